@@ -1,0 +1,381 @@
+#!/usr/bin/env python
+"""Throughput of the point-source model-map path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c1] [--impl ours|reference]
+
+One step = one pass of the hot path over one batch: exposure -> mean PSF ->
+source maps (the three calls of the reference's main.cxx:28-30) for every
+source of the workload.  Workload: config c1 (50 point sources, CAR 200x200
+@ 0.1 deg, 37 energies 100 MeV - 1 TeV, livetime cube nside 64 x 40), seeded
+synthetic inputs.  The metric counts srcmap pixels: one pixel is one
+(source, x, y, energy) element of the [S, H, W, E] model map.
+
+For N > 1 (torchrun) every rank runs its own job of the same size (sources are
+independent; no collective on the data path): weak scaling, value = all ranks'
+pixels / the slowest rank's time.
+
+Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "srcmap pixels/sec at 1e-4 rel err (plain GPU cubature path)"
+UNIT = "srcmap pixels/s (pixel = one (source, x, y, energy) element)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--config", default="c1")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--seed", type=int, default=11)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self, t0: float, t1: float):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9 and p[1].replace(".", "").isdigit():
+                rows.append(p)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        sm = [float(r[1]) for r in rows]
+        busy = [float(r[1]) for r in rows if float(r[3] or 0) > 200.0] or sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(busy), "sm_max_mhz": float(rows[0][2]),
+                "reasons": reasons, "samples": len(rows), "power_w_max": max(float(r[3] or 0) for r in rows)}
+
+
+# ----------------------------------------------------------------------------- our arm
+def to_device_job(job, torch, dev):
+    """Device-resident copies of every input of the three calls."""
+    from xtsrcmaps_b200.api import ExpCube
+    from xtsrcmaps_b200.irf import IrfGrid
+
+    t = lambda a, dt=torch.float64: torch.as_tensor(np.asarray(a), device=dev).to(dt).contiguous()
+
+    def grid(g):
+        return IrfGrid(t(g.cosths), t(g.logEs), t(g.params), g.min_cos_theta)
+
+    return dict(
+        cube=ExpCube(t(job.exp_cube.cosbins, torch.float32), job.exp_cube.nside, 40,
+                     job.exp_cube.cosmin, job.exp_cube.thetabin),
+        wcube=ExpCube(t(job.wexp_cube.cosbins, torch.float32), job.wexp_cube.nside, 40,
+                      job.wexp_cube.cosmin, job.wexp_cube.thetabin),
+        logEs=t(job.logEs), src=t(job.src_sph), af=grid(job.aeff_front), ab=grid(job.aeff_back))
+
+
+def pinned_job(job, torch):
+    """Host copies of the step inputs in pinned (page-locked) memory."""
+    from xtsrcmaps_b200.api import ExpCube
+
+    def pin(a, dt=None):
+        a = np.ascontiguousarray(a if dt is None else np.asarray(a, dt))
+        return torch.from_numpy(a).pin_memory().numpy()
+
+    return dict(
+        cube=ExpCube(pin(job.exp_cube.cosbins), job.exp_cube.nside, 40, job.exp_cube.cosmin, job.exp_cube.thetabin),
+        wcube=ExpCube(pin(job.wexp_cube.cosbins), job.wexp_cube.nside, 40, job.wexp_cube.cosmin, job.wexp_cube.thetabin),
+        logEs=pin(job.logEs, np.float64), src=pin(job.src_sph, np.float64))
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from xtsrcmaps_b200 import api as A
+    from xtsrcmaps_b200.synth import DESCRIPTIONS, make_job
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    A.init(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=dev)
+
+    job = make_job(args.config, seed=args.seed + 1000 * rank)
+    S, H, W, E = job.S, job.wcs.naxis1, job.wcs.naxis2, job.E
+    n_values = job.n_values
+    # IRF set-up (Irf::collect_irf_data, untimed like the reference's ingest)
+    ltf_h = A.livetime_efficiency_factors(job.logEs, job.effic_front)
+    nf_h = A.normalize_rpsf(job.rpsf_front, job.scale_front)
+    nb_h = A.normalize_rpsf(job.rpsf_back, job.scale_back)
+    d = to_device_job(job, torch, dev)
+    from xtsrcmaps_b200.irf import IrfGrid
+
+    tt = lambda a: torch.as_tensor(np.asarray(a), device=dev, dtype=torch.float64)
+    nf = IrfGrid(tt(nf_h.cosths), tt(nf_h.logEs), tt(nf_h.params), nf_h.min_cos_theta)
+    nb = IrfGrid(tt(nb_h.cosths), tt(nb_h.logEs), tt(nb_h.params), nb_h.min_cos_theta)
+    ltf = tt(ltf_h)
+    out = torch.empty((S, H, W, E), dtype=torch.float32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step():
+        ex = A.compute_exposure(d["cube"], d["wcube"], d["logEs"], d["src"], d["af"], d["ab"], ltf)
+        ps = A.compute_psf_data(nf, nb, ex, d["logEs"], ltf)
+        A.point_src_model_map_wcs(job.wcs, d["src"], ex.exposure, ps.uPsf, ps.partial_psf_integral,
+                                  out=out, with_info=False)
+
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    A.profile_enable(True)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    t0 = time.time()
+    for k in range(args.steps):
+        flush.zero_()  # L2 flush between timed steps (outside the events)
+        evs[k][0].record(stream)
+        step()
+        evs[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    t1 = time.time()
+    prof = A.profile_read()
+    A.profile_enable(False)
+    ck = clocks.stop(t0, t1)
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    ms_t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = n_values * world * args.steps / (ms_max * 1e-3)
+
+    # dominant kernel roofline (k_srcmap), measured inside the timed region
+    kname = "k_srcmap"
+    launches, kms = prof.get(kname, (0, 0.0))
+    epad = (E + 3) // 4 * 4
+    alg_bytes = 4 * n_values + 4 * S * 401 * epad + 24 * (H + 1) * (W + 1) + 8 * H * W
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    achieved = alg_bytes / (kms / launches * 1e-3) / 1e9 if launches else None
+    traffic = None
+    try:
+        tr = json.load(open(os.path.join(ROOT, "profiles", "k_srcmap_c1_traffic.json")))
+        traffic = tr.get("dram_bytes_per_launch")
+    except (OSError, ValueError):
+        pass
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "peak_source": peak_src,
+                "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
+                "avg_launch_ms": kms / launches if launches else None,
+                "kernel_share": kms / ms if ms else None}
+    kernels = {k: {"launches": v[0], "ms": round(v[1], 4)} for k, v in prof.items()}
+    gpu_launches = sum(v[0] for v in prof.values())
+
+    # end to end through the public API with host (pinned) buffers
+    e2e = None
+    if not args.no_e2e:
+        hp = pinned_job(job, torch)
+        hout = torch.empty((S, H, W, E), dtype=torch.float32).pin_memory().numpy()
+
+        def step_host():
+            ex = A.compute_exposure(hp["cube"], hp["wcube"], hp["logEs"], hp["src"], job.aeff_front,
+                                    job.aeff_back, ltf_h)
+            ps = A.compute_psf_data(nf_h, nb_h, ex, hp["logEs"], ltf_h)
+            A.point_src_model_map_wcs(job.wcs, hp["src"], ex.exposure, ps.uPsf, ps.partial_psf_integral,
+                                      out=hout, with_info=False)
+            return ex, ps
+
+        for _ in range(2):
+            step_host()
+        ke = max(3, min(args.steps, 20))
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            ex, ps = step_host()
+        te = time.perf_counter() - t0
+        te_t = torch.tensor([te], dtype=torch.float64, device=dev)
+        if dist:
+            dist.all_reduce(te_t, op=dist.ReduceOp.MAX)
+        te = float(te_t.item())
+        C = 40
+        grid_b = lambda g: 8 * (g.cosths.size + g.logEs.size + g.params.size)
+        h2d = (2 * job.exp_cube.cosbins.nbytes + 8 * E + 8 * 2 * S + grid_b(job.aeff_front) + grid_b(job.aeff_back)
+               + 8 * 2 * E  # exposure
+               + grid_b(nf_h) + grid_b(nb_h) + 8 * (C + E + 2 * C * E + 2 * S * C + 2 * E + S * E)  # psf
+               + 8 * (2 * S + S * E + 2 * S * 401 * E))  # srcmap
+        d2h = (8 * (C + 2 * C * E + 2 * S * C + S * E) + 8 * 2 * S * 401 * E + 4 * n_values)
+        e2e = {"value": n_values * world * ke / te, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "steps": ke,
+               "note": "three public calls per step (compute_exposure, compute_psf_data, "
+                       "point_src_model_map_wcs) with pinned host buffers, copies inside the timed region"}
+
+    cpu = None
+    err = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu, err = cpu_baseline(job, out.cpu().numpy())
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (separations, sums and tables f64)",
+        "data": "synthetic (seeded livetime cube, IRF tables and source positions; no public dataset)",
+        "config": {"workload": args.config + ": " + DESCRIPTIONS[args.config], "sources_per_gpu": S,
+                   "map": f"{H}x{W}", "energies": E, "values_per_step_per_gpu": n_values,
+                   "parallelism": f"sources sharded over {world} GPU(s), no data-path collective",
+                   "l2": "256 MiB buffer written between timed steps (L2 flush); the 296 MB map "
+                         "written per step also exceeds the 126 MB L2",
+                   "output_dtype": "float32"},
+        "roofline": roofline, "kernels": kernels, "gpu_launches": gpu_launches,
+        "clocks": ck, "e2e": e2e, "cpu_baseline": cpu, "max_rel_err_vs_fp64_oracle": err,
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- CPU legs
+def _oracle_worker(args):
+    name, seed, lo, hi = args
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import oracle_pipeline
+    from xtsrcmaps_b200.synth import make_job
+
+    job = make_job(name, seed=seed)
+    job.src_sph = job.src_sph[lo:hi]
+    t0 = time.perf_counter()
+    r = oracle_pipeline(job)
+    return time.perf_counter() - t0, r["map"].size
+
+
+def cpu_baseline(job, gpu_map):
+    """The FP64 oracle (a scalar port of the reference path) on the host cores,
+    over the bench's own job; also gives the GPU map's error against FP64."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import max_rel, oracle_pipeline
+
+    t0 = time.perf_counter()
+    r = oracle_pipeline(job)
+    dt = time.perf_counter() - t0
+    reps = 1
+    while time.perf_counter() - t0 < 10.0 and reps < 8:
+        oracle_pipeline(job, with_map=True)
+        reps += 1
+    dt = (time.perf_counter() - t0) / reps
+    err = max_rel(gpu_map, r["map"])
+    return ({"value": job.n_values / dt, "unit": UNIT, "cores": 1, "kind": "port",
+             "sample": f"the full bench job ({job.S} sources, {job.wcs.naxis1}x{job.wcs.naxis2}, "
+                       f"{job.E} energies), FP64 oracle, {reps} repetitions"}, err)
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import multiprocessing as mp
+
+    from xtsrcmaps_b200.synth import DESCRIPTIONS, make_job
+
+    job = make_job(args.config, seed=args.seed)
+    cores = os.cpu_count() or 1
+    S = job.S
+    chunks = [(args.config, args.seed, i * S // cores, (i + 1) * S // cores) for i in range(cores)]
+    chunks = [c for c in chunks if c[3] > c[2]]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(len(chunks)) as pool:
+        for _ in range(max(1, min(args.warmup, 1))):
+            pool.map(_oracle_worker, chunks)
+        times = []
+        nsteps = max(1, min(args.steps, 5))
+        for _ in range(nsteps):
+            t0 = time.perf_counter()
+            pool.map(_oracle_worker, chunks)
+            times.append(time.perf_counter() - t0)
+    ms = 1e3 * sum(times) / len(times)
+    value = job.n_values / (ms * 1e-3)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": nsteps, "warmup": 1, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": args.config + ": " + DESCRIPTIONS[args.config]},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": len(chunks), "kind": "port",
+                         "sample": f"full {args.config} job split by source over {len(chunks)} processes"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local_rank = env_rank()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,165 @@
+/*
+ * xtsrcmaps_b200.h -- C-ABI of the B200 (sm_100a) point-source model-map path.
+ *
+ * The reference (xtsrcmaps) has no plugin or FFI layer; its seam is three C++
+ * namespace functions called from xtsrcmaps/main.cxx:28-30.  Each entry point
+ * below replaces one of them (or one of the finer routines they call) with the
+ * same inputs, outputs, tensor layouts and meaning, as plain pointers and sizes.
+ *
+ * Layouts: row-major, last index contiguous, exactly the reference's
+ * Fermi::Tensor layout (tensor/tensor.hpp:113-122).  S = sources, C = cos-theta
+ * bins of the livetime cube, E = energies, D = 401 PSF separations, H x W map
+ * (H = NAXIS1, the longitude axis; observation/observation.cxx:28-29).
+ *
+ * Pointers: by default every array argument is a HOST pointer; the library
+ * stages it into device memory, runs the kernels on its stream and copies the
+ * results back before returning.  With XTS_DEVICE_PTRS every array argument is
+ * a device pointer on the current CUDA device, the call is asynchronous on the
+ * given stream (NULL = the library's stream) and nothing is copied.
+ *
+ * Errors: every entry point returns XTS_OK (0) or a negative XTS_ERR_* code and
+ * never exits the process; xts_last_error() gives a message for the calling
+ * thread.  The reference instead asserts or calls exit(1) (misc/misc.hxx:41-48).
+ */
+#ifndef XTSRCMAPS_B200_H
+#define XTSRCMAPS_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define XTS_ND 401 /* psf/psf.hxx:20 sep_arr_len */
+
+enum xts_status {
+    XTS_OK = 0,
+    XTS_ERR_ARG = -1,     /* bad shape, null pointer or unsupported option */
+    XTS_ERR_CUDA = -2,    /* a CUDA runtime call failed */
+    XTS_ERR_OOM = -3,     /* device allocation failed */
+    XTS_ERR_TIMEOUT = -4, /* a bounded device-side wait gave up */
+    XTS_ERR_NODEV = -5    /* no usable sm_100 device */
+};
+
+enum xts_flags {
+    XTS_DEVICE_PTRS = 1u << 0, /* array arguments are device pointers */
+    XTS_OUT_F64 = 1u << 1,     /* model map written as double (default float) */
+    XTS_EXPOSURE_TF32 = 1u << 2 /* exposure contraction as 3xTF32 on tcgen05 tensor cores (default: FP64 cores) */
+};
+
+/* FITS celestial WCS (sky_geom/sky_geom.hxx:17-25, WcsConfig). */
+typedef struct xts_wcs {
+    long   naxis1, naxis2;
+    double crpix1, crpix2;
+    double crval1, crval2;
+    double cdelt1, cdelt2;
+    double crota2;  /* degrees */
+    int    proj;    /* 0 = CAR, 1 = AIT */
+    int    galactic;
+} xts_wcs;
+
+/* One padded IRF grid (irf/irf_types.hxx:11-16, IrfData3). */
+typedef struct xts_grid {
+    const double* cosths;  /* [Mc] */
+    int           n_cos;
+    const double* logEs;   /* [Me] */
+    int           n_e;
+    const double* params;  /* [Mc, Me, n_par] */
+    int           n_par;
+    double        min_cos_theta;
+} xts_grid;
+
+/* Livetime cube (observation/obs_types.hxx:24-32, ExposureCubeData). */
+typedef struct xts_expcube {
+    const float* cosbins;  /* [12 nside^2, nbrbins], HEALPix NESTED, equatorial */
+    long         nside;
+    int          nbrbins;
+    double       cosmin;
+    int          thetabin; /* THETABIN != "COSTHETA" */
+} xts_expcube;
+
+/* Outputs of the exposure step (exposure/exposure.hxx:19-26, XtExp). */
+typedef struct xts_exposure_out {
+    double* exp_costhetas;                 /* [C] */
+    double* front_aeff;                    /* [C, E] */
+    double* back_aeff;                     /* [C, E] */
+    double* src_exposure_cosbins;          /* [S, C] */
+    double* src_weighted_exposure_cosbins; /* [S, C] */
+    double* exposure;                      /* [S, E] */
+} xts_exposure_out;
+
+/* Optional per-map results of the model-map step.  Any pointer may be NULL. */
+typedef struct xts_srcmap_info {
+    double* inv_map_integral; /* [S, E] 1 / sum over pixels within radius (0 stays 0) */
+    double* correction;       /* [S, E] containment correction factor */
+    double* psf_radius;       /* [S] degrees */
+    int*    in_fov;           /* [S] */
+} xts_srcmap_info;
+
+/* Library state ------------------------------------------------------------ */
+int         xts_init(int device);       /* select the device, create the stream */
+void        xts_release(void);          /* free every cached device buffer */
+const char* xts_last_error(void);
+int         xts_version(void);
+
+/* Kernel timing for profiling and the roofline report (no counterpart in the
+ * reference, which has no tracing).  While enabled, every kernel the library
+ * launches is bracketed by CUDA events on its stream.  xts_profile_read waits
+ * for the recorded kernels, writes a JSON object
+ * {"kernel": [launches, total_ms], ...} into buf and clears the record; it
+ * returns the length written or a negative error code. */
+int xts_profile_enable(int on);
+int xts_profile_read(char* buf, int buflen);
+
+/* Irf::livetime_efficiency_factors (irf/irf.cxx:70-109) -> ltf [2, E]. */
+int xts_livetime_efficiency_factors(const double* logEs, int E, const float* p0,
+                                    const float* p1, double* ltf, unsigned flags,
+                                    void* stream);
+
+/* irf_private::normalize_rpsf (irf/irf.normalize_rpsf.cpp:11-61): normalises a
+ * King parameter grid [Mc, Me, 6] in place. */
+int xts_normalize_rpsf(double* params, int Mc, int Me, const double* grid_logEs,
+                       float scale0, float scale1, float scale_index,
+                       unsigned flags, void* stream);
+
+/* Exposure::compute_exposure<T> (exposure/exposure.hxx:44-88): steps a1-a5.
+ * front_ltf is Irf::XtIrf::front_LTF [2, E]; C = exp_cube->nbrbins. */
+int xts_compute_exposure(const xts_expcube* exp_cube, const xts_expcube* wexp_cube,
+                         const double* logEs, int E, const double* src_sph, int S,
+                         const xts_grid* aeff_front, const xts_grid* aeff_back,
+                         const double* front_ltf, const xts_exposure_out* out,
+                         unsigned flags, void* stream);
+
+/* Exposure::exposure (exposure/exposure.cxx:159-263, with the DGEMMs of
+ * exposure/exposure.contract.cpp:13-42): step a5 alone, from the gathered
+ * livetime rows ecb, wecb [S, C] and the Aeff tables [C, E] -> exposure [S, E]. */
+int xts_exposure_contract(const double* src_exposure_cosbins,
+                          const double* src_weighted_exposure_cosbins, int S, int C,
+                          const double* front_aeff, const double* back_aeff,
+                          const double* front_ltf, int E, double* exposure,
+                          unsigned flags, void* stream);
+
+/* Psf::compute_psf_data (psf/psf.compute_psf_data.cxx:7-33, which calls
+ * psf/psf.psf_lookup_table_and_partial_integrals.cxx:8-57): steps b3-b7.
+ * psf grids are normalised King grids [Mc, Me, 6]; outputs uPsf and
+ * partial_psf_integral [S, 401, E]. */
+int xts_compute_psf_data(const xts_grid* psf_front, const xts_grid* psf_back,
+                         const double* exp_costhetas, int C, const double* logEs,
+                         int E, const double* front_aeff, const double* back_aeff,
+                         const double* src_exposure_cosbins,
+                         const double* src_weighted_exposure_cosbins, int S,
+                         const double* front_ltf, const double* exposure,
+                         double* upsf, double* partial, unsigned flags, void* stream);
+
+/* ModelMap::point_src_model_map_wcs (model_map/model_map.point_src_model_map_wcs.cxx:6-45,
+ * reached from ModelMap::compute_srcmaps<PointSource>, model_map.compute_src_maps.cxx:6-22):
+ * steps c1-c10 and d1.  model_map is [S, H, W, E], float unless XTS_OUT_F64. */
+int xts_point_src_model_map_wcs(const xts_wcs* wcs, const double* src_sph, int S,
+                                const double* exposure, const double* upsf,
+                                const double* partial, int E, void* model_map,
+                                xts_srcmap_info* info, unsigned flags, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

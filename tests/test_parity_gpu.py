@@ -1,0 +1,197 @@
+"""GPU parity: every step of the point-source path through the C-ABI against the
+FP64 CPU oracle on the same seeded inputs, and against the reference's golden
+vectors where they exist.
+
+Tolerances (the bar of the path's specification):
+  * FP64 steps (exposure, mean PSF, per-map sums): relative 1e-10 or tighter;
+  * FP32 source maps: 1e-5 relative per pixel, per-map totals 1e-7;
+  * FP64 source maps (XTS_OUT_F64): 1e-10 relative per pixel.
+"""
+import numpy as np
+import pytest
+
+from helpers import max_rel, oracle_pipeline
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def api():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from xtsrcmaps_b200 import api as A
+    from xtsrcmaps_b200 import build
+
+    build.build()
+    A.init(0)
+    return A
+
+
+def _job(name, seed=3, n=None):
+    from xtsrcmaps_b200.synth import make_job
+
+    return make_job(name, seed=seed, n_sources=n)
+
+
+def _gpu_pipeline(A, job, out_dtype="float32", tf32=False):
+    ltf = A.livetime_efficiency_factors(job.logEs, job.effic_front)
+    nf = A.normalize_rpsf(job.rpsf_front, job.scale_front)
+    nb = A.normalize_rpsf(job.rpsf_back, job.scale_back)
+    ex = A.compute_exposure(job.exp_cube, job.wexp_cube, job.logEs, job.src_sph, job.aeff_front,
+                            job.aeff_back, ltf, tf32=tf32)
+    ps = A.compute_psf_data(nf, nb, ex, job.logEs, ltf)
+    mm, info = A.point_src_model_map_wcs(job.wcs, job.src_sph, ex.exposure, ps.uPsf,
+                                         ps.partial_psf_integral, out_dtype=out_dtype)
+    return dict(ltf=ltf, nf=nf, nb=nb, ex=ex, ps=ps, map=mm, info=info)
+
+
+@pytest.fixture(scope="module")
+def c1_small(api):
+    job = _job("c1", seed=5, n=6)
+    return job, oracle_pipeline(job), _gpu_pipeline(api, job)
+
+
+def test_irf_setup_vs_oracle(api, c1_small):
+    job, ref, gpu = c1_small
+    assert max_rel(gpu["ltf"], ref["ltf"]) < 1e-15
+    assert max_rel(gpu["nf"].params, ref["nf"].params) < 1e-12
+    assert max_rel(gpu["nb"].params, ref["nb"].params) < 1e-12
+
+
+def test_exposure_vs_oracle(api, c1_small):
+    job, ref, gpu = c1_small
+    ex = gpu["ex"]
+    assert np.array_equal(ex.exp_costhetas, ref["costh"])
+    assert np.array_equal(ex.src_exposure_cosbins, ref["ecb"])  # gather: bit-exact
+    assert np.array_equal(ex.src_weighted_exposure_cosbins, ref["wecb"])
+    assert max_rel(ex.front_aeff, ref["af"]) < 1e-14
+    assert max_rel(ex.back_aeff, ref["ab"]) < 1e-14
+    assert max_rel(ex.exposure, ref["exposure"]) < 1e-13
+
+
+def test_mean_psf_vs_oracle(api, c1_small):
+    job, ref, gpu = c1_small
+    assert max_rel(gpu["ps"].uPsf, ref["upsf"]) < 1e-11
+    assert max_rel(gpu["ps"].partial_psf_integral, ref["partial"], floor=1e-300) < 1e-11
+
+
+def test_srcmap_f32_vs_oracle(api, c1_small):
+    job, ref, gpu = c1_small
+    m, info = gpu["map"], gpu["info"]
+    assert m.dtype == np.float32 and m.shape == ref["map"].shape
+    assert max_rel(m, ref["map"]) < 1e-5
+    np.testing.assert_array_equal(info.in_fov.astype(bool), ref["in_fov"])
+    assert max_rel(info.psf_radius, ref["radius"]) < 1e-13
+    # per-map normalisation sums and their use
+    assert max_rel(info.inv_map_integral, ref["inv_integ"]) < 1e-7
+    assert max_rel(info.correction, ref["factor"]) < 1e-7
+    # totals of the written maps
+    tot_g = m.astype(np.float64).sum(axis=(1, 2))
+    tot_r = ref["map"].sum(axis=(1, 2))
+    assert max_rel(tot_g, tot_r) < 1e-7
+
+
+def test_srcmap_f64_vs_oracle(api, c1_small):
+    job, ref, gpu = c1_small
+    m, info = api.point_src_model_map_wcs(job.wcs, job.src_sph, gpu["ex"].exposure, gpu["ps"].uPsf,
+                                          gpu["ps"].partial_psf_integral, out_dtype="float64")
+    assert m.dtype == np.float64
+    assert max_rel(m, ref["map"]) < 1e-10
+    assert max_rel(info.inv_map_integral, ref["inv_integ"]) < 1e-10
+
+
+def test_config0_full(api):
+    """config 0: one source at the field centre (the point-source pixel itself)."""
+    job = _job("c0", seed=1)
+    ref = oracle_pipeline(job)
+    gpu = _gpu_pipeline(api, job)
+    assert max_rel(gpu["map"], ref["map"]) < 1e-5
+    m64, _ = api.point_src_model_map_wcs(job.wcs, job.src_sph, gpu["ex"].exposure, gpu["ps"].uPsf,
+                                         gpu["ps"].partial_psf_integral, out_dtype="float64")
+    assert max_rel(m64, ref["map"]) < 1e-10
+
+
+def test_device_pointer_mode(api, c1_small):
+    """Same call with CUDA tensors: XTS_DEVICE_PTRS path, asynchronous on torch's stream."""
+    import torch
+
+    job, ref, gpu = c1_small
+    d = torch.device("cuda")
+    ex = gpu["ex"]
+    m, info = api.point_src_model_map_wcs(job.wcs, torch.as_tensor(job.src_sph, device=d),
+                                          torch.as_tensor(ex.exposure, device=d),
+                                          torch.as_tensor(gpu["ps"].uPsf, device=d),
+                                          torch.as_tensor(gpu["ps"].partial_psf_integral, device=d))
+    torch.cuda.synchronize()
+    assert m.is_cuda
+    assert np.array_equal(m.cpu().numpy(), gpu["map"])
+
+
+def test_edge_sources(api):
+    """Sources exactly on a pixel centre, on a pixel corner, just outside the map
+    (in-FOV false) and 80 deg away (LUT clamp at row 400), on a non-square AIT map."""
+    from xtsrcmaps_b200.synth import make_job
+    from xtsrcmaps_b200.wcs import Wcs
+    from oracle import oracle as O
+
+    job = make_job("c0", seed=7)
+    job.wcs = Wcs(60, 44, 30.5, 22.5, 193.98, -5.82, -0.2, 0.2, proj="AIT")
+    pts = [O.pix2sph(job.wcs, 31.0, 20.0), O.pix2sph(job.wcs, 10.5, 7.5), O.pix2sph(job.wcs, 62.0, 10.0)]
+    pts.append((pts[0][0] + 85.0, pts[0][1]))
+    # a source on the unit-vector direction of one rule point: that point's chord is
+    # the blend's radial shrink (~1e-6 rad), below the table's first separation (1e-4 deg)
+    pw = O.square_ptswts(job.wcs)[20, 15, 0:3]
+    d = pw / np.linalg.norm(pw)
+    pts.append((np.degrees(np.arctan2(d[1], d[0])) % 360.0, np.degrees(np.arcsin(d[2]))))
+    job.src_sph = np.array(pts, dtype=np.float64)
+    ref = oracle_pipeline(job)
+    gpu = _gpu_pipeline(api, job)
+    assert max_rel(gpu["map"], ref["map"]) < 1e-5
+    np.testing.assert_array_equal(gpu["info"].in_fov.astype(bool), ref["in_fov"])
+    assert list(ref["in_fov"]) == [True, True, False, False, True]
+
+
+def test_empty_and_single_energy(api):
+    job = _job("c0", seed=2)
+    gpu = _gpu_pipeline(api, job)
+    m, info = api.point_src_model_map_wcs(job.wcs, np.zeros((0, 2)), np.zeros((0, job.E)),
+                                          np.zeros((0, 401, job.E)), np.zeros((0, 401, job.E)))
+    assert m.shape == (0, 100, 100, job.E)
+    ex = gpu["ex"]
+    m1, _ = api.point_src_model_map_wcs(job.wcs, job.src_sph, ex.exposure[:, :1].copy(),
+                                        gpu["ps"].uPsf[:, :, :1].copy(),
+                                        gpu["ps"].partial_psf_integral[:, :, :1].copy())
+    assert max_rel(m1[..., 0], gpu["map"][..., 0]) < 1e-6
+
+
+def test_bad_arguments_raise(api):
+    from xtsrcmaps_b200._lib import XTS_ERR_ARG, XtsError
+    from xtsrcmaps_b200.wcs import Wcs
+
+    w = Wcs(10, 10, 5.5, 5.5, 0.0, 0.0, 0.0, 0.1)  # CDELT1 = 0
+    with pytest.raises(XtsError) as ei:
+        api.point_src_model_map_wcs(w, np.zeros((1, 2)), np.ones((1, 3)), np.ones((1, 401, 3)),
+                                    np.ones((1, 401, 3)))
+    assert ei.value.code == XTS_ERR_ARG
+
+
+def test_golden_exposure_and_psf_on_gpu(api, golden):
+    """The reference's own livetime rows and IRFs through the GPU contraction and
+    mean-PSF kernels, against tests/expected/exposure.bin and uPsf_peak_SE.bin."""
+    from test_oracle_golden import _exposure_inputs
+    from oracle import oracle as O
+    from xtsrcmaps_b200.irf import IrfGrid
+
+    z, g, e, cos, loge, af, ab, ltf, ecb, wecb = _exposure_inputs(golden)
+    ex = api.exposure(ecb, wecb, af, ab, ltf)
+    assert max_rel(ex, e["exposure"]) < 5e-6
+    pf, pb = g["rpsf_front"], g["rpsf_back"]
+    nf = api.normalize_rpsf(pf, g["scale_front"])
+    nb = api.normalize_rpsf(pb, g["scale_back"])
+    from xtsrcmaps_b200.api import XtExp
+
+    xe = XtExp(cos, af, ab, ecb, wecb, ex)
+    ps = api.compute_psf_data(nf, nb, xe, loge, ltf)
+    assert max_rel(ps.uPsf[:, 0, :], golden("psf")["upsf_peak"]) < 2e-6

@@ -1,0 +1,123 @@
+"""ctypes bindings of libxts_cuda.so (include/xtsrcmaps_b200.h).
+
+The library is built in-tree by ``xtsrcmaps_b200/build.py``.  There is no CPU
+fallback: if the shared object is missing or no sm_100 device is visible, the
+calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libxts_cuda.so")
+
+XTS_OK = 0
+XTS_ERR_ARG = -1
+XTS_ERR_CUDA = -2
+XTS_ERR_OOM = -3
+XTS_ERR_TIMEOUT = -4
+XTS_ERR_NODEV = -5
+
+XTS_DEVICE_PTRS = 1 << 0
+XTS_OUT_F64 = 1 << 1
+XTS_EXPOSURE_TF32 = 1 << 2
+
+ND = 401
+
+_vp = C.c_void_p
+
+
+class XtsWcs(C.Structure):
+    _fields_ = [
+        ("naxis1", C.c_long), ("naxis2", C.c_long),
+        ("crpix1", C.c_double), ("crpix2", C.c_double),
+        ("crval1", C.c_double), ("crval2", C.c_double),
+        ("cdelt1", C.c_double), ("cdelt2", C.c_double),
+        ("crota2", C.c_double), ("proj", C.c_int), ("galactic", C.c_int),
+    ]
+
+
+class XtsGrid(C.Structure):
+    _fields_ = [
+        ("cosths", _vp), ("n_cos", C.c_int),
+        ("logEs", _vp), ("n_e", C.c_int),
+        ("params", _vp), ("n_par", C.c_int),
+        ("min_cos_theta", C.c_double),
+    ]
+
+
+class XtsExpcube(C.Structure):
+    _fields_ = [
+        ("cosbins", _vp), ("nside", C.c_long), ("nbrbins", C.c_int),
+        ("cosmin", C.c_double), ("thetabin", C.c_int),
+    ]
+
+
+class XtsExposureOut(C.Structure):
+    _fields_ = [
+        ("exp_costhetas", _vp), ("front_aeff", _vp), ("back_aeff", _vp),
+        ("src_exposure_cosbins", _vp), ("src_weighted_exposure_cosbins", _vp),
+        ("exposure", _vp),
+    ]
+
+
+class XtsSrcmapInfo(C.Structure):
+    _fields_ = [
+        ("inv_map_integral", _vp), ("correction", _vp), ("psf_radius", _vp), ("in_fov", _vp),
+    ]
+
+
+# Every symbol the header declares, with its signature.
+SIGNATURES = {
+    "xts_init": (C.c_int, [C.c_int]),
+    "xts_release": (None, []),
+    "xts_last_error": (C.c_char_p, []),
+    "xts_version": (C.c_int, []),
+    "xts_profile_enable": (C.c_int, [C.c_int]),
+    "xts_profile_read": (C.c_int, [C.c_char_p, C.c_int]),
+    "xts_livetime_efficiency_factors": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, C.c_uint, _vp]),
+    "xts_normalize_rpsf": (C.c_int, [_vp, C.c_int, C.c_int, _vp, C.c_float, C.c_float, C.c_float,
+                                     C.c_uint, _vp]),
+    "xts_compute_exposure": (C.c_int, [C.POINTER(XtsExpcube), C.POINTER(XtsExpcube), _vp, C.c_int,
+                                       _vp, C.c_int, C.POINTER(XtsGrid), C.POINTER(XtsGrid), _vp,
+                                       C.POINTER(XtsExposureOut), C.c_uint, _vp]),
+    "xts_exposure_contract": (C.c_int, [_vp, _vp, C.c_int, C.c_int, _vp, _vp, _vp, C.c_int, _vp,
+                                        C.c_uint, _vp]),
+    "xts_compute_psf_data": (C.c_int, [C.POINTER(XtsGrid), C.POINTER(XtsGrid), _vp, C.c_int, _vp,
+                                       C.c_int, _vp, _vp, _vp, _vp, C.c_int, _vp, _vp, _vp, _vp,
+                                       C.c_uint, _vp]),
+    "xts_point_src_model_map_wcs": (C.c_int, [C.POINTER(XtsWcs), _vp, C.c_int, _vp, _vp, _vp,
+                                              C.c_int, _vp, C.POINTER(XtsSrcmapInfo), C.c_uint, _vp]),
+}
+
+
+class XtsError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"xtsrcmaps_b200 error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m xtsrcmaps_b200.build` "
+                "(there is no CPU fallback)")
+        l = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(l, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = l
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != XTS_OK:
+        msg = lib().xts_last_error()
+        raise XtsError(rc, msg.decode() if msg else "")

@@ -1,0 +1,296 @@
+"""Host-side mirror of the reference's point-source entry points.
+
+The reference's seam is three C++ namespace functions called from
+xtsrcmaps/main.cxx:28-30::
+
+    auto ptexp = Exposure::compute_exposure(cfg, obs, src.point, irf);
+    auto ptpsf = Psf::compute_psf_data(obs, irf, ptexp);
+    maps.pt    = ModelMap::compute_srcmaps(obs, src.point, ptexp, ptpsf);
+
+This module offers the same three calls (plus the finer routines they use) with
+the same inputs, outputs and tensor layouts, executed by the sm_100a kernels of
+``libxts_cuda.so`` through its C-ABI.  Arrays may be numpy arrays (host memory:
+the library stages them on the device and copies results back) or CUDA torch
+tensors (device memory: the call is asynchronous on torch's current stream and
+returns CUDA tensors).  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Any, Optional
+
+import numpy as np
+
+from . import _lib as L
+from .irf import IrfEffic, IrfGrid, IrfScale
+from .wcs import Wcs
+
+ND = L.ND
+
+
+@dataclass
+class ExpCube:
+    """Livetime cube (observation/obs_types.hxx:24-32): cosbins float32 [12 nside^2, nbrbins]."""
+
+    cosbins: Any
+    nside: int
+    nbrbins: int
+    cosmin: float = 0.0
+    thetabin: bool = True
+
+
+@dataclass
+class XtExp:
+    """exposure/exposure.hxx:19-26."""
+
+    exp_costhetas: Any
+    front_aeff: Any
+    back_aeff: Any
+    src_exposure_cosbins: Any
+    src_weighted_exposure_cosbins: Any
+    exposure: Any
+
+
+@dataclass
+class XtPsf:
+    """psf/psf.hxx:14-17."""
+
+    uPsf: Any
+    partial_psf_integral: Any
+
+
+@dataclass
+class SrcmapInfo:
+    inv_map_integral: Any
+    correction: Any
+    psf_radius: Any
+    in_fov: Any
+
+
+# --------------------------------------------------------------------------- plumbing
+def _is_cuda(x) -> bool:
+    return hasattr(x, "is_cuda") and bool(x.is_cuda)
+
+
+class _Call:
+    """Holds the buffers of one C-ABI call and converts arrays to pointers."""
+
+    _NP = {"f64": np.float64, "f32": np.float32, "i32": np.int32}
+
+    def __init__(self, device: bool, like=None):
+        self.device = device
+        self.keep = []
+        if device:
+            import torch
+
+            self.torch = torch
+            self.dev = like.device if like is not None else torch.device("cuda")
+            self.stream = C.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
+        else:
+            self.stream = None
+        self.flags = L.XTS_DEVICE_PTRS if device else 0
+
+    def inp(self, x, kind="f64"):
+        if self.device:
+            t = self.torch
+            dt = {"f64": t.float64, "f32": t.float32, "i32": t.int32}[kind]
+            if not _is_cuda(x):
+                x = t.as_tensor(np.asarray(x), device=self.dev)
+            x = x.to(dt).contiguous()
+            self.keep.append(x)
+            return C.c_void_p(x.data_ptr()), x
+        a = np.ascontiguousarray(np.asarray(x), dtype=self._NP[kind])
+        self.keep.append(a)
+        return C.c_void_p(a.ctypes.data), a
+
+    def out(self, shape, kind="f64"):
+        if self.device:
+            t = self.torch
+            dt = {"f64": t.float64, "f32": t.float32, "i32": t.int32}[kind]
+            x = t.empty(shape, dtype=dt, device=self.dev)
+            self.keep.append(x)
+            return C.c_void_p(x.data_ptr()), x
+        a = np.empty(shape, dtype=self._NP[kind])
+        self.keep.append(a)
+        return C.c_void_p(a.ctypes.data), a
+
+    def grid(self, g: IrfGrid, n_par: int) -> L.XtsGrid:
+        params = g.params
+        if n_par == 1 and getattr(params, "ndim", 3) == 3:
+            params = params[..., 0]
+        cp, c = self.inp(g.cosths)
+        ep, e = self.inp(g.logEs)
+        pp, p = self.inp(params)
+        return L.XtsGrid(cp, len(c), ep, len(e), pp, n_par, float(g.min_cos_theta))
+
+
+def _device_of(*xs) -> Optional[Any]:
+    for x in xs:
+        if _is_cuda(x):
+            return x
+    return None
+
+
+# --------------------------------------------------------------------------- IRF set-up
+def livetime_efficiency_factors(logEs, effic: IrfEffic):
+    """Irf::livetime_efficiency_factors (irf/irf.cxx:70-109) -> [2, E]."""
+    like = _device_of(logEs)
+    c = _Call(like is not None, like)
+    lp, le = c.inp(logEs)
+    p0, _ = c.inp(effic.p0, "f32")
+    p1, _ = c.inp(effic.p1, "f32")
+    op, o = c.out((2, len(le)))
+    L.check(L.lib().xts_livetime_efficiency_factors(lp, len(le), p0, p1, op, c.flags, c.stream))
+    return o
+
+
+def normalize_rpsf(grid: IrfGrid, scale: IrfScale) -> IrfGrid:
+    """irf_private::normalize_rpsf (irf/irf.normalize_rpsf.cpp:11-61); returns a normalised copy."""
+    p = np.array(grid.params, dtype=np.float64, order="C", copy=True)
+    gl = np.ascontiguousarray(grid.logEs, dtype=np.float64)
+    Mc, Me = p.shape[0], p.shape[1]
+    L.check(L.lib().xts_normalize_rpsf(C.c_void_p(p.ctypes.data), Mc, Me, C.c_void_p(gl.ctypes.data),
+                                       scale.scale0, scale.scale1, scale.scale_index, 0, None))
+    return IrfGrid(np.array(grid.cosths), np.array(grid.logEs), p, grid.min_cos_theta)
+
+
+# --------------------------------------------------------------------------- step (a)
+def compute_exposure(exp_cube: ExpCube, wexp_cube: ExpCube, logEs, src_sph, aeff_front: IrfGrid,
+                     aeff_back: IrfGrid, front_ltf, tf32: bool = False) -> XtExp:
+    """Exposure::compute_exposure (exposure/exposure.hxx:44-88)."""
+    like = _device_of(exp_cube.cosbins, src_sph, logEs)
+    c = _Call(like is not None, like)
+    cb, cube = c.inp(exp_cube.cosbins, "f32")
+    wb, _ = c.inp(wexp_cube.cosbins, "f32")
+    C_ = int(exp_cube.nbrbins)
+    cube_s = L.XtsExpcube(cb, int(exp_cube.nside), C_, float(exp_cube.cosmin), int(bool(exp_cube.thetabin)))
+    wcube_s = L.XtsExpcube(wb, int(wexp_cube.nside), int(wexp_cube.nbrbins), float(wexp_cube.cosmin),
+                           int(bool(wexp_cube.thetabin)))
+    lp, le = c.inp(logEs)
+    E = len(le)
+    sp, sa = c.inp(src_sph)
+    S = int(sa.shape[0]) if sa.ndim == 2 else 0
+    af = c.grid(aeff_front, 1)
+    ab = c.grid(aeff_back, 1)
+    ltfp, _ = c.inp(front_ltf)
+    o = [c.out(s) for s in ((C_,), (C_, E), (C_, E), (S, C_), (S, C_), (S, E))]
+    outs = L.XtsExposureOut(*[x[0] for x in o])
+    flags = c.flags | (L.XTS_EXPOSURE_TF32 if tf32 else 0)
+    L.check(L.lib().xts_compute_exposure(C.byref(cube_s), C.byref(wcube_s), lp, E, sp, S, C.byref(af),
+                                         C.byref(ab), ltfp, C.byref(outs), flags, c.stream))
+    return XtExp(*[x[1] for x in o])
+
+
+def exposure(src_exposure_cosbins, src_weighted_exposure_cosbins, front_aeff, back_aeff, front_ltf,
+             tf32: bool = False):
+    """Exposure::exposure (exposure/exposure.cxx:159-263): step a5 from gathered livetime rows."""
+    like = _device_of(src_exposure_cosbins, front_aeff)
+    c = _Call(like is not None, like)
+    xp, xa = c.inp(src_exposure_cosbins)
+    wp, _ = c.inp(src_weighted_exposure_cosbins)
+    afp, afa = c.inp(front_aeff)
+    abp, _ = c.inp(back_aeff)
+    lp, _ = c.inp(front_ltf)
+    S, C_ = int(xa.shape[0]), int(xa.shape[1])
+    E = int(afa.shape[1])
+    op, o = c.out((S, E))
+    flags = c.flags | (L.XTS_EXPOSURE_TF32 if tf32 else 0)
+    L.check(L.lib().xts_exposure_contract(xp, wp, S, C_, afp, abp, lp, E, op, flags, c.stream))
+    return o
+
+
+# --------------------------------------------------------------------------- step (b)
+def compute_psf_data(psf_front: IrfGrid, psf_back: IrfGrid, exp: XtExp, logEs, front_ltf) -> XtPsf:
+    """Psf::compute_psf_data (psf/psf.compute_psf_data.cxx:7-33); King grids already normalised."""
+    like = _device_of(exp.exposure, logEs)
+    c = _Call(like is not None, like)
+    gf = c.grid(psf_front, 6)
+    gb = c.grid(psf_back, 6)
+    cp, ca = c.inp(exp.exp_costhetas)
+    lp, le = c.inp(logEs)
+    afp, _ = c.inp(exp.front_aeff)
+    abp, _ = c.inp(exp.back_aeff)
+    xp, xa = c.inp(exp.src_exposure_cosbins)
+    wp, _ = c.inp(exp.src_weighted_exposure_cosbins)
+    ltfp, _ = c.inp(front_ltf)
+    ep, _ = c.inp(exp.exposure)
+    S, E = int(xa.shape[0]), len(le)
+    up, u = c.out((S, ND, E))
+    pp, p = c.out((S, ND, E))
+    L.check(L.lib().xts_compute_psf_data(C.byref(gf), C.byref(gb), cp, len(ca), lp, E, afp, abp, xp, wp,
+                                         S, ltfp, ep, up, pp, c.flags, c.stream))
+    return XtPsf(u, p)
+
+
+# --------------------------------------------------------------------------- steps (c)+(d)
+def _wcs_struct(w: Wcs) -> L.XtsWcs:
+    return L.XtsWcs(int(w.naxis1), int(w.naxis2), float(w.crpix1), float(w.crpix2), float(w.crval1),
+                    float(w.crval2), float(w.cdelt1), float(w.cdelt2), float(w.crota2), w.proj_code,
+                    int(bool(w.galactic)))
+
+
+def point_src_model_map_wcs(wcs: Wcs, src_sph, exposure, uPsf, partial_integrals,
+                            out_dtype: str = "float32", out=None, with_info: bool = True):
+    """ModelMap::point_src_model_map_wcs (model_map/model_map.point_src_model_map_wcs.cxx:6-45).
+
+    Returns (model_map [S, H, W, E], SrcmapInfo or None).  ``out`` may supply a
+    preallocated output of the right dtype and shape.
+    """
+    like = _device_of(uPsf, exposure, src_sph)
+    c = _Call(like is not None, like)
+    sp, sa = c.inp(src_sph)
+    S = int(sa.shape[0])
+    ep, ea = c.inp(exposure)
+    E = int(ea.shape[1])
+    up, _ = c.inp(uPsf)
+    pp, _ = c.inp(partial_integrals)
+    kind = {"float32": "f32", "float64": "f64"}[out_dtype]
+    shape = (S, int(wcs.naxis1), int(wcs.naxis2), E)
+    if out is None:
+        mp, m = c.out(shape, kind)
+    else:
+        m = out
+        mp = C.c_void_p(m.data_ptr() if c.device else m.ctypes.data)
+    info = None
+    info_s = None
+    if with_info:
+        o = [c.out((S, E)), c.out((S, E)), c.out((S,)), c.out((S,), "i32")]
+        info_s = L.XtsSrcmapInfo(*[x[0] for x in o])
+        info = SrcmapInfo(*[x[1] for x in o])
+    flags = c.flags | (L.XTS_OUT_F64 if kind == "f64" else 0)
+    w = _wcs_struct(wcs)
+    L.check(L.lib().xts_point_src_model_map_wcs(C.byref(w), sp, S, ep, up, pp, E, mp,
+                                                C.byref(info_s) if info_s is not None else None,
+                                                flags, c.stream))
+    return m, info
+
+
+def compute_srcmaps(wcs: Wcs, src_sph, exp: XtExp, psf: XtPsf, out_dtype: str = "float32", out=None):
+    """ModelMap::compute_srcmaps<PointSource> (model_map/model_map.compute_src_maps.cxx:6-22)."""
+    m, _ = point_src_model_map_wcs(wcs, src_sph, exp.exposure, psf.uPsf, psf.partial_psf_integral,
+                                   out_dtype=out_dtype, out=out, with_info=False)
+    return m
+
+
+def init(device: int = 0) -> None:
+    L.check(L.lib().xts_init(int(device)))
+
+
+def profile_enable(on: bool = True) -> None:
+    L.check(L.lib().xts_profile_enable(int(bool(on))))
+
+
+def profile_read() -> dict:
+    """Per-kernel {name: (launches, total_ms)} since profiling was enabled (then cleared)."""
+    import json
+
+    buf = C.create_string_buffer(1 << 16)
+    n = L.lib().xts_profile_read(buf, len(buf))
+    if n < 0:
+        L.check(n)
+    return {k: (int(v[0]), float(v[1])) for k, v in json.loads(buf.value.decode()).items()}
+
+
+def release() -> None:
+    L.lib().xts_release()

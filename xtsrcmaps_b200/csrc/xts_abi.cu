@@ -1,0 +1,416 @@
+// xts_abi.cu -- the extern "C" entry points of include/xtsrcmaps_b200.h: argument
+// checks, host<->device staging, the cached device workspace and error strings.
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <mutex>
+
+#include "xts_internal.cuh"
+
+namespace xts {
+
+static thread_local char g_err[512] = "";
+static std::mutex g_mu;  // serialises calls that share the workspace
+
+int set_error(int code, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int cuda_error(cudaError_t e, const char* what) {
+    int code = (e == cudaErrorMemoryAllocation) ? XTS_ERR_OOM : XTS_ERR_CUDA;
+    return set_error(code, "%s: %s", what, cudaGetErrorString(e));
+}
+
+struct Ctx {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    void* buf[N_SLOTS] = {};
+    size_t cap[N_SLOTS] = {};
+};
+static Ctx g_ctx;
+
+int ensure_device() {
+    if (g_ctx.device >= 0) {
+        cudaError_t e = cudaSetDevice(g_ctx.device);
+        return e == cudaSuccess ? XTS_OK : cuda_error(e, "cudaSetDevice");
+    }
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return set_error(XTS_ERR_NODEV, "no CUDA device visible");
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceProp prop;
+    XTS_CUDA(cudaGetDeviceProperties(&prop, dev));
+    if (prop.major != 10)
+        return set_error(XTS_ERR_NODEV, "device %d is sm_%d%d; this library is built for sm_100a",
+                         dev, prop.major, prop.minor);
+    XTS_CUDA(cudaSetDevice(dev));
+    XTS_CUDA(cudaStreamCreateWithFlags(&g_ctx.stream, cudaStreamNonBlocking));
+    g_ctx.device = dev;
+    return XTS_OK;
+}
+
+cudaStream_t default_stream() { return g_ctx.stream; }
+
+void* workspace(int slot, size_t bytes) {
+    bytes = align_up(bytes ? bytes : 1, 256);
+    if (g_ctx.cap[slot] >= bytes) return g_ctx.buf[slot];
+    if (g_ctx.buf[slot]) {
+        cudaStreamSynchronize(g_ctx.stream);
+        cudaDeviceSynchronize();
+        cudaFree(g_ctx.buf[slot]);
+        g_ctx.buf[slot] = nullptr;
+        g_ctx.cap[slot] = 0;
+    }
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error(XTS_ERR_OOM, "cudaMalloc(%zu) for workspace slot %d: %s", bytes, slot,
+                  cudaGetErrorString(e));
+        return nullptr;
+    }
+    g_ctx.buf[slot] = p;
+    g_ctx.cap[slot] = bytes;
+    return p;
+}
+
+static void release_all() {
+    if (g_ctx.device < 0) return;
+    cudaSetDevice(g_ctx.device);
+    cudaDeviceSynchronize();
+    for (int i = 0; i < N_SLOTS; ++i) {
+        if (g_ctx.buf[i]) cudaFree(g_ctx.buf[i]);
+        g_ctx.buf[i] = nullptr;
+        g_ctx.cap[i] = 0;
+    }
+}
+
+// Kernel timing -------------------------------------------------------------
+struct ProfRec { const char* name; cudaEvent_t a, b; };
+static bool g_prof_on = false;
+static ProfRec g_prof[4096];
+static int g_prof_n = 0;
+static cudaEvent_t g_prof_pool[8192];
+static int g_prof_pool_n = 0, g_prof_pool_used = 0;
+
+static cudaEvent_t prof_event() {
+    if (g_prof_pool_used < g_prof_pool_n) return g_prof_pool[g_prof_pool_used++];
+    if (g_prof_pool_n >= 8192) return nullptr;
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+    g_prof_pool[g_prof_pool_n++] = e;
+    g_prof_pool_used = g_prof_pool_n;
+    return e;
+}
+
+void prof_mark(const char* name, cudaStream_t st, bool begin) {
+    if (!g_prof_on) return;
+    if (begin) {
+        if (g_prof_n >= 4096) return;
+        cudaEvent_t a = prof_event(), b = prof_event();
+        if (!a || !b) return;
+        g_prof[g_prof_n] = {name, a, b};
+        cudaEventRecord(a, st);
+    } else {
+        if (g_prof_n >= 4096 || !g_prof[g_prof_n].name) return;
+        cudaEventRecord(g_prof[g_prof_n].b, st);
+        ++g_prof_n;
+        if (g_prof_n < 4096) g_prof[g_prof_n].name = nullptr;
+    }
+}
+
+// Staging helpers ----------------------------------------------------------
+struct Stager {
+    bool dev;
+    cudaStream_t st;
+    int next_in = S_IN0, next_out = S_OUT0;
+    int rc = XTS_OK;
+    struct Pending { void* host; const void* dptr; size_t bytes; };
+    Pending pend[8];
+    int npend = 0;
+
+    template <typename T>
+    const T* in(const T* p, size_t n) {
+        if (rc || dev || !p || n == 0) return p;
+        void* d = workspace(next_in++, n * sizeof(T));
+        if (!d) { rc = XTS_ERR_OOM; return nullptr; }
+        cudaError_t e = cudaMemcpyAsync(d, p, n * sizeof(T), cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) { rc = cuda_error(e, "cudaMemcpyAsync H2D"); return nullptr; }
+        return (const T*)d;
+    }
+    template <typename T>
+    T* out(T* p, size_t n) {
+        if (rc || dev || !p || n == 0) return p;
+        void* d = workspace(next_out++, n * sizeof(T));
+        if (!d) { rc = XTS_ERR_OOM; return nullptr; }
+        pend[npend++] = {p, d, n * sizeof(T)};
+        return (T*)d;
+    }
+    // scratch output the caller did not ask for
+    template <typename T>
+    T* scratch(size_t n) {
+        if (rc) return nullptr;
+        void* d = workspace(next_out++, n * sizeof(T));
+        if (!d) rc = XTS_ERR_OOM;
+        return (T*)d;
+    }
+    int finish(int launch_rc) {
+        if (rc) return rc;
+        if (launch_rc) return launch_rc;
+        if (dev) return XTS_OK;
+        for (int i = 0; i < npend; ++i) {
+            cudaError_t e = cudaMemcpyAsync(pend[i].host, pend[i].dptr, pend[i].bytes,
+                                            cudaMemcpyDeviceToHost, st);
+            if (e != cudaSuccess) return cuda_error(e, "cudaMemcpyAsync D2H");
+        }
+        XTS_CUDA(cudaStreamSynchronize(st));
+        return XTS_OK;
+    }
+};
+
+static bool grid_ok(const xts_grid* g, int n_par) {
+    return g && g->cosths && g->logEs && g->params && g->n_cos >= 2 && g->n_e >= 2 &&
+           g->n_par == n_par;
+}
+
+static xts_grid stage_grid(Stager& sg, const xts_grid* g) {
+    xts_grid d = *g;
+    d.cosths = sg.in(g->cosths, (size_t)g->n_cos);
+    d.logEs = sg.in(g->logEs, (size_t)g->n_e);
+    d.params = sg.in(g->params, (size_t)g->n_cos * g->n_e * g->n_par);
+    return d;
+}
+
+}  // namespace xts
+
+using namespace xts;
+
+#define XTS_ENTER()                                        \
+    std::lock_guard<std::mutex> lock__(g_mu);              \
+    do {                                                   \
+        int rc__ = ensure_device();                        \
+        if (rc__) return rc__;                             \
+    } while (0)
+
+extern "C" {
+
+int xts_version(void) { return 100; }
+
+const char* xts_last_error(void) { return g_err; }
+
+int xts_init(int device) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (g_ctx.device >= 0 && g_ctx.device != device) release_all();
+    if (g_ctx.device == device) return XTS_OK;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        cudaGetLastError();
+        return set_error(XTS_ERR_NODEV, "device %d not available (%d visible)", device, n);
+    }
+    XTS_CUDA(cudaSetDevice(device));
+    g_ctx.device = -1;
+    if (g_ctx.stream) { cudaStreamDestroy(g_ctx.stream); g_ctx.stream = nullptr; }
+    return ensure_device();
+}
+
+void xts_release(void) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    release_all();
+}
+
+int xts_profile_enable(int on) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    g_prof_on = on != 0;
+    g_prof_n = 0;
+    g_prof_pool_used = 0;
+    g_prof[0].name = nullptr;
+    return XTS_OK;
+}
+
+int xts_profile_read(char* buf, int buflen) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (!buf || buflen < 3) return set_error(XTS_ERR_ARG, "profile_read: buffer too small");
+    const char* names[64];
+    int counts[64];
+    double ms[64];
+    int nk = 0;
+    for (int i = 0; i < g_prof_n; ++i) {
+        cudaError_t e = cudaEventSynchronize(g_prof[i].b);
+        if (e != cudaSuccess) return cuda_error(e, "cudaEventSynchronize");
+        float t = 0.f;
+        cudaEventElapsedTime(&t, g_prof[i].a, g_prof[i].b);
+        int k = 0;
+        while (k < nk && strcmp(names[k], g_prof[i].name) != 0) ++k;
+        if (k == nk) {
+            if (nk == 64) continue;
+            names[nk] = g_prof[i].name; counts[nk] = 0; ms[nk] = 0.; ++nk;
+        }
+        counts[k] += 1;
+        ms[k] += t;
+    }
+    int len = snprintf(buf, buflen, "{");
+    for (int k = 0; k < nk && len < buflen; ++k)
+        len += snprintf(buf + len, buflen - len, "%s\"%s\": [%d, %.6f]", k ? ", " : "", names[k],
+                        counts[k], ms[k]);
+    if (len < buflen) len += snprintf(buf + len, buflen - len, "}");
+    g_prof_n = 0;
+    g_prof_pool_used = 0;
+    g_prof[0].name = nullptr;
+    return len < buflen ? len : set_error(XTS_ERR_ARG, "profile_read: buffer too small");
+}
+
+int xts_livetime_efficiency_factors(const double* logEs, int E, const float* p0, const float* p1,
+                                    double* ltf, unsigned flags, void* stream) {
+    XTS_ENTER();
+    if (E <= 0 || !logEs || !p0 || !p1 || !ltf)
+        return set_error(XTS_ERR_ARG, "livetime_efficiency_factors: bad arguments");
+    Stager sg{(flags & XTS_DEVICE_PTRS) != 0, stream ? (cudaStream_t)stream : g_ctx.stream};
+    const double* d_loge = sg.in(logEs, (size_t)E);
+    const float* d_p0 = sg.in(p0, 6);
+    const float* d_p1 = sg.in(p1, 6);
+    double* d_out = sg.out(ltf, (size_t)2 * E);
+    int rc = sg.rc ? sg.rc : launch_ltf(d_loge, E, d_p0, d_p1, d_out, sg.st);
+    return sg.finish(rc);
+}
+
+int xts_normalize_rpsf(double* params, int Mc, int Me, const double* grid_logEs, float scale0,
+                       float scale1, float scale_index, unsigned flags, void* stream) {
+    XTS_ENTER();
+    if (!params || !grid_logEs || Mc <= 0 || Me <= 0)
+        return set_error(XTS_ERR_ARG, "normalize_rpsf: bad arguments");
+    Stager sg{(flags & XTS_DEVICE_PTRS) != 0, stream ? (cudaStream_t)stream : g_ctx.stream};
+    size_t n = (size_t)Mc * Me * 6;
+    double* d_par = const_cast<double*>(sg.in((const double*)params, n));
+    const double* d_glog = sg.in(grid_logEs, (size_t)Me);
+    if (!sg.dev && !sg.rc) sg.pend[sg.npend++] = {params, d_par, n * sizeof(double)};
+    int rc = sg.rc ? sg.rc
+                   : launch_normalize_rpsf(d_par, Mc, Me, d_glog, scale0, scale1, scale_index, sg.st);
+    return sg.finish(rc);
+}
+
+int xts_compute_exposure(const xts_expcube* cube, const xts_expcube* wcube, const double* logEs,
+                         int E, const double* src_sph, int S, const xts_grid* aeff_front,
+                         const xts_grid* aeff_back, const double* front_ltf,
+                         const xts_exposure_out* out, unsigned flags, void* stream) {
+    XTS_ENTER();
+    if (!cube || !wcube || !cube->cosbins || !wcube->cosbins || !logEs || E <= 0 || S < 0 ||
+        (S > 0 && !src_sph) || !front_ltf || !out)
+        return set_error(XTS_ERR_ARG, "compute_exposure: null argument or bad size");
+    if (cube->nside <= 0 || (cube->nside & (cube->nside - 1)) || cube->nbrbins <= 0 ||
+        wcube->nside != cube->nside || wcube->nbrbins != cube->nbrbins)
+        return set_error(XTS_ERR_ARG, "compute_exposure: livetime cubes need a power-of-two nside and equal shapes");
+    if (!grid_ok(aeff_front, 1) || !grid_ok(aeff_back, 1))
+        return set_error(XTS_ERR_ARG, "compute_exposure: effective-area grids need n_par == 1");
+    int C = cube->nbrbins;
+    long long npix = 12LL * cube->nside * cube->nside;
+    Stager sg{(flags & XTS_DEVICE_PTRS) != 0, stream ? (cudaStream_t)stream : g_ctx.stream};
+    ExposureDev a;
+    a.cube = sg.in(cube->cosbins, (size_t)npix * C);
+    a.wcube = sg.in(wcube->cosbins, (size_t)npix * C);
+    a.nside = cube->nside; a.C = C; a.cosmin = cube->cosmin; a.thetabin = cube->thetabin;
+    a.logEs = sg.in(logEs, (size_t)E); a.E = E;
+    a.src_sph = sg.in(src_sph, (size_t)2 * S); a.S = S;
+    a.af = stage_grid(sg, aeff_front);
+    a.ab = stage_grid(sg, aeff_back);
+    a.ltf = sg.in(front_ltf, (size_t)2 * E);
+    a.exp_costhetas = out->exp_costhetas ? sg.out(out->exp_costhetas, (size_t)C) : sg.scratch<double>(C);
+    a.front_aeff = out->front_aeff ? sg.out(out->front_aeff, (size_t)C * E) : sg.scratch<double>((size_t)C * E);
+    a.back_aeff = out->back_aeff ? sg.out(out->back_aeff, (size_t)C * E) : sg.scratch<double>((size_t)C * E);
+    a.ecb = out->src_exposure_cosbins ? sg.out(out->src_exposure_cosbins, (size_t)S * C) : sg.scratch<double>((size_t)S * C);
+    a.wecb = out->src_weighted_exposure_cosbins ? sg.out(out->src_weighted_exposure_cosbins, (size_t)S * C) : sg.scratch<double>((size_t)S * C);
+    a.exposure = out->exposure ? sg.out(out->exposure, (size_t)S * E) : sg.scratch<double>((size_t)S * E);
+    a.use_tf32 = (flags & XTS_EXPOSURE_TF32) != 0;
+    int rc = sg.rc ? sg.rc : launch_exposure(a, sg.st);
+    return sg.finish(rc);
+}
+
+int xts_exposure_contract(const double* ecb, const double* wecb, int S, int C, const double* af,
+                          const double* ab, const double* ltf, int E, double* exposure,
+                          unsigned flags, void* stream) {
+    XTS_ENTER();
+    if (S < 0 || C <= 0 || E <= 0 || !af || !ab || !ltf || (S > 0 && (!ecb || !wecb || !exposure)))
+        return set_error(XTS_ERR_ARG, "exposure_contract: null argument or bad size");
+    Stager sg{(flags & XTS_DEVICE_PTRS) != 0, stream ? (cudaStream_t)stream : g_ctx.stream};
+    const double* d_ecb = sg.in(ecb, (size_t)S * C);
+    const double* d_wecb = sg.in(wecb, (size_t)S * C);
+    const double* d_af = sg.in(af, (size_t)C * E);
+    const double* d_ab = sg.in(ab, (size_t)C * E);
+    const double* d_ltf = sg.in(ltf, (size_t)2 * E);
+    double* d_out = sg.out(exposure, (size_t)S * E);
+    int rc = sg.rc ? sg.rc
+                   : launch_exposure_contract(d_ecb, d_wecb, S, C, d_af, d_ab, d_ltf, E, d_out,
+                                              (flags & XTS_EXPOSURE_TF32) != 0, sg.st);
+    return sg.finish(rc);
+}
+
+int xts_compute_psf_data(const xts_grid* psf_front, const xts_grid* psf_back,
+                         const double* exp_costhetas, int C, const double* logEs, int E,
+                         const double* front_aeff, const double* back_aeff, const double* ecb,
+                         const double* wecb, int S, const double* front_ltf,
+                         const double* exposure, double* upsf, double* partial, unsigned flags,
+                         void* stream) {
+    XTS_ENTER();
+    if (!grid_ok(psf_front, 6) || !grid_ok(psf_back, 6))
+        return set_error(XTS_ERR_ARG, "compute_psf_data: King grids need n_par == 6");
+    if (!exp_costhetas || C <= 0 || !logEs || E <= 0 || !front_aeff || !back_aeff || S < 0 ||
+        (S > 0 && (!ecb || !wecb || !exposure || !upsf || !partial)) || !front_ltf)
+        return set_error(XTS_ERR_ARG, "compute_psf_data: null argument or bad size");
+    Stager sg{(flags & XTS_DEVICE_PTRS) != 0, stream ? (cudaStream_t)stream : g_ctx.stream};
+    PsfDev a;
+    a.pf = stage_grid(sg, psf_front);
+    a.pb = stage_grid(sg, psf_back);
+    a.costh = sg.in(exp_costhetas, (size_t)C); a.C = C;
+    a.logEs = sg.in(logEs, (size_t)E); a.E = E;
+    a.af = sg.in(front_aeff, (size_t)C * E);
+    a.ab = sg.in(back_aeff, (size_t)C * E);
+    a.ecb = sg.in(ecb, (size_t)S * C);
+    a.wecb = sg.in(wecb, (size_t)S * C); a.S = S;
+    a.ltf = sg.in(front_ltf, (size_t)2 * E);
+    a.exposure = sg.in(exposure, (size_t)S * E);
+    a.upsf = sg.out(upsf, (size_t)S * ND * E);
+    a.partial = sg.out(partial, (size_t)S * ND * E);
+    int rc = sg.rc ? sg.rc : launch_psf(a, sg.st);
+    return sg.finish(rc);
+}
+
+int xts_point_src_model_map_wcs(const xts_wcs* wcs, const double* src_sph, int S,
+                                const double* exposure, const double* upsf, const double* partial,
+                                int E, void* model_map, xts_srcmap_info* info, unsigned flags,
+                                void* stream) {
+    XTS_ENTER();
+    if (!wcs || wcs->naxis1 <= 0 || wcs->naxis2 <= 0 || (wcs->proj != 0 && wcs->proj != 1) ||
+        wcs->cdelt1 == 0. || wcs->cdelt2 == 0.)
+        return set_error(XTS_ERR_ARG, "point_src_model_map_wcs: bad WCS (CAR/AIT, nonzero CDELT)");
+    if (S < 0 || E <= 0 || (S > 0 && (!src_sph || !exposure || !upsf || !partial || !model_map)))
+        return set_error(XTS_ERR_ARG, "point_src_model_map_wcs: null argument or bad size");
+    if ((long long)wcs->naxis1 * wcs->naxis2 > (1LL << 31) - 1 || S > 65535)
+        return set_error(XTS_ERR_ARG, "point_src_model_map_wcs: map or source count too large");
+    bool f64 = (flags & XTS_OUT_F64) != 0;
+    size_t npix = (size_t)wcs->naxis1 * wcs->naxis2;
+    Stager sg{(flags & XTS_DEVICE_PTRS) != 0, stream ? (cudaStream_t)stream : g_ctx.stream};
+    SrcmapDev a;
+    a.wcs = *wcs;
+    a.src_sph = sg.in(src_sph, (size_t)2 * S); a.S = S;
+    a.exposure = sg.in(exposure, (size_t)S * E);
+    a.upsf = sg.in(upsf, (size_t)S * ND * E);
+    a.partial = sg.in(partial, (size_t)S * ND * E); a.E = E;
+    a.out_f64 = f64;
+    a.out = f64 ? (void*)sg.out((double*)model_map, (size_t)S * npix * E)
+                : (void*)sg.out((float*)model_map, (size_t)S * npix * E);
+    a.inv_integ = info ? sg.out(info->inv_map_integral, (size_t)S * E) : nullptr;
+    a.correction = info ? sg.out(info->correction, (size_t)S * E) : nullptr;
+    a.radius = info ? sg.out(info->psf_radius, (size_t)S) : nullptr;
+    a.in_fov = info ? sg.out(info->in_fov, (size_t)S) : nullptr;
+    int rc = sg.rc ? sg.rc : launch_srcmap(a, sg.st);
+    return sg.finish(rc);
+}
+
+}  // extern "C"

@@ -1,0 +1,126 @@
+// xts_internal.cuh -- shared definitions of the CUDA library: constants of the
+// algorithm, error plumbing, the cached device workspace and the launchers each
+// stage exports to the C-ABI layer.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/xtsrcmaps_b200.h"
+
+#define XTS_HD __host__ __device__
+
+namespace xts {
+
+// misc/misc.hxx:15-43 -- constants are part of the algorithm.
+constexpr double PI = 3.141592653589793238462643383279502884197;
+constexpr double TWOPI = 6.283185307179586476925286766559005768394;
+constexpr double HALFPI = 1.570796326794896619231321691639751442099;
+constexpr double INV_HALFPI = 0.6366197723675813430755350534900574;
+constexpr double D2R = 0.017453292519943295769236907684886127134;
+constexpr double R2D = 57.295779513082320876798154814105170332405;
+constexpr double SEP_STEP = 0.033731417579011382769913057686378448039204491;  // ln(7e5)/399
+constexpr double RECIPSTEP = 29.645952402019046699874076387601854602589360539942632073727038565;
+constexpr double REDM1 = 29.148763300179999028597222671574207003288142769360422095500496366;  // 1/(e^step - 1)
+constexpr double LN_1E4 = 9.2103403719761827360719658187374568304044059545150919;
+constexpr int ND = XTS_ND;
+
+// Error plumbing ---------------------------------------------------------------
+int set_error(int code, const char* fmt, ...);
+int cuda_error(cudaError_t e, const char* what);
+
+#define XTS_CUDA(call)                                         \
+    do {                                                       \
+        cudaError_t e__ = (call);                              \
+        if (e__ != cudaSuccess) return ::xts::cuda_error(e__, #call); \
+    } while (0)
+
+#define XTS_CHECK_LAUNCH(name)                                 \
+    do {                                                       \
+        cudaError_t e__ = cudaGetLastError();                  \
+        if (e__ != cudaSuccess) return ::xts::cuda_error(e__, name); \
+    } while (0)
+
+// Optional per-kernel timing (xts_profile_enable): CUDA events recorded on the
+// launching stream around each kernel.  A no-op while profiling is off.
+void prof_mark(const char* name, cudaStream_t st, bool begin);
+
+// Launch a kernel, time it when profiling is on, and check the launch.
+#define XTS_LAUNCH(name, st, ...)                              \
+    do {                                                       \
+        ::xts::prof_mark(name, st, true);                      \
+        __VA_ARGS__;                                           \
+        ::xts::prof_mark(name, st, false);                     \
+        XTS_CHECK_LAUNCH(name);                                \
+    } while (0)
+
+// Grow-only device workspace, one buffer per slot ------------------------------
+enum Slot {
+    // staged inputs / outputs (host-pointer mode)
+    S_IN0, S_IN1, S_IN2, S_IN3, S_IN4, S_IN5, S_IN6, S_IN7, S_IN8, S_IN9, S_IN10, S_IN11,
+    S_IN12, S_IN13, S_IN14, S_IN15, S_IN16, S_IN17,
+    S_OUT0, S_OUT1, S_OUT2, S_OUT3, S_OUT4, S_OUT5, S_OUT6,
+    // internal scratch
+    W_CORNERS, W_CENTERS, W_OMEGA, W_LUT, W_PARTSUM, W_SRCINFO, W_SCALE, W_PSFTAB,
+    W_KING, W_MISC,
+    N_SLOTS
+};
+void* workspace(int slot, size_t bytes);  // nullptr + error set on OOM
+cudaStream_t default_stream();
+int ensure_device();
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// Per-source geometry produced by the boundary-radius kernel (c6).
+struct SrcInfo {
+    double dir[3];
+    double radius_deg;
+    double radius_rad;
+    int in_fov;
+    int pad;
+};
+
+// Stage launchers (device pointers, enqueue on `st`) ----------------------------
+struct ExposureDev {
+    const float* cube; const float* wcube; long long nside; int C; double cosmin; int thetabin;
+    const double* logEs; int E;
+    const double* src_sph; int S;
+    xts_grid af, ab;  // device pointers inside
+    const double* ltf;
+    double* exp_costhetas; double* front_aeff; double* back_aeff;
+    double* ecb; double* wecb; double* exposure;
+    bool use_tf32;
+};
+int launch_exposure(const ExposureDev& a, cudaStream_t st);
+int launch_exposure_contract(const double* ecb, const double* wecb, int S, int C, const double* af,
+                             const double* ab, const double* ltf, int E, double* out, bool tf32,
+                             cudaStream_t st);
+int launch_tf32_exposure(const double* ecb, const double* wecb, int S, int C, const double* af,
+                         const double* ab, const double* ltf, int E, double* out, cudaStream_t st);
+
+int launch_ltf(const double* logEs, int E, const float* p0, const float* p1, double* ltf,
+               cudaStream_t st);
+int launch_normalize_rpsf(double* params, int Mc, int Me, const double* glog, float s0,
+                          float s1, float si, cudaStream_t st);
+
+struct PsfDev {
+    xts_grid pf, pb;  // device pointers inside
+    const double* costh; int C;
+    const double* logEs; int E;
+    const double* af; const double* ab;
+    const double* ecb; const double* wecb; int S;
+    const double* ltf; const double* exposure;
+    double* upsf; double* partial;
+};
+int launch_psf(const PsfDev& a, cudaStream_t st);
+
+struct SrcmapDev {
+    xts_wcs wcs;
+    const double* src_sph; int S;
+    const double* exposure; const double* upsf; const double* partial; int E;
+    void* out; bool out_f64;
+    double* inv_integ; double* correction; double* radius; int* in_fov;  // optional (may be null)
+};
+int launch_srcmap(const SrcmapDev& a, cudaStream_t st);
+
+}  // namespace xts

@@ -1,0 +1,160 @@
+// xts_psf.cu -- step (b): exposure-weighted mean King PSF tables.
+//
+//   b2 separations            psf/psf.hxx:24-31
+//   b3 King table [D,Mc,Me]   psf/psf.king.cxx:9-43
+//   b4 bilerp -> [C,D,E]      psf/psf.bilerp.cxx:6-52
+//   b5 corrected_exposure_psf psf/psf.corrected_exposure_psf.cxx:12-120
+//   b6 mean_psf               psf/psf.mean_psf.cxx:6-33
+//   b7 partial/total, normalise psf/psf.partial_total_integral.cxx:8-52, psf/psf.normalize.cxx:7-24
+//
+// Front and back both use the front livetime-efficiency factors
+// (psf.psf_lookup_table_and_partial_integrals.cxx:151-156), so the two sides'
+// psf*aeff tables are summed before the contraction over cos-theta:
+//   mean[s,d,e] = (sum_c (X[s,c] L0[e] + W[s,c] L1[e]) (Pf Af + Pb Ab)[c,d,e]) / exposure[s,e]
+// which is the reference's four DGEMMs and three sums reassociated.
+#include <math.h>
+
+#include "xts_internal.cuh"
+
+namespace xts {
+
+__device__ __forceinline__ double sep_deg(int d) {  // psf/psf.hxx:24-31
+    const double xstep = log(70. / 1e-4) / (400 - 1.);
+    return d == 0 ? 0.0 : 1e-4 * exp((d - 1) * xstep);
+}
+
+__device__ inline double king_f2(double u, double g) {
+    if (g == 1) g = 1.001;
+    return (1. - 1. / g) * pow(1. + u / g, -g);
+}
+
+// b3: K[side][d][c][e] = evaluate_king(sep[d] rad, 1, params[c,e,:]) (irf/irf.hxx:22-45)
+__global__ void k_king(xts_grid pf, xts_grid pb, double* kf, double* kb) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int side = blockIdx.y;
+    const xts_grid& g = side ? pb : pf;
+    int McMe = g.n_cos * g.n_e;
+    if (i >= ND * McMe) return;
+    int d = i / McMe, ce = i - d * McMe;
+    const double* p = g.params + (size_t)ce * 6;
+    double sep = sep_deg(d) * D2R;
+    double ncore = p[0], ntail = p[1], score = p[2], stail = p[3];
+    double rc = sep / score, uc = rc * rc / 2.;
+    double rt = sep / stail, ut = rt * rt / 2.;
+    (side ? kb : kf)[i] = ncore * king_f2(uc, p[4]) + ntail * ncore * king_f2(ut, p[5]);
+}
+
+__device__ inline void lerp_pars2(const double* g, int n, double v, double* wgt, double* cmpl,
+                                  int* idx) {
+    int lo = 0, hi = n;
+    while (lo < hi) { int m = (lo + hi) >> 1; if (v < g[m]) hi = m; else lo = m + 1; }
+    int i = lo < 1 ? 1 : (lo > n - 1 ? n - 1 : lo);
+    double t = (v - g[i - 1]) / (g[i] - g[i - 1]);
+    *wgt = t; *cmpl = 1. - t; *idx = i;
+}
+
+// b4 + the aeff product of b5, both sides summed: PA[c][d][e].
+__global__ void k_psf_aeff(xts_grid pf, xts_grid pb, const double* kf, const double* kb,
+                           const double* costh, int C, const double* logEs, int E,
+                           const double* af, const double* ab, double* pa) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= C * ND * E) return;
+    int e = i % E;
+    int cd = i / E;
+    int d = cd % ND, c = cd / ND;
+    double v = 0.;
+    for (int side = 0; side < 2; ++side) {
+        const xts_grid& g = side ? pb : pf;
+        const double* K = (side ? kb : kf) + (size_t)d * g.n_cos * g.n_e;
+        double cw, cc, ew, ec; int ci, ei;
+        lerp_pars2(g.cosths, g.n_cos, costh[c], &cw, &cc, &ci);
+        lerp_pars2(g.logEs, g.n_e, logEs[e], &ew, &ec, &ei);
+        int Me = g.n_e;
+        double b = cc * ec * K[(ci - 1) * Me + ei - 1] + cc * ew * K[(ci - 1) * Me + ei] +
+                   cw * ec * K[ci * Me + ei - 1] + cw * ew * K[ci * Me + ei];
+        v += b * (side ? ab : af)[c * E + e];
+    }
+    pa[i] = v;
+}
+
+// b5 + b6: mean[s, de] for a tile of sources; each thread keeps the C values of
+// its (d, e) column in registers and reuses them across the tile's sources.
+constexpr int PSF_TILE_S = 16;
+constexpr int PSF_MAX_C = 64;
+
+__global__ void __launch_bounds__(128) k_mean_psf(const double* pa, int C, int E, const double* ecb,
+                                                  const double* wecb, int S, const double* ltf,
+                                                  const double* expo, double* out) {
+    __shared__ double sx[PSF_TILE_S][PSF_MAX_C];
+    __shared__ double sw[PSF_TILE_S][PSF_MAX_C];
+    int s0 = blockIdx.y * PSF_TILE_S;
+    int ns = min(PSF_TILE_S, S - s0);
+    for (int k = threadIdx.x; k < ns * C; k += blockDim.x) {
+        int s = k / C, c = k - s * C;
+        sx[s][c] = ecb[(size_t)(s0 + s) * C + c];
+        sw[s][c] = wecb[(size_t)(s0 + s) * C + c];
+    }
+    __syncthreads();
+    int DE = ND * E;
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= DE) return;
+    int e = j % E;
+    double col[PSF_MAX_C];
+#pragma unroll 8
+    for (int c = 0; c < C; ++c) col[c] = pa[(size_t)c * DE + j];
+    double l0 = ltf[e], l1 = ltf[E + e];
+    for (int s = 0; s < ns; ++s) {
+        double x = 0., w = 0.;
+#pragma unroll 8
+        for (int c = 0; c < C; ++c) { x = fma(sx[s][c], col[c], x); w = fma(sw[s][c], col[c], w); }
+        out[(size_t)(s0 + s) * DE + j] = (x * l0 + w * l1) / expo[(size_t)(s0 + s) * E + e];
+    }
+}
+
+// b7: per (s, e) exact integral of the linear interpolant of 2 pi u(theta) sin(theta)
+// per separation bin, prefix sum, normalised partials; then uPsf /= total.
+__global__ void k_partial_integral(double* upsf, double* partial, int S, int E) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S * E) return;
+    int s = i / E, e = i - s * E;
+    double* u = upsf + (size_t)s * ND * E + e;
+    double* p = partial + (size_t)s * ND * E + e;
+    double cum = 0.0;
+    p[0] = 0.0;
+    double t1 = 0.0, y1 = TWOPI * u[0] * sin(t1);
+    for (int d = 1; d < ND; ++d) {
+        double t2 = D2R * sep_deg(d);
+        double y2 = TWOPI * u[(size_t)d * E] * sin(t2);
+        double m = (y2 - y1) / (t2 - t1);
+        double b = y1 - t1 * m;
+        double v = 0.5 * m * (t2 * t2 - t1 * t1) + b * (t2 - t1);
+        cum += v;
+        p[(size_t)d * E] = cum;
+        t1 = t2; y1 = y2;
+    }
+    if (cum != 0.)
+        for (int d = 0; d < ND; ++d) p[(size_t)d * E] /= cum;
+    for (int d = 0; d < ND; ++d) u[(size_t)d * E] /= cum;
+}
+
+int launch_psf(const PsfDev& a, cudaStream_t st) {
+    if (a.C > PSF_MAX_C) return set_error(XTS_ERR_ARG, "compute_psf_data: C=%d exceeds %d", a.C, PSF_MAX_C);
+    size_t kf_n = (size_t)ND * a.pf.n_cos * a.pf.n_e, kb_n = (size_t)ND * a.pb.n_cos * a.pb.n_e;
+    double* king = (double*)workspace(W_KING, sizeof(double) * (kf_n + kb_n));
+    double* pa = (double*)workspace(W_PSFTAB, sizeof(double) * (size_t)a.C * ND * a.E);
+    if (!king || !pa) return XTS_ERR_OOM;
+    int mx = (int)(kf_n > kb_n ? kf_n : kb_n);
+    XTS_LAUNCH("k_king", st, k_king<<<dim3((mx + 127) / 128, 2), 128, 0, st>>>(a.pf, a.pb, king, king + kf_n));
+    int n = a.C * ND * a.E;
+    XTS_LAUNCH("k_psf_aeff", st, k_psf_aeff<<<(n + 127) / 128, 128, 0, st>>>(a.pf, a.pb, king, king + kf_n, a.costh, a.C,
+                                               a.logEs, a.E, a.af, a.ab, pa));
+    if (a.S == 0) return XTS_OK;
+    int DE = ND * a.E;
+    dim3 g((DE + 127) / 128, (a.S + PSF_TILE_S - 1) / PSF_TILE_S);
+    XTS_LAUNCH("k_mean_psf", st, k_mean_psf<<<g, 128, 0, st>>>(pa, a.C, a.E, a.ecb, a.wecb, a.S, a.ltf, a.exposure, a.upsf));
+    n = a.S * a.E;
+    XTS_LAUNCH("k_partial_integral", st, k_partial_integral<<<(n + 127) / 128, 128, 0, st>>>(a.upsf, a.partial, a.S, a.E));
+    return XTS_OK;
+}
+
+}  // namespace xts

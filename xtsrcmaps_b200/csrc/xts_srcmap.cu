@@ -1,0 +1,403 @@
+// xts_srcmap.cu -- steps (c) and (d): pixel geometry, per-pixel cubature of the
+// mean PSF, per-map normalisation and the scaled source-map write.
+//
+//   c1 pix2dir / dir_diff             sky_geom/sky_geom.hxx:237-310
+//   c2 square_ptswts (12-point rule)  model_map/mm_cubature/points_weights.hpp:5-56
+//   c3 separation + LUT column        model_map/mm_cubature/convolve_pixel_psf_logsep.hpp:39-55
+//   d1 pixel cubature                 model_map/mm_cubature/cubature.implementation.cxx:21-55
+//   d2 scale_map_by_solid_angle       model_map.scale_map_by_solid_angle.cxx:5-26, math/solid_angle.hpp:42-79
+//   c6 psf_boundary_radius            model_map.psf_boundary_radius.cxx:9-62
+//   c7 map_integral                   model_map.map_integral.cxx:4-48
+//   c8 scale_map_by_exposure          model_map.scale_map_by_exposure.cxx:4-28
+//   c9 map_correction_factor          model_map.map_correction_factor.cxx:3-53,
+//                                     psf/psf.fast_separation_lower_index.cxx:5-22
+//   c10 scale_map_by_correction       model_map.scale_map_by_correction_factor.cxx:4-27
+//
+// The LUT kernel follows the intended semantics of convolve_pixel_psf_logsep:
+// the shipped code never stores its column keys (keys[index] = psfidx is
+// missing), so every point would read rows -1 and 0 of the table.  Here the key
+// is stored, which equals convolve_pixel_psf_searchsep inside [3e-4, 60] deg and
+// keeps logsep's row-400 clamp and its extrapolation below 1e-4 deg.
+//
+// The map is written once: a first pass (k_map_integral) evaluates the
+// cubature only for in-FOV sources and only for pixels whose centre lies within
+// the boundary radius, in FP64, and reduces per tile; k_correction folds the
+// tiles in a fixed order into 1/sum and the containment factor; the write pass
+// (k_srcmap) evaluates every pixel again and stores raw * omega * exposure *
+// factor.  Re-evaluating the disk costs less than writing the raw map and
+// reading it back.
+#include <math.h>
+
+#include <type_traits>
+
+#include "xts_geom.cuh"
+#include "xts_internal.cuh"
+
+namespace xts {
+
+// Sommariva & Festa degree-7 12-point rule on [-1,1]^2 (Padova
+// "cub_square_lowcard"), as tabulated in model_map/mm_cubature/cubature.hpp:209-225.
+static const double SQUARE_DEG7[36] = {
+    3.9383136101878902e-01, -3.6699793434042738e-01, 5.2092862230230441e-01,
+    8.0196847620659251e-01, 8.0992592975809186e-01, 2.3740240561379911e-01,
+    -1.8327327664247231e-02, 9.2596092593108370e-01, 2.4166897208389651e-01,
+    3.6699793434042738e-01, 3.9383136101878902e-01, 5.2092862230230441e-01,
+    -8.0992592975809186e-01, 8.0196847620659251e-01, 2.3740240561379911e-01,
+    -9.2596092593108370e-01, -1.8327327664247231e-02, 2.4166897208389651e-01,
+    -3.9383136101878902e-01, 3.6699793434042738e-01, 5.2092862230230441e-01,
+    -8.0196847620659251e-01, -8.0992592975809186e-01, 2.3740240561379911e-01,
+    1.8327327664247231e-02, -9.2596092593108370e-01, 2.4166897208389651e-01,
+    -3.6699793434042738e-01, -3.9383136101878902e-01, 5.2092862230230441e-01,
+    8.0992592975809186e-01, -8.0196847620659251e-01, 2.3740240561379911e-01,
+    9.2596092593108370e-01, 1.8327327664247231e-02, 2.4166897208389651e-01,
+};
+
+constexpr int NPTS = 12;
+// Per point: 0.25*(1-u)(1-v), 0.25*(1+u)(1-v), 0.25*(1+u)(1+v), 0.25*(1-u)(1+v)
+// (corner weights for LL, LR, UR, UL) and 0.25*w.  Scaling by 0.25 is exact, so
+// these reproduce points_weights.hpp:96-107 bit for bit.
+__constant__ double c_blend[NPTS][5];
+
+static int upload_rule(cudaStream_t st) {
+    static int dev_done = -1;
+    int dev = -1;
+    cudaGetDevice(&dev);
+    if (dev_done == dev) return XTS_OK;
+    double b[NPTS][5];
+    for (int p = 0; p < NPTS; ++p) {
+        double u = SQUARE_DEG7[3 * p], v = SQUARE_DEG7[3 * p + 1];
+        b[p][0] = 0.25 * ((1.0 - u) * (1.0 - v));
+        b[p][1] = 0.25 * ((1.0 + u) * (1.0 - v));
+        b[p][2] = 0.25 * ((1.0 + u) * (1.0 + v));
+        b[p][3] = 0.25 * ((1.0 - u) * (1.0 + v));
+        b[p][4] = 0.25 * SQUARE_DEG7[3 * p + 2];
+    }
+    XTS_CUDA(cudaMemcpyToSymbolAsync(c_blend, b, sizeof(b), 0, cudaMemcpyHostToDevice, st));
+    XTS_CUDA(cudaStreamSynchronize(st));
+    dev_done = dev;
+    return XTS_OK;
+}
+
+// ---------------------------------------------------------------- geometry grids
+// corners[i][j] = pix2dir(i + 0.5, j + 0.5), centres[i][j] = pix2dir(i + 1, j + 1),
+// i in [0, H], j in [0, W] (1-based FITS pixels).
+__global__ void k_grids(WcsDev w, int H, int W, double* corners, double* centers) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    int W1 = W + 1;
+    if (k >= (H + 1) * W1) return;
+    int i = k / W1, j = k - i * W1;
+    double v[3];
+    pix2dir(w, i + 0.5, j + 0.5, v);
+    corners[3 * k] = v[0]; corners[3 * k + 1] = v[1]; corners[3 * k + 2] = v[2];
+    pix2dir(w, i + 1.0, j + 1.0, v);
+    centers[3 * k] = v[0]; centers[3 * k + 1] = v[1]; centers[3 * k + 2] = v[2];
+}
+
+__device__ inline double quad_half(const double* P, const double* Q, const double* R) {
+    double u[3] = {P[0] - Q[0], P[1] - Q[1], P[2] - Q[2]};
+    double v[3] = {P[0] - R[0], P[1] - R[1], P[2] - R[2]};
+    double nu = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    double nv = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    for (int k = 0; k < 3; ++k) { u[k] /= nu; v[k] /= nv; }
+    double c0 = u[1] * v[2] - u[2] * v[1], c1 = u[2] * v[0] - u[0] * v[2], c2 = u[0] * v[1] - u[1] * v[0];
+    return dir_diff(P, Q) * dir_diff(P, R) * sqrt(c0 * c0 + c1 * c1 + c2 * c2);
+}
+
+// d2: solid angle of the quad of pixel centres (h+1,w+1),(h+1,w+2),(h+2,w+2),(h+2,w+1).
+__global__ void k_solid_angle(const double* centers, int H, int W, double* omega) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= H * W) return;
+    int h = k / W, w = k - h * W, W1 = W + 1;
+    const double* A = centers + 3 * (h * W1 + w);
+    const double* B = centers + 3 * (h * W1 + w + 1);
+    const double* C = centers + 3 * ((h + 1) * W1 + w + 1);
+    const double* D = centers + 3 * ((h + 1) * W1 + w);
+    omega[k] = 0.5 * (quad_half(A, B, D) + quad_half(C, B, D));
+}
+
+// c6: in-FOV flag (3.5 pixel buffer) and the minimum distance to the map edge,
+// sampled at the corner grid's border.  One block per source.
+__global__ void k_boundary(WcsDev w, const double* src_sph, int H, int W, const double* corners,
+                           SrcInfo* info) {
+    int s = blockIdx.x;
+    double ra = src_sph[2 * s], dec = src_sph[2 * s + 1];
+    double sd[3];
+    sph2dir(ra, dec, sd);
+    int W1 = W + 1;
+    int nb = 2 * (H + 1) + 2 * (W + 1);
+    double mn = 360.;
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+        int i, j;
+        if (k < H + 1) { i = k; j = 0; }
+        else if (k < 2 * (H + 1)) { i = k - (H + 1); j = W; }
+        else if (k < 2 * (H + 1) + W + 1) { i = 0; j = k - 2 * (H + 1); }
+        else { i = H; j = k - 2 * (H + 1) - (W + 1); }
+        double d = R2D * dir_diff(sd, corners + 3 * (i * W1 + j));
+        mn = mn < d ? mn : d;
+    }
+    for (int o = 16; o > 0; o >>= 1) { double t = __shfl_xor_sync(0xffffffffu, mn, o); mn = mn < t ? mn : t; }
+    __shared__ double red[32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mn;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < (int)(blockDim.x + 31) / 32; ++k) mn = mn < red[k] ? mn : red[k];
+        double r = ra > 180. ? ra - 360. : (ra < -180. ? ra + 360. : ra), p1, p2;
+        sph2pix(w, r, dec, &p1, &p2);
+        const double buf = 3.5;
+        SrcInfo si;
+        si.dir[0] = sd[0]; si.dir[1] = sd[1]; si.dir[2] = sd[2];
+        si.radius_deg = mn;
+        si.radius_rad = D2R * mn;
+        si.in_fov = p1 > buf && p1 < (H - buf) && p2 > buf && p2 < (W - buf);
+        si.pad = 0;
+        info[s] = si;
+    }
+}
+
+// FP32 copy of each source's mean-PSF table, energies padded to Epad.
+__global__ void k_lut32(const double* upsf, int S, int E, int Epad, float* lut) {
+    size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    size_t n = (size_t)S * ND * Epad;
+    if (k >= n) return;
+    int e = (int)(k % Epad);
+    size_t sd = k / Epad;
+    lut[k] = e < E ? (float)upsf[sd * E + e] : 0.f;
+}
+
+// ---------------------------------------------------------------- cubature core
+// c2 + c3 for one pixel: the 12 rule points, their LUT columns and the
+// collapsed interpolation weights, in order of first appearance.
+__device__ __forceinline__ int pixel_columns(const double* corners, int W1, int h, int w,
+                                             const double* src, int* keys, double* va, double* vb) {
+    const double* a = corners + 3 * (h * W1 + w);            // LL (h+0.5, w+0.5)
+    const double* b = corners + 3 * (h * W1 + w + 1);        // LR (h+0.5, w+1.5)
+    const double* c = corners + 3 * ((h + 1) * W1 + w + 1);  // UR (h+1.5, w+1.5)
+    const double* d = corners + 3 * ((h + 1) * W1 + w);      // UL (h+1.5, w+0.5)
+    double A[3] = {a[0], a[1], a[2]}, B[3] = {b[0], b[1], b[2]};
+    double Cc[3] = {c[0], c[1], c[2]}, D[3] = {d[0], d[1], d[2]};
+    int n = 0;
+#pragma unroll
+    for (int p = 0; p < NPTS; ++p) {
+        double nn = c_blend[p][0], pn = c_blend[p][1], pp = c_blend[p][2], np = c_blend[p][3];
+        double wt = c_blend[p][4];
+        double x = (nn * A[0] + pn * B[0] + pp * Cc[0] + np * D[0]) - src[0];
+        double y = (nn * A[1] + pn * B[1] + pp * Cc[1] + np * D[1]) - src[1];
+        double z = (nn * A[2] + pn * B[2] + pp * Cc[2] + np * D[2]) - src[2];
+        double s = 2.0 * R2D * asin(0.5 * sqrt(x * x + y * y + z * z));
+        double j = s < 1e-4 ? 1. : 1. + RECIPSTEP * (LN_1E4 + log(s));
+        int idx = 1 + (int)j;
+        idx = idx > 400 ? 400 : (idx < 2 ? 2 : idx);  // the lower clamp only catches non-finite input
+        double t = REDM1 * (s * 1e4 * exp(SEP_STEP * (2. - idx)) - 1.);
+        int k = 0;
+        while (k < n && keys[k] != idx) ++k;
+        if (k == n) { keys[n] = idx; va[n] = 0.; vb[n] = 0.; ++n; }
+        va[k] += (1.0 - t) * wt;
+        vb[k] += t * wt;
+    }
+    return n;
+}
+
+constexpr int TP = 128;  // pixels per tile (flat h*W + w order)
+
+struct PixCols32 { float va[NPTS], vb[NPTS]; short key[NPTS]; int n; };
+struct PixCols64 { double va[NPTS], vb[NPTS]; short key[NPTS]; int n; };
+
+// c7 pass: per (tile, source) FP64 sums over pixels whose centre lies within
+// the boundary radius of sum_columns (va U[k-1] + vb U[k]) * omega.
+__global__ void __launch_bounds__(TP) k_map_integral(const double* corners, const double* centers,
+                                                     const double* omega, const SrcInfo* info,
+                                                     const double* upsf, int H, int W, int E,
+                                                     int ntiles, double* partsum) {
+    __shared__ PixCols64 cols[TP];
+    __shared__ double som[TP];
+    __shared__ int any;
+    int tile = blockIdx.x, s = blockIdx.y;
+    double* out = partsum + ((size_t)s * ntiles + tile) * E;
+    SrcInfo si = info[s];
+    if (!si.in_fov) {
+        for (int e = threadIdx.x; e < E; e += blockDim.x) out[e] = 0.;
+        return;
+    }
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    int npix = H * W, W1 = W + 1;
+    int pix = tile * TP + threadIdx.x;
+    int n = 0;
+    if (pix < npix) {
+        int h = pix / W, w = pix - h * W;
+        double rad = dir_diff(si.dir, centers + 3 * (h * W1 + w));
+        if (rad <= si.radius_rad) {
+            int keys[NPTS]; double va[NPTS], vb[NPTS];
+            n = pixel_columns(corners, W1, h, w, si.dir, keys, va, vb);
+            for (int k = 0; k < n; ++k) { cols[threadIdx.x].key[k] = (short)keys[k]; cols[threadIdx.x].va[k] = va[k]; cols[threadIdx.x].vb[k] = vb[k]; }
+            som[threadIdx.x] = omega[pix];
+            any = 1;
+        }
+    }
+    cols[threadIdx.x].n = n;
+    __syncthreads();
+    if (!any) {
+        for (int e = threadIdx.x; e < E; e += blockDim.x) out[e] = 0.;
+        return;
+    }
+    const double* U = upsf + (size_t)s * ND * E;
+    for (int e = threadIdx.x; e < E; e += blockDim.x) {
+        double acc = 0.;
+        for (int p = 0; p < TP; ++p) {
+            int np_ = cols[p].n;
+            if (!np_) continue;
+            double raw = 0.;
+            for (int k = 0; k < np_; ++k) {
+                int key = cols[p].key[k];
+                raw += (cols[p].va[k] * U[(size_t)(key - 1) * E + e]) + (cols[p].vb[k] * U[(size_t)key * E + e]);
+            }
+            acc += raw * som[p];
+        }
+        out[e] = acc;
+    }
+}
+
+// c7 (1/sum) + c9 (containment factor) + c8/c10 folded into one per-(s,e) scale.
+__global__ void k_correction(const double* partsum, int ntiles, const SrcInfo* info,
+                             const double* upsf, const double* partial, const double* expo, int S,
+                             int E, double* scale, double* inv_out, double* fac_out,
+                             double* rad_out, int* fov_out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S * E) return;
+    int s = i / E, e = i - s * E;
+    SrcInfo si = info[s];
+    double sum = 0.;
+    for (int t = 0; t < ntiles; ++t) sum += partsum[((size_t)s * ntiles + t) * E + e];
+    double inv = sum != 0. ? 1.0 / sum : sum;
+    double factor;
+    if (!si.in_fov) factor = 1.0;
+    else {
+        double v0 = si.radius_deg;
+        int li = v0 < 1. ? 1 : (int)floor(1. + log(1e4 * v0) * RECIPSTEP);
+        int d = li >= ND - 2 ? ND - 2 : li;
+        const double xstep = log(70. / 1e-4) / (400 - 1.);
+        double t1 = (d == 0 ? 0. : 1e-4 * exp((d - 1) * xstep)) * D2R;
+        double t2 = (1e-4 * exp(d * xstep)) * D2R;
+        const double* U = upsf + (size_t)s * ND * E;
+        double y1 = TWOPI * U[(size_t)d * E + e] * sin(t1);
+        double y2 = TWOPI * U[(size_t)(d + 1) * E + e] * sin(t2);
+        double m = (y2 - y1) / (t2 - t1);
+        double b = y1 - t1 * m;
+        double v = 0.5 * m * (t2 * t2 - t1 * t1) + b * (t2 - t1);
+        double integ = v + partial[(size_t)s * ND * E + (size_t)d * E + e];
+        integ = integ > 1.0 ? 1.0 : integ;
+        factor = integ * inv;
+    }
+    scale[i] = expo[i] * factor;
+    if (inv_out) inv_out[i] = inv;
+    if (fac_out) fac_out[i] = factor;
+    if (e == 0) {
+        if (rad_out) rad_out[s] = si.radius_deg;
+        if (fov_out) fov_out[s] = si.in_fov;
+    }
+}
+
+// d1 + d2 + c8 + c10: evaluate every pixel of a tile and write the scaled map.
+// Phase 1: one thread per pixel computes its columns (FP64 separations).
+// Phase 2: threads walk the tile's output in flat (pixel, energy) order so
+// global stores are coalesced.
+template <bool F64>
+__global__ void __launch_bounds__(TP) k_srcmap(const double* corners, const double* omega,
+                                               const SrcInfo* info, const float* lut32,
+                                               const double* upsf, const double* scale, int H,
+                                               int W, int E, int Epad, void* outp) {
+    __shared__ typename std::conditional<F64, PixCols64, PixCols32>::type cols[TP];
+    __shared__ double som[TP];
+    int tile = blockIdx.x, s = blockIdx.y;
+    int npix = H * W, W1 = W + 1;
+    int pix0 = tile * TP;
+    int npt = min(TP, npix - pix0);
+    SrcInfo si = info[s];
+    if (threadIdx.x < npt) {
+        int pix = pix0 + threadIdx.x;
+        int h = pix / W, w = pix - h * W;
+        int keys[NPTS]; double va[NPTS], vb[NPTS];
+        int n = pixel_columns(corners, W1, h, w, si.dir, keys, va, vb);
+        for (int k = 0; k < n; ++k) {
+            cols[threadIdx.x].key[k] = (short)keys[k];
+            cols[threadIdx.x].va[k] = va[k];
+            cols[threadIdx.x].vb[k] = vb[k];
+        }
+        cols[threadIdx.x].n = n;
+        som[threadIdx.x] = omega[pix];
+    }
+    __syncthreads();
+    const double* sc = scale + (size_t)s * E;
+    size_t base = ((size_t)s * npix + pix0) * E;
+    int nout = npt * E;
+    if (F64) {
+        const double* U = upsf + (size_t)s * ND * E;
+        double* out = (double*)outp + base;
+        for (int f = threadIdx.x; f < nout; f += blockDim.x) {
+            int p = f / E, e = f - p * E;
+            const PixCols64& c = *(const PixCols64*)&cols[p];
+            double raw = 0.;
+            for (int k = 0; k < c.n; ++k)
+                raw += (c.va[k] * U[(size_t)(c.key[k] - 1) * E + e]) + (c.vb[k] * U[(size_t)c.key[k] * E + e]);
+            out[f] = ((raw * som[p]) * sc[e]);
+        }
+    } else {
+        const float* Y = lut32 + (size_t)s * ND * Epad;
+        float* out = (float*)outp + base;
+        for (int f = threadIdx.x; f < nout; f += blockDim.x) {
+            int p = f / E, e = f - p * E;
+            const PixCols32& c = *(const PixCols32*)&cols[p];
+            // compensated (Neumaier) sum over the pixel's columns
+            float acc = 0.f, comp = 0.f;
+            for (int k = 0; k < c.n; ++k) {
+                float term = fmaf(c.va[k], __ldg(Y + (c.key[k] - 1) * Epad + e), c.vb[k] * __ldg(Y + c.key[k] * Epad + e));
+                float t = acc + term;
+                comp += fabsf(acc) >= fabsf(term) ? (acc - t) + term : (term - t) + acc;
+                acc = t;
+            }
+            out[f] = (float)((double)(acc + comp) * (som[p] * sc[e]));
+        }
+    }
+}
+
+int launch_srcmap(const SrcmapDev& a, cudaStream_t st) {
+    int rc = upload_rule(st);
+    if (rc) return rc;
+    int H = (int)a.wcs.naxis1, W = (int)a.wcs.naxis2, S = a.S, E = a.E;
+    WcsDev w = make_wcs(a.wcs);
+    size_t ng = (size_t)(H + 1) * (W + 1);
+    int npix = H * W;
+    int ntiles = (npix + TP - 1) / TP;
+    int Epad = (E + 3) & ~3;
+    double* corners = (double*)workspace(W_CORNERS, sizeof(double) * 3 * ng);
+    double* centers = (double*)workspace(W_CENTERS, sizeof(double) * 3 * ng);
+    double* omega = (double*)workspace(W_OMEGA, sizeof(double) * npix);
+    SrcInfo* info = (SrcInfo*)workspace(W_SRCINFO, sizeof(SrcInfo) * (S > 0 ? S : 1));
+    double* partsum = (double*)workspace(W_PARTSUM, sizeof(double) * (size_t)S * ntiles * E + 8);
+    double* scale = (double*)workspace(W_SCALE, sizeof(double) * (size_t)S * E + 8);
+    float* lut = a.out_f64 ? nullptr : (float*)workspace(W_LUT, sizeof(float) * (size_t)S * ND * Epad + 16);
+    if (!corners || !centers || !omega || !info || !partsum || !scale || (!a.out_f64 && !lut))
+        return XTS_ERR_OOM;
+    XTS_LAUNCH("k_grids", st, k_grids<<<(unsigned)((ng + 127) / 128), 128, 0, st>>>(w, H, W, corners, centers));
+    XTS_LAUNCH("k_solid_angle", st, k_solid_angle<<<(npix + 127) / 128, 128, 0, st>>>(centers, H, W, omega));
+    if (S == 0) return XTS_OK;
+    XTS_LAUNCH("k_boundary", st, k_boundary<<<S, 128, 0, st>>>(w, a.src_sph, H, W, corners, info));
+    if (!a.out_f64) {
+        size_t n = (size_t)S * ND * Epad;
+        XTS_LAUNCH("k_lut32", st, k_lut32<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a.upsf, S, E, Epad, lut));
+    }
+    XTS_LAUNCH("k_map_integral", st, k_map_integral<<<dim3(ntiles, S), TP, 0, st>>>(corners, centers, omega, info, a.upsf, H, W, E,
+                                                   ntiles, partsum));
+    XTS_LAUNCH("k_correction", st, k_correction<<<(S * E + 127) / 128, 128, 0, st>>>(partsum, ntiles, info, a.upsf, a.partial,
+                                                     a.exposure, S, E, scale, a.inv_integ,
+                                                     a.correction, a.radius, a.in_fov));
+    if (a.out_f64)
+        k_srcmap<true><<<dim3(ntiles, S), TP, 0, st>>>(corners, omega, info, lut, a.upsf, scale, H, W,
+                                                       E, Epad, a.out);
+    else
+        XTS_LAUNCH("k_srcmap", st, k_srcmap<false><<<dim3(ntiles, S), TP, 0, st>>>(corners, omega, info, lut, a.upsf, scale, H,
+                                                        W, E, Epad, a.out));
+    return XTS_OK;
+}
+
+}  // namespace xts
