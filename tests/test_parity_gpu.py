@@ -148,7 +148,19 @@ def test_edge_sources(api):
     job.src_sph = np.array(pts, dtype=np.float64)
     ref = oracle_pipeline(job)
     gpu = _gpu_pipeline(api, job)
-    assert max_rel(gpu["map"], ref["map"]) < 1e-5
+    near = [0, 1, 2, 4]
+    assert max_rel(gpu["map"][near], ref["map"][near]) < 1e-5
+    # Beyond the table's last separation (70 deg) the reference extrapolates
+    # linearly past row 400 (convolve_pixel_psf_logsep.hpp:45-47); the values
+    # cross zero, so the error there is measured against the map's largest value.
+    far_ref = ref["map"][3]
+    assert (far_ref < 0).any()
+    scale = np.abs(far_ref).max()
+    assert np.abs(gpu["map"][3] - far_ref).max() / scale < 1e-5
+    m64, _ = api.point_src_model_map_wcs(job.wcs, job.src_sph, gpu["ex"].exposure, gpu["ps"].uPsf,
+                                         gpu["ps"].partial_psf_integral, out_dtype="float64")
+    assert np.abs(m64[3] - far_ref).max() / scale < 1e-10
+    assert max_rel(m64[near], ref["map"][near]) < 1e-10
     np.testing.assert_array_equal(gpu["info"].in_fov.astype(bool), ref["in_fov"])
     assert list(ref["in_fov"]) == [True, True, False, False, True]
 

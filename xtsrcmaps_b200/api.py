@@ -86,7 +86,11 @@ class _Call:
 
             self.torch = torch
             self.dev = like.device if like is not None else torch.device("cuda")
-            self.stream = C.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
+            handle = torch.cuda.current_stream(self.dev).cuda_stream
+            # torch's default stream has handle 0, which the C-ABI reads as "the
+            # library's own stream"; pass cudaStreamLegacy (0x1) so the work stays
+            # ordered with the caller's default-stream work.
+            self.stream = C.c_void_p(handle if handle else 1)
         else:
             self.stream = None
         self.flags = L.XTS_DEVICE_PTRS if device else 0

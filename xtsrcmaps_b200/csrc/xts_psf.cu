@@ -137,6 +137,54 @@ __global__ void k_partial_integral(double* upsf, double* partial, int S, int E) 
     for (int d = 0; d < ND; ++d) u[(size_t)d * E] /= cum;
 }
 
+// Same computation with the source's table staged in shared memory: one block
+// per source, the [401, E] table loaded with coalesced reads, then one thread
+// per energy runs the prefix sum out of shared memory (its global stores are
+// coalesced across the energies), then the block normalises both tables.
+__global__ void k_partial_integral_smem(double* upsf, double* partial, int E) {
+    extern __shared__ double sm[];
+    double* U = sm;                    // [ND][E] raw mean PSF
+    double* TOT = U + (size_t)ND * E;  // [E]
+    double* T = TOT + E;               // [ND] theta (rad)
+    double* ST = T + ND;               // [ND] sin(theta)
+    int s = blockIdx.x;
+    double* us = upsf + (size_t)s * ND * E;
+    double* ps = partial + (size_t)s * ND * E;
+    for (int k = threadIdx.x; k < ND * E; k += blockDim.x) U[k] = us[k];
+    for (int d = threadIdx.x; d < ND; d += blockDim.x) {
+        double t = D2R * sep_deg(d);
+        T[d] = t;
+        ST[d] = sin(t);
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < E; e += blockDim.x) {
+        double cum = 0.0;
+        ps[e] = 0.0;
+        double t1 = T[0], y1 = TWOPI * U[e] * ST[0];
+        for (int d = 1; d < ND; ++d) {
+            double t2 = T[d];
+            double y2 = TWOPI * U[d * E + e] * ST[d];
+            double m = (y2 - y1) / (t2 - t1);
+            double b = y1 - t1 * m;
+            double v = 0.5 * m * (t2 * t2 - t1 * t1) + b * (t2 - t1);
+            cum += v;
+            ps[(size_t)d * E + e] = cum;
+            t1 = t2; y1 = y2;
+        }
+        TOT[e] = cum;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < ND * E; k += blockDim.x) {
+        double tot = TOT[k % E];
+        if (tot != 0.) ps[k] /= tot;
+        us[k] = U[k] / tot;
+    }
+}
+
+constexpr int PARTIAL_SMEM_MAX = 227 * 1024;
+
+static size_t partial_smem_bytes(int E) { return sizeof(double) * ((size_t)ND * E + E + 2 * ND); }
+
 int launch_psf(const PsfDev& a, cudaStream_t st) {
     if (a.C > PSF_MAX_C) return set_error(XTS_ERR_ARG, "compute_psf_data: C=%d exceeds %d", a.C, PSF_MAX_C);
     size_t kf_n = (size_t)ND * a.pf.n_cos * a.pf.n_e, kb_n = (size_t)ND * a.pb.n_cos * a.pb.n_e;
@@ -152,8 +200,14 @@ int launch_psf(const PsfDev& a, cudaStream_t st) {
     int DE = ND * a.E;
     dim3 g((DE + 127) / 128, (a.S + PSF_TILE_S - 1) / PSF_TILE_S);
     XTS_LAUNCH("k_mean_psf", st, k_mean_psf<<<g, 128, 0, st>>>(pa, a.C, a.E, a.ecb, a.wecb, a.S, a.ltf, a.exposure, a.upsf));
-    n = a.S * a.E;
-    XTS_LAUNCH("k_partial_integral", st, k_partial_integral<<<(n + 127) / 128, 128, 0, st>>>(a.upsf, a.partial, a.S, a.E));
+    size_t smem = partial_smem_bytes(a.E);
+    if (smem <= PARTIAL_SMEM_MAX) {
+        XTS_CUDA(cudaFuncSetAttribute(k_partial_integral_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        XTS_LAUNCH("k_partial_integral", st, k_partial_integral_smem<<<a.S, 256, smem, st>>>(a.upsf, a.partial, a.E));
+    } else {
+        n = a.S * a.E;
+        XTS_LAUNCH("k_partial_integral", st, k_partial_integral<<<(n + 127) / 128, 128, 0, st>>>(a.upsf, a.partial, a.S, a.E));
+    }
     return XTS_OK;
 }
 
