@@ -360,6 +360,101 @@ __global__ void __launch_bounds__(TP) k_srcmap(const double* corners, const doub
     }
 }
 
+// c7 as a row histogram: sum_pix omega * value(pix, e) = sum_r Hist[r] * uPsf[r][e]
+// with Hist[r] = sum over pixels in the radius of omega * (interpolation weight
+// on row r).  Each block accumulates one chunk of pixels of one in-FOV source
+// into a shared FP64 histogram; k_correction_hist folds the chunks.
+__global__ void __launch_bounds__(256) k_map_integral_hist(const double* corners, const double* centers,
+                                                           const double* omega, const SrcInfo* info,
+                                                           int H, int W, int nch, double* hist_out) {
+    __shared__ double hist[ND];
+    int s = blockIdx.y, ch = blockIdx.x;
+    SrcInfo si = info[s];
+    double* out = hist_out + ((size_t)s * nch + ch) * ND;
+    if (!si.in_fov) {
+        for (int r = threadIdx.x; r < ND; r += blockDim.x) out[r] = 0.;
+        return;
+    }
+    for (int r = threadIdx.x; r < ND; r += blockDim.x) hist[r] = 0.;
+    __syncthreads();
+    // chord^2 of the radius; pixels within a relative 1e-12 of it take the
+    // reference's own test 2 asin(|d|/2) <= radius
+    double ch2 = 2.0 * sin(0.5 * si.radius_rad);
+    ch2 *= ch2;
+    int npix = H * W, W1 = W + 1;
+    for (int pix = ch * blockDim.x + threadIdx.x; pix < npix; pix += nch * blockDim.x) {
+        int h = pix / W, w = pix - h * W;
+        const double* c = centers + 3 * (h * W1 + w);
+        double x = si.dir[0] - c[0], y = si.dir[1] - c[1], z = si.dir[2] - c[2];
+        double d2 = x * x + y * y + z * z;
+        bool inside;
+        if (d2 < ch2 * (1.0 - 1e-12)) inside = true;
+        else if (d2 > ch2 * (1.0 + 1e-12)) inside = false;
+        else inside = dir_diff(si.dir, c) <= si.radius_rad;
+        if (!inside) continue;
+        int keys[NPTS]; double va[NPTS], vb[NPTS];
+        int n = pixel_columns(corners, W1, h, w, si.dir, keys, va, vb);
+        double om = omega[pix];
+        for (int k = 0; k < n; ++k) {
+            atomicAdd(&hist[keys[k] - 1], va[k] * om);
+            atomicAdd(&hist[keys[k]], vb[k] * om);
+        }
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < ND; r += blockDim.x) out[r] = hist[r];
+}
+
+// c7 (1/sum) + c9 (containment factor) + c8/c10 folded into one per-(s,e) scale.
+// One block per source: fold the chunk histograms, then one thread per energy.
+__global__ void __launch_bounds__(256) k_correction_hist(const double* hist_in, int nch, const SrcInfo* info,
+                                                         const double* upsf, const double* partial,
+                                                         const double* expo, int E, double* scale,
+                                                         double* inv_out, double* fac_out,
+                                                         double* rad_out, int* fov_out) {
+    __shared__ double hsum[ND];
+    int s = blockIdx.x;
+    SrcInfo si = info[s];
+    for (int r = threadIdx.x; r < ND; r += blockDim.x) {
+        double v = 0.;
+        for (int c = 0; c < nch; ++c) v += hist_in[((size_t)s * nch + c) * ND + r];
+        hsum[r] = v;
+    }
+    __syncthreads();
+    const double* U = upsf + (size_t)s * ND * E;
+    for (int e = threadIdx.x; e < E; e += blockDim.x) {
+        int i = s * E + e;
+        double sum = 0.;
+        if (si.in_fov)
+            for (int r = 0; r < ND; ++r) sum = fma(hsum[r], U[(size_t)r * E + e], sum);
+        double inv = sum != 0. ? 1.0 / sum : sum;
+        double factor;
+        if (!si.in_fov) factor = 1.0;
+        else {
+            double v0 = si.radius_deg;
+            int li = v0 < 1. ? 1 : (int)floor(1. + log(1e4 * v0) * RECIPSTEP);
+            int d = li >= ND - 2 ? ND - 2 : li;
+            const double xstep = log(70. / 1e-4) / (400 - 1.);
+            double t1 = (d == 0 ? 0. : 1e-4 * exp((d - 1) * xstep)) * D2R;
+            double t2 = (1e-4 * exp(d * xstep)) * D2R;
+            double y1 = TWOPI * U[(size_t)d * E + e] * sin(t1);
+            double y2 = TWOPI * U[(size_t)(d + 1) * E + e] * sin(t2);
+            double m = (y2 - y1) / (t2 - t1);
+            double b = y1 - t1 * m;
+            double v = 0.5 * m * (t2 * t2 - t1 * t1) + b * (t2 - t1);
+            double integ = v + partial[(size_t)s * ND * E + (size_t)d * E + e];
+            integ = integ > 1.0 ? 1.0 : integ;
+            factor = integ * inv;
+        }
+        scale[i] = expo[i] * factor;
+        if (inv_out) inv_out[i] = inv;
+        if (fac_out) fac_out[i] = factor;
+        if (e == 0) {
+            if (rad_out) rad_out[s] = si.radius_deg;
+            if (fov_out) fov_out[s] = si.in_fov;
+        }
+    }
+}
+
 int launch_srcmap(const SrcmapDev& a, cudaStream_t st) {
     int rc = upload_rule(st);
     if (rc) return rc;
@@ -369,35 +464,32 @@ int launch_srcmap(const SrcmapDev& a, cudaStream_t st) {
     int npix = H * W;
     int ntiles = (npix + TP - 1) / TP;
     int Epad = (E + 3) & ~3;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    int nch = S > 0 ? (4 * nsm + S - 1) / S : 1;
+    int maxch = (npix + 255) / 256;
+    nch = nch < 1 ? 1 : (nch > maxch ? maxch : nch);
     double* corners = (double*)workspace(W_CORNERS, sizeof(double) * 3 * ng);
     double* centers = (double*)workspace(W_CENTERS, sizeof(double) * 3 * ng);
     double* omega = (double*)workspace(W_OMEGA, sizeof(double) * npix);
     SrcInfo* info = (SrcInfo*)workspace(W_SRCINFO, sizeof(SrcInfo) * (S > 0 ? S : 1));
-    double* partsum = (double*)workspace(W_PARTSUM, sizeof(double) * (size_t)S * ntiles * E + 8);
+    double* hist = (double*)workspace(W_PARTSUM, sizeof(double) * (size_t)S * nch * ND + 8);
     double* scale = (double*)workspace(W_SCALE, sizeof(double) * (size_t)S * E + 8);
-    float* lut = a.out_f64 ? nullptr : (float*)workspace(W_LUT, sizeof(float) * (size_t)S * ND * Epad + 16);
-    if (!corners || !centers || !omega || !info || !partsum || !scale || (!a.out_f64 && !lut))
-        return XTS_ERR_OOM;
+    if (!corners || !centers || !omega || !info || !hist || !scale) return XTS_ERR_OOM;
     XTS_LAUNCH("k_grids", st, k_grids<<<(unsigned)((ng + 127) / 128), 128, 0, st>>>(w, H, W, corners, centers));
     XTS_LAUNCH("k_solid_angle", st, k_solid_angle<<<(npix + 127) / 128, 128, 0, st>>>(centers, H, W, omega));
     if (S == 0) return XTS_OK;
     XTS_LAUNCH("k_boundary", st, k_boundary<<<S, 128, 0, st>>>(w, a.src_sph, H, W, corners, info));
-    if (!a.out_f64) {
-        size_t n = (size_t)S * ND * Epad;
-        XTS_LAUNCH("k_lut32", st, k_lut32<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a.upsf, S, E, Epad, lut));
+    XTS_LAUNCH("k_map_integral", st, k_map_integral_hist<<<dim3(nch, S), 256, 0, st>>>(corners, centers, omega, info, H, W, nch, hist));
+    XTS_LAUNCH("k_correction", st, k_correction_hist<<<S, 256, 0, st>>>(hist, nch, info, a.upsf, a.partial, a.exposure, E,
+                                                                        scale, a.inv_integ, a.correction, a.radius, a.in_fov));
+    if (a.out_f64) {
+        XTS_LAUNCH("k_srcmap_f64", st, k_srcmap<true><<<dim3(ntiles, S), TP, 0, st>>>(corners, omega, info, nullptr, a.upsf, scale,
+                                                                                        H, W, E, Epad, a.out));
+        return XTS_OK;
     }
-    XTS_LAUNCH("k_map_integral", st, k_map_integral<<<dim3(ntiles, S), TP, 0, st>>>(corners, centers, omega, info, a.upsf, H, W, E,
-                                                   ntiles, partsum));
-    XTS_LAUNCH("k_correction", st, k_correction<<<(S * E + 127) / 128, 128, 0, st>>>(partsum, ntiles, info, a.upsf, a.partial,
-                                                     a.exposure, S, E, scale, a.inv_integ,
-                                                     a.correction, a.radius, a.in_fov));
-    if (a.out_f64)
-        k_srcmap<true><<<dim3(ntiles, S), TP, 0, st>>>(corners, omega, info, lut, a.upsf, scale, H, W,
-                                                       E, Epad, a.out);
-    else
-        XTS_LAUNCH("k_srcmap", st, k_srcmap<false><<<dim3(ntiles, S), TP, 0, st>>>(corners, omega, info, lut, a.upsf, scale, H,
-                                                        W, E, Epad, a.out));
-    return XTS_OK;
+    return launch_srcmap_fast(corners, omega, info, a.upsf, scale, S, H, W, E, (float*)a.out, st);
 }
 
 }  // namespace xts
