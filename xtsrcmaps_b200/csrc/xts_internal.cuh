@@ -122,6 +122,9 @@ struct SrcmapDev {
     double* inv_integ; double* correction; double* radius; int* in_fov;  // optional (may be null)
 };
 int launch_srcmap(const SrcmapDev& a, cudaStream_t st);
+int launch_map_integral_fast(const double* corners, const double* centers, const double* omega,
+                             const SrcInfo* info, int S, int H, int W, int nch, double* hist,
+                             cudaStream_t st);
 int launch_srcmap_fast(const double* corners, const double* omega, const SrcInfo* info,
                        const double* upsf, const double* scale, int S, int H, int W, int E,
                        float* out, cudaStream_t st);

@@ -85,30 +85,33 @@ constexpr int PSF_MAX_C = 64;
 __global__ void __launch_bounds__(128) k_mean_psf(const double* pa, int C, int E, const double* ecb,
                                                   const double* wecb, int S, const double* ltf,
                                                   const double* expo, double* out) {
-    __shared__ double sx[PSF_TILE_S][PSF_MAX_C];
-    __shared__ double sw[PSF_TILE_S][PSF_MAX_C];
+    __shared__ double sx[PSF_MAX_C][PSF_TILE_S];
+    __shared__ double sw[PSF_MAX_C][PSF_TILE_S];
     int s0 = blockIdx.y * PSF_TILE_S;
     int ns = min(PSF_TILE_S, S - s0);
-    for (int k = threadIdx.x; k < ns * C; k += blockDim.x) {
+    for (int k = threadIdx.x; k < PSF_TILE_S * C; k += blockDim.x) {
         int s = k / C, c = k - s * C;
-        sx[s][c] = ecb[(size_t)(s0 + s) * C + c];
-        sw[s][c] = wecb[(size_t)(s0 + s) * C + c];
+        bool ok = s < ns;
+        sx[c][s] = ok ? ecb[(size_t)(s0 + s) * C + c] : 0.;
+        sw[c][s] = ok ? wecb[(size_t)(s0 + s) * C + c] : 0.;
     }
     __syncthreads();
     int DE = ND * E;
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= DE) return;
     int e = j % E;
-    double col[PSF_MAX_C];
-#pragma unroll 8
-    for (int c = 0; c < C; ++c) col[c] = pa[(size_t)c * DE + j];
-    double l0 = ltf[e], l1 = ltf[E + e];
-    for (int s = 0; s < ns; ++s) {
-        double x = 0., w = 0.;
-#pragma unroll 8
-        for (int c = 0; c < C; ++c) { x = fma(sx[s][c], col[c], x); w = fma(sw[s][c], col[c], w); }
-        out[(size_t)(s0 + s) * DE + j] = (x * l0 + w * l1) / expo[(size_t)(s0 + s) * E + e];
+    double x[PSF_TILE_S], w[PSF_TILE_S];
+#pragma unroll
+    for (int s = 0; s < PSF_TILE_S; ++s) { x[s] = 0.; w[s] = 0.; }
+    for (int c = 0; c < C; ++c) {
+        const double col = pa[(size_t)c * DE + j];
+#pragma unroll
+        for (int s = 0; s < PSF_TILE_S; ++s) { x[s] = fma(sx[c][s], col, x[s]); w[s] = fma(sw[c][s], col, w[s]); }
     }
+    double l0 = ltf[e], l1 = ltf[E + e];
+#pragma unroll
+    for (int s = 0; s < PSF_TILE_S; ++s)
+        if (s < ns) out[(size_t)(s0 + s) * DE + j] = (x[s] * l0 + w[s] * l1) / expo[(size_t)(s0 + s) * E + e];
 }
 
 // b7: per (s, e) exact integral of the linear interpolant of 2 pi u(theta) sin(theta)
@@ -143,10 +146,13 @@ __global__ void k_partial_integral(double* upsf, double* partial, int S, int E) 
 // coalesced across the energies), then the block normalises both tables.
 __global__ void k_partial_integral_smem(double* upsf, double* partial, int E) {
     extern __shared__ double sm[];
-    double* U = sm;                    // [ND][E] raw mean PSF
-    double* TOT = U + (size_t)ND * E;  // [E]
-    double* T = TOT + E;               // [ND] theta (rad)
-    double* ST = T + ND;               // [ND] sin(theta)
+    double* U = sm;                     // [ND][E] raw mean PSF
+    double* TOT = U + (size_t)ND * E;   // [E]
+    double* T = TOT + E;                // [ND] theta (rad)
+    double* ST = T + ND;                // [ND] 2 pi sin(theta)
+    double* IDT = ST + ND;              // [ND] 1 / (theta[d] - theta[d-1])
+    double* HA = IDT + ND;              // [ND] (theta[d]^2 - theta[d-1]^2) / 2
+    double* DT = HA + ND;               // [ND] theta[d] - theta[d-1]
     int s = blockIdx.x;
     double* us = upsf + (size_t)s * ND * E;
     double* ps = partial + (size_t)s * ND * E;
@@ -154,22 +160,29 @@ __global__ void k_partial_integral_smem(double* upsf, double* partial, int E) {
     for (int d = threadIdx.x; d < ND; d += blockDim.x) {
         double t = D2R * sep_deg(d);
         T[d] = t;
-        ST[d] = sin(t);
+        ST[d] = TWOPI * sin(t);
+    }
+    __syncthreads();
+    for (int d = 1 + threadIdx.x; d < ND; d += blockDim.x) {
+        double t1 = T[d - 1], t2 = T[d];
+        DT[d] = t2 - t1;
+        IDT[d] = 1.0 / (t2 - t1);
+        HA[d] = 0.5 * (t2 * t2 - t1 * t1);
     }
     __syncthreads();
     for (int e = threadIdx.x; e < E; e += blockDim.x) {
         double cum = 0.0;
         ps[e] = 0.0;
-        double t1 = T[0], y1 = TWOPI * U[e] * ST[0];
+        double y1 = U[e] * ST[0];
+#pragma unroll 4
         for (int d = 1; d < ND; ++d) {
-            double t2 = T[d];
-            double y2 = TWOPI * U[d * E + e] * ST[d];
-            double m = (y2 - y1) / (t2 - t1);
-            double b = y1 - t1 * m;
-            double v = 0.5 * m * (t2 * t2 - t1 * t1) + b * (t2 - t1);
+            double y2 = U[d * E + e] * ST[d];
+            double m = (y2 - y1) * IDT[d];
+            double b = y1 - T[d - 1] * m;
+            double v = m * HA[d] + b * DT[d];
             cum += v;
             ps[(size_t)d * E + e] = cum;
-            t1 = t2; y1 = y2;
+            y1 = y2;
         }
         TOT[e] = cum;
     }
@@ -183,7 +196,7 @@ __global__ void k_partial_integral_smem(double* upsf, double* partial, int E) {
 
 constexpr int PARTIAL_SMEM_MAX = 227 * 1024;
 
-static size_t partial_smem_bytes(int E) { return sizeof(double) * ((size_t)ND * E + E + 2 * ND); }
+static size_t partial_smem_bytes(int E) { return sizeof(double) * ((size_t)ND * E + E + 5 * ND); }
 
 int launch_psf(const PsfDev& a, cudaStream_t st) {
     if (a.C > PSF_MAX_C) return set_error(XTS_ERR_ARG, "compute_psf_data: C=%d exceeds %d", a.C, PSF_MAX_C);

@@ -481,7 +481,12 @@ int launch_srcmap(const SrcmapDev& a, cudaStream_t st) {
     XTS_LAUNCH("k_solid_angle", st, k_solid_angle<<<(npix + 127) / 128, 128, 0, st>>>(centers, H, W, omega));
     if (S == 0) return XTS_OK;
     XTS_LAUNCH("k_boundary", st, k_boundary<<<S, 128, 0, st>>>(w, a.src_sph, H, W, corners, info));
-    XTS_LAUNCH("k_map_integral", st, k_map_integral_hist<<<dim3(nch, S), 256, 0, st>>>(corners, centers, omega, info, H, W, nch, hist));
+    if (a.out_f64) {  // the reference's own per-point FP64 arithmetic throughout
+        XTS_LAUNCH("k_map_integral_f64", st, k_map_integral_hist<<<dim3(nch, S), 256, 0, st>>>(corners, centers, omega, info, H, W, nch, hist));
+    } else {
+        rc = launch_map_integral_fast(corners, centers, omega, info, S, H, W, nch, hist, st);
+        if (rc) return rc;
+    }
     XTS_LAUNCH("k_correction", st, k_correction_hist<<<S, 256, 0, st>>>(hist, nch, info, a.upsf, a.partial, a.exposure, E,
                                                                         scale, a.inv_integ, a.correction, a.radius, a.in_fov));
     if (a.out_f64) {

@@ -167,7 +167,75 @@ constexpr size_t OFF_STAGE = OFF_META + sizeof(int) * FT;
 
 size_t srcmap_fast_smem(int E) { return OFF_STAGE + sizeof(float) * ((size_t)FT * E + 8); }
 
-__global__ void __launch_bounds__(FT, 2)
+// Interpolation weight outside the tabulated range (s < 1e-4 deg or s >= 70 deg):
+// the reference's own FP64 formula (convolve_pixel_psf_logsep.hpp:45-47).  Kept
+// out of line: it runs for a handful of points per map.
+__device__ __noinline__ float t_exact(double q, int idx) {
+    const double sdeg = 2.0 * R2D * asin(0.5 * sqrt(q));
+    return (float)(REDM1 * (sdeg * 1e4 * exp(SEP_STEP * (2. - idx)) - 1.));
+}
+
+// Row and interpolation weight of one rule point from its FP64 squared chord q.
+// The FP32 starting guess is within one row of the bracket (|error| < 0.3 rows
+// up to 70 deg, where the row is clamped to 400 anyway); one branch-free
+// correction against the FP64 squared chords gives the reference's row.
+__device__ __forceinline__ int point_row(double q, const double* sq, const float4* scoef, float* t_out) {
+    const float qf = (float)q;
+    // ln s_deg ~ ln(180/pi) + ln(q)/2 + q/24;  j = 1 + (ln 1e4 + ln s_deg)/step
+    const float lns = fmaf(0.34657359f, __log2f(fmaxf(qf, 1e-37f)), fmaf(qf, 1.f / 24.f, 4.0482950f));
+    const float jf = fmaf(29.645952f, lns, 1.f + 29.645952f * 9.2103404f);
+    int idx = 1 + (int)fminf(fmaxf(jf, 1.f), 399.f);  // [2, 400]
+    const double qa = sq[idx - 1], qb = sq[idx];
+    const int dn = (q < qa) & (idx > 2);
+    const int up = (q >= qb) & (idx < 400);
+    idx += up - dn;
+    const double qlo = up ? qb : (dn ? sq[idx - 1] : qa);
+    const float4 c0 = scoef[2 * (idx - 1)], c1 = scoef[2 * (idx - 1) + 1];
+    const float dl = (float)(q - qlo) * c0.x;  // q / q_lo - 1
+    if (dl >= -0.002f && dl <= 0.072f) {
+        const float zz = fmaf(dl, 1.f / DPOLY_H, -DPOLY_C / DPOLY_H);
+        const float P = fmaf(fmaf(fmaf(fmaf(c1.y, zz, c1.x), zz, c0.w), zz, c0.z), zz, c0.y);
+        *t_out = (float)REDM1 * (dl * P);
+    } else {
+        *t_out = t_exact(q, idx);
+    }
+    return idx;
+}
+
+// Bilinear form of the rule points of pixel (h, w) relative to the source:
+// p(u, v) - src = A + B u + C v + D uv (points_weights.hpp:93-107).
+struct PixGeom { double Ax, Ay, Az, Bx, By, Bz, Cx, Cy, Cz, Dx, Dy, Dz; };
+
+__device__ __forceinline__ PixGeom pixel_geom(const double* corners, int W1, int h, int w, const SrcInfo& si) {
+    const double* a = corners + 3 * (h * W1 + w);            // LL
+    const double* b = corners + 3 * (h * W1 + w + 1);        // LR
+    const double* c = corners + 3 * ((h + 1) * W1 + w + 1);  // UR
+    const double* d = corners + 3 * ((h + 1) * W1 + w);      // UL
+    PixGeom g;
+    g.Ax = 0.25 * ((a[0] + b[0]) + (c[0] + d[0])) - si.dir[0];
+    g.Ay = 0.25 * ((a[1] + b[1]) + (c[1] + d[1])) - si.dir[1];
+    g.Az = 0.25 * ((a[2] + b[2]) + (c[2] + d[2])) - si.dir[2];
+    g.Bx = 0.25 * ((b[0] + c[0]) - (a[0] + d[0]));
+    g.By = 0.25 * ((b[1] + c[1]) - (a[1] + d[1]));
+    g.Bz = 0.25 * ((b[2] + c[2]) - (a[2] + d[2]));
+    g.Cx = 0.25 * ((c[0] + d[0]) - (a[0] + b[0]));
+    g.Cy = 0.25 * ((c[1] + d[1]) - (a[1] + b[1]));
+    g.Cz = 0.25 * ((c[2] + d[2]) - (a[2] + b[2]));
+    g.Dx = 0.25 * ((a[0] + c[0]) - (b[0] + d[0]));
+    g.Dy = 0.25 * ((a[1] + c[1]) - (b[1] + d[1]));
+    g.Dz = 0.25 * ((a[2] + c[2]) - (b[2] + d[2]));
+    return g;
+}
+
+__device__ __forceinline__ double point_q(const PixGeom& g, int p) {
+    const double u = c_rule_uv[p][0], v = c_rule_uv[p][1], uv = c_rule_uv[p][2];
+    const double x = fma(g.Dx, uv, fma(g.Cx, v, fma(g.Bx, u, g.Ax)));
+    const double y = fma(g.Dy, uv, fma(g.Cy, v, fma(g.By, u, g.Ay)));
+    const double z = fma(g.Dz, uv, fma(g.Cz, v, fma(g.Bz, u, g.Az)));
+    return fma(x, x, fma(y, y, z * z));
+}
+
+__global__ void __launch_bounds__(FT, 3)
 k_srcmap_fast(const double* __restrict__ corners, const double* __restrict__ omega,
               const SrcInfo* __restrict__ info, const float* __restrict__ lut,
               const SepTab* __restrict__ septab, int H, int W, int E, int Epad, int nchunk,
@@ -183,11 +251,11 @@ k_srcmap_fast(const double* __restrict__ corners, const double* __restrict__ ome
     for (int k = threadIdx.x; k < ND + 1; k += FT) sq[k] = septab->q[k];
     for (int k = threadIdx.x; k < 2 * ND; k += FT) scoef[k] = ((const float4*)septab->coef)[k];
     const SrcInfo si = info[s];
-    const double sx = si.dir[0], sy = si.dir[1], sz = si.dir[2];
     const int npix = H * W, W1 = W + 1;
     const int ntiles = (npix + FT - 1) / FT;
     const float* Y = lut + (size_t)s * ND * Epad;
     const int t = threadIdx.x;
+    float* wr = wwin + t * WST;
     __syncthreads();
 
     for (int tile = blockIdx.x; tile < ntiles; tile += nchunk) {
@@ -197,130 +265,103 @@ k_srcmap_fast(const double* __restrict__ corners, const double* __restrict__ ome
         const int m = (int)(g0 & 3);                          // staging residue
         const int nflat = np * E;
 
-        // ---------------- phase 1: this thread's pixel (overlaps the previous tile's store)
+        // ---------------- phase 1: this thread's pixel (overlaps the previous tile's store).
+        // The RW-row window is anchored on the pixel centre's row; a point whose
+        // rows fall outside it makes the pixel "wide" (only next to the source).
         int nrows = 0, rbase = 0;
         bool wide = false;
-        float om = 0.f;
-        int idxs[12];
-        float ts[12];
+        const int pix = p0 + t;
         if (t < np) {
-            const int pix = p0 + t, h = pix / W, w = pix - h * W;
-            const double* a = corners + 3 * (h * W1 + w);            // LL
-            const double* b = corners + 3 * (h * W1 + w + 1);        // LR
-            const double* c = corners + 3 * ((h + 1) * W1 + w + 1);  // UR
-            const double* d = corners + 3 * ((h + 1) * W1 + w);      // UL
-            const double Ax = 0.25 * ((a[0] + b[0]) + (c[0] + d[0])) - sx;
-            const double Ay = 0.25 * ((a[1] + b[1]) + (c[1] + d[1])) - sy;
-            const double Az = 0.25 * ((a[2] + b[2]) + (c[2] + d[2])) - sz;
-            const double Bx = 0.25 * ((b[0] + c[0]) - (a[0] + d[0]));
-            const double By = 0.25 * ((b[1] + c[1]) - (a[1] + d[1]));
-            const double Bz = 0.25 * ((b[2] + c[2]) - (a[2] + d[2]));
-            const double Cx = 0.25 * ((c[0] + d[0]) - (a[0] + b[0]));
-            const double Cy = 0.25 * ((c[1] + d[1]) - (a[1] + b[1]));
-            const double Cz = 0.25 * ((c[2] + d[2]) - (a[2] + b[2]));
-            const double Dx = 0.25 * ((a[0] + c[0]) - (b[0] + d[0]));
-            const double Dy = 0.25 * ((a[1] + c[1]) - (b[1] + d[1]));
-            const double Dz = 0.25 * ((a[2] + c[2]) - (b[2] + d[2]));
-            int imin = 1 << 20, imax = 0;
+            const int h = pix / W, w = pix - h * W;
+            const PixGeom g = pixel_geom(corners, W1, h, w, si);
+            float tc;
+            const int ic = point_row(fma(g.Ax, g.Ax, fma(g.Ay, g.Ay, g.Az * g.Az)), sq, scoef, &tc);
+            rbase = min(max(ic - 1 - RW / 2, 0), ND - RW);
+#pragma unroll
+            for (int j = 0; j < RW; ++j) wr[j] = 0.f;
+            int lo = RW, hi = -1;
 #pragma unroll
             for (int p = 0; p < 12; ++p) {
-                const double u = c_rule_uv[p][0], v = c_rule_uv[p][1], uv = c_rule_uv[p][2];
-                const double x = fma(Dx, uv, fma(Cx, v, fma(Bx, u, Ax)));
-                const double y = fma(Dy, uv, fma(Cy, v, fma(By, u, Ay)));
-                const double z = fma(Dz, uv, fma(Cz, v, fma(Bz, u, Az)));
-                const double q = fma(x, x, fma(y, y, z * z));
-                // starting guess in FP32: ln s_deg ~ ln(180/pi) + ln(q)/2 + q/24
-                const float qf = (float)q;
-                const float lns = 4.0482950f + 0.34657359f * __log2f(fmaxf(qf, 1e-37f)) + qf * (1.f / 24.f);
-                const float jf = 1.f + 29.645952f * (9.2103404f + lns);
-                int idx = 1 + (int)fminf(fmaxf(jf, 0.f), 500.f);
-                idx = min(max(idx, 2), 400);
-                // exact row against the FP64 squared chords, clamped to [2, 400]
-#pragma unroll
-                for (int it = 0; it < 3; ++it) {
-                    if (idx > 2 && q < sq[idx - 1]) --idx;
-                    else if (idx < 400 && q >= sq[idx]) ++idx;
-                }
-                const double qlo = sq[idx - 1];
-                const float4 c0 = scoef[2 * (idx - 1)], c1 = scoef[2 * (idx - 1) + 1];
-                const float dl = (float)(q - qlo) * c0.x;  // q / q_lo - 1
                 float tt;
-                if (dl >= -0.002f && dl <= 0.072f) {
-                    const float zz = fmaf(dl, 1.f / DPOLY_H, -DPOLY_C / DPOLY_H);
-                    const float P = fmaf(fmaf(fmaf(fmaf(c1.y, zz, c1.x), zz, c0.w), zz, c0.z), zz, c0.y);
-                    tt = (float)REDM1 * (dl * P);
-                } else {  // outside the table: the reference's own FP64 formula
-                    const double sdeg = 2.0 * R2D * asin(0.5 * sqrt(q));
-                    tt = (float)(REDM1 * (sdeg * 1e4 * exp(SEP_STEP * (2. - idx)) - 1.));
-                }
-                idxs[p] = idx;
-                ts[p] = tt;
-                imin = min(imin, idx);
-                imax = max(imax, idx);
-            }
-            rbase = imin - 1;
-            nrows = imax - imin + 2;
-            om = (float)omega[pix];
-            if (nrows <= RW) {
-                float* wr = wwin + t * WST;
-#pragma unroll
-                for (int j = 0; j < RW; ++j) wr[j] = 0.f;
-#pragma unroll
-                for (int p = 0; p < 12; ++p) {
+                const int r = point_row(point_q(g, p), sq, scoef, &tt) - 1 - rbase;
+                if (r >= 0 && r < RW - 1) {  // thread-private window in shared memory
                     const float wgt = (float)c_rule_uv[p][3];
-                    const int r = idxs[p] - 1 - rbase;
-                    wr[r] = fmaf(1.f - ts[p], wgt, wr[r]);
-                    wr[r + 1] = fmaf(ts[p], wgt, wr[r + 1]);
+                    wr[r] = fmaf(1.f - tt, wgt, wr[r]);
+                    wr[r + 1] = fmaf(tt, wgt, wr[r + 1]);
+                    lo = min(lo, r);
+                    hi = max(hi, r + 1);
+                } else {
+                    wide = true;
                 }
-#pragma unroll
-                for (int j = 0; j < RW; ++j) wr[j] *= om;
-            } else {
-                wide = true;
-                nrows = 0;
+            }
+            if (!wide) {
+                const float om = (float)omega[pix];
+                nrows = hi - lo + 1;
+                for (int j = 0; j < nrows; ++j) wr[j] = wr[j + lo] * om;
+                rbase += lo;
             }
         }
         if (t == 0) bulk_wait_read();  // the previous tile's bulk store has read the stage
         meta[t] = (rbase & 0xffff) | (nrows << 16);
         __syncthreads();
 
-        // wide pixels (points spanning more than RW rows, next to the source):
-        // evaluated point by point by their own thread, compensated sum
+        // wide pixels: evaluated point by point by their own thread, compensated sum
         if (wide) {
+            const int h = pix / W, w = pix - h * W;
+            const PixGeom g = pixel_geom(corners, W1, h, w, si);
+            const float om = (float)omega[pix];
             float* dst = stage + m + t * E;
-            for (int e = 0; e < E; ++e) {
-                float acc = 0.f, comp = 0.f;
-#pragma unroll
+            for (int e0 = 0; e0 < E; e0 += 4) {
+                float acc[4] = {0.f, 0.f, 0.f, 0.f}, comp[4] = {0.f, 0.f, 0.f, 0.f};
                 for (int p = 0; p < 12; ++p) {
+                    float tt;
+                    const int idx = point_row(point_q(g, p), sq, scoef, &tt);
                     const float wgt = (float)c_rule_uv[p][3];
-                    const float* yl = Y + (size_t)(idxs[p] - 1) * Epad + e;
-                    const float term = fmaf((1.f - ts[p]) * wgt, __ldg(yl), ts[p] * wgt * __ldg(yl + Epad));
-                    const float s2 = acc + term;
-                    comp += fabsf(acc) >= fabsf(term) ? (acc - s2) + term : (term - s2) + acc;
-                    acc = s2;
+                    const float* yl = Y + (size_t)(idx - 1) * Epad + e0;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const float term = fmaf((1.f - tt) * wgt, __ldg(yl + k), tt * wgt * __ldg(yl + Epad + k));
+                        const float s2 = acc[k] + term;
+                        comp[k] += fabsf(acc[k]) >= fabsf(term) ? (acc[k] - s2) + term : (term - s2) + acc[k];
+                        acc[k] = s2;
+                    }
                 }
-                dst[e] = (acc + comp) * om;
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (e0 + k < E) dst[e0 + k] = (acc[k] + comp[k]) * om;
             }
         }
 
-        // ---------------- phase 2: flat (pixel, energy) order, coalesced stage writes
+        // ---------------- phase 2: flat (pixel, energy) order, four independent outputs per thread
         {
-            int f = t;
-            int p = f / E, e = f - p * E;
             const int dp = FT / E, de = FT - dp * E;
-            for (; f < nflat; f += FT) {
-                const int mt = meta[p];
-                const int nr = mt >> 16;
-                if (nr) {
-                    const int rb = (short)(mt & 0xffff);
-                    const float* wr = wwin + p * WST;
-                    const float* yp = Y + (size_t)rb * Epad + e;
-                    float acc = 0.f;
-                    for (int j = 0; j < nr; ++j) acc = fmaf(wr[j], __ldg(yp + j * Epad), acc);
-                    stage[m + f] = acc;
+            int f = t, p = t / E;
+            int e = t - p * E;
+            while (f < nflat) {
+                float res[4];
+                int fo[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    fo[k] = -1;
+                    res[k] = 0.f;
+                    if (f < nflat) {
+                        const int mt = meta[p];
+                        const int nr = mt >> 16;
+                        const float* wk = wwin + p * WST;
+                        const float* yp = Y + (size_t)(short)(mt & 0xffff) * Epad + e;
+                        float a = 0.f;
+                        for (int j = 0; j < nr; ++j) a = fmaf(wk[j], __ldg(yp + j * Epad), a);
+                        res[k] = a;
+                        fo[k] = nr ? f : -1;  // nr == 0: wide pixel, already staged
+                    }
+                    f += FT;
+                    p += dp;
+                    e += de;
+                    if (e >= E) { e -= E; ++p; }
                 }
-                p += dp;
-                e += de;
-                if (e >= E) { e -= E; ++p; }
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (fo[k] >= 0) stage[m + fo[k]] = res[k];
             }
         }
         fence_async_shared();
@@ -339,6 +380,133 @@ k_srcmap_fast(const double* __restrict__ corners, const double* __restrict__ ome
     }
     if (t == 0) bulk_wait_all();
     __syncthreads();
+}
+
+// c7 map integral, FP64, without atomics in the common case.  For each tile of
+// 256 pixels of one in-FOV source, every pixel whose centre lies within the
+// boundary radius (the reference's test 2 asin(|d|/2) <= radius, evaluated on the
+// squared chord with an exact fallback next to the threshold) builds its FP64
+// row window (interpolation weights times solid angle); then one thread per
+// table row sums the tile's windows in a fixed order into the block's row
+// histogram.  Pixels whose points leave the window (next to the source) add
+// their 24 weights with shared-memory atomics.  The caller folds the block
+// histograms with the mean-PSF table: sum_pix omega value(pix, e) = sum_r H[r] U[r][e].
+constexpr size_t MI_OFF_SQ = 0;
+constexpr size_t MI_OFF_COEF = (8 * (ND + 1) + 15) / 16 * 16;
+constexpr size_t MI_OFF_HIST = MI_OFF_COEF + sizeof(float4) * 2 * ND;
+constexpr size_t MI_OFF_WTS = MI_OFF_HIST + (8 * ND + 15) / 16 * 16;
+constexpr size_t MI_OFF_BASE = MI_OFF_WTS + sizeof(double) * FT * RW;
+constexpr size_t MI_SMEM = MI_OFF_BASE + sizeof(int) * (FT + 4);
+
+__global__ void __launch_bounds__(FT) k_map_integral_fast(const double* __restrict__ corners, const double* __restrict__ centers,
+                                                          const double* __restrict__ omega, const SrcInfo* __restrict__ info,
+                                                          const SepTab* __restrict__ septab, int H, int W, int nch,
+                                                          double* __restrict__ hist_out) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* sq = (double*)(smem + MI_OFF_SQ);
+    float4* scoef = (float4*)(smem + MI_OFF_COEF);
+    double* hist = (double*)(smem + MI_OFF_HIST);
+    double* wts = (double*)(smem + MI_OFF_WTS);  // [FT][RW]
+    int* wbase = (int*)(smem + MI_OFF_BASE);     // [FT], plus [FT] = row min, [FT+1] = row max
+    const int s = blockIdx.y, t = threadIdx.x;
+    const SrcInfo si = info[s];
+    double* out = hist_out + ((size_t)s * nch + blockIdx.x) * ND;
+    if (!si.in_fov) {
+        for (int r = t; r < ND; r += FT) out[r] = 0.;
+        return;
+    }
+    for (int k = t; k < ND + 1; k += FT) sq[k] = septab->q[k];
+    for (int k = t; k < 2 * ND; k += FT) scoef[k] = ((const float4*)septab->coef)[k];
+    for (int r = t; r < ND; r += FT) hist[r] = 0.;
+    double ch2 = 2.0 * sin(0.5 * si.radius_rad);
+    ch2 *= ch2;
+    const int npix = H * W, W1 = W + 1;
+    const int ntiles = (npix + FT - 1) / FT;
+    __syncthreads();
+    for (int tile = blockIdx.x; tile < ntiles; tile += nch) {
+        if (t == 0) { wbase[FT] = ND; wbase[FT + 1] = -1; }
+        const int pix = tile * FT + t;
+        int rb = -1;
+        bool inside = false;
+        if (pix < npix) {
+            const int h = pix / W, w = pix - h * W;
+            const double* c = centers + 3 * (h * W1 + w);
+            const double x = si.dir[0] - c[0], y = si.dir[1] - c[1], z = si.dir[2] - c[2];
+            const double d2 = x * x + y * y + z * z;
+            if (d2 < ch2 * (1.0 - 1e-12)) inside = true;
+            else if (d2 > ch2 * (1.0 + 1e-12)) inside = false;
+            else inside = dir_diff(si.dir, c) <= si.radius_rad;
+        }
+        __syncthreads();
+        if (!__syncthreads_or(inside)) continue;
+        if (inside) {
+            const int h = pix / W, w = pix - h * W;
+            const PixGeom g = pixel_geom(corners, W1, h, w, si);
+            const double om = omega[pix];
+            float tc;
+            const int ic = point_row(fma(g.Ax, g.Ax, fma(g.Ay, g.Ay, g.Az * g.Az)), sq, scoef, &tc);
+            const int base = min(max(ic - 1 - RW / 2, 0), ND - RW);
+            double* wd = wts + t * RW;
+#pragma unroll
+            for (int j = 0; j < RW; ++j) wd[j] = 0.;
+            bool wide = false;
+#pragma unroll
+            for (int p = 0; p < 12; ++p) {
+                float tt;
+                const int idx = point_row(point_q(g, p), sq, scoef, &tt);
+                const int r = idx - 1 - base;
+                const double wgt = c_rule_uv[p][3];
+                const double wa = (double)(1.f - tt) * wgt * om, wb = (double)tt * wgt * om;
+                if (r >= 0 && r < RW - 1) {
+                    wd[r] += wa;
+                    wd[r + 1] += wb;
+                } else {
+                    wide = true;
+                    atomicAdd(&hist[idx - 1], wa);
+                    atomicAdd(&hist[idx], wb);
+                }
+            }
+            rb = base;
+            atomicMin(&wbase[FT], base);
+            atomicMax(&wbase[FT + 1], base + RW - 1);
+        }
+        wbase[t] = rb;
+        __syncthreads();
+        const int rmin = wbase[FT], rmax = wbase[FT + 1];
+        // 8 threads per row, each over 32 pixels, combined in a fixed shuffle order
+        const int sub = t & 7;
+        for (int r0 = rmin; r0 <= rmax; r0 += FT / 8) {
+            const int r = r0 + (t >> 3);
+            double acc = 0.;
+            if (r <= rmax) {
+                for (int p = sub * 32; p < sub * 32 + 32; ++p) {
+                    const int b0 = wbase[p];
+                    const int k = r - b0;
+                    if (b0 >= 0 && k >= 0 && k < RW) acc += wts[p * RW + k];
+                }
+            }
+            acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+            acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+            acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+            if (sub == 0 && r <= rmax) hist[r] += acc;
+        }
+        __syncthreads();
+    }
+    __syncthreads();
+    for (int r = t; r < ND; r += FT) out[r] = hist[r];
+}
+
+int launch_map_integral_fast(const double* corners, const double* centers, const double* omega,
+                             const SrcInfo* info, int S, int H, int W, int nch, double* hist,
+                             cudaStream_t st) {
+    int rc = upload_rule_uv(st);
+    if (rc) return rc;
+    const SepTab* tab = nullptr;
+    rc = build_septab(st, &tab);
+    if (rc) return rc;
+    XTS_CUDA(cudaFuncSetAttribute(k_map_integral_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MI_SMEM));
+    XTS_LAUNCH("k_map_integral", st, k_map_integral_fast<<<dim3(nch, S), FT, MI_SMEM, st>>>(corners, centers, omega, info, tab, H, W, nch, hist));
+    return XTS_OK;
 }
 
 int launch_srcmap_fast(const double* corners, const double* omega, const SrcInfo* info,
