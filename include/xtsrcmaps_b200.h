@@ -44,7 +44,8 @@ enum xts_status {
 enum xts_flags {
     XTS_DEVICE_PTRS = 1u << 0, /* array arguments are device pointers */
     XTS_OUT_F64 = 1u << 1,     /* model map written as double (default float) */
-    XTS_EXPOSURE_TF32 = 1u << 2 /* exposure contraction as 3xTF32 on tcgen05 tensor cores (default: FP64 cores) */
+    XTS_EXPOSURE_TF32 = 1u << 2, /* exposure contraction as 3xTF32 on tcgen05 tensor cores (default: FP64 cores) */
+    XTS_CUDA_CORES = 1u << 3     /* FP32 source maps on CUDA cores only (default: tcgen05 tensor cores) */
 };
 
 /* FITS celestial WCS (sky_geom/sky_geom.hxx:17-25, WcsConfig). */

@@ -93,6 +93,16 @@ def test_srcmap_f32_vs_oracle(api, c1_small):
     assert max_rel(tot_g, tot_r) < 1e-7
 
 
+def test_srcmap_cuda_core_path_vs_oracle(api, c1_small):
+    """The CUDA-core FP32 path (XTS_CUDA_CORES) against the oracle and the
+    default tensor-core path."""
+    job, ref, gpu = c1_small
+    m, info = api.point_src_model_map_wcs(job.wcs, job.src_sph, gpu["ex"].exposure, gpu["ps"].uPsf,
+                                          gpu["ps"].partial_psf_integral, tensor_cores=False)
+    assert max_rel(m, ref["map"]) < 1e-5
+    assert max_rel(m, gpu["map"]) < 2e-6
+
+
 def test_srcmap_f64_vs_oracle(api, c1_small):
     job, ref, gpu = c1_small
     m, info = api.point_src_model_map_wcs(job.wcs, job.src_sph, gpu["ex"].exposure, gpu["ps"].uPsf,

@@ -235,7 +235,8 @@ def _wcs_struct(w: Wcs) -> L.XtsWcs:
 
 
 def point_src_model_map_wcs(wcs: Wcs, src_sph, exposure, uPsf, partial_integrals,
-                            out_dtype: str = "float32", out=None, with_info: bool = True):
+                            out_dtype: str = "float32", out=None, with_info: bool = True,
+                            tensor_cores: bool = True):
     """ModelMap::point_src_model_map_wcs (model_map/model_map.point_src_model_map_wcs.cxx:6-45).
 
     Returns (model_map [S, H, W, E], SrcmapInfo or None).  ``out`` may supply a
@@ -262,7 +263,7 @@ def point_src_model_map_wcs(wcs: Wcs, src_sph, exposure, uPsf, partial_integrals
         o = [c.out((S, E)), c.out((S, E)), c.out((S,)), c.out((S,), "i32")]
         info_s = L.XtsSrcmapInfo(*[x[0] for x in o])
         info = SrcmapInfo(*[x[1] for x in o])
-    flags = c.flags | (L.XTS_OUT_F64 if kind == "f64" else 0)
+    flags = c.flags | (L.XTS_OUT_F64 if kind == "f64" else 0) | (0 if tensor_cores else L.XTS_CUDA_CORES)
     w = _wcs_struct(wcs)
     L.check(L.lib().xts_point_src_model_map_wcs(C.byref(w), sp, S, ep, up, pp, E, mp,
                                                 C.byref(info_s) if info_s is not None else None,

@@ -409,8 +409,11 @@ int xts_point_src_model_map_wcs(const xts_wcs* wcs, const double* src_sph, int S
     a.correction = info ? sg.out(info->correction, (size_t)S * E) : nullptr;
     a.radius = info ? sg.out(info->psf_radius, (size_t)S) : nullptr;
     a.in_fov = info ? sg.out(info->in_fov, (size_t)S) : nullptr;
+    a.cuda_cores = (flags & XTS_CUDA_CORES) != 0;
     int rc = sg.rc ? sg.rc : launch_srcmap(a, sg.st);
-    return sg.finish(rc);
+    rc = sg.finish(rc);
+    if (rc == XTS_OK && !sg.dev && S > 0) rc = srcmap_status(sg.st);
+    return rc;
 }
 
 }  // extern "C"

@@ -120,11 +120,16 @@ struct SrcmapDev {
     const double* exposure; const double* upsf; const double* partial; int E;
     void* out; bool out_f64;
     double* inv_integ; double* correction; double* radius; int* in_fov;  // optional (may be null)
+    bool cuda_cores;  // FP32 map on CUDA cores instead of tcgen05 tensor cores
 };
 int launch_srcmap(const SrcmapDev& a, cudaStream_t st);
 int launch_map_integral_fast(const double* corners, const double* centers, const double* omega,
                              const SrcInfo* info, int S, int H, int W, int nch, double* hist,
                              cudaStream_t st);
+int launch_srcmap_tc(const double* corners, const double* omega, const SrcInfo* info,
+                     const double* upsf, const double* scale, int S, int H, int W, int E, float* out,
+                     int* status, cudaStream_t st);
+int srcmap_status(cudaStream_t st);  // 0, or XTS_ERR_TIMEOUT if a bounded device wait gave up
 int launch_srcmap_fast(const double* corners, const double* omega, const SrcInfo* info,
                        const double* upsf, const double* scale, int S, int H, int W, int E,
                        float* out, cudaStream_t st);

@@ -455,6 +455,19 @@ __global__ void __launch_bounds__(256) k_correction_hist(const double* hist_in, 
     }
 }
 
+int srcmap_status(cudaStream_t st) {
+    int* status = (int*)workspace(W_MISC, 64);
+    if (!status) return XTS_ERR_OOM;
+    int v = 0;
+    XTS_CUDA(cudaMemcpyAsync(&v, status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    XTS_CUDA(cudaStreamSynchronize(st));
+    if (v) {
+        cudaMemsetAsync(status, 0, sizeof(int), st);
+        return set_error(XTS_ERR_TIMEOUT, "source-map kernel: a bounded device wait gave up");
+    }
+    return XTS_OK;
+}
+
 int launch_srcmap(const SrcmapDev& a, cudaStream_t st) {
     int rc = upload_rule(st);
     if (rc) return rc;
@@ -492,6 +505,14 @@ int launch_srcmap(const SrcmapDev& a, cudaStream_t st) {
     if (a.out_f64) {
         XTS_LAUNCH("k_srcmap_f64", st, k_srcmap<true><<<dim3(ntiles, S), TP, 0, st>>>(corners, omega, info, nullptr, a.upsf, scale,
                                                                                         H, W, E, Epad, a.out));
+        return XTS_OK;
+    }
+    if (E <= 128 && !a.cuda_cores) {
+        int* status = (int*)workspace(W_MISC, 64);
+        if (!status) return XTS_ERR_OOM;
+        XTS_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
+        rc = launch_srcmap_tc(corners, omega, info, a.upsf, scale, S, H, W, E, (float*)a.out, status, st);
+        if (rc) return rc;
         return XTS_OK;
     }
     return launch_srcmap_fast(corners, omega, info, a.upsf, scale, S, H, W, E, (float*)a.out, st);
