@@ -10,8 +10,9 @@
 // [R0, R0 + 32 nk) are processed in chunks of KC = 32:
 //   * A = W[:, chunk] (128 x 32, K-major, 128-byte swizzle) is written to shared
 //     memory by the threads, split into TF32 hi and lo parts;
-//   * B = Y'[chunk rows, 0..N) (32 x N, MN-major, 128-byte swizzle) is loaded by
-//     TMA from the hi and lo tables (rows past 400 read as zeros);
+//   * B = Y'[chunk rows, 0..N) (N x 32, K-major, 128-byte swizzle) is loaded by
+//     TMA from transposed hi and lo tables [s][e][row] (rows past 400 and
+//     energies past E read as zeros; tf32 MMAs need B K-major);
 //   * one thread issues tcgen05.mma.kind::tf32 (M = 128, N = 16 ceil(E/16), K = 8)
 //     for A_hi B_hi + A_lo B_hi + A_hi B_lo into an FP32 accumulator in tensor
 //     memory (3xTF32: ~2^-21 relative per product, FP32 accumulation);
@@ -45,8 +46,8 @@ XTS_HD inline TcLayout tc_layout(int E) {
     size_t o = 0;
     L.a_hi = o; o += TM * KC * 4;
     L.a_lo = o; o += TM * KC * 4;
-    L.b_hi = o; o += (size_t)L.na * KC * 128;
-    L.b_lo = o; o += (size_t)L.na * KC * 128;
+    L.b_hi = o; o += (size_t)L.N * 128;
+    L.b_lo = o; o += (size_t)L.N * 128;
     L.sq = o; o += (8 * (ND + 1) + 15) / 16 * 16;
     L.coef = o; o += 16 * 2 * ND;
     L.win = o; o += (4 * TM * WST + 15) / 16 * 16;
@@ -78,9 +79,9 @@ __device__ __forceinline__ unsigned long long sw128_desc(unsigned addr, unsigned
            ((unsigned long long)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46) | (2ull << 61);
 }
 
-// Instruction descriptor: D f32, A/B tf32, A K-major, B MN-major, M = 128, N.
+// Instruction descriptor: D f32, A/B tf32, both K-major, M = 128, N.
 __host__ __device__ constexpr unsigned tf32_idesc(int N) {
-    return (1u << 4) | (2u << 7) | (2u << 10) | (1u << 16) | ((unsigned)(N >> 3) << 17) | ((unsigned)(TM >> 4) << 24);
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((unsigned)(N >> 3) << 17) | ((unsigned)(TM >> 4) << 24);
 }
 
 __device__ __forceinline__ unsigned tf32_round(float v) {
@@ -202,7 +203,7 @@ k_srcmap_tc(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ C
         }
         meta[t] = make_int4(rbase, nrows, wslot, pix);
         __syncthreads();
-        const int R0 = cnt[1], Rmax = cnt[2], nwide = cnt[0];
+        const int R0 = cnt[1] & ~3, Rmax = cnt[2], nwide = cnt[0];  // TMA x coordinate: multiple of 4
         const int nk = Rmax >= R0 ? (Rmax - R0) / KC + 1 : 0;
 
         // ---------------- tensor cores: K chunks of 32 rows
@@ -211,16 +212,14 @@ k_srcmap_tc(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ C
             if (t == 0) {
                 if (c > 0) { ok = mbar_wait(bar_mma, ph_mma); ph_mma ^= 1; }  // previous chunk done with A, B
                 if (ok) {
-                    const unsigned bytes = (unsigned)(2 * na * KC * 128);
+                    const unsigned bytes = (unsigned)(2 * N * 128);
                     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(bar_tma), "r"(bytes) : "memory");
-                    for (int a = 0; a < na; ++a) {
-                        asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
-                                     :: "r"(smem_u32(smem + L.b_hi + (size_t)a * KC * 128)), "l"((unsigned long long)&tm_hi),
-                                        "r"(32 * a), "r"(rc), "r"(s), "r"(bar_tma) : "memory");
-                        asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
-                                     :: "r"(smem_u32(smem + L.b_lo + (size_t)a * KC * 128)), "l"((unsigned long long)&tm_lo),
-                                        "r"(32 * a), "r"(rc), "r"(s), "r"(bar_tma) : "memory");
-                    }
+                    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+                                 :: "r"(smem_u32(smem + L.b_hi)), "l"((unsigned long long)&tm_hi),
+                                    "r"(rc), "r"(0), "r"(s), "r"(bar_tma) : "memory");
+                    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+                                 :: "r"(smem_u32(smem + L.b_lo)), "l"((unsigned long long)&tm_lo),
+                                    "r"(rc), "r"(0), "r"(s), "r"(bar_tma) : "memory");
                 } else {
                     cnt[3] = 1;
                 }
@@ -262,16 +261,18 @@ k_srcmap_tc(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ C
                     for (int ks = 0; ks < KC / 8; ++ks) {
                         const unsigned long long dah = sw128_desc(a_hi + 32 * ks, 16, 1024);
                         const unsigned long long dal = sw128_desc(a_lo + 32 * ks, 16, 1024);
-                        const unsigned long long dbh = sw128_desc(b_hi + 1024 * ks, KC * 128, 1024);
-                        const unsigned long long dbl = sw128_desc(b_lo + 1024 * ks, KC * 128, 1024);
-                        const unsigned long long da[3] = {dah, dal, dah};
-                        const unsigned long long db[3] = {dbh, dbh, dbl};
+                        const unsigned long long dbh = sw128_desc(b_hi + 32 * ks, 16, 1024);
+                        const unsigned long long dbl = sw128_desc(b_lo + 32 * ks, 16, 1024);
+                        // small cross terms first, the full-size hi*hi term last, so that
+                        // the accumulator's FP32 rounding acts once at full magnitude per step
+                        const unsigned long long da[3] = {dal, dah, dah};
+                        const unsigned long long db[3] = {dbh, dbl, dbh};
 #pragma unroll
                         for (int term = 0; term < 3; ++term) {
                             const unsigned acc = (c > 0 || ks > 0 || term > 0) ? 1u : 0u;
                             asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                                         "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n"
-                                         :: "r"(tmem), "l"(da[term]), "l"(db[term]), "r"(idesc), "r"(acc));
+                                         "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n"
+                                         :: "r"(tmem), "l"(da[term]), "l"(db[term]), "r"(idesc), "r"(acc), "r"(0u));
                         }
                     }
                     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
@@ -383,19 +384,36 @@ static EncodeTiledFn encode_fn() {
     return fn;
 }
 
-// 3-D map over a [S][ND][Epad] float table, boxes of 32 energies x 32 rows.
-static int make_table_map(CUtensorMap* m, const float* base, int S, int Epad) {
+// 3-D map over a transposed [S][E][NDP] float table (rows contiguous), boxes of
+// 32 rows x N energies; rows past 400 and energies past E read as zeros.
+constexpr int NDP = 404;  // row stride of the transposed tables (16-byte multiple)
+
+static int make_table_map(CUtensorMap* m, const float* base, int S, int E, int N) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return set_error(XTS_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
-    cuuint64_t dims[3] = {(cuuint64_t)Epad, (cuuint64_t)ND, (cuuint64_t)S};
-    cuuint64_t strides[2] = {(cuuint64_t)Epad * 4, (cuuint64_t)ND * Epad * 4};
-    cuuint32_t box[3] = {32, (cuuint32_t)KC, 1};
+    cuuint64_t dims[3] = {(cuuint64_t)ND, (cuuint64_t)E, (cuuint64_t)S};
+    cuuint64_t strides[2] = {(cuuint64_t)NDP * 4, (cuuint64_t)NDP * E * 4};
+    cuuint32_t box[3] = {(cuuint32_t)KC, (cuuint32_t)N, 1};
     cuuint32_t es[3] = {1, 1, 1};
     CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)base, dims, strides, box, es,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return set_error(XTS_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
     return XTS_OK;
+}
+
+// Transposed 3xTF32 split of the scaled table: hi = tf32(Y'), lo = Y' - hi, [s][e][row].
+__global__ void k_lut_split_t(const float* lut, int S, int E, int Epad, float* hi, float* lo) {
+    size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    size_t n = (size_t)S * E * NDP;
+    if (k >= n) return;
+    int r = (int)(k % NDP);
+    size_t se = k / NDP;
+    int e = (int)(se % E), s = (int)(se / E);
+    float v = r < ND ? lut[((size_t)s * ND + r) * Epad + e] : 0.f;
+    float h = __uint_as_float(tf32_round(v));
+    hi[k] = h;
+    lo[k] = v - h;
 }
 
 size_t srcmap_tc_smem(int E) { return tc_layout(E).total + 1024; }
@@ -409,15 +427,17 @@ int launch_srcmap_tc(const double* corners, const double* omega, const SrcInfo* 
     rc = build_septab(st, &tab);
     if (rc) return rc;
     int Epad = (E + 3) & ~3;
-    size_t n = (size_t)S * ND * Epad;
-    float* lut = (float*)workspace(W_LUT, sizeof(float) * 3 * n + 64);
+    const int N = tc_layout(E).N;
+    size_t n = (size_t)S * ND * Epad, nt = (size_t)S * E * NDP;
+    float* lut = (float*)workspace(W_LUT, sizeof(float) * (n + 2 * nt) + 64);
     if (!lut) return XTS_ERR_OOM;
-    float* hi = lut + n;
-    float* lo = hi + n;
-    XTS_LAUNCH("k_lut_scaled", st, k_lut_scaled<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(upsf, scale, S, E, Epad, lut, hi, lo));
+    float* hi = lut + ((n + 3) & ~(size_t)3);
+    float* lo = hi + nt;
+    XTS_LAUNCH("k_lut_scaled", st, k_lut_scaled<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(upsf, scale, S, E, Epad, lut, nullptr, nullptr));
+    XTS_LAUNCH("k_lut_split_t", st, k_lut_split_t<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(lut, S, E, Epad, hi, lo));
     CUtensorMap mhi, mlo;
-    if ((rc = make_table_map(&mhi, hi, S, Epad))) return rc;
-    if ((rc = make_table_map(&mlo, lo, S, Epad))) return rc;
+    if ((rc = make_table_map(&mhi, hi, S, E, N))) return rc;
+    if ((rc = make_table_map(&mlo, lo, S, E, N))) return rc;
     size_t smem = srcmap_tc_smem(E);
     XTS_CUDA(cudaFuncSetAttribute(k_srcmap_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int dev = 0, nsm = 148;
