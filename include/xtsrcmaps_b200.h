@@ -152,6 +152,29 @@ int xts_compute_psf_data(const xts_grid* psf_front, const xts_grid* psf_back,
                          const double* front_ltf, const double* exposure,
                          double* upsf, double* partial, unsigned flags, void* stream);
 
+/* xts_compute_psf_data for callers that cannot allocate device memory.  This
+ * entry point has no counterpart in the reference: it exists for hosts that must
+ * not call cudaMalloc while they run (work recorded into a stream capture, a
+ * service whose memory pool owns the device, a real-time loop).  Every pointer
+ * is a DEVICE pointer (no flags argument; XTS_DEVICE_PTRS is implied) and the
+ * launches go to `stream` (NULL = the legacy default stream) on the current
+ * device, without xts_init.  The King and psf*aeff scratch tables live in one
+ * fixed 8 MiB device array that the library holds on every GPU that loads it
+ * until the process exits: shapes needing more than XTS_NOALLOC_SCRATCH_DOUBLES
+ * doubles, 401 * (Mc*Me front + Mc*Me back) + C * 401 * E (+ up to 31 of
+ * padding), fail with XTS_ERR_ARG and launch nothing.  All calls share that
+ * array and the last call's contents stay in it; calls that overlap on the GPU
+ * race on it, so order them on one stream.  The first call on a device looks the
+ * array up (cudaGetSymbolAddress) and must come before any stream capture. */
+#define XTS_NOALLOC_SCRATCH_DOUBLES (1u << 20)
+int xts_compute_psf_data_noalloc(const xts_grid* psf_front, const xts_grid* psf_back,
+                                 const double* exp_costhetas, int C, const double* logEs,
+                                 int E, const double* front_aeff, const double* back_aeff,
+                                 const double* src_exposure_cosbins,
+                                 const double* src_weighted_exposure_cosbins, int S,
+                                 const double* front_ltf, const double* exposure,
+                                 double* upsf, double* partial, void* stream);
+
 /* ModelMap::point_src_model_map_wcs (model_map/model_map.point_src_model_map_wcs.cxx:6-45,
  * reached from ModelMap::compute_srcmaps<PointSource>, model_map.compute_src_maps.cxx:6-22):
  * steps c1-c10 and d1.  model_map is [S, H, W, E], float unless XTS_OUT_F64. */

@@ -224,4 +224,30 @@ int launch_psf(const PsfDev& a, cudaStream_t st) {
     return XTS_OK;
 }
 
+// The same launches with caller-provided scratch: king holds both sides' King
+// tables (401 * (Mc * Me front + Mc * Me back) doubles), pa the summed psf * aeff
+// table (C * 401 * E doubles).  Nothing here allocates.
+int launch_psf_scratch(const PsfDev& a, double* king, double* pa, cudaStream_t st) {
+    if (a.C > PSF_MAX_C) return set_error(XTS_ERR_ARG, "compute_psf_data: C=%d exceeds %d", a.C, PSF_MAX_C);
+    size_t kf_n = (size_t)ND * a.pf.n_cos * a.pf.n_e, kb_n = (size_t)ND * a.pb.n_cos * a.pb.n_e;
+    int mx = (int)(kf_n > kb_n ? kf_n : kb_n);
+    XTS_LAUNCH("k_king", st, k_king<<<dim3((mx + 127) / 128, 2), 128, 0, st>>>(a.pf, a.pb, king, king + kf_n));
+    int n = a.C * ND * a.E;
+    XTS_LAUNCH("k_psf_aeff", st, k_psf_aeff<<<(n + 127) / 128, 128, 0, st>>>(a.pf, a.pb, king, king + kf_n, a.costh, a.C,
+                                               a.logEs, a.E, a.af, a.ab, pa));
+    if (a.S == 0) return XTS_OK;
+    int DE = ND * a.E;
+    dim3 g((DE + 127) / 128, (a.S + PSF_TILE_S - 1) / PSF_TILE_S);
+    XTS_LAUNCH("k_mean_psf", st, k_mean_psf<<<g, 128, 0, st>>>(pa, a.C, a.E, a.ecb, a.wecb, a.S, a.ltf, a.exposure, a.upsf));
+    size_t smem = partial_smem_bytes(a.E);
+    if (smem <= PARTIAL_SMEM_MAX) {
+        XTS_CUDA(cudaFuncSetAttribute(k_partial_integral_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        XTS_LAUNCH("k_partial_integral", st, k_partial_integral_smem<<<a.S, 256, smem, st>>>(a.upsf, a.partial, a.E));
+    } else {
+        n = a.S * a.E;
+        XTS_LAUNCH("k_partial_integral", st, k_partial_integral<<<(n + 127) / 128, 128, 0, st>>>(a.upsf, a.partial, a.S, a.E));
+    }
+    return XTS_OK;
+}
+
 }  // namespace xts
