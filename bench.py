@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=11)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--kernel", default="windows", choices=["windows", "cuda_cores", "tcgen05"],
+                    help="FP32 source-map write pass")
     return ap.parse_args()
 
 
@@ -173,7 +175,7 @@ def run_ours(args, rank, world, local_rank):
         with torch.cuda.stream(stream):
             ex = A.compute_exposure(d["cube"], d["wcube"], d["logEs"], d["src"], d["af"], d["ab"], ltf)
             ps = A.compute_psf_data(nf, nb, ex, d["logEs"], ltf)
-            A.point_src_model_map_wcs(job.wcs, d["src"], ex.exposure, ps.uPsf, ps.partial_psf_integral,
+            A.point_src_model_map_wcs(job.wcs, d["src"], ex.exposure, ps.uPsf, ps.partial_psf_integral, kernel=args.kernel,
                                       out=out, with_info=False)
 
     for _ in range(max(3, args.warmup)):
@@ -245,7 +247,7 @@ def run_ours(args, rank, world, local_rank):
             ex = A.compute_exposure(hp["cube"], hp["wcube"], hp["logEs"], hp["src"], job.aeff_front,
                                     job.aeff_back, ltf_h)
             ps = A.compute_psf_data(nf_h, nb_h, ex, hp["logEs"], ltf_h)
-            A.point_src_model_map_wcs(job.wcs, hp["src"], ex.exposure, ps.uPsf, ps.partial_psf_integral,
+            A.point_src_model_map_wcs(job.wcs, hp["src"], ex.exposure, ps.uPsf, ps.partial_psf_integral, kernel=args.kernel,
                                       out=hout, with_info=False)
             return ex, ps
 

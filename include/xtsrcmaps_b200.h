@@ -45,7 +45,10 @@ enum xts_flags {
     XTS_DEVICE_PTRS = 1u << 0, /* array arguments are device pointers */
     XTS_OUT_F64 = 1u << 1,     /* model map written as double (default float) */
     XTS_EXPOSURE_TF32 = 1u << 2, /* exposure contraction as 3xTF32 on tcgen05 tensor cores (default: FP64 cores) */
-    XTS_CUDA_CORES = 1u << 3     /* FP32 source maps on CUDA cores only (default: tcgen05 tensor cores) */
+    XTS_CUDA_CORES = 1u << 3,    /* FP32 source maps by the single-pass CUDA-core kernel (geometry and
+                                    map integral in separate passes; default: the two-pass window path) */
+    XTS_TCGEN05 = 1u << 4        /* FP32 source maps with the window-times-table product on tcgen05
+                                    tensor cores (3xTF32); default: the two-pass window path */
 };
 
 /* FITS celestial WCS (sky_geom/sky_geom.hxx:17-25, WcsConfig). */

@@ -93,14 +93,18 @@ def test_srcmap_f32_vs_oracle(api, c1_small):
     assert max_rel(tot_g, tot_r) < 1e-7
 
 
-def test_srcmap_cuda_core_path_vs_oracle(api, c1_small):
-    """The CUDA-core FP32 path (XTS_CUDA_CORES) against the oracle and the
-    default tensor-core path."""
+@pytest.mark.parametrize("kernel", ["cuda_cores", "tcgen05"])
+def test_srcmap_other_fp32_kernels_vs_oracle(api, c1_small, kernel):
+    """The single-pass CUDA-core kernel (XTS_CUDA_CORES) and the tcgen05 kernel
+    (XTS_TCGEN05) against the oracle and the default two-pass window path."""
     job, ref, gpu = c1_small
     m, info = api.point_src_model_map_wcs(job.wcs, job.src_sph, gpu["ex"].exposure, gpu["ps"].uPsf,
-                                          gpu["ps"].partial_psf_integral, tensor_cores=False)
+                                          gpu["ps"].partial_psf_integral, kernel=kernel)
     assert max_rel(m, ref["map"]) < 1e-5
     assert max_rel(m, gpu["map"]) < 2e-6
+    assert max_rel(info.inv_map_integral, ref["inv_integ"]) < 1e-7
+    tot_g = m.astype(np.float64).sum(axis=(1, 2))
+    assert max_rel(tot_g, ref["map"].sum(axis=(1, 2))) < 1e-7
 
 
 def test_srcmap_f64_vs_oracle(api, c1_small):

@@ -236,12 +236,16 @@ def _wcs_struct(w: Wcs) -> L.XtsWcs:
 
 def point_src_model_map_wcs(wcs: Wcs, src_sph, exposure, uPsf, partial_integrals,
                             out_dtype: str = "float32", out=None, with_info: bool = True,
-                            tensor_cores: bool = True):
+                            kernel: str = "windows"):
     """ModelMap::point_src_model_map_wcs (model_map/model_map.point_src_model_map_wcs.cxx:6-45).
 
     Returns (model_map [S, H, W, E], SrcmapInfo or None).  ``out`` may supply a
-    preallocated output of the right dtype and shape.
+    preallocated output of the right dtype and shape (16-byte aligned).
+    ``kernel`` picks the FP32 write pass: "windows" (default: geometry pass +
+    streaming write pass), "cuda_cores" (single-pass CUDA-core kernel) or
+    "tcgen05" (window-times-table product on tensor cores).
     """
+    kflag = {"windows": 0, "cuda_cores": L.XTS_CUDA_CORES, "tcgen05": L.XTS_TCGEN05}[kernel]
     like = _device_of(uPsf, exposure, src_sph)
     c = _Call(like is not None, like)
     sp, sa = c.inp(src_sph)
@@ -263,7 +267,7 @@ def point_src_model_map_wcs(wcs: Wcs, src_sph, exposure, uPsf, partial_integrals
         o = [c.out((S, E)), c.out((S, E)), c.out((S,)), c.out((S,), "i32")]
         info_s = L.XtsSrcmapInfo(*[x[0] for x in o])
         info = SrcmapInfo(*[x[1] for x in o])
-    flags = c.flags | (L.XTS_OUT_F64 if kind == "f64" else 0) | (0 if tensor_cores else L.XTS_CUDA_CORES)
+    flags = c.flags | (L.XTS_OUT_F64 if kind == "f64" else 0) | kflag
     w = _wcs_struct(wcs)
     L.check(L.lib().xts_point_src_model_map_wcs(C.byref(w), sp, S, ep, up, pp, E, mp,
                                                 C.byref(info_s) if info_s is not None else None,

@@ -395,6 +395,9 @@ int xts_point_src_model_map_wcs(const xts_wcs* wcs, const double* src_sph, int S
         return set_error(XTS_ERR_ARG, "point_src_model_map_wcs: map or source count too large");
     bool f64 = (flags & XTS_OUT_F64) != 0;
     size_t npix = (size_t)wcs->naxis1 * wcs->naxis2;
+    // the FP32 write passes store with TMA bulk copies, which need a 16-byte aligned base
+    if ((flags & XTS_DEVICE_PTRS) && !f64 && ((uintptr_t)model_map & 15))
+        return set_error(XTS_ERR_ARG, "point_src_model_map_wcs: device model_map must be 16-byte aligned");
     Stager sg{(flags & XTS_DEVICE_PTRS) != 0, stream ? (cudaStream_t)stream : g_ctx.stream};
     SrcmapDev a;
     a.wcs = *wcs;
@@ -409,7 +412,7 @@ int xts_point_src_model_map_wcs(const xts_wcs* wcs, const double* src_sph, int S
     a.correction = info ? sg.out(info->correction, (size_t)S * E) : nullptr;
     a.radius = info ? sg.out(info->psf_radius, (size_t)S) : nullptr;
     a.in_fov = info ? sg.out(info->in_fov, (size_t)S) : nullptr;
-    a.cuda_cores = (flags & XTS_CUDA_CORES) != 0;
+    a.kernel = (flags & XTS_TCGEN05) ? SRCMAP_TCGEN05 : (flags & XTS_CUDA_CORES) ? SRCMAP_ONEPASS : SRCMAP_WINDOWS;
     int rc = sg.rc ? sg.rc : launch_srcmap(a, sg.st);
     rc = sg.finish(rc);
     if (rc == XTS_OK && !sg.dev && S > 0) rc = srcmap_status(sg.st);

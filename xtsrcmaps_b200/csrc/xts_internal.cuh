@@ -62,7 +62,7 @@ enum Slot {
     S_OUT0, S_OUT1, S_OUT2, S_OUT3, S_OUT4, S_OUT5, S_OUT6,
     // internal scratch
     W_CORNERS, W_CENTERS, W_OMEGA, W_LUT, W_PARTSUM, W_SRCINFO, W_SCALE, W_PSFTAB,
-    W_KING, W_MISC,
+    W_KING, W_MISC, W_WIN, W_WMETA, W_SPARSE,
     N_SLOTS
 };
 void* workspace(int slot, size_t bytes);  // nullptr + error set on OOM
@@ -120,8 +120,9 @@ struct SrcmapDev {
     const double* exposure; const double* upsf; const double* partial; int E;
     void* out; bool out_f64;
     double* inv_integ; double* correction; double* radius; int* in_fov;  // optional (may be null)
-    bool cuda_cores;  // FP32 map on CUDA cores instead of tcgen05 tensor cores
+    int kernel;  // FP32 write pass: SRCMAP_WINDOWS, SRCMAP_ONEPASS or SRCMAP_TCGEN05
 };
+enum { SRCMAP_WINDOWS = 0, SRCMAP_ONEPASS = 1, SRCMAP_TCGEN05 = 2 };
 int launch_srcmap(const SrcmapDev& a, cudaStream_t st);
 int launch_map_integral_fast(const double* corners, const double* centers, const double* omega,
                              const SrcInfo* info, int S, int H, int W, int nch, double* hist,
@@ -129,7 +130,17 @@ int launch_map_integral_fast(const double* corners, const double* centers, const
 int launch_srcmap_tc(const double* corners, const double* omega, const SrcInfo* info,
                      const double* upsf, const double* scale, int S, int H, int W, int E, float* out,
                      int* status, cudaStream_t st);
-int srcmap_status(cudaStream_t st);  // 0, or XTS_ERR_TIMEOUT if a bounded device wait gave up
+int srcmap_status(cudaStream_t st);
+int launch_correction(const double* hist, int nch, const SrcInfo* info, int S, const double* upsf,
+                      const double* partial, const double* exposure, int E, double* scale,
+                      double* inv_integ, double* correction, double* radius, int* in_fov,
+                      cudaStream_t st);
+bool srcmap_win_supported(int E);
+int launch_srcmap_win(const double* corners, const double* centers, const double* omega,
+                      const SrcInfo* info, int S, int H, int W, int E, int nch, double* hist,
+                      const double* upsf, const double* partial, const double* exposure,
+                      double* scale, double* inv_integ, double* correction, double* radius,
+                      int* in_fov, int* status, float* out, cudaStream_t st);  // 0, or XTS_ERR_TIMEOUT if a bounded device wait gave up
 int launch_srcmap_fast(const double* corners, const double* omega, const SrcInfo* info,
                        const double* upsf, const double* scale, int S, int H, int W, int E,
                        float* out, cudaStream_t st);

@@ -455,6 +455,15 @@ __global__ void __launch_bounds__(256) k_correction_hist(const double* hist_in, 
     }
 }
 
+int launch_correction(const double* hist, int nch, const SrcInfo* info, int S, const double* upsf,
+                      const double* partial, const double* exposure, int E, double* scale,
+                      double* inv_integ, double* correction, double* radius, int* in_fov,
+                      cudaStream_t st) {
+    XTS_LAUNCH("k_correction", st, k_correction_hist<<<S, 256, 0, st>>>(hist, nch, info, upsf, partial, exposure, E,
+                                                                        scale, inv_integ, correction, radius, in_fov));
+    return XTS_OK;
+}
+
 int srcmap_status(cudaStream_t st) {
     int* status = (int*)workspace(W_MISC, 64);
     if (!status) return XTS_ERR_OOM;
@@ -494,20 +503,29 @@ int launch_srcmap(const SrcmapDev& a, cudaStream_t st) {
     XTS_LAUNCH("k_solid_angle", st, k_solid_angle<<<(npix + 127) / 128, 128, 0, st>>>(centers, H, W, omega));
     if (S == 0) return XTS_OK;
     XTS_LAUNCH("k_boundary", st, k_boundary<<<S, 128, 0, st>>>(w, a.src_sph, H, W, corners, info));
+    if (!a.out_f64 && a.kernel == SRCMAP_WINDOWS && srcmap_win_supported(E)) {
+        int* status = (int*)workspace(W_MISC, 64);
+        if (!status) return XTS_ERR_OOM;
+        XTS_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
+        return launch_srcmap_win(corners, centers, omega, info, S, H, W, E, nch, hist, a.upsf, a.partial,
+                                 a.exposure, scale, a.inv_integ, a.correction, a.radius, a.in_fov, status,
+                                 (float*)a.out, st);
+    }
     if (a.out_f64) {  // the reference's own per-point FP64 arithmetic throughout
         XTS_LAUNCH("k_map_integral_f64", st, k_map_integral_hist<<<dim3(nch, S), 256, 0, st>>>(corners, centers, omega, info, H, W, nch, hist));
     } else {
         rc = launch_map_integral_fast(corners, centers, omega, info, S, H, W, nch, hist, st);
         if (rc) return rc;
     }
-    XTS_LAUNCH("k_correction", st, k_correction_hist<<<S, 256, 0, st>>>(hist, nch, info, a.upsf, a.partial, a.exposure, E,
-                                                                        scale, a.inv_integ, a.correction, a.radius, a.in_fov));
+    rc = launch_correction(hist, nch, info, S, a.upsf, a.partial, a.exposure, E, scale, a.inv_integ,
+                           a.correction, a.radius, a.in_fov, st);
+    if (rc) return rc;
     if (a.out_f64) {
         XTS_LAUNCH("k_srcmap_f64", st, k_srcmap<true><<<dim3(ntiles, S), TP, 0, st>>>(corners, omega, info, nullptr, a.upsf, scale,
                                                                                         H, W, E, Epad, a.out));
         return XTS_OK;
     }
-    if (E <= 128 && !a.cuda_cores) {
+    if (a.kernel == SRCMAP_TCGEN05 && E <= 128) {
         int* status = (int*)workspace(W_MISC, 64);
         if (!status) return XTS_ERR_OOM;
         XTS_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));

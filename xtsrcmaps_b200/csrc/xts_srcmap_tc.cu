@@ -31,7 +31,6 @@ namespace xts {
 
 constexpr int TM = 128;  // pixels per tile == MMA M == threads per block
 constexpr int KC = 32;   // table rows per K chunk (128 bytes of TF32: one swizzle atom)
-constexpr int WAIT_LIMIT = 1 << 21;  // try_wait polls before a wait is declared failed
 
 struct TcLayout {  // shared-memory byte offsets, all multiples of 16 (A, B: 1024)
     int na, N, E;
@@ -58,18 +57,6 @@ XTS_HD inline TcLayout tc_layout(int E) {
     L.bars = o; o += 64;
     L.total = o;
     return L;
-}
-
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
-    for (int i = 0; i < WAIT_LIMIT; ++i) {
-        unsigned done;
-        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
-                     : "=r"(done) : "r"(bar), "r"(parity) : "memory");
-        if (done) return true;
-    }
-    return false;
 }
 
 // UMMA shared-memory descriptors (sm_100 format: start >> 4 in [0,14), LBO >> 4 in

@@ -1,0 +1,438 @@
+// xts_srcmap_win.cu -- the FP32 source-map path in two passes over the pixels.
+//
+// Pass A, k_pixel_windows (geometry, once per pixel and source): the 12 rule
+// points of the pixel give LUT rows and interpolation weights (xts_point.cuh);
+// their weights times the pixel's solid angle are summed into a dense window of
+// at most RW consecutive table rows.  For pixels inside the boundary radius of
+// an in-FOV source the FP64 window also enters the block's row histogram, whose
+// dot product with uPsf is the map integral of c7 (model_map.map_integral.cxx:4-48):
+//     sum_pix omega * value(pix, e) = sum_r Hist[r] * uPsf[r][e].
+// Every pixel's window is written once as a 36-byte record (8 FP32 weights and
+// the first row / row count).  Pixels whose points leave the window (those next
+// to the source) are "wide": they get a sparse record of their 24 (row, weight)
+// pairs from a shared pool instead, or, if the pool is full, are evaluated point
+// by point in pass B.
+//
+// Pass B, k_srcmap_win (the write pass, d1 + d2 + c8 + c10): the source's scaled
+// table Y' = uPsf * exposure * correction (FP32, [401][EQ] float4, EQ odd so
+// different rows fall in different shared-memory bank groups) is brought into
+// shared memory by one TMA bulk copy; each thread reads its pixel's window
+// record and forms value[e] = sum_j W[j] * Y'[row_j][e] for all energies in
+// registers (rows rbase + j, or the 24 rows of a sparse record).  Values are
+// staged and written by one TMA bulk store per tile, so the pass streams the
+// window records in and the map out; the next tile's records are loaded while
+// the current one is computed.
+#include "xts_point.cuh"
+
+namespace xts {
+
+// ============================================================================ pass A
+constexpr int WT = 256;  // pixels per tile == threads per block
+
+constexpr size_t WA_OFF_SQ = 0;
+constexpr size_t WA_OFF_COEF = (8 * (ND + 1) + 15) / 16 * 16;
+constexpr size_t WA_OFF_HIST = WA_OFF_COEF + sizeof(float4) * 2 * ND;
+constexpr size_t WA_OFF_WTS = WA_OFF_HIST + (8 * ND + 15) / 16 * 16;
+constexpr size_t WA_OFF_BASE = WA_OFF_WTS + sizeof(double) * WT * RW;
+constexpr size_t WA_SMEM = WA_OFF_BASE + sizeof(int) * (WT + 4);
+
+constexpr int NSP = 24;  // entries of a sparse record: 12 points x 2 rows
+constexpr int META_OVERFLOW = -0x7fffffff - 1;  // wide pixel without a sparse record
+
+__global__ void __launch_bounds__(WT, 3) k_pixel_windows(const double* __restrict__ corners, const double* __restrict__ centers,
+                                                      const double* __restrict__ omega, const SrcInfo* __restrict__ info,
+                                                      const SepTab* __restrict__ septab, int H, int W, int nch,
+                                                      double* __restrict__ hist_out, float4* __restrict__ win,
+                                                      int* __restrict__ wmeta, float2* __restrict__ sparse,
+                                                      int sparse_cap, int* __restrict__ sparse_count) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* sq = (double*)(smem + WA_OFF_SQ);
+    float4* scoef = (float4*)(smem + WA_OFF_COEF);
+    double* hist = (double*)(smem + WA_OFF_HIST);
+    double* wts = (double*)(smem + WA_OFF_WTS);  // [RW][WT] FP64 windows (row-major by window slot)
+    int* wbase = (int*)(smem + WA_OFF_BASE);     // [WT] first row (-1: not in radius); [WT..WT+3] row min/max by parity
+    const int s = blockIdx.y, t = threadIdx.x;
+    const SrcInfo si = info[s];
+    for (int k = t; k < ND + 1; k += WT) sq[k] = septab->q[k];
+    for (int k = t; k < 2 * ND; k += WT) scoef[k] = ((const float4*)septab->coef)[k];
+    for (int r = t; r < ND; r += WT) hist[r] = 0.;
+    if (t < 4) wbase[WT + t] = (t & 1) ? -1 : ND;
+    double ch2 = 2.0 * sin(0.5 * si.radius_rad);
+    ch2 *= ch2;
+    const int npix = H * W, W1 = W + 1;
+    const int ntiles = (npix + WT - 1) / WT;
+    const size_t sp = (size_t)s * npix;
+    __syncthreads();
+    int it = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += nch, ++it) {
+        const int par = 2 * (it & 1);
+        // the other parity's min/max slots were last read before the previous
+        // iteration's closing barrier; reset them for the next iteration
+        if (t == 0) { wbase[WT + 2 - par] = ND; wbase[WT + 3 - par] = -1; }
+        const int pix = tile * WT + t;
+        bool inside = false;
+        int rb = -1;
+        if (pix < npix) {
+            const int h = pix / W, w = pix - h * W;
+            if (si.in_fov) {
+                const double* c = centers + 3 * (h * W1 + w);
+                const double x = si.dir[0] - c[0], y = si.dir[1] - c[1], z = si.dir[2] - c[2];
+                const double d2 = x * x + y * y + z * z;
+                if (d2 < ch2 * (1.0 - 1e-12)) inside = true;
+                else if (d2 > ch2 * (1.0 + 1e-12)) inside = false;
+                else inside = dir_diff(si.dir, c) <= si.radius_rad;
+            }
+            const PixGeom g = pixel_geom(corners, W1, h, w, si);
+            const double om = omega[pix];
+            float tc;
+            const int ic = point_row(fma(g.Ax, g.Ax, fma(g.Ay, g.Ay, g.Az * g.Az)), sq, scoef, &tc);
+            const int base = min(max(ic - 1 - RW / 2, 0), ND - RW);
+            double* wd = wts + t;  // slot j at wd[j * WT]: lanes hit consecutive words
+#pragma unroll
+            for (int j = 0; j < RW; ++j) wd[j * WT] = 0.;
+            bool wide = false;
+            int lo = RW, hi = -1;
+#pragma unroll
+            for (int p = 0; p < 12; ++p) {
+                float tt;
+                const int idx = point_row(point_q(g, p), sq, scoef, &tt);
+                const int r = idx - 1 - base;
+                const double wgt = c_rule_uv[p][3];
+                const double wa = (double)(1.f - tt) * wgt * om, wb = (double)tt * wgt * om;
+                if (r >= 0 && r < RW - 1) {
+                    wd[r * WT] += wa;
+                    wd[(r + 1) * WT] += wb;
+                    lo = min(lo, r);
+                    hi = max(hi, r + 1);
+                } else {
+                    wide = true;
+                    if (inside) {
+                        atomicAdd(&hist[idx - 1], wa);
+                        atomicAdd(&hist[idx], wb);
+                    }
+                }
+            }
+            // the FP32 window record of the write pass, shifted to its first row
+            float f[RW];
+#pragma unroll
+            for (int j = 0; j < RW; ++j) f[j] = 0.f;
+            int meta;
+            if (!wide) {
+#pragma unroll
+                for (int j = 0; j < RW; ++j)
+                    if (j <= hi - lo) f[j] = (float)wd[min(j + lo, RW - 1) * WT];
+                meta = (base + lo) | ((hi - lo + 1) << 16);
+            } else {
+                const int slot = atomicAdd(sparse_count, 1);
+                if (slot < sparse_cap) {  // the 12 points again (rare: pixels next to the source)
+                    float2* rec = sparse + (size_t)slot * NSP;
+                    for (int p = 0; p < 12; ++p) {
+                        float tt;
+                        const int idx = point_row(point_q(g, p), sq, scoef, &tt);
+                        const double wgt = c_rule_uv[p][3];
+                        rec[2 * p] = make_float2((float)((double)(1.f - tt) * wgt * om), __int_as_float(idx - 1));
+                        rec[2 * p + 1] = make_float2((float)((double)tt * wgt * om), __int_as_float(idx));
+                    }
+                    meta = -1 - slot;
+                } else {
+                    meta = META_OVERFLOW;
+                }
+            }
+            win[2 * (sp + pix)] = make_float4(f[0], f[1], f[2], f[3]);
+            win[2 * (sp + pix) + 1] = make_float4(f[4], f[5], f[6], f[7]);
+            wmeta[sp + pix] = meta;
+            if (inside) {
+                rb = base;
+                atomicMin(&wbase[WT + par], base);
+                atomicMax(&wbase[WT + 1 + par], base + RW - 1);
+            }
+        }
+        wbase[t] = rb;
+        if (__syncthreads_or(inside)) {
+            const int rmin = wbase[WT + par], rmax = wbase[WT + 1 + par];
+            // 8 threads per row, each over 32 pixels (p = sub mod 8), combined in a
+            // fixed shuffle order; the four rows of a warp start at different pixels
+            // so that their window reads spread over the banks
+            const int sub = t & 7, a = (t >> 3) & 3;
+            for (int r0 = rmin; r0 <= rmax; r0 += WT / 8) {
+                const int r = r0 + (t >> 3);
+                double acc = 0.;
+                if (r <= rmax) {
+                    for (int i = 0; i < 32; ++i) {
+                        const int p = ((i + a) & 31) * 8 + sub;
+                        const int b0 = wbase[p];
+                        const int k = r - b0;
+                        if (b0 >= 0 && k >= 0 && k < RW) acc += wts[k * WT + p];
+                    }
+                }
+                acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+                acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+                acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+                if (sub == 0 && r <= rmax) hist[r] += acc;
+            }
+        }
+        __syncthreads();
+    }
+    double* out = hist_out + ((size_t)s * nch + blockIdx.x) * ND;
+    for (int r = t; r < ND; r += WT) out[r] = hist[r];
+}
+
+// ============================================================================ pass B
+constexpr int BT = 256;  // pixels per tile == threads per block
+constexpr int BQ = 13;   // float4 quads of a table row at most: E <= 52
+
+// Table row stride in float4 units: ceil(E/4), made odd.
+static int win_row_quads(int E) {
+    int nq = (E + 3) / 4;
+    return (nq & 1) ? nq : nq + 1;
+}
+
+struct WinLayout { size_t tab, stage, bar, total; };
+static __host__ __device__ WinLayout win_layout(int E, int EQ) {
+    WinLayout L;
+    L.tab = 0;                                            // [ND + RW][EQ] float4 (RW zero guard rows)
+    L.stage = (size_t)(ND + RW) * EQ * 16;                // [BT * E + 8] floats
+    L.bar = (L.stage + sizeof(float) * ((size_t)BT * E + 8) + 15) / 16 * 16;
+    L.total = L.bar + 16;
+    return L;
+}
+
+// One pixel's record as read by pass B.
+struct PixRec { int meta; float4 wa, wb; };
+
+__device__ __forceinline__ PixRec load_rec(const float4* win, const int* wmeta, size_t k, bool valid) {
+    PixRec r;
+    r.meta = 0;
+    r.wa = make_float4(0.f, 0.f, 0.f, 0.f);
+    r.wb = r.wa;
+    if (valid) {
+        r.meta = __ldg(wmeta + k);
+        r.wa = __ldg(win + 2 * k);
+        r.wb = __ldg(win + 2 * k + 1);
+    }
+    return r;
+}
+
+__global__ void __launch_bounds__(BT, 2)
+k_srcmap_win(const float4* __restrict__ win, const int* __restrict__ wmeta, const float2* __restrict__ sparse,
+             const float* __restrict__ lut, const double* __restrict__ corners, const double* __restrict__ omega,
+             const SrcInfo* __restrict__ info, const SepTab* __restrict__ septab,
+             int S, int s_base, int H, int W, int E, int EQ, int* status, float* __restrict__ out) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const WinLayout L = win_layout(E, EQ);
+    float4* tab = (float4*)(smem + L.tab);
+    float* stage = (float*)(smem + L.stage);
+    const unsigned bar = smem_u32(smem + L.bar);
+    const int t = threadIdx.x;
+    const int nq = (E + 3) >> 2;
+    const int npix = H * W, W1 = W + 1;
+    const int ntiles = (npix + BT - 1) / BT;
+    const long long T = (long long)S * ntiles;
+    const long long f0 = T * blockIdx.x / gridDim.x, f1 = T * (blockIdx.x + 1) / gridDim.x;
+    const unsigned tab_bytes = (unsigned)(ND * EQ * 16);
+
+    for (int k = t; k < RW * EQ; k += BT) tab[ND * EQ + k] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (t == 0) mbar_init(bar, 1);
+    __syncthreads();
+
+    int cur = -1;
+    unsigned phase = 0;
+    PixRec rec;
+    {
+        const int s = (int)(f0 / ntiles), p0 = (int)(f0 - (long long)s * ntiles) * BT;
+        rec = load_rec(win, wmeta, (size_t)s * npix + p0 + t, f0 < f1 && p0 + t < npix);
+    }
+    for (long long f = f0; f < f1; ++f) {
+        const int s = (int)(f / ntiles);
+        const int tile = (int)(f - (long long)s * ntiles);
+        const int p0 = tile * BT;
+        const int np = min(BT, npix - p0);
+        const long long g0 = ((long long)(s_base + s) * npix + p0) * E;  // first flat output of the whole map
+        const int m = (int)(g0 & 3);                                      // staging residue
+        const int nflat = np * E;
+        const int pix = p0 + t;
+
+        // the next tile's records, in flight while this tile is computed
+        PixRec nxt;
+        {
+            const long long fn = f + 1;
+            const int sn = (int)(fn / ntiles), pn = (int)(fn - (long long)sn * ntiles) * BT;
+            nxt = load_rec(win, wmeta, (size_t)sn * npix + pn + t, fn < f1 && pn + t < npix);
+        }
+        if (s != cur) {
+            __syncthreads();  // every thread is done with the previous source's table
+            if (t == 0) {
+                fence_async_shared();
+                bulk_load(tab, lut + (size_t)s * ND * EQ * 4, tab_bytes, bar);
+            }
+            cur = s;
+            const bool ok = mbar_wait(bar, phase);
+            phase ^= 1;
+            if (!__syncthreads_and(ok)) {
+                if (t == 0) {
+                    atomicExch(status, 1);
+                    mbar_wait(bar, phase ^ 1);  // bounded: let the copy land before the block exits
+                    bulk_wait_all();
+                }
+                return;
+            }
+        }
+        if (t == 0) bulk_wait_read();  // the previous tile's bulk store has read the stage
+        __syncthreads();
+
+        // entries of this pixel: window rows rbase + j (j < nr), or a sparse record
+        const int meta = rec.meta;
+        const bool valid = t < np;
+        const bool sp = valid && meta < 0 && meta != META_OVERFLOW;
+        const bool slow = valid && meta == META_OVERFLOW;
+        const int nent = sp ? NSP : (meta >= 0 ? (meta >> 16) : 0);
+        const int rb = meta >= 0 ? (meta & 0xffff) : 0;
+        const float2* se = sparse + (size_t)(sp ? -1 - meta : 0) * NSP;
+        const int kmax = __reduce_max_sync(0xffffffffu, nent);
+        const float w[RW] = {rec.wa.x, rec.wa.y, rec.wa.z, rec.wa.w, rec.wb.x, rec.wb.y, rec.wb.z, rec.wb.w};
+        float4 acc[BQ];
+#pragma unroll
+        for (int q = 0; q < BQ; ++q) acc[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int j = 0; j < NSP; ++j) {
+            if (j < kmax) {  // warp-uniform; entries past a pixel's own count carry weight 0
+                float wj = j < RW ? w[j < RW ? j : 0] : 0.f;
+                int row = rb + (j < RW ? j : 0);
+                if (sp) {
+                    const float2 e = __ldg(se + j);
+                    wj = e.x;
+                    row = __float_as_int(e.y);
+                }
+                const float4* yr = tab + row * EQ;
+#pragma unroll
+                for (int q = 0; q < BQ; ++q) {
+                    if (q < nq) {
+                        const float4 y = yr[q];
+                        acc[q].x = fmaf(wj, y.x, acc[q].x);
+                        acc[q].y = fmaf(wj, y.y, acc[q].y);
+                        acc[q].z = fmaf(wj, y.z, acc[q].z);
+                        acc[q].w = fmaf(wj, y.w, acc[q].w);
+                    }
+                }
+            }
+        }
+        float* dst = stage + m + t * E;
+        if (valid && !slow) {
+#pragma unroll
+            for (int q = 0; q < BQ; ++q) {
+                if (q < nq) {
+                    const int e = 4 * q;
+                    dst[e] = acc[q].x;
+                    if (e + 1 < E) dst[e + 1] = acc[q].y;
+                    if (e + 2 < E) dst[e + 2] = acc[q].z;
+                    if (e + 3 < E) dst[e + 3] = acc[q].w;
+                }
+            }
+        }
+        if (slow) {  // sparse pool full: point by point from the shared table, compensated sum
+            const SrcInfo si = info[s];
+            const int h = pix / W, wc = pix - h * W;
+            const PixGeom g = pixel_geom(corners, W1, h, wc, si);
+            const float om = (float)omega[pix];
+            const float* Y = (const float*)tab;
+            const int ES = 4 * EQ;
+            for (int e = 0; e < E; ++e) {
+                float acc1 = 0.f, comp = 0.f;
+                for (int p = 0; p < 12; ++p) {
+                    float tt;
+                    const int idx = point_row(point_q(g, p), septab->q, (const float4*)septab->coef, &tt);
+                    const float wgt = (float)c_rule_uv[p][3];
+                    const float* yl = Y + (idx - 1) * ES + e;
+                    const float term = fmaf((1.f - tt) * wgt, yl[0], tt * wgt * yl[ES]);
+                    const float s2 = acc1 + term;
+                    comp += fabsf(acc1) >= fabsf(term) ? (acc1 - s2) + term : (term - s2) + acc1;
+                    acc1 = s2;
+                }
+                dst[e] = (acc1 + comp) * om;
+            }
+        }
+        fence_async_shared();
+        __syncthreads();
+        // TMA bulk store of the 16-byte aligned body, threads for the edges
+        const long long ga = (g0 + 3) & ~3LL, gb = (g0 + nflat) & ~3LL;
+        if (t == 0 && gb > ga)
+            bulk_store(out + ga, stage + m + (int)(ga - g0), (unsigned)((gb - ga) * 4));
+        if (t < 8) {
+            const long long g = t < 4 ? g0 + t : gb + (t - 4);
+            const bool head = t < 4 && g < ga && g < g0 + nflat;
+            const bool tail = t >= 4 && g >= gb && g >= ga && g < g0 + nflat;
+            if (head || tail) out[g] = stage[m + (int)(g - g0)];
+        }
+        rec = nxt;
+    }
+    if (t == 0) bulk_wait_all();
+}
+
+// ============================================================================ host
+bool srcmap_win_supported(int E) {
+    return E >= 1 && E <= 4 * BQ && win_layout(E, win_row_quads(E)).total <= 227 * 1024;
+}
+
+// Window records of one source chunk: 36 bytes per (source, pixel).
+static size_t win_bytes_per_source(int npix) { return (size_t)npix * 36; }
+
+int launch_srcmap_win(const double* corners, const double* centers, const double* omega,
+                      const SrcInfo* info, int S, int H, int W, int E, int nch, double* hist,
+                      const double* upsf, const double* partial, const double* exposure,
+                      double* scale, double* inv_integ, double* correction, double* radius,
+                      int* in_fov, int* status, float* out, cudaStream_t st) {
+    int rc = upload_rule_uv(st);
+    if (rc) return rc;
+    const SepTab* tab = nullptr;
+    rc = build_septab(st, &tab);
+    if (rc) return rc;
+    const int npix = H * W;
+    const int EQ = win_row_quads(E);
+    const WinLayout L = win_layout(E, EQ);
+    // sources per chunk: window records of at most ~2 GiB
+    const size_t budget = (size_t)2 << 30;
+    int Sc = (int)(budget / win_bytes_per_source(npix));
+    Sc = Sc < 1 ? 1 : (Sc > S ? S : Sc);
+    float4* win = (float4*)workspace(W_WIN, (size_t)Sc * npix * 32 + 16);
+    int* wmeta = (int*)workspace(W_WMETA, (size_t)Sc * npix * 4 + 16);
+    float* lut = (float*)workspace(W_LUT, sizeof(float) * (size_t)Sc * ND * EQ * 4 + 16);
+    // sparse records for wide pixels: room for 1/8 of the chunk's pixels (at least 64k)
+    long long cap = (long long)Sc * npix / 8;
+    cap = cap < 65536 ? 65536 : cap;
+    cap = cap > (long long)Sc * npix ? (long long)Sc * npix : cap;
+    float2* sparse = (float2*)workspace(W_SPARSE, sizeof(float2) * NSP * (size_t)cap + 16);
+    if (!win || !wmeta || !lut || !sparse) return XTS_ERR_OOM;
+    int* sparse_count = status + 1;
+    XTS_CUDA(cudaFuncSetAttribute(k_pixel_windows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WA_SMEM));
+    XTS_CUDA(cudaFuncSetAttribute(k_srcmap_win, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
+    int dev = 0, nsm = 148, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    XTS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_srcmap_win, BT, L.total));
+    if (per_sm < 1) return set_error(XTS_ERR_ARG, "source-map write pass does not fit on an SM (E=%d)", E);
+    for (int s0 = 0; s0 < S; s0 += Sc) {
+        const int n = S - s0 < Sc ? S - s0 : Sc;
+        const size_t oE = (size_t)s0 * E;
+        XTS_CUDA(cudaMemsetAsync(sparse_count, 0, sizeof(int), st));
+        XTS_LAUNCH("k_pixel_windows", st, k_pixel_windows<<<dim3(nch, n), WT, WA_SMEM, st>>>(
+                                              corners, centers, omega, info + s0, tab, H, W, nch,
+                                              hist + (size_t)s0 * nch * ND, win, wmeta, sparse, (int)cap,
+                                              sparse_count));
+        rc = launch_correction(hist + (size_t)s0 * nch * ND, nch, info + s0, n, upsf + oE * ND, partial + oE * ND,
+                               exposure + oE, E, scale + oE, inv_integ ? inv_integ + oE : nullptr,
+                               correction ? correction + oE : nullptr, radius ? radius + s0 : nullptr,
+                               in_fov ? in_fov + s0 : nullptr, st);
+        if (rc) return rc;
+        const size_t nl = (size_t)n * ND * EQ * 4;
+        XTS_LAUNCH("k_lut_scaled", st, k_lut_scaled<<<(unsigned)((nl + 255) / 256), 256, 0, st>>>(
+                                           upsf + oE * ND, scale + oE, n, E, EQ * 4, lut, nullptr, nullptr));
+        const long long T = (long long)n * ((npix + BT - 1) / BT);
+        long long G = (long long)nsm * per_sm;
+        if (G > T) G = T;
+        XTS_LAUNCH("k_srcmap", st, k_srcmap_win<<<(unsigned)G, BT, L.total, st>>>(
+                                       win, wmeta, sparse, lut, corners, omega, info + s0, tab, n, s0, H, W, E, EQ, status, out));
+    }
+    return XTS_OK;
+}
+
+}  // namespace xts
