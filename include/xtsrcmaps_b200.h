@@ -111,7 +111,9 @@ int         xts_version(void);
  * launches is bracketed by CUDA events on its stream.  xts_profile_read waits
  * for the recorded kernels, writes a JSON object
  * {"kernel": [launches, total_ms], ...} into buf and clears the record; it
- * returns the length written or a negative error code. */
+ * returns the length written or a negative error code.  With on = 2 the record
+ * is kept across reads: launches captured into a CUDA graph carry their events
+ * as event-record nodes, and each read reports the graph's latest replay. */
 int xts_profile_enable(int on);
 int xts_profile_read(char* buf, int buflen);
 

@@ -286,8 +286,11 @@ def init(device: int = 0) -> None:
     L.check(L.lib().xts_init(int(device)))
 
 
-def profile_enable(on: bool = True) -> None:
-    L.check(L.lib().xts_profile_enable(int(bool(on))))
+def profile_enable(on: bool = True, keep: bool = False) -> None:
+    """Time every library kernel with CUDA events.  ``keep`` keeps the record
+    across reads, for launches captured into a CUDA graph (each read then
+    reports the latest replay)."""
+    L.check(L.lib().xts_profile_enable(2 if (on and keep) else int(bool(on))))
 
 
 def profile_read() -> dict:

@@ -96,6 +96,7 @@ static void release_all() {
 // Kernel timing -------------------------------------------------------------
 struct ProfRec { const char* name; cudaEvent_t a, b; };
 static bool g_prof_on = false;
+static bool g_prof_keep = false;  // records survive reads (launches captured into a CUDA graph)
 static ProfRec g_prof[4096];
 static int g_prof_n = 0;
 static cudaEvent_t g_prof_pool[8192];
@@ -111,6 +112,16 @@ static cudaEvent_t prof_event() {
     return e;
 }
 
+// Inside a stream capture the event becomes an event-record node of the graph,
+// re-recorded on every replay.
+static void prof_record(cudaEvent_t ev, cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusActive)
+        cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal);
+    else
+        cudaEventRecord(ev, st);
+}
+
 void prof_mark(const char* name, cudaStream_t st, bool begin) {
     if (!g_prof_on) return;
     if (begin) {
@@ -118,10 +129,10 @@ void prof_mark(const char* name, cudaStream_t st, bool begin) {
         cudaEvent_t a = prof_event(), b = prof_event();
         if (!a || !b) return;
         g_prof[g_prof_n] = {name, a, b};
-        cudaEventRecord(a, st);
+        prof_record(a, st);
     } else {
         if (g_prof_n >= 4096 || !g_prof[g_prof_n].name) return;
-        cudaEventRecord(g_prof[g_prof_n].b, st);
+        prof_record(g_prof[g_prof_n].b, st);
         ++g_prof_n;
         if (g_prof_n < 4096) g_prof[g_prof_n].name = nullptr;
     }
@@ -229,6 +240,7 @@ void xts_release(void) {
 int xts_profile_enable(int on) {
     std::lock_guard<std::mutex> lock(g_mu);
     g_prof_on = on != 0;
+    g_prof_keep = on == 2;
     g_prof_n = 0;
     g_prof_pool_used = 0;
     g_prof[0].name = nullptr;
@@ -261,9 +273,11 @@ int xts_profile_read(char* buf, int buflen) {
         len += snprintf(buf + len, buflen - len, "%s\"%s\": [%d, %.6f]", k ? ", " : "", names[k],
                         counts[k], ms[k]);
     if (len < buflen) len += snprintf(buf + len, buflen - len, "}");
-    g_prof_n = 0;
-    g_prof_pool_used = 0;
-    g_prof[0].name = nullptr;
+    if (!g_prof_keep) {
+        g_prof_n = 0;
+        g_prof_pool_used = 0;
+        g_prof[0].name = nullptr;
+    }
     return len < buflen ? len : set_error(XTS_ERR_ARG, "profile_read: buffer too small");
 }
 

@@ -237,25 +237,28 @@ __device__ __forceinline__ double point_q(const PixGeom& g, int p) {
 }
 
 // Scaled FP32 table Y'[s][d][e] = uPsf * (exposure * correction), energies
-// padded to Epad with zeros.  With hi/lo given, also the 3xTF32 split:
+// padded to Epad with zeros; launched as lut_scaled_grid(S) x 256 threads.  With hi/lo given, also the 3xTF32 split:
 // hi = tf32(Y'), lo = Y' - hi.
 static __global__ void k_lut_scaled(const double* upsf, const double* scale, int S, int E, int Epad,
                              float* lut, float* hi, float* lo) {
-    size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    size_t n = (size_t)S * ND * Epad;
-    if (k >= n) return;
-    int e = (int)(k % Epad);
-    size_t sd = k / Epad;
-    int s = (int)(sd / ND);
-    float v = e < E ? (float)(upsf[sd * E + e] * scale[(size_t)s * E + e]) : 0.f;
-    if (lut) lut[k] = v;
-    if (hi) {
-        unsigned hb;
-        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hb) : "f"(v));
-        float h = __uint_as_float(hb);
-        hi[k] = h;
-        lo[k] = v - h;
+    const unsigned sd = blockIdx.x * 8 + (threadIdx.x >> 5);  // (source, row), one warp per row
+    if (sd >= (unsigned)S * ND) return;
+    const unsigned s = sd / ND;
+    for (int e = threadIdx.x & 31; e < Epad; e += 32) {
+        const size_t k = (size_t)sd * Epad + e;
+        const float v = e < E ? (float)(upsf[(size_t)sd * E + e] * scale[(size_t)s * E + e]) : 0.f;
+        if (lut) lut[k] = v;
+        if (hi) {
+            unsigned hb;
+            asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hb) : "f"(v));
+            const float h = __uint_as_float(hb);
+            hi[k] = h;
+            lo[k] = v - h;
+        }
     }
 }
+
+// Launch shape of k_lut_scaled: 256 threads, one warp per (source, row).
+static inline unsigned lut_scaled_grid(int S) { return (unsigned)(((size_t)S * ND + 7) / 8); }
 
 }  // namespace xts

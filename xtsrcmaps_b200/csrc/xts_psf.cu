@@ -115,88 +115,68 @@ __global__ void __launch_bounds__(128) k_mean_psf(const double* pa, int C, int E
 }
 
 // b7: per (s, e) exact integral of the linear interpolant of 2 pi u(theta) sin(theta)
-// per separation bin, prefix sum, normalised partials; then uPsf /= total.
-__global__ void k_partial_integral(double* upsf, double* partial, int S, int E) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= S * E) return;
-    int s = i / E, e = i - s * E;
+// over each separation bin (psf.partial_total_integral.cxx:8-52), prefix sum,
+// normalised partials, then uPsf /= total (psf.normalize.cxx:7-24).  One warp per
+// (source, energy): each lane integrates a run of 13 bins, the runs are joined by
+// a shuffle scan, and every lane normalises its own rows.
+constexpr int PSCAN_ROWS = (ND - 1 + 31) / 32;  // bins per lane
+
+__global__ void __launch_bounds__(256) k_partial_scan(double* upsf, double* partial, int E) {
+    __shared__ double th[ND], st[ND];  // theta (rad) and 2 pi sin(theta) of the separations
+    for (int d = threadIdx.x; d < ND; d += blockDim.x) {
+        th[d] = D2R * sep_deg(d);
+        st[d] = TWOPI * sin(th[d]);
+    }
+    __syncthreads();
+    const int s = blockIdx.x, lane = threadIdx.x & 31;
+    const int e = blockIdx.y * 8 + (threadIdx.x >> 5);
+    if (e >= E) return;  // whole warp
     double* u = upsf + (size_t)s * ND * E + e;
     double* p = partial + (size_t)s * ND * E + e;
-    double cum = 0.0;
-    p[0] = 0.0;
-    double t1 = 0.0, y1 = TWOPI * u[0] * sin(t1);
-    for (int d = 1; d < ND; ++d) {
-        double t2 = D2R * sep_deg(d);
-        double y2 = TWOPI * u[(size_t)d * E] * sin(t2);
-        double m = (y2 - y1) / (t2 - t1);
-        double b = y1 - t1 * m;
-        double v = 0.5 * m * (t2 * t2 - t1 * t1) + b * (t2 - t1);
-        cum += v;
-        p[(size_t)d * E] = cum;
-        t1 = t2; y1 = y2;
-    }
-    if (cum != 0.)
-        for (int d = 0; d < ND; ++d) p[(size_t)d * E] /= cum;
-    for (int d = 0; d < ND; ++d) u[(size_t)d * E] /= cum;
-}
-
-// Same computation with the source's table staged in shared memory: one block
-// per source, the [401, E] table loaded with coalesced reads, then one thread
-// per energy runs the prefix sum out of shared memory (its global stores are
-// coalesced across the energies), then the block normalises both tables.
-__global__ void k_partial_integral_smem(double* upsf, double* partial, int E) {
-    extern __shared__ double sm[];
-    double* U = sm;                     // [ND][E] raw mean PSF
-    double* TOT = U + (size_t)ND * E;   // [E]
-    double* T = TOT + E;                // [ND] theta (rad)
-    double* ST = T + ND;                // [ND] 2 pi sin(theta)
-    double* IDT = ST + ND;              // [ND] 1 / (theta[d] - theta[d-1])
-    double* HA = IDT + ND;              // [ND] (theta[d]^2 - theta[d-1]^2) / 2
-    double* DT = HA + ND;               // [ND] theta[d] - theta[d-1]
-    int s = blockIdx.x;
-    double* us = upsf + (size_t)s * ND * E;
-    double* ps = partial + (size_t)s * ND * E;
-    for (int k = threadIdx.x; k < ND * E; k += blockDim.x) U[k] = us[k];
-    for (int d = threadIdx.x; d < ND; d += blockDim.x) {
-        double t = D2R * sep_deg(d);
-        T[d] = t;
-        ST[d] = TWOPI * sin(t);
-    }
-    __syncthreads();
-    for (int d = 1 + threadIdx.x; d < ND; d += blockDim.x) {
-        double t1 = T[d - 1], t2 = T[d];
-        DT[d] = t2 - t1;
-        IDT[d] = 1.0 / (t2 - t1);
-        HA[d] = 0.5 * (t2 * t2 - t1 * t1);
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < E; e += blockDim.x) {
-        double cum = 0.0;
-        ps[e] = 0.0;
-        double y1 = U[e] * ST[0];
-#pragma unroll 4
-        for (int d = 1; d < ND; ++d) {
-            double y2 = U[d * E + e] * ST[d];
-            double m = (y2 - y1) * IDT[d];
-            double b = y1 - T[d - 1] * m;
-            double v = m * HA[d] + b * DT[d];
-            cum += v;
-            ps[(size_t)d * E + e] = cum;
-            y1 = y2;
+    const int d0 = 1 + lane * PSCAN_ROWS;
+    const int d1 = min(ND, d0 + PSCAN_ROWS);
+    double cum[PSCAN_ROWS];
+    double run = 0.0;
+    if (d0 < ND) {
+        double t1 = th[d0 - 1];
+        double y1 = u[(size_t)(d0 - 1) * E] * st[d0 - 1];
+#pragma unroll
+        for (int k = 0; k < PSCAN_ROWS; ++k) {
+            const int d = d0 + k;
+            if (d < d1) {
+                const double t2 = th[d];
+                const double y2 = u[(size_t)d * E] * st[d];
+                const double m = (y2 - y1) / (t2 - t1);
+                const double b = y1 - t1 * m;
+                run += 0.5 * m * (t2 * t2 - t1 * t1) + b * (t2 - t1);
+                t1 = t2;
+                y1 = y2;
+            }
+            cum[k] = run;
         }
-        TOT[e] = cum;
     }
-    __syncthreads();
-    for (int k = threadIdx.x; k < ND * E; k += blockDim.x) {
-        double tot = TOT[k % E];
-        if (tot != 0.) ps[k] /= tot;
-        us[k] = U[k] / tot;
+    double incl = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const double base = incl - run;
+    const double tot = __shfl_sync(0xffffffffu, incl, 31);
+    if (lane == 0) {
+        p[0] = 0.0;
+        u[0] = u[0] / tot;
+    }
+#pragma unroll
+    for (int k = 0; k < PSCAN_ROWS; ++k) {
+        const int d = d0 + k;
+        if (d < d1) {
+            const double c = base + cum[k];
+            p[(size_t)d * E] = tot != 0. ? c / tot : c;
+            u[(size_t)d * E] = u[(size_t)d * E] / tot;
+        }
     }
 }
-
-constexpr int PARTIAL_SMEM_MAX = 227 * 1024;
-
-static size_t partial_smem_bytes(int E) { return sizeof(double) * ((size_t)ND * E + E + 5 * ND); }
 
 int launch_psf(const PsfDev& a, cudaStream_t st) {
     if (a.C > PSF_MAX_C) return set_error(XTS_ERR_ARG, "compute_psf_data: C=%d exceeds %d", a.C, PSF_MAX_C);
@@ -213,14 +193,7 @@ int launch_psf(const PsfDev& a, cudaStream_t st) {
     int DE = ND * a.E;
     dim3 g((DE + 127) / 128, (a.S + PSF_TILE_S - 1) / PSF_TILE_S);
     XTS_LAUNCH("k_mean_psf", st, k_mean_psf<<<g, 128, 0, st>>>(pa, a.C, a.E, a.ecb, a.wecb, a.S, a.ltf, a.exposure, a.upsf));
-    size_t smem = partial_smem_bytes(a.E);
-    if (smem <= PARTIAL_SMEM_MAX) {
-        XTS_CUDA(cudaFuncSetAttribute(k_partial_integral_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        XTS_LAUNCH("k_partial_integral", st, k_partial_integral_smem<<<a.S, 256, smem, st>>>(a.upsf, a.partial, a.E));
-    } else {
-        n = a.S * a.E;
-        XTS_LAUNCH("k_partial_integral", st, k_partial_integral<<<(n + 127) / 128, 128, 0, st>>>(a.upsf, a.partial, a.S, a.E));
-    }
+    XTS_LAUNCH("k_partial_integral", st, k_partial_scan<<<dim3(a.S, (a.E + 7) / 8), 256, 0, st>>>(a.upsf, a.partial, a.E));
     return XTS_OK;
 }
 
@@ -239,14 +212,7 @@ int launch_psf_scratch(const PsfDev& a, double* king, double* pa, cudaStream_t s
     int DE = ND * a.E;
     dim3 g((DE + 127) / 128, (a.S + PSF_TILE_S - 1) / PSF_TILE_S);
     XTS_LAUNCH("k_mean_psf", st, k_mean_psf<<<g, 128, 0, st>>>(pa, a.C, a.E, a.ecb, a.wecb, a.S, a.ltf, a.exposure, a.upsf));
-    size_t smem = partial_smem_bytes(a.E);
-    if (smem <= PARTIAL_SMEM_MAX) {
-        XTS_CUDA(cudaFuncSetAttribute(k_partial_integral_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        XTS_LAUNCH("k_partial_integral", st, k_partial_integral_smem<<<a.S, 256, smem, st>>>(a.upsf, a.partial, a.E));
-    } else {
-        n = a.S * a.E;
-        XTS_LAUNCH("k_partial_integral", st, k_partial_integral<<<(n + 127) / 128, 128, 0, st>>>(a.upsf, a.partial, a.S, a.E));
-    }
+    XTS_LAUNCH("k_partial_integral", st, k_partial_scan<<<dim3(a.S, (a.E + 7) / 8), 256, 0, st>>>(a.upsf, a.partial, a.E));
     return XTS_OK;
 }
 

@@ -405,7 +405,8 @@ __global__ void __launch_bounds__(256) k_map_integral_hist(const double* corners
 }
 
 // c7 (1/sum) + c9 (containment factor) + c8/c10 folded into one per-(s,e) scale.
-// One block per source: fold the chunk histograms, then one thread per energy.
+// Block (s, group of 8 energies): fold the source's chunk histograms, then one
+// warp per energy.
 __global__ void __launch_bounds__(256) k_correction_hist(const double* hist_in, int nch, const SrcInfo* info,
                                                          const double* upsf, const double* partial,
                                                          const double* expo, int E, double* scale,
@@ -421,11 +422,19 @@ __global__ void __launch_bounds__(256) k_correction_hist(const double* hist_in, 
     }
     __syncthreads();
     const double* U = upsf + (size_t)s * ND * E;
-    for (int e = threadIdx.x; e < E; e += blockDim.x) {
+    // one warp per energy (8 energies per block): lanes split the rows, then a
+    // fixed shuffle order
+    const int lane = threadIdx.x & 31;
+    {
+        const int e = blockIdx.y * 8 + (threadIdx.x >> 5);
+        if (e >= E) return;
         int i = s * E + e;
         double sum = 0.;
-        if (si.in_fov)
-            for (int r = 0; r < ND; ++r) sum = fma(hsum[r], U[(size_t)r * E + e], sum);
+        if (si.in_fov) {
+            for (int r = lane; r < ND; r += 32) sum = fma(hsum[r], U[(size_t)r * E + e], sum);
+            for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        }
+        if (lane != 0) return;
         double inv = sum != 0. ? 1.0 / sum : sum;
         double factor;
         if (!si.in_fov) factor = 1.0;
@@ -459,7 +468,7 @@ int launch_correction(const double* hist, int nch, const SrcInfo* info, int S, c
                       const double* partial, const double* exposure, int E, double* scale,
                       double* inv_integ, double* correction, double* radius, int* in_fov,
                       cudaStream_t st) {
-    XTS_LAUNCH("k_correction", st, k_correction_hist<<<S, 256, 0, st>>>(hist, nch, info, upsf, partial, exposure, E,
+    XTS_LAUNCH("k_correction", st, k_correction_hist<<<dim3(S, (E + 7) / 8), 256, 0, st>>>(hist, nch, info, upsf, partial, exposure, E,
                                                                         scale, inv_integ, correction, radius, in_fov));
     return XTS_OK;
 }

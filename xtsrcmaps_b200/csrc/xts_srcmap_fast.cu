@@ -309,7 +309,7 @@ int launch_srcmap_fast(const double* corners, const double* omega, const SrcInfo
     float* lut = (float*)workspace(W_LUT, sizeof(float) * (size_t)S * ND * Epad + 16);
     if (!lut) return XTS_ERR_OOM;
     size_t n = (size_t)S * ND * Epad;
-    XTS_LAUNCH("k_lut_scaled", st, k_lut_scaled<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(upsf, scale, S, E, Epad, lut, nullptr, nullptr));
+    XTS_LAUNCH("k_lut_scaled", st, k_lut_scaled<<<lut_scaled_grid(S), 256, 0, st>>>(upsf, scale, S, E, Epad, lut, nullptr, nullptr));
     size_t smem = srcmap_fast_smem(E);
     if (smem > 227 * 1024) return set_error(XTS_ERR_ARG, "E=%d too large for the fast source-map kernel", E);
     XTS_CUDA(cudaFuncSetAttribute(k_srcmap_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

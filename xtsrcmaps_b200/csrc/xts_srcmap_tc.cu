@@ -420,7 +420,7 @@ int launch_srcmap_tc(const double* corners, const double* omega, const SrcInfo* 
     if (!lut) return XTS_ERR_OOM;
     float* hi = lut + ((n + 3) & ~(size_t)3);
     float* lo = hi + nt;
-    XTS_LAUNCH("k_lut_scaled", st, k_lut_scaled<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(upsf, scale, S, E, Epad, lut, nullptr, nullptr));
+    XTS_LAUNCH("k_lut_scaled", st, k_lut_scaled<<<lut_scaled_grid(S), 256, 0, st>>>(upsf, scale, S, E, Epad, lut, nullptr, nullptr));
     XTS_LAUNCH("k_lut_split_t", st, k_lut_split_t<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(lut, S, E, Epad, hi, lo));
     CUtensorMap mhi, mlo;
     if ((rc = make_table_map(&mhi, hi, S, E, N))) return rc;

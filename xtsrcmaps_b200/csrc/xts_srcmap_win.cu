@@ -4,7 +4,7 @@
 // points of the pixel give LUT rows and interpolation weights (xts_point.cuh);
 // their weights times the pixel's solid angle are summed into a dense window of
 // at most RW consecutive table rows.  For pixels inside the boundary radius of
-// an in-FOV source the FP64 window also enters the block's row histogram, whose
+// an in-FOV source the window also enters the block's FP64 row histogram, whose
 // dot product with uPsf is the map integral of c7 (model_map.map_integral.cxx:4-48):
 //     sum_pix omega * value(pix, e) = sum_r Hist[r] * uPsf[r][e].
 // Every pixel's window is written once as a 36-byte record (8 FP32 weights and
@@ -33,7 +33,7 @@ constexpr size_t WA_OFF_SQ = 0;
 constexpr size_t WA_OFF_COEF = (8 * (ND + 1) + 15) / 16 * 16;
 constexpr size_t WA_OFF_HIST = WA_OFF_COEF + sizeof(float4) * 2 * ND;
 constexpr size_t WA_OFF_WTS = WA_OFF_HIST + (8 * ND + 15) / 16 * 16;
-constexpr size_t WA_OFF_BASE = WA_OFF_WTS + sizeof(double) * WT * RW;
+constexpr size_t WA_OFF_BASE = WA_OFF_WTS + sizeof(float) * WT * RW;
 constexpr size_t WA_SMEM = WA_OFF_BASE + sizeof(int) * (WT + 4);
 
 constexpr int NSP = 24;  // entries of a sparse record: 12 points x 2 rows
@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(WT, 3) k_pixel_windows(const double* __restric
     double* sq = (double*)(smem + WA_OFF_SQ);
     float4* scoef = (float4*)(smem + WA_OFF_COEF);
     double* hist = (double*)(smem + WA_OFF_HIST);
-    double* wts = (double*)(smem + WA_OFF_WTS);  // [RW][WT] FP64 windows (row-major by window slot)
+    float* wts = (float*)(smem + WA_OFF_WTS);    // [RW][WT] windows (row-major by window slot)
     int* wbase = (int*)(smem + WA_OFF_BASE);     // [WT] first row (-1: not in radius); [WT..WT+3] row min/max by parity
     const int s = blockIdx.y, t = threadIdx.x;
     const SrcInfo si = info[s];
@@ -83,13 +83,13 @@ __global__ void __launch_bounds__(WT, 3) k_pixel_windows(const double* __restric
                 else inside = dir_diff(si.dir, c) <= si.radius_rad;
             }
             const PixGeom g = pixel_geom(corners, W1, h, w, si);
-            const double om = omega[pix];
+            const float om = (float)omega[pix];
             float tc;
             const int ic = point_row(fma(g.Ax, g.Ax, fma(g.Ay, g.Ay, g.Az * g.Az)), sq, scoef, &tc);
             const int base = min(max(ic - 1 - RW / 2, 0), ND - RW);
-            double* wd = wts + t;  // slot j at wd[j * WT]: lanes hit consecutive words
+            float* wd = wts + t;  // slot j at wd[j * WT]: lanes hit consecutive words
 #pragma unroll
-            for (int j = 0; j < RW; ++j) wd[j * WT] = 0.;
+            for (int j = 0; j < RW; ++j) wd[j * WT] = 0.f;
             bool wide = false;
             int lo = RW, hi = -1;
 #pragma unroll
@@ -97,8 +97,8 @@ __global__ void __launch_bounds__(WT, 3) k_pixel_windows(const double* __restric
                 float tt;
                 const int idx = point_row(point_q(g, p), sq, scoef, &tt);
                 const int r = idx - 1 - base;
-                const double wgt = c_rule_uv[p][3];
-                const double wa = (double)(1.f - tt) * wgt * om, wb = (double)tt * wgt * om;
+                const float wo = (float)c_rule_uv[p][3] * om;
+                const float wa = (1.f - tt) * wo, wb = tt * wo;
                 if (r >= 0 && r < RW - 1) {
                     wd[r * WT] += wa;
                     wd[(r + 1) * WT] += wb;
@@ -107,8 +107,8 @@ __global__ void __launch_bounds__(WT, 3) k_pixel_windows(const double* __restric
                 } else {
                     wide = true;
                     if (inside) {
-                        atomicAdd(&hist[idx - 1], wa);
-                        atomicAdd(&hist[idx], wb);
+                        atomicAdd(&hist[idx - 1], (double)wa);
+                        atomicAdd(&hist[idx], (double)wb);
                     }
                 }
             }
@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(WT, 3) k_pixel_windows(const double* __restric
             if (!wide) {
 #pragma unroll
                 for (int j = 0; j < RW; ++j)
-                    if (j <= hi - lo) f[j] = (float)wd[min(j + lo, RW - 1) * WT];
+                    if (j <= hi - lo) f[j] = wd[min(j + lo, RW - 1) * WT];
                 meta = (base + lo) | ((hi - lo + 1) << 16);
             } else {
                 const int slot = atomicAdd(sparse_count, 1);
@@ -129,9 +129,9 @@ __global__ void __launch_bounds__(WT, 3) k_pixel_windows(const double* __restric
                     for (int p = 0; p < 12; ++p) {
                         float tt;
                         const int idx = point_row(point_q(g, p), sq, scoef, &tt);
-                        const double wgt = c_rule_uv[p][3];
-                        rec[2 * p] = make_float2((float)((double)(1.f - tt) * wgt * om), __int_as_float(idx - 1));
-                        rec[2 * p + 1] = make_float2((float)((double)tt * wgt * om), __int_as_float(idx));
+                        const float wo = (float)c_rule_uv[p][3] * om;
+                        rec[2 * p] = make_float2((1.f - tt) * wo, __int_as_float(idx - 1));
+                        rec[2 * p + 1] = make_float2(tt * wo, __int_as_float(idx));
                     }
                     meta = -1 - slot;
                 } else {
@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(WT, 3) k_pixel_windows(const double* __restric
                         const int p = ((i + a) & 31) * 8 + sub;
                         const int b0 = wbase[p];
                         const int k = r - b0;
-                        if (b0 >= 0 && k >= 0 && k < RW) acc += wts[k * WT + p];
+                        if (b0 >= 0 && k >= 0 && k < RW) acc += (double)wts[k * WT + p];
                     }
                 }
                 acc += __shfl_xor_sync(0xffffffffu, acc, 1);
@@ -191,8 +191,8 @@ struct WinLayout { size_t tab, stage, bar, total; };
 static __host__ __device__ WinLayout win_layout(int E, int EQ) {
     WinLayout L;
     L.tab = 0;                                            // [ND + RW][EQ] float4 (RW zero guard rows)
-    L.stage = (size_t)(ND + RW) * EQ * 16;                // [BT * E + 8] floats
-    L.bar = (L.stage + sizeof(float) * ((size_t)BT * E + 8) + 15) / 16 * 16;
+    L.stage = (size_t)(ND + RW) * EQ * 16;                // per warp [32 * E + 8] floats
+    L.bar = (L.stage + sizeof(float) * (size_t)(BT / 32) * (32 * E + 8) + 15) / 16 * 16;
     L.total = L.bar + 16;
     return L;
 }
@@ -213,6 +213,10 @@ __device__ __forceinline__ PixRec load_rec(const float4* win, const int* wmeta, 
     return r;
 }
 
+// Warps run independently: each owns 32 pixels of the tile, a slice of the
+// stage and its own TMA bulk store, so no block barrier is needed except when the
+// block moves on to the next source's table.
+template <int NQ>
 __global__ void __launch_bounds__(BT, 2)
 k_srcmap_win(const float4* __restrict__ win, const int* __restrict__ wmeta, const float2* __restrict__ sparse,
              const float* __restrict__ lut, const double* __restrict__ corners, const double* __restrict__ omega,
@@ -221,10 +225,9 @@ k_srcmap_win(const float4* __restrict__ win, const int* __restrict__ wmeta, cons
     extern __shared__ __align__(16) unsigned char smem[];
     const WinLayout L = win_layout(E, EQ);
     float4* tab = (float4*)(smem + L.tab);
-    float* stage = (float*)(smem + L.stage);
     const unsigned bar = smem_u32(smem + L.bar);
-    const int t = threadIdx.x;
-    const int nq = (E + 3) >> 2;
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    float* stage = (float*)(smem + L.stage) + warp * (32 * E + 8);
     const int npix = H * W, W1 = W + 1;
     const int ntiles = (npix + BT - 1) / BT;
     const long long T = (long long)S * ntiles;
@@ -244,23 +247,30 @@ k_srcmap_win(const float4* __restrict__ win, const int* __restrict__ wmeta, cons
     }
     for (long long f = f0; f < f1; ++f) {
         const int s = (int)(f / ntiles);
-        const int tile = (int)(f - (long long)s * ntiles);
-        const int p0 = tile * BT;
-        const int np = min(BT, npix - p0);
-        const long long g0 = ((long long)(s_base + s) * npix + p0) * E;  // first flat output of the whole map
-        const int m = (int)(g0 & 3);                                      // staging residue
-        const int nflat = np * E;
-        const int pix = p0 + t;
+        const int px0 = (int)(f - (long long)s * ntiles) * BT + warp * 32;  // this warp's first pixel
+        const int npw = min(32, npix - px0);                                // may be <= 0 in the last tile
+        const long long g0 = ((long long)(s_base + s) * npix + px0) * E;    // first flat output of the whole map
+        const int m = (int)(g0 & 3);                                        // staging residue
+        const int nflat = npw > 0 ? npw * E : 0;
+        const int pix = px0 + lane;
 
-        // the next tile's records, in flight while this tile is computed
+        // the next tile's records, in flight while this tile is computed, and the
+        // one after that on its way into L2
         PixRec nxt;
         {
             const long long fn = f + 1;
             const int sn = (int)(fn / ntiles), pn = (int)(fn - (long long)sn * ntiles) * BT;
             nxt = load_rec(win, wmeta, (size_t)sn * npix + pn + t, fn < f1 && pn + t < npix);
+            const long long f2 = f + 2;
+            const int s2 = (int)(f2 / ntiles), p2 = (int)(f2 - (long long)s2 * ntiles) * BT;
+            if (f2 < f1 && p2 + t < npix) {
+                const size_t k2 = (size_t)s2 * npix + p2 + t;
+                asm volatile("prefetch.global.L2 [%0];" :: "l"(win + 2 * k2));
+                if ((t & 31) == 0) asm volatile("prefetch.global.L2 [%0];" :: "l"(wmeta + k2));
+            }
         }
         if (s != cur) {
-            __syncthreads();  // every thread is done with the previous source's table
+            __syncthreads();  // every warp is done with the previous source's table
             if (t == 0) {
                 fence_async_shared();
                 bulk_load(tab, lut + (size_t)s * ND * EQ * 4, tab_bytes, bar);
@@ -272,17 +282,14 @@ k_srcmap_win(const float4* __restrict__ win, const int* __restrict__ wmeta, cons
                 if (t == 0) {
                     atomicExch(status, 1);
                     mbar_wait(bar, phase ^ 1);  // bounded: let the copy land before the block exits
-                    bulk_wait_all();
                 }
+                if (lane == 0) bulk_wait_all();
                 return;
             }
         }
-        if (t == 0) bulk_wait_read();  // the previous tile's bulk store has read the stage
-        __syncthreads();
-
         // entries of this pixel: window rows rbase + j (j < nr), or a sparse record
         const int meta = rec.meta;
-        const bool valid = t < np;
+        const bool valid = lane < npw;
         const bool sp = valid && meta < 0 && meta != META_OVERFLOW;
         const bool slow = valid && meta == META_OVERFLOW;
         const int nent = sp ? NSP : (meta >= 0 ? (meta >> 16) : 0);
@@ -290,23 +297,17 @@ k_srcmap_win(const float4* __restrict__ win, const int* __restrict__ wmeta, cons
         const float2* se = sparse + (size_t)(sp ? -1 - meta : 0) * NSP;
         const int kmax = __reduce_max_sync(0xffffffffu, nent);
         const float w[RW] = {rec.wa.x, rec.wa.y, rec.wa.z, rec.wa.w, rec.wb.x, rec.wb.y, rec.wb.z, rec.wb.w};
-        float4 acc[BQ];
+        float4 acc[NQ];
 #pragma unroll
-        for (int q = 0; q < BQ; ++q) acc[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int q = 0; q < NQ; ++q) acc[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (kmax <= RW) {  // window records only (warp-uniform)
 #pragma unroll
-        for (int j = 0; j < NSP; ++j) {
-            if (j < kmax) {  // warp-uniform; entries past a pixel's own count carry weight 0
-                float wj = j < RW ? w[j < RW ? j : 0] : 0.f;
-                int row = rb + (j < RW ? j : 0);
-                if (sp) {
-                    const float2 e = __ldg(se + j);
-                    wj = e.x;
-                    row = __float_as_int(e.y);
-                }
-                const float4* yr = tab + row * EQ;
+            for (int j = 0; j < RW; ++j) {
+                if (j < kmax) {  // rows past a pixel's own window carry weight 0
+                    const float4* yr = tab + (rb + j) * EQ;
+                    const float wj = w[j];
 #pragma unroll
-                for (int q = 0; q < BQ; ++q) {
-                    if (q < nq) {
+                    for (int q = 0; q < NQ; ++q) {
                         const float4 y = yr[q];
                         acc[q].x = fmaf(wj, y.x, acc[q].x);
                         acc[q].y = fmaf(wj, y.y, acc[q].y);
@@ -315,18 +316,43 @@ k_srcmap_win(const float4* __restrict__ win, const int* __restrict__ wmeta, cons
                     }
                 }
             }
+        } else {  // some lanes hold sparse records (pixels next to the source)
+#pragma unroll 1
+            for (int j = 0; j < NSP; ++j) {
+                float wj = 0.f;
+                int row = rb;
+#pragma unroll
+                for (int i = 0; i < RW; ++i)
+                    if (i == j) wj = w[i];
+                if (j < RW) row = rb + j;
+                if (sp) {
+                    const float2 e = __ldg(se + j);
+                    wj = e.x;
+                    row = __float_as_int(e.y);
+                }
+                const float4* yr = tab + row * EQ;
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) {
+                    const float4 y = yr[q];
+                    acc[q].x = fmaf(wj, y.x, acc[q].x);
+                    acc[q].y = fmaf(wj, y.y, acc[q].y);
+                    acc[q].z = fmaf(wj, y.z, acc[q].z);
+                    acc[q].w = fmaf(wj, y.w, acc[q].w);
+                }
+            }
         }
-        float* dst = stage + m + t * E;
+        // the stage is reused only now: the previous bulk store's read-out overlapped the sums
+        if (lane == 0) bulk_wait_read();
+        __syncwarp();
+        float* dst = stage + m + lane * E;
         if (valid && !slow) {
 #pragma unroll
-            for (int q = 0; q < BQ; ++q) {
-                if (q < nq) {
-                    const int e = 4 * q;
-                    dst[e] = acc[q].x;
-                    if (e + 1 < E) dst[e + 1] = acc[q].y;
-                    if (e + 2 < E) dst[e + 2] = acc[q].z;
-                    if (e + 3 < E) dst[e + 3] = acc[q].w;
-                }
+            for (int q = 0; q < NQ; ++q) {
+                const int e = 4 * q;
+                dst[e] = acc[q].x;
+                if (q < NQ - 1 || e + 1 < E) dst[e + 1] = acc[q].y;
+                if (q < NQ - 1 || e + 2 < E) dst[e + 2] = acc[q].z;
+                if (q < NQ - 1 || e + 3 < E) dst[e + 3] = acc[q].w;
             }
         }
         if (slow) {  // sparse pool full: point by point from the shared table, compensated sum
@@ -352,21 +378,46 @@ k_srcmap_win(const float4* __restrict__ win, const int* __restrict__ wmeta, cons
             }
         }
         fence_async_shared();
-        __syncthreads();
-        // TMA bulk store of the 16-byte aligned body, threads for the edges
-        const long long ga = (g0 + 3) & ~3LL, gb = (g0 + nflat) & ~3LL;
-        if (t == 0 && gb > ga)
-            bulk_store(out + ga, stage + m + (int)(ga - g0), (unsigned)((gb - ga) * 4));
-        if (t < 8) {
-            const long long g = t < 4 ? g0 + t : gb + (t - 4);
-            const bool head = t < 4 && g < ga && g < g0 + nflat;
-            const bool tail = t >= 4 && g >= gb && g >= ga && g < g0 + nflat;
-            if (head || tail) out[g] = stage[m + (int)(g - g0)];
+        __syncwarp();
+        // TMA bulk store of the warp's 16-byte aligned body, lanes for the edges
+        if (nflat > 0) {
+            const long long ga = (g0 + 3) & ~3LL, gb = (g0 + nflat) & ~3LL;
+            if (lane == 0 && gb > ga)
+                bulk_store(out + ga, stage + m + (int)(ga - g0), (unsigned)((gb - ga) * 4));
+            if (lane < 8) {
+                const long long g = lane < 4 ? g0 + lane : gb + (lane - 4);
+                const bool head = lane < 4 && g < ga && g < g0 + nflat;
+                const bool tail = lane >= 4 && g >= gb && g >= ga && g < g0 + nflat;
+                if (head || tail) out[g] = stage[m + (int)(g - g0)];
+            }
         }
         rec = nxt;
     }
-    if (t == 0) bulk_wait_all();
+    if (lane == 0) bulk_wait_all();
 }
+
+template <int NQ>
+static int launch_write_pass(unsigned G, size_t smem, cudaStream_t st, const float4* win, const int* wmeta,
+                             const float2* sparse, const float* lut, const double* corners, const double* omega,
+                             const SrcInfo* info, const SepTab* tab, int S, int s_base, int H, int W, int E, int EQ,
+                             int* status, float* out, int* per_sm, int nsm, bool query) {
+    if (query) {
+        XTS_CUDA(cudaFuncSetAttribute(k_srcmap_win<NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        XTS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_srcmap_win<NQ>, BT, smem));
+        return XTS_OK;
+    }
+    XTS_LAUNCH("k_srcmap", st, k_srcmap_win<NQ><<<G, BT, smem, st>>>(win, wmeta, sparse, lut, corners, omega, info, tab,
+                                                                    S, s_base, H, W, E, EQ, status, out));
+    return XTS_OK;
+}
+
+typedef int (*WritePassFn)(unsigned, size_t, cudaStream_t, const float4*, const int*, const float2*, const float*,
+                           const double*, const double*, const SrcInfo*, const SepTab*, int, int, int, int, int, int,
+                           int*, float*, int*, int, bool);
+static const WritePassFn k_write_pass[BQ] = {
+    launch_write_pass<1>, launch_write_pass<2>, launch_write_pass<3>, launch_write_pass<4>, launch_write_pass<5>,
+    launch_write_pass<6>, launch_write_pass<7>, launch_write_pass<8>, launch_write_pass<9>, launch_write_pass<10>,
+    launch_write_pass<11>, launch_write_pass<12>, launch_write_pass<13>};
 
 // ============================================================================ host
 bool srcmap_win_supported(int E) {
@@ -404,11 +455,13 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
     if (!win || !wmeta || !lut || !sparse) return XTS_ERR_OOM;
     int* sparse_count = status + 1;
     XTS_CUDA(cudaFuncSetAttribute(k_pixel_windows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WA_SMEM));
-    XTS_CUDA(cudaFuncSetAttribute(k_srcmap_win, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
     int dev = 0, nsm = 148, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    XTS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_srcmap_win, BT, L.total));
+    const WritePassFn wp = k_write_pass[(E + 3) / 4 - 1];
+    rc = wp(0, L.total, st, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, 0, 0, E, EQ,
+            nullptr, nullptr, &per_sm, nsm, true);
+    if (rc) return rc;
     if (per_sm < 1) return set_error(XTS_ERR_ARG, "source-map write pass does not fit on an SM (E=%d)", E);
     for (int s0 = 0; s0 < S; s0 += Sc) {
         const int n = S - s0 < Sc ? S - s0 : Sc;
@@ -423,14 +476,14 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
                                correction ? correction + oE : nullptr, radius ? radius + s0 : nullptr,
                                in_fov ? in_fov + s0 : nullptr, st);
         if (rc) return rc;
-        const size_t nl = (size_t)n * ND * EQ * 4;
-        XTS_LAUNCH("k_lut_scaled", st, k_lut_scaled<<<(unsigned)((nl + 255) / 256), 256, 0, st>>>(
+        XTS_LAUNCH("k_lut_scaled", st, k_lut_scaled<<<lut_scaled_grid(n), 256, 0, st>>>(
                                            upsf + oE * ND, scale + oE, n, E, EQ * 4, lut, nullptr, nullptr));
         const long long T = (long long)n * ((npix + BT - 1) / BT);
         long long G = (long long)nsm * per_sm;
         if (G > T) G = T;
-        XTS_LAUNCH("k_srcmap", st, k_srcmap_win<<<(unsigned)G, BT, L.total, st>>>(
-                                       win, wmeta, sparse, lut, corners, omega, info + s0, tab, n, s0, H, W, E, EQ, status, out));
+        rc = wp((unsigned)G, L.total, st, win, wmeta, sparse, lut, corners, omega, info + s0, tab, n, s0, H, W, E, EQ,
+                status, out, nullptr, nsm, false);
+        if (rc) return rc;
     }
     return XTS_OK;
 }
