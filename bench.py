@@ -299,44 +299,60 @@ def run_ours(args, rank, world, local_rank):
     kernels = {k: {"launches": v[0], "ms": round(v[1], 4)} for k, v in prof.items()}
     gpu_launches = sum(v[0] for v in prof.values())
 
-    # end to end through the public API with host (pinned) buffers
+    # end to end through the public API with host (pinned) buffers: the fused
+    # call that replaces main.cxx:28-30, and the three separate calls
     e2e = None
     if not args.no_e2e:
         hp = pinned_job(job, torch)
         hout = torch.empty((S, H, W, E), dtype=torch.float32).pin_memory().numpy()
 
-        def step_host():
+        def step_fused():
+            A.point_source_maps(job.wcs, hp["src"], hp["cube"], hp["wcube"], hp["logEs"], job.aeff_front,
+                                job.aeff_back, nf_h, nb_h, ltf_h, out=hout, with_info=False, kernel=args.kernel)
+
+        def step_three():
             ex = A.compute_exposure(hp["cube"], hp["wcube"], hp["logEs"], hp["src"], job.aeff_front,
                                     job.aeff_back, ltf_h)
             ps = A.compute_psf_data(nf_h, nb_h, ex, hp["logEs"], ltf_h)
-            A.point_src_model_map_wcs(job.wcs, hp["src"], ex.exposure, ps.uPsf, ps.partial_psf_integral, kernel=args.kernel,
-                                      out=hout, with_info=False)
-            return ex, ps
+            A.point_src_model_map_wcs(job.wcs, hp["src"], ex.exposure, ps.uPsf, ps.partial_psf_integral,
+                                      kernel=args.kernel, out=hout, with_info=False)
 
-        for _ in range(2):
-            step_host()
         ke = max(3, min(args.steps, 20))
-        if dist:
-            dist.barrier()
-        t0 = time.perf_counter()
-        for _ in range(ke):
-            ex, ps = step_host()
-        te = time.perf_counter() - t0
-        te_t = torch.tensor([te], dtype=torch.float64, device=dev)
-        if dist:
-            dist.all_reduce(te_t, op=dist.ReduceOp.MAX)
-        te = float(te_t.item())
-        C = 40
+
+        def wall(fn):
+            for _ in range(3):
+                fn()
+            if dist:
+                dist.barrier()
+            t0_ = time.perf_counter()
+            for _ in range(ke):
+                fn()
+            te_ = time.perf_counter() - t0_
+            te_t = torch.tensor([te_], dtype=torch.float64, device=dev)
+            if dist:
+                dist.all_reduce(te_t, op=dist.ReduceOp.MAX)
+            return float(te_t.item())
+
+        te = wall(step_fused)
+        te3 = wall(step_three)
+        C = int(job.exp_cube.nbrbins)
         grid_b = lambda g: 8 * (g.cosths.size + g.logEs.size + g.params.size)
         h2d = (2 * job.exp_cube.cosbins.nbytes + 8 * E + 8 * 2 * S + grid_b(job.aeff_front) + grid_b(job.aeff_back)
-               + 8 * 2 * E  # exposure
-               + grid_b(nf_h) + grid_b(nb_h) + 8 * (C + E + 2 * C * E + 2 * S * C + 2 * E + S * E)  # psf
-               + 8 * (2 * S + S * E + 2 * S * 401 * E))  # srcmap
-        d2h = (8 * (C + 2 * C * E + 2 * S * C + S * E) + 8 * 2 * S * 401 * E + 4 * n_values)
+               + grid_b(nf_h) + grid_b(nb_h) + 8 * 2 * E)
+        d2h = 4 * n_values
+        h2d3 = (2 * job.exp_cube.cosbins.nbytes + 8 * E + 8 * 2 * S + grid_b(job.aeff_front) + grid_b(job.aeff_back)
+                + 8 * 2 * E  # exposure
+                + grid_b(nf_h) + grid_b(nb_h) + 8 * (C + E + 2 * C * E + 2 * S * C + 2 * E + S * E)  # psf
+                + 8 * (2 * S + S * E + 2 * S * 401 * E))  # srcmap
+        d2h3 = (8 * (C + 2 * C * E + 2 * S * C + S * E) + 8 * 2 * S * 401 * E + 4 * n_values)
         e2e = {"value": n_values * world * ke / te, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "steps": ke,
-               "note": "three public calls per step (compute_exposure, compute_psf_data, "
-                       "point_src_model_map_wcs) with pinned host buffers, copies inside the timed region"}
+               "note": "one public call per step (point_source_maps: the three calls of main.cxx:28-30 fused) "
+                       "from pinned host buffers to a pinned host map, copies inside the timed region",
+               "three_calls": {"value": n_values * world * ke / te3, "h2d_bytes_per_step": int(h2d3),
+                               "d2h_bytes_per_step": int(d2h3),
+                               "note": "compute_exposure, compute_psf_data, point_src_model_map_wcs as "
+                                       "separate host-buffer calls"}}
 
     cpu = None
     err = None

@@ -188,6 +188,21 @@ int xts_point_src_model_map_wcs(const xts_wcs* wcs, const double* src_sph, int S
                                 const double* partial, int E, void* model_map,
                                 xts_srcmap_info* info, unsigned flags, void* stream);
 
+/* The three calls of xtsrcmaps/main.cxx:28-30 in one: Exposure::compute_exposure
+ * (exposure/exposure.hxx:44-88), Psf::compute_psf_data (psf/psf.compute_psf_data.cxx:7-33)
+ * and ModelMap::compute_srcmaps<PointSource> (model_map/model_map.compute_src_maps.cxx:6-22),
+ * with the exposure and mean-PSF tables kept in device memory between the steps.
+ * Inputs are those of xts_compute_exposure plus the normalised King grids of
+ * xts_compute_psf_data and the map WCS; outputs those of
+ * xts_point_src_model_map_wcs.  With host pointers the maps are copied out in
+ * chunks of sources while later chunks are still being computed. */
+int xts_point_source_maps(const xts_expcube* exp_cube, const xts_expcube* wexp_cube,
+                          const double* logEs, int E, const double* src_sph, int S,
+                          const xts_grid* aeff_front, const xts_grid* aeff_back,
+                          const xts_grid* psf_front, const xts_grid* psf_back,
+                          const double* front_ltf, const xts_wcs* wcs, void* model_map,
+                          xts_srcmap_info* info, unsigned flags, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -221,3 +221,38 @@ def test_golden_exposure_and_psf_on_gpu(api, golden):
     xe = XtExp(cos, af, ab, ecb, wecb, ex)
     ps = api.compute_psf_data(nf, nb, xe, loge, ltf)
     assert max_rel(ps.uPsf[:, 0, :], golden("psf")["upsf_peak"]) < 2e-6
+
+
+@pytest.mark.parametrize("out_dtype", ["float32", "float64"])
+def test_point_source_maps_fused_call(api, c1_small, out_dtype):
+    """xts_point_source_maps (the three calls of main.cxx:28-30 in one) gives the
+    same maps and per-map results as the three separate calls, with host buffers
+    (chunked copy-out) and with device tensors."""
+    import torch
+
+    job, ref, gpu = c1_small
+    m, info = api.point_source_maps(job.wcs, job.src_sph, job.exp_cube, job.wexp_cube, job.logEs,
+                                    job.aeff_front, job.aeff_back, gpu["nf"], gpu["nb"], gpu["ltf"],
+                                    out_dtype=out_dtype)
+    m3, info3 = api.point_src_model_map_wcs(job.wcs, job.src_sph, gpu["ex"].exposure, gpu["ps"].uPsf,
+                                            gpu["ps"].partial_psf_integral, out_dtype=out_dtype)
+    # the map integrals add the points of pixels next to the source with FP64
+    # atomics, so two runs agree to rounding, not bit for bit
+    same = 1e-6 if out_dtype == "float32" else 1e-13
+    assert max_rel(m, m3) < same
+    assert max_rel(info.inv_map_integral, info3.inv_map_integral) < 1e-13
+    assert max_rel(info.correction, info3.correction) < 1e-13
+    tol = 1e-5 if out_dtype == "float32" else 1e-10
+    assert max_rel(m, ref["map"]) < tol
+    d = torch.device("cuda")
+    tg = lambda g: type(g)(*[torch.as_tensor(np.asarray(v), device=d) if isinstance(v, np.ndarray) else v
+                             for v in (g.cosths, g.logEs, g.params, g.min_cos_theta)])
+    from xtsrcmaps_b200.api import ExpCube
+
+    tc = lambda c: ExpCube(torch.as_tensor(c.cosbins, device=d), c.nside, c.nbrbins, c.cosmin, c.thetabin)
+    md, _ = api.point_source_maps(job.wcs, torch.as_tensor(job.src_sph, device=d), tc(job.exp_cube),
+                                  tc(job.wexp_cube), torch.as_tensor(job.logEs, device=d), tg(job.aeff_front),
+                                  tg(job.aeff_back), tg(gpu["nf"]), tg(gpu["nb"]),
+                                  torch.as_tensor(gpu["ltf"], device=d), out_dtype=out_dtype)
+    torch.cuda.synchronize()
+    assert max_rel(md.cpu().numpy(), m) < same

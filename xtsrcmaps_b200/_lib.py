@@ -92,6 +92,10 @@ SIGNATURES = {
     "xts_compute_psf_data_noalloc": (C.c_int, [C.POINTER(XtsGrid), C.POINTER(XtsGrid), _vp, C.c_int,
                                                _vp, C.c_int, _vp, _vp, _vp, _vp, C.c_int, _vp, _vp,
                                                _vp, _vp, _vp]),
+    "xts_point_source_maps": (C.c_int, [C.POINTER(XtsExpcube), C.POINTER(XtsExpcube), _vp, C.c_int, _vp,
+                                        C.c_int, C.POINTER(XtsGrid), C.POINTER(XtsGrid), C.POINTER(XtsGrid),
+                                        C.POINTER(XtsGrid), _vp, C.POINTER(XtsWcs), _vp,
+                                        C.POINTER(XtsSrcmapInfo), C.c_uint, _vp]),
     "xts_point_src_model_map_wcs": (C.c_int, [C.POINTER(XtsWcs), _vp, C.c_int, _vp, _vp, _vp,
                                               C.c_int, _vp, C.POINTER(XtsSrcmapInfo), C.c_uint, _vp]),
 }

@@ -26,9 +26,13 @@ int cuda_error(cudaError_t e, const char* what) {
     return set_error(code, "%s: %s", what, cudaGetErrorString(e));
 }
 
+constexpr int N_CHUNK_EV = 16;  // source chunks of a pipelined host-mode map
+
 struct Ctx {
     int device = -1;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;    // device-to-host copies of finished map chunks
+    cudaEvent_t chunk_ev[N_CHUNK_EV] = {};
     void* buf[N_SLOTS] = {};
     size_t cap[N_SLOTS] = {};
 };
@@ -53,6 +57,9 @@ int ensure_device() {
                          dev, prop.major, prop.minor);
     XTS_CUDA(cudaSetDevice(dev));
     XTS_CUDA(cudaStreamCreateWithFlags(&g_ctx.stream, cudaStreamNonBlocking));
+    if (!g_ctx.copy_stream) XTS_CUDA(cudaStreamCreateWithFlags(&g_ctx.copy_stream, cudaStreamNonBlocking));
+    for (int i = 0; i < N_CHUNK_EV; ++i)
+        if (!g_ctx.chunk_ev[i]) XTS_CUDA(cudaEventCreateWithFlags(&g_ctx.chunk_ev[i], cudaEventDisableTiming));
     g_ctx.device = dev;
     return XTS_OK;
 }
@@ -151,6 +158,7 @@ struct Stager {
     template <typename T>
     const T* in(const T* p, size_t n) {
         if (rc || dev || !p || n == 0) return p;
+        if (next_in > S_IN17) { rc = set_error(XTS_ERR_ARG, "too many staged inputs"); return nullptr; }
         void* d = workspace(next_in++, n * sizeof(T));
         if (!d) { rc = XTS_ERR_OOM; return nullptr; }
         cudaError_t e = cudaMemcpyAsync(d, p, n * sizeof(T), cudaMemcpyHostToDevice, st);
@@ -160,15 +168,26 @@ struct Stager {
     template <typename T>
     T* out(T* p, size_t n) {
         if (rc || dev || !p || n == 0) return p;
+        if (next_out > S_OUT15 || npend == 8) { rc = set_error(XTS_ERR_ARG, "too many staged outputs"); return nullptr; }
         void* d = workspace(next_out++, n * sizeof(T));
         if (!d) { rc = XTS_ERR_OOM; return nullptr; }
         pend[npend++] = {p, d, n * sizeof(T)};
         return (T*)d;
     }
+    // drop a pending copy-out (the caller copies that output itself)
+    void unpend(const void* host) {
+        for (int i = 0; i < npend; ++i)
+            if (pend[i].host == host) {
+                for (int j = i + 1; j < npend; ++j) pend[j - 1] = pend[j];
+                --npend;
+                return;
+            }
+    }
     // scratch output the caller did not ask for
     template <typename T>
     T* scratch(size_t n) {
         if (rc) return nullptr;
+        if (next_out > S_OUT15) { rc = set_error(XTS_ERR_ARG, "too many staged outputs"); return nullptr; }
         void* d = workspace(next_out++, n * sizeof(T));
         if (!d) rc = XTS_ERR_OOM;
         return (T*)d;
@@ -186,6 +205,75 @@ struct Stager {
         return XTS_OK;
     }
 };
+
+// Pipelined copy-out of a host-mode model map: each finished chunk of sources
+// gets an event on the compute stream; once every chunk is launched, the copy
+// stream waits for each event in turn and copies that chunk (copies into
+// pageable memory block the calling thread, so they are issued only after all
+// kernels are queued).
+struct ChunkCopy {
+    char* host = nullptr;
+    const char* dev = nullptr;
+    size_t bytes_per_source = 0;
+    int n = 0;
+    int s0[N_CHUNK_EV], ns[N_CHUNK_EV];
+    int issue(cudaStream_t st) {
+        for (int i = 0; i < n; ++i) {
+            XTS_CUDA(cudaStreamWaitEvent(g_ctx.copy_stream, g_ctx.chunk_ev[i], 0));
+            const size_t off = (size_t)s0[i] * bytes_per_source;
+            XTS_CUDA(cudaMemcpyAsync(host + off, dev + off, (size_t)ns[i] * bytes_per_source,
+                                     cudaMemcpyDeviceToHost, g_ctx.copy_stream));
+        }
+        return XTS_OK;
+    }
+};
+
+static int chunk_done(void* ctx, int s0, int n, cudaStream_t st) {
+    ChunkCopy* c = (ChunkCopy*)ctx;
+    if (c->n > 0 && c->n == N_CHUNK_EV) {  // merge into the last chunk (its event is re-recorded)
+        c->ns[c->n - 1] = s0 + n - c->s0[c->n - 1];
+        XTS_CUDA(cudaEventRecord(g_ctx.chunk_ev[c->n - 1], st));
+        return XTS_OK;
+    }
+    c->s0[c->n] = s0;
+    c->ns[c->n] = n;
+    XTS_CUDA(cudaEventRecord(g_ctx.chunk_ev[c->n], st));
+    c->n++;
+    return XTS_OK;
+}
+
+static int srcmap_kernel(unsigned flags) {
+    return (flags & XTS_TCGEN05) ? SRCMAP_TCGEN05 : (flags & XTS_CUDA_CORES) ? SRCMAP_ONEPASS : SRCMAP_WINDOWS;
+}
+
+// The model-map step with its outputs staged by sg.  In host mode the map is
+// copied out by source chunks on the copy stream while later chunks are
+// computed (window path); the other outputs are copied at the end.
+static int run_srcmap(Stager& sg, SrcmapDev& a, void* model_map, size_t npix, bool f64) {
+    const int S = a.S, E = a.E;
+    ChunkCopy cc;
+    if (!sg.dev && !sg.rc && S > 0 && npix * E > 0) {
+        cc.host = (char*)model_map;
+        cc.dev = (const char*)a.out;
+        cc.bytes_per_source = npix * E * (f64 ? 8 : 4);
+        sg.unpend(model_map);  // the map is not in the final copy list
+        a.chunk_sources = (S + 7) / 8;  // about 8 chunks (at most N_CHUNK_EV events are used)
+        a.on_chunk = chunk_done;
+        a.on_chunk_ctx = &cc;
+    }
+    int rc = sg.rc ? sg.rc : launch_srcmap(a, sg.st);
+    if (cc.host && rc == XTS_OK) {
+        if (cc.n == 0) rc = chunk_done(&cc, 0, S, sg.st);  // path without chunk hooks: one chunk
+        if (rc == XTS_OK) rc = cc.issue(sg.st);
+    }
+    rc = sg.finish(rc);
+    if (cc.host && cc.n) {
+        cudaError_t e = cudaStreamSynchronize(g_ctx.copy_stream);
+        if (rc == XTS_OK && e != cudaSuccess) rc = cuda_error(e, "map copy-out");
+    }
+    if (rc == XTS_OK && !sg.dev && S > 0) rc = srcmap_status(sg.st);
+    return rc;
+}
 
 static bool grid_ok(const xts_grid* g, int n_par) {
     return g && g->cosths && g->logEs && g->params && g->n_cos >= 2 && g->n_e >= 2 &&
@@ -229,6 +317,9 @@ int xts_init(int device) {
     XTS_CUDA(cudaSetDevice(device));
     g_ctx.device = -1;
     if (g_ctx.stream) { cudaStreamDestroy(g_ctx.stream); g_ctx.stream = nullptr; }
+    if (g_ctx.copy_stream) { cudaStreamDestroy(g_ctx.copy_stream); g_ctx.copy_stream = nullptr; }
+    for (int i = 0; i < N_CHUNK_EV; ++i)
+        if (g_ctx.chunk_ev[i]) { cudaEventDestroy(g_ctx.chunk_ev[i]); g_ctx.chunk_ev[i] = nullptr; }
     return ensure_device();
 }
 
@@ -426,11 +517,84 @@ int xts_point_src_model_map_wcs(const xts_wcs* wcs, const double* src_sph, int S
     a.correction = info ? sg.out(info->correction, (size_t)S * E) : nullptr;
     a.radius = info ? sg.out(info->psf_radius, (size_t)S) : nullptr;
     a.in_fov = info ? sg.out(info->in_fov, (size_t)S) : nullptr;
-    a.kernel = (flags & XTS_TCGEN05) ? SRCMAP_TCGEN05 : (flags & XTS_CUDA_CORES) ? SRCMAP_ONEPASS : SRCMAP_WINDOWS;
-    int rc = sg.rc ? sg.rc : launch_srcmap(a, sg.st);
-    rc = sg.finish(rc);
-    if (rc == XTS_OK && !sg.dev && S > 0) rc = srcmap_status(sg.st);
-    return rc;
+    a.kernel = srcmap_kernel(flags);
+    return run_srcmap(sg, a, model_map, npix, f64);
+}
+
+int xts_point_source_maps(const xts_expcube* cube, const xts_expcube* wcube, const double* logEs,
+                          int E, const double* src_sph, int S, const xts_grid* aeff_front,
+                          const xts_grid* aeff_back, const xts_grid* psf_front,
+                          const xts_grid* psf_back, const double* front_ltf, const xts_wcs* wcs,
+                          void* model_map, xts_srcmap_info* info, unsigned flags, void* stream) {
+    XTS_ENTER();
+    if (!cube || !wcube || !cube->cosbins || !wcube->cosbins || !logEs || E <= 0 || S < 0 ||
+        (S > 0 && (!src_sph || !model_map)) || !front_ltf)
+        return set_error(XTS_ERR_ARG, "point_source_maps: null argument or bad size");
+    if (cube->nside <= 0 || (cube->nside & (cube->nside - 1)) || cube->nbrbins <= 0 ||
+        wcube->nside != cube->nside || wcube->nbrbins != cube->nbrbins)
+        return set_error(XTS_ERR_ARG, "point_source_maps: livetime cubes need a power-of-two nside and equal shapes");
+    if (!grid_ok(aeff_front, 1) || !grid_ok(aeff_back, 1))
+        return set_error(XTS_ERR_ARG, "point_source_maps: effective-area grids need n_par == 1");
+    if (!grid_ok(psf_front, 6) || !grid_ok(psf_back, 6))
+        return set_error(XTS_ERR_ARG, "point_source_maps: King grids need n_par == 6");
+    if (!wcs || wcs->naxis1 <= 0 || wcs->naxis2 <= 0 || (wcs->proj != 0 && wcs->proj != 1) ||
+        wcs->cdelt1 == 0. || wcs->cdelt2 == 0.)
+        return set_error(XTS_ERR_ARG, "point_source_maps: bad WCS (CAR/AIT, nonzero CDELT)");
+    if ((long long)wcs->naxis1 * wcs->naxis2 > (1LL << 31) - 1 || S > 65535)
+        return set_error(XTS_ERR_ARG, "point_source_maps: map or source count too large");
+    const bool f64 = (flags & XTS_OUT_F64) != 0;
+    const size_t npix = (size_t)wcs->naxis1 * wcs->naxis2;
+    if ((flags & XTS_DEVICE_PTRS) && !f64 && ((uintptr_t)model_map & 15))
+        return set_error(XTS_ERR_ARG, "point_source_maps: device model_map must be 16-byte aligned");
+    const int C = cube->nbrbins;
+    const long long nhp = 12LL * cube->nside * cube->nside;
+    Stager sg{(flags & XTS_DEVICE_PTRS) != 0, stream ? (cudaStream_t)stream : g_ctx.stream};
+    // (a) exposure; its outputs stay in device memory
+    ExposureDev ea;
+    ea.cube = sg.in(cube->cosbins, (size_t)nhp * C);
+    ea.wcube = sg.in(wcube->cosbins, (size_t)nhp * C);
+    ea.nside = cube->nside; ea.C = C; ea.cosmin = cube->cosmin; ea.thetabin = cube->thetabin;
+    ea.logEs = sg.in(logEs, (size_t)E); ea.E = E;
+    ea.src_sph = sg.in(src_sph, (size_t)2 * S); ea.S = S;
+    ea.af = stage_grid(sg, aeff_front);
+    ea.ab = stage_grid(sg, aeff_back);
+    ea.ltf = sg.in(front_ltf, (size_t)2 * E);
+    ea.exp_costhetas = sg.scratch<double>(C);
+    ea.front_aeff = sg.scratch<double>((size_t)C * E);
+    ea.back_aeff = sg.scratch<double>((size_t)C * E);
+    ea.ecb = sg.scratch<double>((size_t)S * C);
+    ea.wecb = sg.scratch<double>((size_t)S * C);
+    ea.exposure = sg.scratch<double>((size_t)S * E);
+    ea.use_tf32 = (flags & XTS_EXPOSURE_TF32) != 0;
+    // (b) mean PSF tables
+    PsfDev pa;
+    pa.pf = stage_grid(sg, psf_front);
+    pa.pb = stage_grid(sg, psf_back);
+    pa.costh = ea.exp_costhetas; pa.C = C;
+    pa.logEs = ea.logEs; pa.E = E;
+    pa.af = ea.front_aeff; pa.ab = ea.back_aeff;
+    pa.ecb = ea.ecb; pa.wecb = ea.wecb; pa.S = S;
+    pa.ltf = ea.ltf; pa.exposure = ea.exposure;
+    pa.upsf = sg.scratch<double>((size_t)S * ND * E);
+    pa.partial = sg.scratch<double>((size_t)S * ND * E);
+    // (c)+(d) model maps
+    SrcmapDev ma;
+    ma.wcs = *wcs;
+    ma.src_sph = ea.src_sph; ma.S = S;
+    ma.exposure = ea.exposure; ma.upsf = pa.upsf; ma.partial = pa.partial; ma.E = E;
+    ma.out_f64 = f64;
+    ma.out = f64 ? (void*)sg.out((double*)model_map, (size_t)S * npix * E)
+                 : (void*)sg.out((float*)model_map, (size_t)S * npix * E);
+    ma.inv_integ = info ? sg.out(info->inv_map_integral, (size_t)S * E) : nullptr;
+    ma.correction = info ? sg.out(info->correction, (size_t)S * E) : nullptr;
+    ma.radius = info ? sg.out(info->psf_radius, (size_t)S) : nullptr;
+    ma.in_fov = info ? sg.out(info->in_fov, (size_t)S) : nullptr;
+    ma.kernel = srcmap_kernel(flags);
+    int rc = sg.rc;
+    if (rc == XTS_OK) rc = launch_exposure(ea, sg.st);
+    if (rc == XTS_OK) rc = launch_psf(pa, sg.st);
+    if (rc != XTS_OK) return sg.finish(rc);
+    return run_srcmap(sg, ma, model_map, npix, f64);
 }
 
 }  // extern "C"

@@ -59,7 +59,8 @@ enum Slot {
     // staged inputs / outputs (host-pointer mode)
     S_IN0, S_IN1, S_IN2, S_IN3, S_IN4, S_IN5, S_IN6, S_IN7, S_IN8, S_IN9, S_IN10, S_IN11,
     S_IN12, S_IN13, S_IN14, S_IN15, S_IN16, S_IN17,
-    S_OUT0, S_OUT1, S_OUT2, S_OUT3, S_OUT4, S_OUT5, S_OUT6,
+    S_OUT0, S_OUT1, S_OUT2, S_OUT3, S_OUT4, S_OUT5, S_OUT6, S_OUT7, S_OUT8, S_OUT9, S_OUT10,
+    S_OUT11, S_OUT12, S_OUT13, S_OUT14, S_OUT15,
     // internal scratch
     W_CORNERS, W_CENTERS, W_OMEGA, W_LUT, W_PARTSUM, W_SRCINFO, W_SCALE, W_PSFTAB,
     W_KING, W_MISC, W_WIN, W_WMETA, W_SPARSE,
@@ -121,6 +122,11 @@ struct SrcmapDev {
     void* out; bool out_f64;
     double* inv_integ; double* correction; double* radius; int* in_fov;  // optional (may be null)
     int kernel;  // FP32 write pass: SRCMAP_WINDOWS, SRCMAP_ONEPASS or SRCMAP_TCGEN05
+    // Optional: sources per chunk of the write pass, and a hook called on the
+    // launching stream after each chunk's maps are enqueued (pipelined copy-out).
+    int chunk_sources = 0;
+    int (*on_chunk)(void* ctx, int s0, int n, cudaStream_t st) = nullptr;
+    void* on_chunk_ctx = nullptr;
 };
 enum { SRCMAP_WINDOWS = 0, SRCMAP_ONEPASS = 1, SRCMAP_TCGEN05 = 2 };
 int launch_srcmap(const SrcmapDev& a, cudaStream_t st);
@@ -137,10 +143,12 @@ int launch_correction(const double* hist, int nch, const SrcInfo* info, int S, c
                       cudaStream_t st);
 bool srcmap_win_supported(int E);
 int launch_srcmap_win(const double* corners, const double* centers, const double* omega,
-                      const SrcInfo* info, int S, int H, int W, int E, int nch, double* hist,
+                      const SrcInfo* info, int S, int H, int W, int E,
                       const double* upsf, const double* partial, const double* exposure,
                       double* scale, double* inv_integ, double* correction, double* radius,
-                      int* in_fov, int* status, float* out, cudaStream_t st);  // 0, or XTS_ERR_TIMEOUT if a bounded device wait gave up
+                      int* in_fov, int* status, float* out, int chunk_sources,
+                      int (*on_chunk)(void*, int, int, cudaStream_t), void* on_chunk_ctx,
+                      cudaStream_t st);  // 0, or XTS_ERR_TIMEOUT if a bounded device wait gave up
 int launch_srcmap_fast(const double* corners, const double* omega, const SrcInfo* info,
                        const double* upsf, const double* scale, int S, int H, int W, int E,
                        float* out, cudaStream_t st);

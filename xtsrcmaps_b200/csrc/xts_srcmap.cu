@@ -516,9 +516,9 @@ int launch_srcmap(const SrcmapDev& a, cudaStream_t st) {
         int* status = (int*)workspace(W_MISC, 64);
         if (!status) return XTS_ERR_OOM;
         XTS_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
-        return launch_srcmap_win(corners, centers, omega, info, S, H, W, E, nch, hist, a.upsf, a.partial,
+        return launch_srcmap_win(corners, centers, omega, info, S, H, W, E, a.upsf, a.partial,
                                  a.exposure, scale, a.inv_integ, a.correction, a.radius, a.in_fov, status,
-                                 (float*)a.out, st);
+                                 (float*)a.out, a.chunk_sources, a.on_chunk, a.on_chunk_ctx, st);
     }
     if (a.out_f64) {  // the reference's own per-point FP64 arithmetic throughout
         XTS_LAUNCH("k_map_integral_f64", st, k_map_integral_hist<<<dim3(nch, S), 256, 0, st>>>(corners, centers, omega, info, H, W, nch, hist));

@@ -428,10 +428,12 @@ bool srcmap_win_supported(int E) {
 static size_t win_bytes_per_source(int npix) { return (size_t)npix * 36; }
 
 int launch_srcmap_win(const double* corners, const double* centers, const double* omega,
-                      const SrcInfo* info, int S, int H, int W, int E, int nch, double* hist,
+                      const SrcInfo* info, int S, int H, int W, int E,
                       const double* upsf, const double* partial, const double* exposure,
                       double* scale, double* inv_integ, double* correction, double* radius,
-                      int* in_fov, int* status, float* out, cudaStream_t st) {
+                      int* in_fov, int* status, float* out, int chunk_sources,
+                      int (*on_chunk)(void*, int, int, cudaStream_t), void* on_chunk_ctx,
+                      cudaStream_t st) {
     int rc = upload_rule_uv(st);
     if (rc) return rc;
     const SepTab* tab = nullptr;
@@ -443,6 +445,7 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
     // sources per chunk: window records of at most ~2 GiB
     const size_t budget = (size_t)2 << 30;
     int Sc = (int)(budget / win_bytes_per_source(npix));
+    if (chunk_sources > 0 && chunk_sources < Sc) Sc = chunk_sources;
     Sc = Sc < 1 ? 1 : (Sc > S ? S : Sc);
     float4* win = (float4*)workspace(W_WIN, (size_t)Sc * npix * 32 + 16);
     int* wmeta = (int*)workspace(W_WMETA, (size_t)Sc * npix * 4 + 16);
@@ -452,12 +455,18 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
     cap = cap < 65536 ? 65536 : cap;
     cap = cap > (long long)Sc * npix ? (long long)Sc * npix : cap;
     float2* sparse = (float2*)workspace(W_SPARSE, sizeof(float2) * NSP * (size_t)cap + 16);
-    if (!win || !wmeta || !lut || !sparse) return XTS_ERR_OOM;
-    int* sparse_count = status + 1;
-    XTS_CUDA(cudaFuncSetAttribute(k_pixel_windows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WA_SMEM));
     int dev = 0, nsm = 148, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    // pass A: about four blocks per SM over the chunk's sources; the row
+    // histograms of a chunk ([Sc][nch][401]) are reused by the next chunk
+    int nch = (4 * nsm + Sc - 1) / Sc;
+    const int maxch = (npix + WT - 1) / WT;
+    nch = nch < 1 ? 1 : (nch > maxch ? maxch : nch);
+    double* hist = (double*)workspace(W_PARTSUM, sizeof(double) * (size_t)Sc * nch * ND + 8);
+    if (!win || !wmeta || !lut || !sparse || !hist) return XTS_ERR_OOM;
+    int* sparse_count = status + 1;
+    XTS_CUDA(cudaFuncSetAttribute(k_pixel_windows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WA_SMEM));
     const WritePassFn wp = k_write_pass[(E + 3) / 4 - 1];
     rc = wp(0, L.total, st, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, 0, 0, E, EQ,
             nullptr, nullptr, &per_sm, nsm, true);
@@ -469,9 +478,9 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
         XTS_CUDA(cudaMemsetAsync(sparse_count, 0, sizeof(int), st));
         XTS_LAUNCH("k_pixel_windows", st, k_pixel_windows<<<dim3(nch, n), WT, WA_SMEM, st>>>(
                                               corners, centers, omega, info + s0, tab, H, W, nch,
-                                              hist + (size_t)s0 * nch * ND, win, wmeta, sparse, (int)cap,
+                                              hist, win, wmeta, sparse, (int)cap,
                                               sparse_count));
-        rc = launch_correction(hist + (size_t)s0 * nch * ND, nch, info + s0, n, upsf + oE * ND, partial + oE * ND,
+        rc = launch_correction(hist, nch, info + s0, n, upsf + oE * ND, partial + oE * ND,
                                exposure + oE, E, scale + oE, inv_integ ? inv_integ + oE : nullptr,
                                correction ? correction + oE : nullptr, radius ? radius + s0 : nullptr,
                                in_fov ? in_fov + s0 : nullptr, st);
@@ -484,6 +493,7 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
         rc = wp((unsigned)G, L.total, st, win, wmeta, sparse, lut, corners, omega, info + s0, tab, n, s0, H, W, E, EQ,
                 status, out, nullptr, nsm, false);
         if (rc) return rc;
+        if (on_chunk && (rc = on_chunk(on_chunk_ctx, s0, n, st))) return rc;
     }
     return XTS_OK;
 }
