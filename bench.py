@@ -286,7 +286,8 @@ def run_ours(args, rank, world, local_rank):
     traffic = None
     try:
         tr = json.load(open(os.path.join(ROOT, "profiles", "k_srcmap_c1_traffic.json")))
-        traffic = tr.get("dram_bytes_per_launch")
+        if tr.get("workload") == args.config and args.kernel == "windows":
+            traffic = tr.get("dram_bytes_per_launch")
     except (OSError, ValueError):
         pass
     roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",

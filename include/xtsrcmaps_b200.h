@@ -44,7 +44,7 @@ enum xts_status {
 enum xts_flags {
     XTS_DEVICE_PTRS = 1u << 0, /* array arguments are device pointers */
     XTS_OUT_F64 = 1u << 1,     /* model map written as double (default float) */
-    XTS_EXPOSURE_TF32 = 1u << 2, /* exposure contraction as 3xTF32 on tcgen05 tensor cores (default: FP64 cores) */
+    /* 1u << 2 is reserved */
     XTS_CUDA_CORES = 1u << 3,    /* FP32 source maps by the single-pass CUDA-core kernel (geometry and
                                     map integral in separate passes; default: the two-pass window path) */
     XTS_TCGEN05 = 1u << 4        /* FP32 source maps with the window-times-table product on tcgen05

@@ -35,12 +35,12 @@ def _job(name, seed=3, n=None):
     return make_job(name, seed=seed, n_sources=n)
 
 
-def _gpu_pipeline(A, job, out_dtype="float32", tf32=False):
+def _gpu_pipeline(A, job, out_dtype="float32"):
     ltf = A.livetime_efficiency_factors(job.logEs, job.effic_front)
     nf = A.normalize_rpsf(job.rpsf_front, job.scale_front)
     nb = A.normalize_rpsf(job.rpsf_back, job.scale_back)
     ex = A.compute_exposure(job.exp_cube, job.wexp_cube, job.logEs, job.src_sph, job.aeff_front,
-                            job.aeff_back, ltf, tf32=tf32)
+                            job.aeff_back, ltf)
     ps = A.compute_psf_data(nf, nb, ex, job.logEs, ltf)
     mm, info = A.point_src_model_map_wcs(job.wcs, job.src_sph, ex.exposure, ps.uPsf,
                                          ps.partial_psf_integral, out_dtype=out_dtype)

@@ -21,7 +21,6 @@ XTS_ERR_NODEV = -5
 
 XTS_DEVICE_PTRS = 1 << 0
 XTS_OUT_F64 = 1 << 1
-XTS_EXPOSURE_TF32 = 1 << 2
 XTS_CUDA_CORES = 1 << 3
 XTS_TCGEN05 = 1 << 4
 

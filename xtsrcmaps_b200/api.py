@@ -183,7 +183,7 @@ def normalize_rpsf(grid: IrfGrid, scale: IrfScale) -> IrfGrid:
 
 # --------------------------------------------------------------------------- step (a)
 def compute_exposure(exp_cube: ExpCube, wexp_cube: ExpCube, logEs, src_sph, aeff_front: IrfGrid,
-                     aeff_back: IrfGrid, front_ltf, tf32: bool = False) -> XtExp:
+                     aeff_back: IrfGrid, front_ltf) -> XtExp:
     """Exposure::compute_exposure (exposure/exposure.hxx:44-88)."""
     like = _device_of(exp_cube.cosbins, src_sph, logEs)
     c = _Call(like is not None, like)
@@ -202,14 +202,13 @@ def compute_exposure(exp_cube: ExpCube, wexp_cube: ExpCube, logEs, src_sph, aeff
     ltfp, _ = c.inp(front_ltf)
     o = [c.out(s) for s in ((C_,), (C_, E), (C_, E), (S, C_), (S, C_), (S, E))]
     outs = L.XtsExposureOut(*[x[0] for x in o])
-    flags = c.flags | (L.XTS_EXPOSURE_TF32 if tf32 else 0)
+    flags = c.flags
     L.check(L.lib().xts_compute_exposure(C.byref(cube_s), C.byref(wcube_s), lp, E, sp, S, C.byref(af),
                                          C.byref(ab), ltfp, C.byref(outs), flags, c.stream))
     return XtExp(*[x[1] for x in o])
 
 
-def exposure(src_exposure_cosbins, src_weighted_exposure_cosbins, front_aeff, back_aeff, front_ltf,
-             tf32: bool = False):
+def exposure(src_exposure_cosbins, src_weighted_exposure_cosbins, front_aeff, back_aeff, front_ltf):
     """Exposure::exposure (exposure/exposure.cxx:159-263): step a5 from gathered livetime rows."""
     like = _device_of(src_exposure_cosbins, front_aeff)
     c = _Call(like is not None, like)
@@ -221,8 +220,7 @@ def exposure(src_exposure_cosbins, src_weighted_exposure_cosbins, front_aeff, ba
     S, C_ = int(xa.shape[0]), int(xa.shape[1])
     E = int(afa.shape[1])
     op, o = c.out((S, E))
-    flags = c.flags | (L.XTS_EXPOSURE_TF32 if tf32 else 0)
-    L.check(L.lib().xts_exposure_contract(xp, wp, S, C_, afp, abp, lp, E, op, flags, c.stream))
+    L.check(L.lib().xts_exposure_contract(xp, wp, S, C_, afp, abp, lp, E, op, c.flags, c.stream))
     return o
 
 
@@ -300,7 +298,7 @@ def point_src_model_map_wcs(wcs: Wcs, src_sph, exposure, uPsf, partial_integrals
 def point_source_maps(wcs: Wcs, src_sph, exp_cube: ExpCube, wexp_cube: ExpCube, logEs, aeff_front: IrfGrid,
                       aeff_back: IrfGrid, psf_front: IrfGrid, psf_back: IrfGrid, front_ltf,
                       out_dtype: str = "float32", out=None, with_info: bool = True,
-                      kernel: str = "windows", tf32: bool = False):
+                      kernel: str = "windows"):
     """The three calls of main.cxx:28-30 (compute_exposure, compute_psf_data,
     compute_srcmaps<PointSource>) in one library call; the exposure and mean-PSF
     tables stay in device memory.  ``psf_front``/``psf_back`` are normalised King
@@ -337,7 +335,7 @@ def point_source_maps(wcs: Wcs, src_sph, exp_cube: ExpCube, wexp_cube: ExpCube, 
         info_s = L.XtsSrcmapInfo(*[x[0] for x in o])
         info = SrcmapInfo(*[x[1] for x in o])
     kflag = {"windows": 0, "cuda_cores": L.XTS_CUDA_CORES, "tcgen05": L.XTS_TCGEN05}[kernel]
-    flags = c.flags | (L.XTS_OUT_F64 if kind == "f64" else 0) | kflag | (L.XTS_EXPOSURE_TF32 if tf32 else 0)
+    flags = c.flags | (L.XTS_OUT_F64 if kind == "f64" else 0) | kflag
     w = _wcs_struct(wcs)
     L.check(L.lib().xts_point_source_maps(C.byref(cube_s), C.byref(wcube_s), lp, E, sp, S, C.byref(af),
                                           C.byref(ab), C.byref(gf), C.byref(gb), ltfp, C.byref(w), mp,

@@ -432,7 +432,6 @@ int xts_compute_exposure(const xts_expcube* cube, const xts_expcube* wcube, cons
     a.ecb = out->src_exposure_cosbins ? sg.out(out->src_exposure_cosbins, (size_t)S * C) : sg.scratch<double>((size_t)S * C);
     a.wecb = out->src_weighted_exposure_cosbins ? sg.out(out->src_weighted_exposure_cosbins, (size_t)S * C) : sg.scratch<double>((size_t)S * C);
     a.exposure = out->exposure ? sg.out(out->exposure, (size_t)S * E) : sg.scratch<double>((size_t)S * E);
-    a.use_tf32 = (flags & XTS_EXPOSURE_TF32) != 0;
     int rc = sg.rc ? sg.rc : launch_exposure(a, sg.st);
     return sg.finish(rc);
 }
@@ -452,7 +451,7 @@ int xts_exposure_contract(const double* ecb, const double* wecb, int S, int C, c
     double* d_out = sg.out(exposure, (size_t)S * E);
     int rc = sg.rc ? sg.rc
                    : launch_exposure_contract(d_ecb, d_wecb, S, C, d_af, d_ab, d_ltf, E, d_out,
-                                              (flags & XTS_EXPOSURE_TF32) != 0, sg.st);
+                                              sg.st);
     return sg.finish(rc);
 }
 
@@ -565,7 +564,6 @@ int xts_point_source_maps(const xts_expcube* cube, const xts_expcube* wcube, con
     ea.ecb = sg.scratch<double>((size_t)S * C);
     ea.wecb = sg.scratch<double>((size_t)S * C);
     ea.exposure = sg.scratch<double>((size_t)S * E);
-    ea.use_tf32 = (flags & XTS_EXPOSURE_TF32) != 0;
     // (b) mean PSF tables
     PsfDev pa;
     pa.pf = stage_grid(sg, psf_front);

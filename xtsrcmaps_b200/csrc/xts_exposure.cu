@@ -92,11 +92,10 @@ __global__ void k_exposure_f64(const double* ecb, const double* wecb, int S, int
 }
 
 int launch_exposure_contract(const double* ecb, const double* wecb, int S, int C, const double* af,
-                             const double* ab, const double* ltf, int E, double* out, bool tf32,
+                             const double* ab, const double* ltf, int E, double* out,
                              cudaStream_t st) {
     int n = S * E;
     if (n == 0) return XTS_OK;
-    if (tf32) return launch_tf32_exposure(ecb, wecb, S, C, af, ab, ltf, E, out, st);
     XTS_LAUNCH("k_exposure_f64", st, k_exposure_f64<<<(n + 127) / 128, 128, 0, st>>>(ecb, wecb, S, C, af, ab, ltf, E, out));
     return XTS_OK;
 }
@@ -112,7 +111,7 @@ int launch_exposure(const ExposureDev& a, cudaStream_t st) {
                                                       a.C, a.ecb, a.wecb));
     }
     return launch_exposure_contract(a.ecb, a.wecb, a.S, a.C, a.front_aeff, a.back_aeff, a.ltf, a.E,
-                                    a.exposure, a.use_tf32, st);
+                                    a.exposure, st);
 }
 
 // a4: piecewise-linear efficiency in log E.  Row 1 from p0, row 0 from p1, and

@@ -90,14 +90,10 @@ struct ExposureDev {
     const double* ltf;
     double* exp_costhetas; double* front_aeff; double* back_aeff;
     double* ecb; double* wecb; double* exposure;
-    bool use_tf32;
 };
 int launch_exposure(const ExposureDev& a, cudaStream_t st);
 int launch_exposure_contract(const double* ecb, const double* wecb, int S, int C, const double* af,
-                             const double* ab, const double* ltf, int E, double* out, bool tf32,
-                             cudaStream_t st);
-int launch_tf32_exposure(const double* ecb, const double* wecb, int S, int C, const double* af,
-                         const double* ab, const double* ltf, int E, double* out, cudaStream_t st);
+                             const double* ab, const double* ltf, int E, double* out, cudaStream_t st);
 
 int launch_ltf(const double* logEs, int E, const float* p0, const float* p1, double* ltf,
                cudaStream_t st);
