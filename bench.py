@@ -397,57 +397,98 @@ def _oracle_worker(args):
     return time.perf_counter() - t0, r["map"].size
 
 
+def _reference_runner(job):
+    """One full pass of the CPU reference over ``job``: the reference's own code
+    compiled under oracle/_ref when it is there (its OpenMP on every host core),
+    else None.  Returns (run, threads, description)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import irf_setup, reference_pipeline
+    from oracle import oracle_ref as R
+
+    if not R.available():
+        return None, 0, ""
+    threads = R.set_threads(os.cpu_count() or 1)
+    setup = irf_setup(job)  # Irf::collect_irf_data, outside the timed pass as on the GPU
+    busy = min(threads, (job.S + 15) // 16)
+    desc = (f"the reference's compiled exposure, mean-PSF and model-map code (oracle/_ref), OpenMP with "
+            f"{threads} threads; its source loops use schedule(static, 16), so {busy} thread(s) share "
+            f"the {job.S} sources of the cubature")
+    return (lambda: reference_pipeline(job, setup)), threads, desc
+
+
 def cpu_baseline(job, gpu_map):
-    """The FP64 oracle (a scalar port of the reference path) on the host cores,
-    over the bench's own job; also gives the GPU map's error against FP64."""
+    """The CPU reference (compiled reference code, else the FP64 oracle port) on
+    the host cores over the bench's own job, repeated for about 10 s; also the
+    GPU map's error against the FP64 oracle."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from helpers import max_rel, oracle_pipeline
 
-    t0 = time.perf_counter()
     r = oracle_pipeline(job)
-    dt = time.perf_counter() - t0
-    reps = 1
-    while time.perf_counter() - t0 < 10.0 and reps < 8:
-        oracle_pipeline(job, with_map=True)
+    err = max_rel(gpu_map, r["map"])
+    run, threads, desc = _reference_runner(job)
+    kind = "reference"
+    if run is None:
+        run, threads, kind = (lambda: oracle_pipeline(job)), 1, "port"
+        desc = "the FP64 oracle (a scalar C restatement of the reference path) on one core"
+    run()
+    t0 = time.perf_counter()
+    reps = 0
+    while reps < 1 or (time.perf_counter() - t0 < 10.0 and reps < 20):
+        run()
         reps += 1
     dt = (time.perf_counter() - t0) / reps
-    err = max_rel(gpu_map, r["map"])
-    return ({"value": job.n_values / dt, "unit": UNIT, "cores": 1, "kind": "port",
-             "sample": f"the full bench job ({job.S} sources, {job.wcs.naxis1}x{job.wcs.naxis2}, "
-                       f"{job.E} energies), FP64 oracle, {reps} repetitions"}, err)
+    return ({"value": job.n_values / dt, "unit": UNIT, "cores": threads, "kind": kind,
+             "sample": f"the full bench job ({job.S} sources, {job.wcs.naxis1}x{job.wcs.naxis2}, {job.E} "
+                       f"energies) {reps} times: {desc}"}, err)
 
 
 def run_reference(args, rank, world):
+    """--impl reference: the CPU reference on this box's host cores (rank 0 only)."""
     if rank != 0:
         return
-    import multiprocessing as mp
-
     from xtsrcmaps_b200.synth import DESCRIPTIONS, make_job
 
     job = make_job(args.config, seed=args.seed)
-    cores = os.cpu_count() or 1
-    S = job.S
-    chunks = [(args.config, args.seed, i * S // cores, (i + 1) * S // cores) for i in range(cores)]
-    chunks = [c for c in chunks if c[3] > c[2]]
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(len(chunks)) as pool:
-        for _ in range(max(1, min(args.warmup, 1))):
-            pool.map(_oracle_worker, chunks)
+    run, threads, desc = _reference_runner(job)
+    if run is not None:
+        kind = "reference"
+        for _ in range(max(1, min(args.warmup, 2))):
+            run()
         times = []
-        nsteps = max(1, min(args.steps, 5))
-        for _ in range(nsteps):
+        t_all = time.perf_counter()
+        for _ in range(args.steps):  # each step is the whole workload; stop after ~60 s
             t0 = time.perf_counter()
-            pool.map(_oracle_worker, chunks)
+            run()
             times.append(time.perf_counter() - t0)
+            if time.perf_counter() - t_all > 60.0:
+                break
+        sample = f"the whole {args.config} job per step: {desc}"
+    else:  # the oracle port, one process per block of sources
+        import multiprocessing as mp
+
+        kind = "port"
+        cores = os.cpu_count() or 1
+        S = job.S
+        chunks = [(args.config, args.seed, i * S // cores, (i + 1) * S // cores) for i in range(cores)]
+        chunks = [c for c in chunks if c[3] > c[2]]
+        threads = len(chunks)
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(len(chunks)) as pool:
+            pool.map(_oracle_worker, chunks)
+            times = []
+            for _ in range(max(1, min(args.steps, 5))):
+                t0 = time.perf_counter()
+                pool.map(_oracle_worker, chunks)
+                times.append(time.perf_counter() - t0)
+        sample = f"the whole {args.config} job per step, FP64 oracle split by source over {threads} processes"
     ms = 1e3 * sum(times) / len(times)
     value = job.n_values / (ms * 1e-3)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-        "steps": nsteps, "warmup": 1, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "steps": len(times), "warmup": max(1, min(args.warmup, 2)), "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
         "config": {"workload": args.config + ": " + DESCRIPTIONS[args.config]},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": len(chunks), "kind": "port",
-                         "sample": f"full {args.config} job split by source over {len(chunks)} processes"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

@@ -27,6 +27,34 @@ def oracle_pipeline(job, with_map: bool = True):
     return out
 
 
+def irf_setup(job):
+    """IRF set-up outside the timed path (Irf::collect_irf_data): livetime
+    efficiency factors and normalised King grids, with the FP64 oracle."""
+    ltf = O.livetime_efficiency_factors(job.logEs, job.effic_front.p0, job.effic_front.p1)
+    return ltf, normalized(job.rpsf_front, job.scale_front), normalized(job.rpsf_back, job.scale_back)
+
+
+def reference_pipeline(job, setup=None, with_map: bool = True):
+    """The same steps through the reference's own code compiled under oracle/_ref
+    (oracle/oracle_ref.py): exposure, mean PSF and the model map.  The effective
+    area tables come from the oracle's restatement of Irf::aeff_value, whose
+    reference translation unit needs <mdspan>."""
+    from oracle import oracle_ref as R
+
+    ltf, nf, nb = setup if setup is not None else irf_setup(job)
+    cube, wcube = job.exp_cube, job.wexp_cube
+    cos = O.costhetas(cube.nbrbins, cube.cosmin, cube.thetabin)
+    af = O.aeff_value(cos, job.logEs, job.aeff_front)
+    ab = O.aeff_value(cos, job.logEs, job.aeff_back)
+    cos, ecb, wecb, expo = R.exposure(cube.cosbins, wcube.cosbins, cube.nside, cube.cosmin, cube.thetabin,
+                                      job.src_sph, af, ab, ltf)
+    upsf, partial = R.psf(nf, nb, cos, job.logEs, af, ab, ecb, wecb, ltf, expo)
+    out = dict(costh=cos, ecb=ecb, wecb=wecb, af=af, ab=ab, ltf=ltf, exposure=expo, upsf=upsf, partial=partial)
+    if with_map:
+        out["map"] = R.point_src_model_map_wcs(job.wcs, job.src_sph, expo, upsf, partial)
+    return out
+
+
 def normalized(grid: IrfGrid, scale) -> IrfGrid:
     p = O.normalize_rpsf(grid.params, grid.logEs, scale.scale0, scale.scale1, scale.scale_index)
     return IrfGrid(grid.cosths, grid.logEs, p, grid.min_cos_theta)

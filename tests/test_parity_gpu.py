@@ -256,3 +256,21 @@ def test_point_source_maps_fused_call(api, c1_small, out_dtype):
                                   torch.as_tensor(gpu["ltf"], device=d), out_dtype=out_dtype)
     torch.cuda.synchronize()
     assert max_rel(md.cpu().numpy(), m) < same
+
+
+def test_srcmap_vs_compiled_reference(api, c1_small):
+    """GPU maps (FP32 and FP64) against ModelMap::point_src_model_map_wcs of the
+    reference's own code compiled under oracle/_ref, fed the same exposure and
+    mean-PSF tables."""
+    from oracle import oracle_ref as R
+
+    if not R.available():
+        pytest.skip("oracle/_ref/libxts_ref.so not built")
+    job, ref, gpu = c1_small
+    rm = R.point_src_model_map_wcs(job.wcs, job.src_sph, ref["exposure"], ref["upsf"], ref["partial"])
+    m32, _ = api.point_src_model_map_wcs(job.wcs, job.src_sph, ref["exposure"], ref["upsf"], ref["partial"])
+    m64, _ = api.point_src_model_map_wcs(job.wcs, job.src_sph, ref["exposure"], ref["upsf"], ref["partial"],
+                                         out_dtype="float64")
+    assert max_rel(m32, rm) < 1e-5
+    assert max_rel(m32.astype(np.float64).sum(axis=(1, 2)), rm.sum(axis=(1, 2))) < 1e-7
+    assert max_rel(m64, rm) < 1e-10
