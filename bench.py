@@ -153,7 +153,14 @@ def run_ours(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=dev)
 
-    job = make_job(args.config, seed=args.seed + 1000 * rank)
+    # one global source list, CONFIGS[config]["S"] sources per GPU, sharded over
+    # the ranks (weak scaling); every rank holds the same livetime cube and IRFs
+    from xtsrcmaps_b200.shard import shard_sources
+    from xtsrcmaps_b200.synth import CONFIGS
+
+    per_gpu = CONFIGS[args.config]["S"]
+    job = make_job(args.config, seed=args.seed, n_sources=per_gpu * world)
+    job.src_sph = job.src_sph[shard_sources(job.S, world)[rank]]
     S, H, W, E = job.S, job.wcs.naxis1, job.wcs.naxis2, job.E
     n_values = job.n_values
     # IRF set-up (Irf::collect_irf_data, untimed like the reference's ingest)
