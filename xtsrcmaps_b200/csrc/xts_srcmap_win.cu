@@ -240,14 +240,15 @@ k_srcmap_win(const float4* __restrict__ win, const int* __restrict__ wmeta, cons
 
     int cur = -1;
     unsigned phase = 0;
-    PixRec rec;
-    {
-        const int s = (int)(f0 / ntiles), p0 = (int)(f0 - (long long)s * ntiles) * BT;
-        rec = load_rec(win, wmeta, (size_t)s * npix + p0 + t, f0 < f1 && p0 + t < npix);
-    }
+    // (source, tile) of f, advanced by counting: no 64-bit division per tile
+    int s = (int)(f0 / ntiles), tile = (int)(f0 - (long long)s * ntiles);
+    PixRec rec = load_rec(win, wmeta, (size_t)s * npix + tile * BT + t, f0 < f1 && tile * BT + t < npix);
     for (long long f = f0; f < f1; ++f) {
-        const int s = (int)(f / ntiles);
-        const int px0 = (int)(f - (long long)s * ntiles) * BT + warp * 32;  // this warp's first pixel
+        int sn = s, tn = tile + 1;  // the next tile
+        if (tn == ntiles) { tn = 0; ++sn; }
+        int s2 = sn, t2 = tn + 1;   // and the one after
+        if (t2 == ntiles) { t2 = 0; ++s2; }
+        const int px0 = tile * BT + warp * 32;  // this warp's first pixel
         const int npw = min(32, npix - px0);                                // may be <= 0 in the last tile
         const long long g0 = ((long long)(s_base + s) * npix + px0) * E;    // first flat output of the whole map
         const int m = (int)(g0 & 3);                                        // staging residue
@@ -258,12 +259,10 @@ k_srcmap_win(const float4* __restrict__ win, const int* __restrict__ wmeta, cons
         // one after that on its way into L2
         PixRec nxt;
         {
-            const long long fn = f + 1;
-            const int sn = (int)(fn / ntiles), pn = (int)(fn - (long long)sn * ntiles) * BT;
-            nxt = load_rec(win, wmeta, (size_t)sn * npix + pn + t, fn < f1 && pn + t < npix);
-            const long long f2 = f + 2;
-            const int s2 = (int)(f2 / ntiles), p2 = (int)(f2 - (long long)s2 * ntiles) * BT;
-            if (f2 < f1 && p2 + t < npix) {
+            const int pn = tn * BT;
+            nxt = load_rec(win, wmeta, (size_t)sn * npix + pn + t, f + 1 < f1 && pn + t < npix);
+            const int p2 = t2 * BT;
+            if (f + 2 < f1 && p2 + t < npix) {
                 const size_t k2 = (size_t)s2 * npix + p2 + t;
                 asm volatile("prefetch.global.L2 [%0];" :: "l"(win + 2 * k2));
                 if ((t & 31) == 0) asm volatile("prefetch.global.L2 [%0];" :: "l"(wmeta + k2));
@@ -392,6 +391,8 @@ k_srcmap_win(const float4* __restrict__ win, const int* __restrict__ wmeta, cons
             }
         }
         rec = nxt;
+        s = sn;
+        tile = tn;
     }
     if (lane == 0) bulk_wait_all();
 }
