@@ -188,6 +188,21 @@ int xts_point_src_model_map_wcs(const xts_wcs* wcs, const double* src_sph, int S
                                 const double* partial, int E, void* model_map,
                                 xts_srcmap_info* info, unsigned flags, void* stream);
 
+/* The model map of xts_point_src_model_map_wcs with adaptive cubature of each
+ * pixel in place of the fixed 12-point rule: the Genz-Malik degree-7/5 rule on
+ * the pixel (17 points), regions halved along the dimension with the larger
+ * fourth difference until max_e |R5 - R7| / |R7| <= rtol or max_depth levels.
+ * This is the design of the reference's uncompiled math/genz_malik.hxx:18-195,
+ * math/genz_malik.cxx:66-217 and model_map/model_map.pixel_mean_psf_genz.cxx:21-108,
+ * with rectangular sub-regions and the estimate kept at the depth limit.  The
+ * map is float [S, H, W, E]; rtol in [1e-6, 1], max_depth in [0, 16] (the
+ * reference's design uses 6); only XTS_DEVICE_PTRS applies. */
+int xts_point_src_model_map_wcs_adaptive(const xts_wcs* wcs, const double* src_sph, int S,
+                                         const double* exposure, const double* upsf,
+                                         const double* partial, int E, double rtol, int max_depth,
+                                         float* model_map, xts_srcmap_info* info, unsigned flags,
+                                         void* stream);
+
 /* The three calls of xtsrcmaps/main.cxx:28-30 in one: Exposure::compute_exposure
  * (exposure/exposure.hxx:44-88), Psf::compute_psf_data (psf/psf.compute_psf_data.cxx:7-33)
  * and ModelMap::compute_srcmaps<PointSource> (model_map/model_map.compute_src_maps.cxx:6-22),

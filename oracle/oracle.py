@@ -304,3 +304,41 @@ def convolve_pixel_logsep(pw48, lut, src3) -> np.ndarray:
     o, op = _out(E)
     lib().xo_convolve_pixel_logsep(op, C.c_int(E), pp, lp, s3p)
     return o
+
+
+def adaptive_cubature_map(wcs, src_sph, upsf, rtol: float, max_depth: int = 6):
+    """Pixel-mean PSF [S, H, W, E] by adaptive Genz-Malik cubature (SURVEY row d3;
+    math/genz_malik.hxx:18-85 design, published rule with rectangular sub-regions)
+    and the number of regions evaluated per (source, pixel)."""
+    w = _wcs(wcs)
+    s, sp = _d(src_sph)
+    u, up = _d(upsf)
+    S, E = s.shape[0], u.shape[2]
+    H, W = int(wcs.naxis1), int(wcs.naxis2)
+    out, op = _out((S, H, W, E))
+    n = np.zeros((S, H, W), dtype=np.int32)
+    lib().xo_adaptive_cubature_map(C.byref(w), sp, C.c_int(S), up, C.c_int(E), C.c_double(rtol),
+                                   C.c_int(max_depth), op, n.ctypes.data_as(_ip))
+    return out, n
+
+
+def point_src_model_map_wcs_adaptive(wcs, src_sph, expo, upsf, partial, rtol: float, max_depth: int = 6):
+    """ModelMap::point_src_model_map_wcs with the adaptive cubature in place of the
+    12-point rule; returns the same dict as point_src_model_map_wcs plus 'nregions'."""
+    w = _wcs(wcs)
+    s, sp = _d(src_sph)
+    ex, exp_ = _d(expo)
+    u, up = _d(upsf)
+    p, pp = _d(partial)
+    S, E = ex.shape
+    H, W = int(wcs.naxis1), int(wcs.naxis2)
+    m, mp = _out((S, H, W, E))
+    inv, ip = _out((S, E))
+    fac, fp = _out((S, E))
+    rad, rp = _out((S,))
+    fov = np.zeros(S, dtype=np.int32)
+    n = np.zeros((S, H, W), dtype=np.int32)
+    lib().xo_point_src_model_map_wcs_adaptive(C.byref(w), sp, C.c_int(S), exp_, up, pp, C.c_int(E),
+                                              C.c_double(rtol), C.c_int(max_depth), mp, ip, fp, rp,
+                                              fov.ctypes.data_as(_ip), n.ctypes.data_as(_ip))
+    return dict(map=m, inv_integ=inv, factor=fac, radius=rad, in_fov=fov.astype(bool), nregions=n)

@@ -713,12 +713,12 @@ void xo_map_correction_factor(const double* inv, const double* radius, const int
 }
 
 /* model_map/model_map.point_src_model_map_wcs.cxx:6-45 */
-void xo_point_src_model_map_wcs(const xo_wcs* w, const double* src_sph, int S,
-                                const double* expo, const double* upsf,
-                                const double* partial, int E, double* out,
-                                double* inv, double* factor, double* radius, int* in_fov) {
+/* Steps after the cubature (model_map.point_src_model_map_wcs.cxx:22-44): solid
+ * angle, boundary radius, map integral, exposure, correction factor. */
+static void finish_model_map(const xo_wcs* w, const double* src_sph, int S, const double* expo,
+                             const double* upsf, const double* partial, int E, double* out,
+                             double* inv, double* factor, double* radius, int* in_fov) {
     long Nh = w->naxis1, Nw = w->naxis2;
-    xo_cubature_map(w, Nh, Nw, src_sph, S, upsf, E, out);
     double* om = (double*)malloc(sizeof(double) * Nh * Nw);
     xo_solid_angle(w, Nh, Nw, om);
     for (int s = 0; s < S; ++s)
@@ -734,4 +734,154 @@ void xo_point_src_model_map_wcs(const xo_wcs* w, const double* src_sph, int S,
         for (long p = 0; p < Nh * Nw; ++p)
             for (int e = 0; e < E; ++e) out[((size_t)s * Nh * Nw + p) * E + e] *= factor[(size_t)s * E + e];
     free(om);
+}
+
+void xo_point_src_model_map_wcs(const xo_wcs* w, const double* src_sph, int S,
+                                const double* expo, const double* upsf,
+                                const double* partial, int E, double* out,
+                                double* inv, double* factor, double* radius, int* in_fov) {
+    xo_cubature_map(w, w->naxis1, w->naxis2, src_sph, S, upsf, E, out);
+    finish_model_map(w, src_sph, S, expo, upsf, partial, E, out, inv, factor, radius, in_fov);
+}
+
+/* ---- adaptive cubature: the published Genz-Malik degree-7/5 rule for d = 2
+ * (A.C. Genz, A.A. Malik, J. Comput. Appl. Math. 6 (1980) 295-302; weights as
+ * updated by Bernstein, Espelid and Genz), the design the reference lays out in
+ * math/genz_malik.hxx:18-85 and math/genz_malik.cxx:66-217 (not compiled there).
+ * Differences from that code, which follow the published algorithm instead:
+ * sub-regions are rectangles with a half-width per dimension (region_split at
+ * genz_malik.cxx:189-217 halves one scalar half-width for both dimensions while
+ * splitting only one), and regions still above the tolerance at the depth limit
+ * keep their estimate (integrate_region at genz_malik.hxx:150-194 drops them).
+ * The integrand is the keys-fixed logsep interpolation of the mean PSF at the
+ * pixel's bilinear blend of its corner unit vectors, as for the 12-point rule. */
+static const double GM_L2 = 0.35856858280031809199064515390793749545406372969943071; /* sqrt(9/70) */
+static const double GM_L4 = 0.94868329805051379959966806332981556011586654179756505; /* sqrt(9/10) */
+static const double GM_L5 = 0.68824720161168529772162873429362352512689535661564885; /* sqrt(9/19) */
+
+/* point offsets in half-widths along (dimension 0, dimension 1) */
+static const signed char GM_OFF[17][2] = {
+    {0, 0},
+    {-2, 0}, {0, -2}, {2, 0}, {0, 2},         /* +-l2 on one axis  (code 2) */
+    {-4, 0}, {0, -4}, {4, 0}, {0, 4},         /* +-l4 on one axis  (code 4) */
+    {-4, -4}, {4, -4}, {-4, 4}, {4, 4},       /* (+-l4, +-l4) */
+    {-5, -5}, {-5, 5}, {5, -5}, {5, 5},       /* (+-l5, +-l5) */
+};
+
+void xo_gm_rule(double* w7 /*[17]*/, double* w5 /*[17]*/, double* lam /*[6] by code*/) {
+    const double a = (12824. - 9120. * 2. + 400. * 4.) / 19683., b = 980. / 6561.;
+    const double c = (1820. - 400. * 2.) / 19683., d = 200. / 19683., f = 6859. / 19683. / 4.;
+    const double a5 = (729. - 950. * 2. + 50. * 4.) / 729., b5 = 245. / 486.;
+    const double c5 = (265. - 100. * 2.) / 1458., d5 = 25. / 729.;
+    for (int p = 0; p < 17; ++p) {
+        w7[p] = p == 0 ? a : p < 5 ? b : p < 9 ? c : p < 13 ? d : f;
+        w5[p] = p == 0 ? a5 : p < 5 ? b5 : p < 9 ? c5 : p < 13 ? d5 : 0.;
+    }
+    for (int k = 0; k < 6; ++k) lam[k] = 0.;
+    lam[2] = GM_L2; lam[4] = GM_L4; lam[5] = GM_L5;
+}
+
+/* mean PSF over one pixel [E] by adaptive Genz-Malik cubature; returns the
+ * number of regions evaluated.  abcd: corner unit vectors LL, LR, UR, UL;
+ * dimension 0 runs along the map's first axis (h), dimension 1 along w. */
+int xo_adaptive_pixel(const double* abcd /*[4][3]*/, const double* lut /*[D,E]*/, int E,
+                      const double* src, double rtol, int max_depth, double* mean /*[E]*/) {
+    double w7[17], w5[17], lam[6];
+    xo_gm_rule(w7, w5, lam);
+    struct { double c0, c1, h0, h1; int depth; } stack[64];
+    int top = 0, nreg = 0;
+    stack[top].c0 = 0.; stack[top].c1 = 0.; stack[top].h0 = 1.; stack[top].h1 = 1.; stack[top].depth = 0; ++top;
+    double* f = (double*)malloc(sizeof(double) * 17 * E);
+    for (int e = 0; e < E; ++e) mean[e] = 0.;
+    while (top > 0) {
+        --top;
+        const double c0 = stack[top].c0, c1 = stack[top].c1, h0 = stack[top].h0, h1 = stack[top].h1;
+        const int depth = stack[top].depth;
+        ++nreg;
+        for (int p = 0; p < 17; ++p) {
+            const int o0 = GM_OFF[p][0], o1 = GM_OFF[p][1];
+            const double x0 = c0 + (o0 < 0 ? -lam[-o0] : lam[o0]) * h0;   /* v: along h */
+            const double x1 = c1 + (o1 < 0 ? -lam[-o1] : lam[o1]) * h1;   /* u: along w */
+            const double u = x1, v = x0;
+            const double nn = (1.0 - u) * (1.0 - v), pn = (1.0 + u) * (1.0 - v);
+            const double pp = (1.0 + u) * (1.0 + v), np = (1.0 - u) * (1.0 + v);
+            double q[3];
+            for (int k = 0; k < 3; ++k)
+                q[k] = 0.25 * (nn * abcd[k] + pn * abcd[3 + k] + pp * abcd[6 + k] + np * abcd[9 + k]) - src[k];
+            const double sd = 2.0 * R2D * asin(0.5 * sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]));
+            const double j = sd < 1e-4 ? 1. : 1. + RECIPSTEP * (LN_1E4 + log(sd));
+            int idx = 1 + (int)(unsigned short)j;
+            if (idx > 400) idx = 400;
+            const double t = REDM1 * (sd * 1e4 * exp(SEP_STEP * (2. - idx)) - 1.);
+            const double* YL = lut + (size_t)E * (idx - 1);
+            const double* YR = lut + (size_t)E * idx;
+            for (int e = 0; e < E; ++e) f[p * E + e] = (1.0 - t) * YL[e] + t * YR[e];
+        }
+        const double area = h0 * h1;  /* fraction of the pixel */
+        double rel = 0.;
+        for (int e = 0; e < E; ++e) {
+            double v7 = 0., v5 = 0.;
+            for (int p = 0; p < 17; ++p) { v7 += w7[p] * f[p * E + e]; v5 += w5[p] * f[p * E + e]; }
+            const double err = fabs(v5 - v7);
+            const double r = v7 != 0. ? err / fabs(v7) : (err != 0. ? INFINITY : 0.);
+            if (r > rel) rel = r;
+        }
+        if (rel <= rtol || depth >= max_depth) {
+            for (int e = 0; e < E; ++e) {
+                double v7 = 0.;
+                for (int p = 0; p < 17; ++p) v7 += w7[p] * f[p * E + e];
+                mean[e] += area * v7;
+            }
+            continue;
+        }
+        /* split the dimension with the larger fourth divided difference */
+        double dd[2] = {0., 0.};
+        for (int e = 0; e < E; ++e) {
+            const double f0 = 2. * f[e];
+            dd[0] += fabs((f[1 * E + e] + f[3 * E + e] - f0) - (1. / 7.) * (f[5 * E + e] + f[7 * E + e] - f0));
+            dd[1] += fabs((f[2 * E + e] + f[4 * E + e] - f0) - (1. / 7.) * (f[6 * E + e] + f[8 * E + e] - f0));
+        }
+        const int dim = dd[0] >= dd[1] ? 0 : 1;
+        for (int side = 1; side >= -1; side -= 2) {  /* the lower half is evaluated first */
+            stack[top].c0 = c0; stack[top].c1 = c1; stack[top].h0 = h0; stack[top].h1 = h1;
+            stack[top].depth = depth + 1;
+            if (dim == 0) { stack[top].h0 = 0.5 * h0; stack[top].c0 = c0 + side * 0.5 * h0; }
+            else { stack[top].h1 = 0.5 * h1; stack[top].c1 = c1 + side * 0.5 * h1; }
+            ++top;
+        }
+    }
+    free(f);
+    return nreg;
+}
+
+void xo_adaptive_cubature_map(const xo_wcs* w, const double* src_sph, int S, const double* upsf,
+                              int E, double rtol, int max_depth, double* out /*[S,H,W,E]*/,
+                              int* nregions /*[S,H,W] or NULL*/) {
+    long Nh = w->naxis1, Nw = w->naxis2;
+    for (int s = 0; s < S; ++s) {
+        double src[3];
+        xo_sph2dir(src_sph[2 * s], src_sph[2 * s + 1], src);
+        for (long h = 0; h < Nh; ++h)
+            for (long x = 0; x < Nw; ++x) {
+                double abcd[12];
+                const double ph = 1. + h, pw = 1. + x;
+                xo_pix2dir(w, ph - 0.5, pw - 0.5, abcd);     /* LL */
+                xo_pix2dir(w, ph - 0.5, pw + 0.5, abcd + 3); /* LR */
+                xo_pix2dir(w, ph + 0.5, pw + 0.5, abcd + 6); /* UR */
+                xo_pix2dir(w, ph + 0.5, pw - 0.5, abcd + 9); /* UL */
+                const size_t k = ((size_t)s * Nh + h) * Nw + x;
+                const int n = xo_adaptive_pixel(abcd, upsf + (size_t)s * XO_ND * E, E, src, rtol,
+                                                max_depth, out + k * E);
+                if (nregions) nregions[k] = n;
+            }
+    }
+}
+
+void xo_point_src_model_map_wcs_adaptive(const xo_wcs* w, const double* src_sph, int S,
+                                         const double* expo, const double* upsf,
+                                         const double* partial, int E, double rtol, int max_depth,
+                                         double* out, double* inv, double* factor, double* radius,
+                                         int* in_fov, int* nregions) {
+    xo_adaptive_cubature_map(w, src_sph, S, upsf, E, rtol, max_depth, out, nregions);
+    finish_model_map(w, src_sph, S, expo, upsf, partial, E, out, inv, factor, radius, in_fov);
 }

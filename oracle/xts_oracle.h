@@ -117,6 +117,19 @@ void xo_point_src_model_map_wcs(const xo_wcs* w, const double* src_sph, int S,
                                 double* out /*[S,H,W,E]*/, double* inv_integ,
                                 double* factor, double* radius, int* in_fov);
 
+/* ---- row d3: adaptive Genz-Malik cubature (see xts_oracle.c) ---- */
+void xo_gm_rule(double* w7 /*[17]*/, double* w5 /*[17]*/, double* lam /*[6]*/);
+int xo_adaptive_pixel(const double* abcd /*[4][3]*/, const double* lut /*[D,E]*/, int E,
+                      const double* src3, double rtol, int max_depth, double* mean /*[E]*/);
+void xo_adaptive_cubature_map(const xo_wcs* w, const double* src_sph, int S, const double* upsf,
+                              int E, double rtol, int max_depth, double* out /*[S,H,W,E]*/,
+                              int* nregions /*[S,H,W] or NULL*/);
+void xo_point_src_model_map_wcs_adaptive(const xo_wcs* w, const double* src_sph, int S,
+                                         const double* expo, const double* upsf,
+                                         const double* partial, int E, double rtol, int max_depth,
+                                         double* out, double* inv_integ, double* factor,
+                                         double* radius, int* in_fov, int* nregions);
+
 #ifdef __cplusplus
 }
 #endif

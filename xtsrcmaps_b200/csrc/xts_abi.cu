@@ -520,6 +520,45 @@ int xts_point_src_model_map_wcs(const xts_wcs* wcs, const double* src_sph, int S
     return run_srcmap(sg, a, model_map, npix, f64);
 }
 
+int xts_point_src_model_map_wcs_adaptive(const xts_wcs* wcs, const double* src_sph, int S,
+                                         const double* exposure, const double* upsf,
+                                         const double* partial, int E, double rtol, int max_depth,
+                                         float* model_map, xts_srcmap_info* info, unsigned flags,
+                                         void* stream) {
+    XTS_ENTER();
+    if (!wcs || wcs->naxis1 <= 0 || wcs->naxis2 <= 0 || (wcs->proj != 0 && wcs->proj != 1) ||
+        wcs->cdelt1 == 0. || wcs->cdelt2 == 0.)
+        return set_error(XTS_ERR_ARG, "point_src_model_map_wcs_adaptive: bad WCS (CAR/AIT, nonzero CDELT)");
+    if (S < 0 || E <= 0 || E > 256 || (S > 0 && (!src_sph || !exposure || !upsf || !partial || !model_map)))
+        return set_error(XTS_ERR_ARG, "point_src_model_map_wcs_adaptive: null argument or bad size (E <= 256)");
+    if (!(rtol >= 1e-6 && rtol <= 1.0) || max_depth < 0 || max_depth > 16)
+        return set_error(XTS_ERR_ARG, "point_src_model_map_wcs_adaptive: rtol must lie in [1e-6, 1] and "
+                                      "max_depth in [0, 16]");
+    if ((long long)wcs->naxis1 * wcs->naxis2 * E > 0xffffffffLL || S > 65535)
+        return set_error(XTS_ERR_ARG, "point_src_model_map_wcs_adaptive: map or source count too large");
+    if (flags & ~(unsigned)XTS_DEVICE_PTRS)
+        return set_error(XTS_ERR_ARG, "point_src_model_map_wcs_adaptive: only XTS_DEVICE_PTRS applies");
+    const size_t npix = (size_t)wcs->naxis1 * wcs->naxis2;
+    Stager sg{(flags & XTS_DEVICE_PTRS) != 0, stream ? (cudaStream_t)stream : g_ctx.stream};
+    SrcmapDev a;
+    a.wcs = *wcs;
+    a.src_sph = sg.in(src_sph, (size_t)2 * S); a.S = S;
+    a.exposure = sg.in(exposure, (size_t)S * E);
+    a.upsf = sg.in(upsf, (size_t)S * ND * E);
+    a.partial = sg.in(partial, (size_t)S * ND * E); a.E = E;
+    a.out_f64 = false;
+    a.out = sg.out(model_map, (size_t)S * npix * E);
+    a.inv_integ = info ? sg.out(info->inv_map_integral, (size_t)S * E) : nullptr;
+    a.correction = info ? sg.out(info->correction, (size_t)S * E) : nullptr;
+    a.radius = info ? sg.out(info->psf_radius, (size_t)S) : nullptr;
+    a.in_fov = info ? sg.out(info->in_fov, (size_t)S) : nullptr;
+    a.kernel = SRCMAP_WINDOWS;
+    a.adaptive = true;
+    a.rtol = rtol;
+    a.max_depth = max_depth;
+    return run_srcmap(sg, a, model_map, npix, false);
+}
+
 int xts_point_source_maps(const xts_expcube* cube, const xts_expcube* wcube, const double* logEs,
                           int E, const double* src_sph, int S, const xts_grid* aeff_front,
                           const xts_grid* aeff_back, const xts_grid* psf_front,

@@ -1,0 +1,381 @@
+// xts_adaptive.cu -- adaptive cubature of the pixel-mean PSF:
+// the published Genz-Malik degree-7/5 rule for two dimensions (A.C. Genz,
+// A.A. Malik, J. Comput. Appl. Math. 6 (1980) 295-302; weights as updated by
+// Bernstein, Espelid and Genz), the design the reference lays out in
+// math/genz_malik.hxx:18-85 and math/genz_malik.cxx:66-217 (not compiled there),
+// with rectangular sub-regions and the estimate kept at the depth limit.
+//
+// Work is scheduled by region, not by pixel, so that pixels needing many regions
+// (next to the source) do not hold up the others: level 0 evaluates every
+// (source, pixel)'s whole-pixel region, one thread each, and writes accepted
+// pixels' means; an unaccepted region pushes its two halves onto a device-side
+// queue.  Each further level is one persistent grid-stride launch over the
+// previous level's queue, one region per thread; accepted regions add area * R7
+// into their pixel's mean with FP32 atomics.  The queue has a fixed capacity; a
+// region whose halves do not fit is accepted as it is.
+//
+// A region's 17 points give LUT rows and interpolation weights exactly as the
+// 12-point rule's do (xts_point.cuh: FP64 chord of the corner-vector blend,
+// exact row, per-row t polynomial).  When they span at most AW consecutive rows,
+// four row windows are formed (the degree-7 value, degree-5 minus degree-7, and
+// the two fourth divided differences that choose the split dimension) and dotted
+// with the source's FP32 mean-PSF rows for every energy; otherwise the points
+// are evaluated one by one.  A region is accepted when
+// max_e |R5 - R7| / |R7| <= rtol or at the depth limit; otherwise it is halved
+// along the dimension with the larger summed fourth difference.
+//
+// k_adaptive_integral then sums mean * solid angle over the pixels inside the
+// boundary radius (FP64, fixed order), k_correction_sums forms the scales, and
+// k_scale_map writes value = mean * solid angle * exposure * correction.
+#include "xts_point.cuh"
+
+namespace xts {
+
+constexpr int AT = 256;     // threads per block
+constexpr int AW = 8;       // rows of a region window
+constexpr int AMAXD = 16;   // deepest subdivision accepted by the entry point
+
+// Points of the rule in half-widths along (dimension 0 = map axis h, dimension 1
+// = map axis w) and the coefficients of the four windows per point.
+struct GmRule {
+    float off0[17], off1[17];
+    float w7[17], wd[17], d0[17], d1[17];
+};
+static __constant__ GmRule c_gm;
+static int upload_gm(cudaStream_t st) {
+    static int dev_done = -1;
+    int dev = -1;
+    cudaGetDevice(&dev);
+    if (dev_done == dev) return XTS_OK;
+    const double l2 = sqrt(9. / 70.), l4 = sqrt(9. / 10.), l5 = sqrt(9. / 19.);
+    // centre; +-l2 on each axis; +-l4 on each axis; (+-l4, +-l4); (+-l5, +-l5)
+    const double o[17][2] = {{0, 0},     {-l2, 0},   {0, -l2},  {l2, 0},   {0, l2},   {-l4, 0},
+                             {0, -l4},   {l4, 0},    {0, l4},   {-l4, -l4}, {l4, -l4}, {-l4, l4},
+                             {l4, l4},   {-l5, -l5}, {-l5, l5}, {l5, -l5},  {l5, l5}};
+    const double a7 = (12824. - 9120. * 2. + 400. * 4.) / 19683., b7 = 980. / 6561.;
+    const double c7 = (1820. - 400. * 2.) / 19683., d7 = 200. / 19683., f7 = 6859. / 19683. / 4.;
+    const double a5 = (729. - 950. * 2. + 50. * 4.) / 729., b5 = 245. / 486.;
+    const double c5 = (265. - 100. * 2.) / 1458., d5 = 25. / 729.;
+    GmRule g;
+    for (int p = 0; p < 17; ++p) {
+        const double w7 = p == 0 ? a7 : p < 5 ? b7 : p < 9 ? c7 : p < 13 ? d7 : f7;
+        const double w5 = p == 0 ? a5 : p < 5 ? b5 : p < 9 ? c5 : p < 13 ? d5 : 0.;
+        g.off0[p] = (float)o[p][0];
+        g.off1[p] = (float)o[p][1];
+        g.w7[p] = (float)w7;
+        g.wd[p] = (float)(w5 - w7);
+        // fourth differences: (f(-l2) + f(+l2) - 2 f0) - (l2/l4)^2 (f(-l4) + f(+l4) - 2 f0)
+        double e0 = 0., e1 = 0.;
+        if (p == 0) e0 = e1 = -2. + 2. / 7.;
+        if (p == 1 || p == 3) e0 = 1.;
+        if (p == 5 || p == 7) e0 = -1. / 7.;
+        if (p == 2 || p == 4) e1 = 1.;
+        if (p == 6 || p == 8) e1 = -1. / 7.;
+        g.d0[p] = (float)e0;
+        g.d1[p] = (float)e1;
+    }
+    XTS_CUDA(cudaMemcpyToSymbolAsync(c_gm, &g, sizeof(g), 0, cudaMemcpyHostToDevice, st));
+    XTS_CUDA(cudaStreamSynchronize(st));
+    dev_done = dev;
+    return XTS_OK;
+}
+
+// One queued region: its pixel (source * npix + pixel) and its rectangle in the
+// pixel's [-1, 1]^2 parameter square.
+struct QRegion { int sp; float c0, c1, h0, h1; };
+
+constexpr size_t AO_SQ = 0;
+constexpr size_t AO_COEF = (8 * (ND + 1) + 15) / 16 * 16;
+constexpr size_t AO_WIN = AO_COEF + sizeof(float4) * 2 * ND;  // [4][AW][AT] floats
+constexpr size_t A_SMEM = AO_WIN + sizeof(float) * 4 * AW * AT;
+
+// Evaluates one region.  Returns true when it is accepted, after adding
+// area * R7 into mean[e] (atomically when `atomic`); otherwise sets *dim.
+__device__ __noinline__ bool gm_region(const PixGeom& g, float c0, float c1, float h0, float h1, bool last,
+                                          const double* sq, const float4* scoef, float* wk, const float* Y, int E,
+                                          float rtol, float* mean, bool atomic, int* dim) {
+    int ix[17];
+    float tt[17];
+    int rmin = ND, rmax = 0;
+#pragma unroll
+    for (int p = 0; p < 17; ++p) {
+        const double u = c1 + c_gm.off1[p] * h1;  // along w
+        const double v = c0 + c_gm.off0[p] * h0;  // along h
+        const double x = fma(g.Dx, u * v, fma(g.Cx, v, fma(g.Bx, u, g.Ax)));
+        const double y = fma(g.Dy, u * v, fma(g.Cy, v, fma(g.By, u, g.Ay)));
+        const double z = fma(g.Dz, u * v, fma(g.Cz, v, fma(g.Bz, u, g.Az)));
+        ix[p] = point_row(fma(x, x, fma(y, y, z * z)), sq, scoef, &tt[p]);
+        rmin = min(rmin, ix[p] - 1);
+        rmax = max(rmax, ix[p]);
+    }
+    const float area = h0 * h1;  // fraction of the pixel
+    const int nr = rmax - rmin + 1;
+    const bool windowed = nr <= AW;
+    float w7[AW], wd[AW], e0[AW], e1[AW];
+    if (windowed) {  // the four row windows of this region
+#pragma unroll
+        for (int j = 0; j < 4 * AW; ++j) wk[j * AT] = 0.f;
+#pragma unroll
+        for (int p = 0; p < 17; ++p) {
+            const int r = ix[p] - 1 - rmin;
+            const float a = 1.f - tt[p], b = tt[p];
+            wk[(0 * AW + r) * AT] += a * c_gm.w7[p];
+            wk[(0 * AW + r + 1) * AT] += b * c_gm.w7[p];
+            wk[(1 * AW + r) * AT] += a * c_gm.wd[p];
+            wk[(1 * AW + r + 1) * AT] += b * c_gm.wd[p];
+            wk[(2 * AW + r) * AT] += a * c_gm.d0[p];
+            wk[(2 * AW + r + 1) * AT] += b * c_gm.d0[p];
+            wk[(3 * AW + r) * AT] += a * c_gm.d1[p];
+            wk[(3 * AW + r + 1) * AT] += b * c_gm.d1[p];
+        }
+#pragma unroll
+        for (int j = 0; j < AW; ++j) {
+            w7[j] = wk[(0 * AW + j) * AT];
+            wd[j] = wk[(1 * AW + j) * AT];
+            e0[j] = wk[(2 * AW + j) * AT];
+            e1[j] = wk[(3 * AW + j) * AT];
+        }
+    }
+    const float* y0 = Y + (size_t)rmin * E;
+    // R7, R5 - R7 and the two fourth differences at energy e: from the windows,
+    // or point by point when the rows are too far apart
+    auto rule = [&](int e, float& v7, float& vd, float& a0, float& a1) {
+        v7 = vd = a0 = a1 = 0.f;
+        if (windowed) {
+#pragma unroll
+            for (int j = 0; j < AW; ++j) {
+                if (j < nr) {
+                    const float yv = __ldg(y0 + (size_t)j * E + e);
+                    v7 = fmaf(w7[j], yv, v7);
+                    vd = fmaf(wd[j], yv, vd);
+                    a0 = fmaf(e0[j], yv, a0);
+                    a1 = fmaf(e1[j], yv, a1);
+                }
+            }
+        } else {
+            for (int p = 0; p < 17; ++p) {
+                const float* yl = Y + (size_t)(ix[p] - 1) * E + e;
+                const float f = fmaf(tt[p], __ldg(yl + E) - __ldg(yl), __ldg(yl));
+                v7 = fmaf(c_gm.w7[p], f, v7);
+                vd = fmaf(c_gm.wd[p], f, vd);
+                a0 = fmaf(c_gm.d0[p], f, a0);
+                a1 = fmaf(c_gm.d1[p], f, a1);
+            }
+        }
+    };
+    float rel = 0.f, dd0 = 0.f, dd1 = 0.f;
+    if (!last) {
+        for (int e = 0; e < E; ++e) {
+            float v7, vd, a0, a1;
+            rule(e, v7, vd, a0, a1);
+            const float r = fabsf(vd) <= rtol * fabsf(v7) ? 0.f : (v7 != 0.f ? fabsf(vd) / fabsf(v7) : 3.4e38f);
+            rel = fmaxf(rel, r);
+            dd0 += fabsf(a0);
+            dd1 += fabsf(a1);
+        }
+    }
+    if (last || rel <= rtol) {
+        for (int e = 0; e < E; ++e) {
+            float v7, vd, a0, a1;
+            rule(e, v7, vd, a0, a1);
+            if (atomic) atomicAdd(mean + e, area * v7);
+            else mean[e] = area * v7;
+        }
+        return true;
+    }
+    *dim = dd0 >= dd1 ? 0 : 1;
+    return false;
+}
+
+// Pushes the two halves of a region (lower half first in the queue), or returns
+// false when the queue is full.
+__device__ __forceinline__ bool push_halves(QRegion* q, int* qcount, int qcap, int sp, float c0, float c1,
+                                            float h0, float h1, int dim) {
+    const int k = atomicAdd(qcount, 2);
+    if (k + 2 > qcap) return false;
+    QRegion a {sp, c0, c1, h0, h1}, b = a;
+    if (dim == 0) {
+        a.h0 = b.h0 = 0.5f * h0;
+        a.c0 = c0 - 0.5f * h0;
+        b.c0 = c0 + 0.5f * h0;
+    } else {
+        a.h1 = b.h1 = 0.5f * h1;
+        a.c1 = c1 - 0.5f * h1;
+        b.c1 = c1 + 0.5f * h1;
+    }
+    q[k] = a;
+    q[k + 1] = b;
+    return true;
+}
+
+__device__ __forceinline__ void load_tables(const SepTab* septab, double* sq, float4* scoef) {
+    for (int k = threadIdx.x; k < ND + 1; k += blockDim.x) sq[k] = septab->q[k];
+    for (int k = threadIdx.x; k < 2 * ND; k += blockDim.x) scoef[k] = ((const float4*)septab->coef)[k];
+    __syncthreads();
+}
+
+// Level 0: one thread per (source, pixel), the whole pixel as one region.
+__global__ void __launch_bounds__(AT, 2)
+k_adaptive_level0(const double* __restrict__ corners, const SrcInfo* __restrict__ info,
+                  const SepTab* __restrict__ septab, const float* __restrict__ lut, int H, int W, int E, float rtol,
+                  int max_depth, float* __restrict__ mean, QRegion* __restrict__ q, int* qcount, int qcap) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* sq = (double*)(smem + AO_SQ);
+    float4* scoef = (float4*)(smem + AO_COEF);
+    float* wk = (float*)(smem + AO_WIN) + threadIdx.x;
+    load_tables(septab, sq, scoef);
+    const int s = blockIdx.y, npix = H * W;
+    const int pix = blockIdx.x * AT + threadIdx.x;
+    if (pix >= npix) return;
+    const SrcInfo si = info[s];
+    const int h = pix / W, w = pix - h * W;
+    const PixGeom g = pixel_geom(corners, W + 1, h, w, si);
+    const int sp = s * npix + pix;
+    float* m = mean + (size_t)sp * E;
+    int dim = 0;
+    if (gm_region(g, 0.f, 0.f, 1.f, 1.f, max_depth == 0, sq, scoef, wk, lut + (size_t)s * ND * E, E, rtol, m,
+                  false, &dim))
+        return;
+    for (int e = 0; e < E; ++e) m[e] = 0.f;
+    if (!push_halves(q, qcount, qcap, sp, 0.f, 0.f, 1.f, 1.f, dim))  // queue full: keep the estimate
+        gm_region(g, 0.f, 0.f, 1.f, 1.f, true, sq, scoef, wk, lut + (size_t)s * ND * E, E, rtol, m, false, &dim);
+}
+
+// Level >= 1: persistent grid-stride over the previous level's queue.
+__global__ void __launch_bounds__(AT, 2)
+k_adaptive_level(const double* __restrict__ corners, const SrcInfo* __restrict__ info,
+                 const SepTab* __restrict__ septab, const float* __restrict__ lut, int H, int W, int E, float rtol,
+                 int level, int max_depth, float* __restrict__ mean, const QRegion* __restrict__ qin,
+                 const int* qin_count, QRegion* __restrict__ qout, int* qout_count, int qcap) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* sq = (double*)(smem + AO_SQ);
+    float4* scoef = (float4*)(smem + AO_COEF);
+    float* wk = (float*)(smem + AO_WIN) + threadIdx.x;
+    load_tables(septab, sq, scoef);
+    const int n = min(*qin_count, qcap);
+    const int npix = H * W;
+    const bool last = level >= max_depth;
+    for (int k = blockIdx.x * AT + threadIdx.x; k < n; k += gridDim.x * AT) {
+        const QRegion r = qin[k];
+        const int s = r.sp / npix, pix = r.sp - s * npix;
+        const SrcInfo si = info[s];
+        const int h = pix / W, w = pix - h * W;
+        const PixGeom g = pixel_geom(corners, W + 1, h, w, si);
+        const float* Y = lut + (size_t)s * ND * E;
+        float* m = mean + (size_t)r.sp * E;
+        int dim = 0;
+        if (gm_region(g, r.c0, r.c1, r.h0, r.h1, last, sq, scoef, wk, Y, E, rtol, m, true, &dim)) continue;
+        if (!push_halves(qout, qout_count, qcap, r.sp, r.c0, r.c1, r.h0, r.h1, dim))
+            gm_region(g, r.c0, r.c1, r.h0, r.h1, true, sq, scoef, wk, Y, E, rtol, m, true, &dim);
+    }
+}
+
+// c7 on the adaptive map: per block (chunk, source) the FP64 sums over pixels
+// inside the boundary radius of mean * solid angle, in a fixed order.
+__global__ void __launch_bounds__(AT) k_adaptive_integral(const double* __restrict__ centers,
+                                                          const double* __restrict__ omega,
+                                                          const SrcInfo* __restrict__ info,
+                                                          const float* __restrict__ mean, int H, int W, int E,
+                                                          int nch, double* __restrict__ sums_out) {
+    __shared__ double part[AT];
+    const int s = blockIdx.y, t = threadIdx.x;
+    const SrcInfo si = info[s];
+    const int npix = H * W, W1 = W + 1;
+    double ch2 = 2.0 * sin(0.5 * si.radius_rad);
+    ch2 *= ch2;
+    // thread (g, e): energy e over pixels g, g + G, ... of the block's range
+    const int G = AT / E, g = t / E, e = t - g * E;
+    const int p_lo = (int)((long long)npix * blockIdx.x / nch), p_hi = (int)((long long)npix * (blockIdx.x + 1) / nch);
+    double acc = 0.;
+    if (si.in_fov && t < G * E) {
+        for (int pix = p_lo + g; pix < p_hi; pix += G) {
+            const int h = pix / W, w = pix - h * W;
+            const double* c = centers + 3 * (h * W1 + w);
+            const double x = si.dir[0] - c[0], y = si.dir[1] - c[1], z = si.dir[2] - c[2];
+            const double d2 = x * x + y * y + z * z;
+            bool inside;
+            if (d2 < ch2 * (1.0 - 1e-12)) inside = true;
+            else if (d2 > ch2 * (1.0 + 1e-12)) inside = false;
+            else inside = dir_diff(si.dir, c) <= si.radius_rad;
+            if (inside) acc += (double)mean[((size_t)s * npix + pix) * E + e] * omega[pix];
+        }
+    }
+    part[t] = acc;
+    __syncthreads();
+    for (int ee = t; ee < E; ee += AT) {
+        double v = 0.;
+        for (int gg = 0; gg < G; ++gg) v += part[gg * E + ee];
+        sums_out[((size_t)s * nch + blockIdx.x) * E + ee] = v;
+    }
+}
+
+// c8 + c10 and the solid angle: value = mean * omega * exposure * correction.
+__global__ void k_scale_map(float* __restrict__ out, const double* __restrict__ omega,
+                            const double* __restrict__ scale, int npix, int E) {
+    __shared__ float sc[256];
+    const int s = blockIdx.y;
+    for (int e = threadIdx.x; e < E; e += blockDim.x) sc[e] = (float)scale[(size_t)s * E + e];
+    __syncthreads();
+    const unsigned n = (unsigned)npix * (unsigned)E;
+    float* o = out + (size_t)s * n;
+    for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const unsigned pix = k / (unsigned)E;
+        o[k] = (float)((double)o[k] * omega[pix]) * sc[k - pix * (unsigned)E];
+    }
+}
+
+bool srcmap_adaptive_supported(int E) { return E >= 1 && E <= 256; }
+
+int launch_adaptive_map(const double* corners, const double* centers, const double* omega, const SrcInfo* info,
+                        const double* upsf, int S, int H, int W, int E, double rtol, int max_depth, int nch,
+                        double* sums, float* out, cudaStream_t st) {
+    int rc = upload_gm(st);
+    if (rc) return rc;
+    const SepTab* tab = nullptr;
+    rc = build_septab(st, &tab);
+    if (rc) return rc;
+    const int npix = H * W;
+    // the mean PSF rows in FP32, [S][401][E]
+    float* lut = (float*)workspace(W_LUT, sizeof(float) * (size_t)S * ND * E + 16);
+    // two region queues (ping-pong) and their counters
+    long long cap = 4LL * S * npix;
+    cap = cap < (1 << 20) ? (1 << 20) : cap;
+    cap = cap > (1 << 26) ? (1 << 26) : cap;
+    QRegion* q = (QRegion*)workspace(W_SPARSE, sizeof(QRegion) * 2 * (size_t)cap + 16);
+    int* counts = (int*)workspace(W_WMETA, sizeof(int) * 64);
+    if (!lut || !q || !counts) return XTS_ERR_OOM;
+    XTS_LAUNCH("k_lut_scaled", st, k_lut_scaled<<<lut_scaled_grid(S), 256, 0, st>>>(upsf, nullptr, S, E, E, lut,
+                                                                                       nullptr, nullptr));
+    XTS_CUDA(cudaFuncSetAttribute(k_adaptive_level0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A_SMEM));
+    XTS_CUDA(cudaFuncSetAttribute(k_adaptive_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A_SMEM));
+    XTS_CUDA(cudaMemsetAsync(counts, 0, sizeof(int) * (AMAXD + 2), st));
+    XTS_LAUNCH("k_adaptive_map", st, k_adaptive_level0<<<dim3((npix + AT - 1) / AT, S), AT, A_SMEM, st>>>(
+                                         corners, info, tab, lut, H, W, E, (float)rtol, max_depth, out, q, counts,
+                                         (int)cap));
+    int dev = 0, nsm = 148, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    XTS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adaptive_level, AT, A_SMEM));
+    const int G = nsm * (per_sm > 0 ? per_sm : 1);
+    for (int level = 1; level <= max_depth; ++level) {
+        QRegion* qin = q + (size_t)((level - 1) & 1) * cap;
+        QRegion* qout = q + (size_t)(level & 1) * cap;
+        XTS_LAUNCH("k_adaptive_map", st, k_adaptive_level<<<G, AT, A_SMEM, st>>>(
+                                             corners, info, tab, lut, H, W, E, (float)rtol, level, max_depth, out,
+                                             qin, counts + level - 1, qout, counts + level, (int)cap));
+    }
+    XTS_LAUNCH("k_adaptive_integral", st, k_adaptive_integral<<<dim3(nch, S), AT, 0, st>>>(centers, omega, info,
+                                                                                          out, H, W, E, nch, sums));
+    return XTS_OK;
+}
+
+int launch_scale_map(float* out, const double* omega, const double* scale, int S, int npix, int E,
+                     cudaStream_t st) {
+    const unsigned n = (unsigned)npix * (unsigned)E;
+    unsigned gx = (n + 255) / 256;
+    if (gx > 1024) gx = 1024;
+    XTS_LAUNCH("k_scale_map", st, k_scale_map<<<dim3(gx, S), 256, 0, st>>>(out, omega, scale, npix, E));
+    return XTS_OK;
+}
+
+}  // namespace xts

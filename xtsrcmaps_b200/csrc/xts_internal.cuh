@@ -123,6 +123,10 @@ struct SrcmapDev {
     int chunk_sources = 0;
     int (*on_chunk)(void* ctx, int s0, int n, cudaStream_t st) = nullptr;
     void* on_chunk_ctx = nullptr;
+    // adaptive Genz-Malik cubature in place of the 12-point rule (FP32 map)
+    bool adaptive = false;
+    double rtol = 1e-4;
+    int max_depth = 6;
 };
 enum { SRCMAP_WINDOWS = 0, SRCMAP_ONEPASS = 1, SRCMAP_TCGEN05 = 2 };
 int launch_srcmap(const SrcmapDev& a, cudaStream_t st);
@@ -138,6 +142,12 @@ int launch_correction(const double* hist, int nch, const SrcInfo* info, int S, c
                       double* inv_integ, double* correction, double* radius, int* in_fov,
                       cudaStream_t st);
 bool srcmap_win_supported(int E);
+bool srcmap_adaptive_supported(int E);
+int launch_adaptive_map(const double* corners, const double* centers, const double* omega, const SrcInfo* info,
+                        const double* upsf, int S, int H, int W, int E, double rtol, int max_depth, int nch,
+                        double* sums, float* out, cudaStream_t st);
+int launch_scale_map(float* out, const double* omega, const double* scale, int S, int npix, int E,
+                     cudaStream_t st);
 int launch_srcmap_win(const double* corners, const double* centers, const double* omega,
                       const SrcInfo* info, int S, int H, int W, int E,
                       const double* upsf, const double* partial, const double* exposure,

@@ -237,7 +237,8 @@ __device__ __forceinline__ double point_q(const PixGeom& g, int p) {
 }
 
 // Scaled FP32 table Y'[s][d][e] = uPsf * (exposure * correction), energies
-// padded to Epad with zeros; launched as lut_scaled_grid(S) x 256 threads.  With hi/lo given, also the 3xTF32 split:
+// padded to Epad with zeros (scale NULL: uPsf itself); launched as
+// lut_scaled_grid(S) x 256 threads.  With hi/lo given, also the 3xTF32 split:
 // hi = tf32(Y'), lo = Y' - hi.
 static __global__ void k_lut_scaled(const double* upsf, const double* scale, int S, int E, int Epad,
                              float* lut, float* hi, float* lo) {
@@ -246,7 +247,7 @@ static __global__ void k_lut_scaled(const double* upsf, const double* scale, int
     const unsigned s = sd / ND;
     for (int e = threadIdx.x & 31; e < Epad; e += 32) {
         const size_t k = (size_t)sd * Epad + e;
-        const float v = e < E ? (float)(upsf[(size_t)sd * E + e] * scale[(size_t)s * E + e]) : 0.f;
+        const float v = e < E ? (float)(upsf[(size_t)sd * E + e] * (scale ? scale[(size_t)s * E + e] : 1.0)) : 0.f;
         if (lut) lut[k] = v;
         if (hi) {
             unsigned hb;

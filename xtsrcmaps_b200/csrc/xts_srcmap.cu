@@ -404,6 +404,29 @@ __global__ void __launch_bounds__(256) k_map_integral_hist(const double* corners
     for (int r = threadIdx.x; r < ND; r += blockDim.x) out[r] = hist[r];
 }
 
+// c9 map_correction_factor (model_map.map_correction_factor.cxx:3-53): the PSF
+// integral out to the boundary radius over the whole bin at the radius's lower
+// index (fast_separation_lower_index, psf.fast_separation_lower_index.cxx:5-22,
+// with its `v < 1.` rule), capped at 1, times 1/map integral; 1 out of FOV.
+__device__ double correction_factor(const SrcInfo& si, const double* U, const double* partial_s, int E, int e,
+                                    double inv) {
+    if (!si.in_fov) return 1.0;
+    const double v0 = si.radius_deg;
+    const int li = v0 < 1. ? 1 : (int)floor(1. + log(1e4 * v0) * RECIPSTEP);
+    const int d = li >= ND - 2 ? ND - 2 : li;
+    const double xstep = log(70. / 1e-4) / (400 - 1.);
+    const double t1 = (d == 0 ? 0. : 1e-4 * exp((d - 1) * xstep)) * D2R;
+    const double t2 = (1e-4 * exp(d * xstep)) * D2R;
+    const double y1 = TWOPI * U[(size_t)d * E + e] * sin(t1);
+    const double y2 = TWOPI * U[(size_t)(d + 1) * E + e] * sin(t2);
+    const double m = (y2 - y1) / (t2 - t1);
+    const double b = y1 - t1 * m;
+    const double v = 0.5 * m * (t2 * t2 - t1 * t1) + b * (t2 - t1);
+    double integ = v + partial_s[(size_t)d * E + e];
+    integ = integ > 1.0 ? 1.0 : integ;
+    return integ * inv;
+}
+
 // c7 (1/sum) + c9 (containment factor) + c8/c10 folded into one per-(s,e) scale.
 // Block (s, group of 8 energies): fold the source's chunk histograms, then one
 // warp per energy.
@@ -435,25 +458,8 @@ __global__ void __launch_bounds__(256) k_correction_hist(const double* hist_in, 
             for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
         }
         if (lane != 0) return;
-        double inv = sum != 0. ? 1.0 / sum : sum;
-        double factor;
-        if (!si.in_fov) factor = 1.0;
-        else {
-            double v0 = si.radius_deg;
-            int li = v0 < 1. ? 1 : (int)floor(1. + log(1e4 * v0) * RECIPSTEP);
-            int d = li >= ND - 2 ? ND - 2 : li;
-            const double xstep = log(70. / 1e-4) / (400 - 1.);
-            double t1 = (d == 0 ? 0. : 1e-4 * exp((d - 1) * xstep)) * D2R;
-            double t2 = (1e-4 * exp(d * xstep)) * D2R;
-            double y1 = TWOPI * U[(size_t)d * E + e] * sin(t1);
-            double y2 = TWOPI * U[(size_t)(d + 1) * E + e] * sin(t2);
-            double m = (y2 - y1) / (t2 - t1);
-            double b = y1 - t1 * m;
-            double v = 0.5 * m * (t2 * t2 - t1 * t1) + b * (t2 - t1);
-            double integ = v + partial[(size_t)s * ND * E + (size_t)d * E + e];
-            integ = integ > 1.0 ? 1.0 : integ;
-            factor = integ * inv;
-        }
+        const double inv = sum != 0. ? 1.0 / sum : sum;
+        const double factor = correction_factor(si, U, partial + (size_t)s * ND * E, E, e, inv);
         scale[i] = expo[i] * factor;
         if (inv_out) inv_out[i] = inv;
         if (fac_out) fac_out[i] = factor;
@@ -471,6 +477,51 @@ int launch_correction(const double* hist, int nch, const SrcInfo* info, int S, c
     XTS_LAUNCH("k_correction", st, k_correction_hist<<<dim3(S, (E + 7) / 8), 256, 0, st>>>(hist, nch, info, upsf, partial, exposure, E,
                                                                         scale, inv_integ, correction, radius, in_fov));
     return XTS_OK;
+}
+
+// c7 + c9 for the adaptive map, whose per-block FP64 sums over the pixels inside
+// the boundary radius [S][nch][E] are folded in a fixed order.
+__global__ void __launch_bounds__(256) k_correction_sums(const double* sums, int nch, const SrcInfo* info,
+                                                         const double* upsf, const double* partial,
+                                                         const double* expo, int E, double* scale,
+                                                         double* inv_out, double* fac_out,
+                                                         double* rad_out, int* fov_out) {
+    const int s = blockIdx.x;
+    const SrcInfo si = info[s];
+    const double* U = upsf + (size_t)s * ND * E;
+    for (int e = threadIdx.x; e < E; e += blockDim.x) {
+        const int i = s * E + e;
+        double sum = 0.;
+        if (si.in_fov)
+            for (int c = 0; c < nch; ++c) sum += sums[((size_t)s * nch + c) * E + e];
+        const double inv = sum != 0. ? 1.0 / sum : sum;
+        const double factor = correction_factor(si, U, partial + (size_t)s * ND * E, E, e, inv);
+        scale[i] = expo[i] * factor;
+        if (inv_out) inv_out[i] = inv;
+        if (fac_out) fac_out[i] = factor;
+        if (e == 0) {
+            if (rad_out) rad_out[s] = si.radius_deg;
+            if (fov_out) fov_out[s] = si.in_fov;
+        }
+    }
+}
+
+// The model map with adaptive cubature: pixel means * solid angle, map integral
+// sums, correction, then one scaling pass over the map.
+static int launch_srcmap_adaptive(const SrcmapDev& a, const double* corners, const double* centers,
+                                  const double* omega, const SrcInfo* info, double* scale, int nch,
+                                  cudaStream_t st) {
+    const int H = (int)a.wcs.naxis1, W = (int)a.wcs.naxis2, S = a.S, E = a.E;
+    const int npix = H * W;
+    double* sums = (double*)workspace(W_PARTSUM, sizeof(double) * (size_t)S * nch * E + 8);
+    if (!sums) return XTS_ERR_OOM;
+    int rc = launch_adaptive_map(corners, centers, omega, info, a.upsf, S, H, W, E, a.rtol, a.max_depth, nch,
+                                 sums, (float*)a.out, st);
+    if (rc) return rc;
+    XTS_LAUNCH("k_correction", st, k_correction_sums<<<S, 128, 0, st>>>(sums, nch, info, a.upsf, a.partial,
+                                                                        a.exposure, E, scale, a.inv_integ,
+                                                                        a.correction, a.radius, a.in_fov));
+    return launch_scale_map((float*)a.out, omega, scale, S, npix, E, st);
 }
 
 int srcmap_status(cudaStream_t st) {
@@ -512,6 +563,11 @@ int launch_srcmap(const SrcmapDev& a, cudaStream_t st) {
     XTS_LAUNCH("k_solid_angle", st, k_solid_angle<<<(npix + 127) / 128, 128, 0, st>>>(centers, H, W, omega));
     if (S == 0) return XTS_OK;
     XTS_LAUNCH("k_boundary", st, k_boundary<<<S, 128, 0, st>>>(w, a.src_sph, H, W, corners, info));
+    if (a.adaptive) {
+        if (a.out_f64 || !srcmap_adaptive_supported(E))
+            return set_error(XTS_ERR_ARG, "adaptive cubature: FP32 maps with E <= 256 only");
+        return launch_srcmap_adaptive(a, corners, centers, omega, info, scale, nch, st);
+    }
     if (!a.out_f64 && a.kernel == SRCMAP_WINDOWS && srcmap_win_supported(E)) {
         int* status = (int*)workspace(W_MISC, 64);
         if (!status) return XTS_ERR_OOM;
