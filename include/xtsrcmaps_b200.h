@@ -145,6 +145,18 @@ int xts_exposure_contract(const double* src_exposure_cosbins,
                           const double* front_ltf, int E, double* exposure,
                           unsigned flags, void* stream);
 
+/* The exposure of every HEALPix pixel of the livetime cube [12 nside^2, E]: the
+ * contraction of Exposure::exposure (exposure/exposure.cxx:159-263, DGEMMs of
+ * exposure/exposure.contract.cpp:13-42) applied to all cube rows instead of the
+ * rows gathered at the sources (exposure/exposure.cxx:42-63), so a source's
+ * exposure is the map row at its NESTED pixel.  Computed on tcgen05 tensor
+ * cores as 3xTF32 with FP32 accumulation (relative error ~1e-6; the per-source
+ * xts_compute_exposure stays FP64).  Needs nbrbins <= 64 and a multiple of 4. */
+int xts_exposure_map(const xts_expcube* exp_cube, const xts_expcube* wexp_cube,
+                     const double* logEs, int E, const xts_grid* aeff_front,
+                     const xts_grid* aeff_back, const double* front_ltf,
+                     double* exposure_map, unsigned flags, void* stream);
+
 /* Psf::compute_psf_data (psf/psf.compute_psf_data.cxx:7-33, which calls
  * psf/psf.psf_lookup_table_and_partial_integrals.cxx:8-57): steps b3-b7.
  * psf grids are normalised King grids [Mc, Me, 6]; outputs uPsf and

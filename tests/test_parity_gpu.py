@@ -316,3 +316,25 @@ def test_adaptive_map_accuracy_gain(api):
     e_ad, e_pl = max_rel(ad, truth), max_rel(pl, truth)
     assert e_pl > 5e-4
     assert e_ad < 0.5 * e_pl
+
+
+@pytest.mark.parametrize("name", ["c0", "c1"])
+def test_exposure_map_tensor_cores(api, name):
+    """The full-sky exposure contraction on tcgen05 (3xTF32, FP32 accumulation)
+    against the FP64 oracle applied to every livetime-cube row, and its rows at
+    the sources' NESTED pixels against the FP64 per-source exposures."""
+    from oracle import oracle as O
+
+    job = _job(name, seed=4)
+    ref = oracle_pipeline(job, with_map=False)
+    cube, wcube = job.exp_cube, job.wexp_cube
+    m = api.exposure_map(cube, wcube, job.logEs, job.aeff_front, job.aeff_back, ref["ltf"])
+    npix = 12 * cube.nside ** 2
+    assert m.shape == (npix, job.E)
+    want = O.exposure(cube.cosbins.astype(np.float64), wcube.cosbins.astype(np.float64), ref["af"], ref["ab"],
+                      ref["ltf"])
+    rel = np.abs(m - want) / np.abs(want)
+    assert rel.max() < 5e-6
+    assert rel.mean() < 1e-6
+    pix = [O.ang2pix_nest(np.pi / 2 - np.radians(dec), np.radians(ra), cube.nside) for ra, dec in job.src_sph]
+    assert max_rel(m[pix], ref["exposure"]) < 5e-6

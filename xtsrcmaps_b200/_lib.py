@@ -95,6 +95,8 @@ SIGNATURES = {
                                         C.c_int, C.POINTER(XtsGrid), C.POINTER(XtsGrid), C.POINTER(XtsGrid),
                                         C.POINTER(XtsGrid), _vp, C.POINTER(XtsWcs), _vp,
                                         C.POINTER(XtsSrcmapInfo), C.c_uint, _vp]),
+    "xts_exposure_map": (C.c_int, [C.POINTER(XtsExpcube), C.POINTER(XtsExpcube), _vp, C.c_int,
+                                   C.POINTER(XtsGrid), C.POINTER(XtsGrid), _vp, _vp, C.c_uint, _vp]),
     "xts_point_src_model_map_wcs_adaptive": (C.c_int, [C.POINTER(XtsWcs), _vp, C.c_int, _vp, _vp, _vp,
                                                        C.c_int, C.c_double, C.c_int, _vp,
                                                        C.POINTER(XtsSrcmapInfo), C.c_uint, _vp]),

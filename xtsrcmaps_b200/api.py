@@ -208,6 +208,30 @@ def compute_exposure(exp_cube: ExpCube, wexp_cube: ExpCube, logEs, src_sph, aeff
     return XtExp(*[x[1] for x in o])
 
 
+def exposure_map(exp_cube: ExpCube, wexp_cube: ExpCube, logEs, aeff_front: IrfGrid, aeff_back: IrfGrid,
+                 front_ltf):
+    """Exposure of every HEALPix pixel [12 nside^2, E] (the contraction of
+    exposure/exposure.cxx:159-263 over all livetime-cube rows) on tcgen05 tensor
+    cores as 3xTF32; a source's exposure is the row at its NESTED pixel."""
+    like = _device_of(exp_cube.cosbins, logEs)
+    c = _Call(like is not None, like)
+    cb, cube = c.inp(exp_cube.cosbins, "f32")
+    wb, _ = c.inp(wexp_cube.cosbins, "f32")
+    cube_s = L.XtsExpcube(cb, int(exp_cube.nside), int(exp_cube.nbrbins), float(exp_cube.cosmin),
+                          int(bool(exp_cube.thetabin)))
+    wcube_s = L.XtsExpcube(wb, int(wexp_cube.nside), int(wexp_cube.nbrbins), float(wexp_cube.cosmin),
+                           int(bool(wexp_cube.thetabin)))
+    lp, le = c.inp(logEs)
+    E = len(le)
+    af = c.grid(aeff_front, 1)
+    ab = c.grid(aeff_back, 1)
+    ltfp, _ = c.inp(front_ltf)
+    op, o = c.out((12 * int(exp_cube.nside) ** 2, E))
+    L.check(L.lib().xts_exposure_map(C.byref(cube_s), C.byref(wcube_s), lp, E, C.byref(af), C.byref(ab), ltfp,
+                                     op, c.flags, c.stream))
+    return o
+
+
 def exposure(src_exposure_cosbins, src_weighted_exposure_cosbins, front_aeff, back_aeff, front_ltf):
     """Exposure::exposure (exposure/exposure.cxx:159-263): step a5 from gathered livetime rows."""
     like = _device_of(src_exposure_cosbins, front_aeff)

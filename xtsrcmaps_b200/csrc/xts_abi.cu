@@ -520,6 +520,51 @@ int xts_point_src_model_map_wcs(const xts_wcs* wcs, const double* src_sph, int S
     return run_srcmap(sg, a, model_map, npix, f64);
 }
 
+int xts_exposure_map(const xts_expcube* cube, const xts_expcube* wcube, const double* logEs, int E,
+                     const xts_grid* aeff_front, const xts_grid* aeff_back, const double* front_ltf,
+                     double* exposure_map, unsigned flags, void* stream) {
+    XTS_ENTER();
+    if (!cube || !wcube || !cube->cosbins || !wcube->cosbins || !logEs || E <= 0 || !front_ltf || !exposure_map)
+        return set_error(XTS_ERR_ARG, "exposure_map: null argument or bad size");
+    if (cube->nside <= 0 || (cube->nside & (cube->nside - 1)) || cube->nbrbins <= 0 ||
+        wcube->nside != cube->nside || wcube->nbrbins != cube->nbrbins)
+        return set_error(XTS_ERR_ARG, "exposure_map: livetime cubes need a power-of-two nside and equal shapes");
+    if (!grid_ok(aeff_front, 1) || !grid_ok(aeff_back, 1))
+        return set_error(XTS_ERR_ARG, "exposure_map: effective-area grids need n_par == 1");
+    const int C = cube->nbrbins;
+    if (!exposure_map_supported(C, E))
+        return set_error(XTS_ERR_ARG, "exposure_map: needs nbrbins <= 64 and a multiple of 4, E <= 256");
+    const long long npix = 12LL * cube->nside * cube->nside;
+    Stager sg{(flags & XTS_DEVICE_PTRS) != 0, stream ? (cudaStream_t)stream : g_ctx.stream};
+    ExposureDev ea;
+    ea.cube = sg.in(cube->cosbins, (size_t)npix * C);
+    ea.wcube = sg.in(wcube->cosbins, (size_t)npix * C);
+    ea.nside = cube->nside; ea.C = C; ea.cosmin = cube->cosmin; ea.thetabin = cube->thetabin;
+    ea.logEs = sg.in(logEs, (size_t)E); ea.E = E;
+    ea.src_sph = nullptr; ea.S = 0;
+    ea.af = stage_grid(sg, aeff_front);
+    ea.ab = stage_grid(sg, aeff_back);
+    ea.ltf = sg.in(front_ltf, (size_t)2 * E);
+    ea.exp_costhetas = sg.scratch<double>(C);
+    ea.front_aeff = sg.scratch<double>((size_t)C * E);
+    ea.back_aeff = sg.scratch<double>((size_t)C * E);
+    ea.ecb = ea.wecb = ea.exposure = nullptr;
+    double* out = sg.out(exposure_map, (size_t)npix * E);
+    int* status = (int*)workspace(W_MISC, 64);
+    int rc = sg.rc ? sg.rc : (status ? XTS_OK : XTS_ERR_OOM);
+    if (rc == XTS_OK) {
+        cudaError_t e = cudaMemsetAsync(status, 0, sizeof(int), sg.st);
+        if (e != cudaSuccess) rc = cuda_error(e, "cudaMemsetAsync");
+    }
+    if (rc == XTS_OK) rc = launch_exposure(ea, sg.st);  // cos-theta bins and effective-area tables
+    if (rc == XTS_OK)
+        rc = launch_exposure_map_tc(ea.cube, ea.wcube, npix, C, ea.front_aeff, ea.back_aeff, ea.ltf, E, out, status,
+                                    sg.st);
+    rc = sg.finish(rc);
+    if (rc == XTS_OK && !sg.dev) rc = srcmap_status(sg.st);
+    return rc;
+}
+
 int xts_point_src_model_map_wcs_adaptive(const xts_wcs* wcs, const double* src_sph, int S,
                                          const double* exposure, const double* upsf,
                                          const double* partial, int E, double rtol, int max_depth,

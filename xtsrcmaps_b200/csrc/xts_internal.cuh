@@ -63,7 +63,7 @@ enum Slot {
     S_OUT11, S_OUT12, S_OUT13, S_OUT14, S_OUT15,
     // internal scratch
     W_CORNERS, W_CENTERS, W_OMEGA, W_LUT, W_PARTSUM, W_SRCINFO, W_SCALE, W_PSFTAB,
-    W_KING, W_MISC, W_WIN, W_WMETA, W_SPARSE,
+    W_KING, W_MISC, W_WIN, W_WMETA, W_SPARSE, W_MISC2, W_EXPMAP,
     N_SLOTS
 };
 void* workspace(int slot, size_t bytes);  // nullptr + error set on OOM
@@ -142,6 +142,10 @@ int launch_correction(const double* hist, int nch, const SrcInfo* info, int S, c
                       double* inv_integ, double* correction, double* radius, int* in_fov,
                       cudaStream_t st);
 bool srcmap_win_supported(int E);
+bool exposure_map_supported(int C, int E);
+int launch_exposure_map_tc(const float* cube, const float* wcube, long long npix, int C, const double* front_aeff,
+                           const double* back_aeff, const double* ltf, int E, double* out, int* status,
+                           cudaStream_t st);
 bool srcmap_adaptive_supported(int E);
 int launch_adaptive_map(const double* corners, const double* centers, const double* omega, const SrcInfo* info,
                         const double* upsf, int S, int H, int W, int E, double rtol, int max_depth, int nch,

@@ -532,7 +532,7 @@ int srcmap_status(cudaStream_t st) {
     XTS_CUDA(cudaStreamSynchronize(st));
     if (v) {
         cudaMemsetAsync(status, 0, sizeof(int), st);
-        return set_error(XTS_ERR_TIMEOUT, "source-map kernel: a bounded device wait gave up");
+        return set_error(XTS_ERR_TIMEOUT, "a bounded device-side wait gave up (tensor-memory or TMA pipeline)");
     }
     return XTS_OK;
 }
