@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="time eager launches instead of a CUDA graph")
     ap.add_argument("--no-adaptive", action="store_true", help="skip the adaptive-cubature measurement")
+    ap.add_argument("--exposure-map-nside", type=int, default=0,
+                    help="time only the full-sky exposure map at this nside and exit")
     ap.add_argument("--kernel", default="windows", choices=["windows", "cuda_cores", "tcgen05"],
                     help="FP32 source-map write pass")
     return ap.parse_args()
@@ -277,12 +279,13 @@ def run_ours(args, rank, world, local_rank):
     # of the 12-point rule (rtol 1e-4, depth 6), eager launches, same timing rules
     adaptive = None
     if not args.no_adaptive:
+        out_a = torch.empty_like(out)  # its own buffer: `out` keeps the 12-point map for the error check
         def step_adaptive():
             with torch.cuda.stream(stream):
                 ex = A.compute_exposure(d["cube"], d["wcube"], d["logEs"], d["src"], d["af"], d["ab"], ltf)
                 ps = A.compute_psf_data(nf, nb, ex, d["logEs"], ltf)
                 A.point_src_model_map_wcs_adaptive(job.wcs, d["src"], ex.exposure, ps.uPsf, ps.partial_psf_integral,
-                                                   rtol=1e-4, max_depth=6, out=out, with_info=False)
+                                                   rtol=1e-4, max_depth=6, out=out_a, with_info=False)
 
         for _ in range(max(3, args.warmup)):
             step_adaptive()
@@ -532,8 +535,58 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_exposure_map(args):
+    """--exposure-map-nside N: the full-sky exposure map (tcgen05, 3xTF32) on a
+    seeded livetime cube of that nside with the c4 energy grid; one JSON line."""
+    import torch
+
+    from xtsrcmaps_b200 import api as A
+    from xtsrcmaps_b200.api import ExpCube
+    from xtsrcmaps_b200.synth import make_job
+
+    A.init(0)
+    dev = torch.device("cuda", 0)
+    job = make_job("c4", seed=args.seed, n_sources=1)
+    nside, C = int(args.exposure_map_nside), 40
+    npix = 12 * nside * nside
+    rng = np.random.default_rng(args.seed)
+    cube = (2e5 * rng.lognormal(0.0, 0.2, (npix, C))).astype(np.float32)
+    c = ExpCube(torch.as_tensor(cube, device=dev), nside, C, 0.0, True)
+    w = ExpCube(torch.as_tensor(0.9 * cube, device=dev), nside, C, 0.0, True)
+    ltf = torch.as_tensor(A.livetime_efficiency_factors(job.logEs, job.effic_front), device=dev)
+    tg = lambda g: type(g)(*[torch.as_tensor(np.asarray(v), device=dev) if isinstance(v, np.ndarray) else v
+                             for v in (g.cosths, g.logEs, g.params, g.min_cos_theta)])
+    le, af, ab = torch.as_tensor(job.logEs, device=dev), tg(job.aeff_front), tg(job.aeff_back)
+    for _ in range(max(3, args.warmup)):
+        A.exposure_map(c, w, le, af, ab, ltf)
+    torch.cuda.synchronize(dev)
+    A.profile_enable(True)
+    for _ in range(args.steps):
+        A.exposure_map(c, w, le, af, ab, ltf)
+    torch.cuda.synchronize(dev)
+    prof = A.profile_read()
+    A.profile_enable(False)
+    n, kms = prof["k_exposure_map_tc"]
+    ms = kms / n
+    alg = 2 * npix * C * 4 + npix * job.E * 8
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    print(json.dumps({"metric": "exposure-map pixels/s (full sky, tcgen05 3xTF32)", "value": npix / (ms * 1e-3),
+                      "unit": "HEALPix pixels/s", "kernel_ms": ms, "launches": n, "nside": nside, "C": C, "E": job.E,
+                      "roofline": {"bound": "hbm", "achieved": alg / ms / 1e6, "peak": peak, "unit": "GB/s",
+                                   "frac": alg / ms / 1e6 / peak, "alg_bytes_per_launch": alg},
+                      "useful_tflops": 2 * npix * 2 * C * job.E * 2 / ms / 1e9}), flush=True)
+
+
 def main():
     args = parse()
+    if args.exposure_map_nside:
+        run_exposure_map(args)
+        return
     rank, world, local_rank = env_rank()
     if args.impl == "reference":
         run_reference(args, rank, world)
