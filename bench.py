@@ -182,7 +182,15 @@ def run_ours(args, rank, world, local_rank):
 
     stream = torch.cuda.Stream(dev)
 
+    # one step = the public call that replaces main.cxx:28-30 (point_source_maps:
+    # exposure, mean PSF and model maps; the map geometry runs on a second stream
+    # beside exposure and PSF); step3 = the three separate calls, for comparison
     def step():
+        with torch.cuda.stream(stream):
+            A.point_source_maps(job.wcs, d["src"], d["cube"], d["wcube"], d["logEs"], d["af"], d["ab"], nf, nb,
+                                ltf, out=out, with_info=False, kernel=args.kernel)
+
+    def step3():
         with torch.cuda.stream(stream):
             ex = A.compute_exposure(d["cube"], d["wcube"], d["logEs"], d["src"], d["af"], d["ab"], ltf)
             ps = A.compute_psf_data(nf, nb, ex, d["logEs"], ltf)
@@ -190,6 +198,7 @@ def run_ours(args, rank, world, local_rank):
                                       out=out, with_info=False)
 
     for _ in range(max(3, args.warmup)):
+        step3()
         step()
     torch.cuda.synchronize(dev)
 
@@ -198,11 +207,11 @@ def run_ours(args, rank, world, local_rank):
     # launch.  Two graphs: a plain one for the timed steps, and one whose kernels
     # are bracketed by the library's timers (event-record nodes) for the per-kernel
     # table and the roofline, replayed over the same number of steps afterwards.
-    def capture(profiled):
+    def capture(profiled, fn=step):
         A.profile_enable(True, keep=True) if profiled else A.profile_enable(False)
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g, stream=stream):
-            step()
+            fn()
         for _ in range(max(3, args.warmup)):
             with torch.cuda.stream(stream):
                 g.replay()
@@ -211,15 +220,16 @@ def run_ours(args, rank, world, local_rank):
             A.profile_read()
         return g
 
-    graph = gprof = None
+    graph = gprof = graph3 = None
     graph_note = "eager launches"
     if not args.no_graph:
         try:
             graph = capture(False)
-            gprof = capture(True)
-            graph_note = "one CUDA graph per step (three public calls captured once)"
+            graph3 = capture(False, step3)
+            gprof = capture(True)  # last: enabling or disabling the profiler clears its records
+            graph_note = "one CUDA graph per step (the fused public call captured once)"
         except Exception as exc:  # capture refused: time eager launches
-            graph = gprof = None
+            graph = gprof = graph3 = None
             graph_note = "eager launches (graph capture failed: %s)" % str(exc).splitlines()[0][:120]
             A.profile_enable(False)
             torch.cuda.synchronize(dev)
@@ -266,12 +276,15 @@ def run_ours(args, rank, world, local_rank):
         # per-kernel times: the instrumented graph (its timers were recorded at
         # capture and are kept), read after every replay
         ms_prof = timed(replay(gprof), lambda: add_prof(A.profile_read()))
+        ms3 = timed(replay(graph3))
     else:
         A.profile_enable(True)
         ms = timed(step)
         t1 = time.time()
         add_prof(A.profile_read())
         ms_prof = ms
+        A.profile_enable(False)
+        ms3 = timed(step3)
     A.profile_enable(False)
     ck = clocks.stop(t0, t1)
 
@@ -420,6 +433,9 @@ def run_ours(args, rank, world, local_rank):
         "roofline": roofline, "kernels": kernels, "gpu_launches": gpu_launches,
         "clocks": ck, "e2e": e2e, "cpu_baseline": cpu, "max_rel_err_vs_fp64_oracle": err,
         "adaptive": adaptive,
+        "three_calls_device": {"ms_per_step": ms3 / args.steps, "value": n_values * world * args.steps / (ms3 * 1e-3),
+                               "note": "compute_exposure, compute_psf_data, point_src_model_map_wcs as three "
+                                       "device-pointer calls on one stream (no geometry overlap)"},
     }
     print(json.dumps(line), flush=True)
 

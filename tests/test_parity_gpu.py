@@ -258,6 +258,41 @@ def test_point_source_maps_fused_call(api, c1_small, out_dtype):
     assert max_rel(md.cpu().numpy(), m) < same
 
 
+def test_fused_call_graph_capture(api, c1_small):
+    """The fused device-pointer call runs its map geometry on a second stream that
+    forks from and joins the caller's stream: captured into a CUDA graph and
+    replayed twice (on a poisoned output) it reproduces the eager maps."""
+    import torch
+
+    from xtsrcmaps_b200.api import ExpCube
+
+    job, ref, gpu = c1_small
+    d = torch.device("cuda")
+    tg = lambda g: type(g)(*[torch.as_tensor(np.asarray(v), device=d) if isinstance(v, np.ndarray) else v
+                             for v in (g.cosths, g.logEs, g.params, g.min_cos_theta)])
+    tc = lambda c: ExpCube(torch.as_tensor(c.cosbins, device=d), c.nside, c.nbrbins, c.cosmin, c.thetabin)
+    args = (job.wcs, torch.as_tensor(job.src_sph, device=d), tc(job.exp_cube), tc(job.wexp_cube),
+            torch.as_tensor(job.logEs, device=d), tg(job.aeff_front), tg(job.aeff_back), tg(gpu["nf"]),
+            tg(gpu["nb"]), torch.as_tensor(gpu["ltf"], device=d))
+    st = torch.cuda.Stream()
+    with torch.cuda.stream(st):
+        eager, _ = api.point_source_maps(*args, with_info=False)
+        out = torch.empty_like(eager)
+        api.point_source_maps(*args, out=out, with_info=False)  # warm: workspaces sized
+    st.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=st):
+        api.point_source_maps(*args, out=out, with_info=False)
+    for _ in range(2):
+        with torch.cuda.stream(st):
+            out.fill_(float("nan"))
+            g.replay()
+        st.synchronize()
+        assert max_rel(out.cpu().numpy(), eager.cpu().numpy()) < 1e-6
+    assert max_rel(out.cpu().numpy(), ref["map"]) < 1e-5
+    del g
+
+
 def test_srcmap_vs_compiled_reference(api, c1_small):
     """GPU maps (FP32 and FP64) against ModelMap::point_src_model_map_wcs of the
     reference's own code compiled under oracle/_ref, fed the same exposure and

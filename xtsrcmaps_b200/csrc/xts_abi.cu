@@ -32,6 +32,8 @@ struct Ctx {
     int device = -1;
     cudaStream_t stream = nullptr;
     cudaStream_t copy_stream = nullptr;    // device-to-host copies of finished map chunks
+    cudaStream_t geo_stream = nullptr;     // map geometry of the fused call, beside exposure and PSF
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     cudaEvent_t chunk_ev[N_CHUNK_EV] = {};
     void* buf[N_SLOTS] = {};
     size_t cap[N_SLOTS] = {};
@@ -58,6 +60,9 @@ int ensure_device() {
     XTS_CUDA(cudaSetDevice(dev));
     XTS_CUDA(cudaStreamCreateWithFlags(&g_ctx.stream, cudaStreamNonBlocking));
     if (!g_ctx.copy_stream) XTS_CUDA(cudaStreamCreateWithFlags(&g_ctx.copy_stream, cudaStreamNonBlocking));
+    if (!g_ctx.geo_stream) XTS_CUDA(cudaStreamCreateWithFlags(&g_ctx.geo_stream, cudaStreamNonBlocking));
+    if (!g_ctx.fork_ev) XTS_CUDA(cudaEventCreateWithFlags(&g_ctx.fork_ev, cudaEventDisableTiming));
+    if (!g_ctx.join_ev) XTS_CUDA(cudaEventCreateWithFlags(&g_ctx.join_ev, cudaEventDisableTiming));
     for (int i = 0; i < N_CHUNK_EV; ++i)
         if (!g_ctx.chunk_ev[i]) XTS_CUDA(cudaEventCreateWithFlags(&g_ctx.chunk_ev[i], cudaEventDisableTiming));
     g_ctx.device = dev;
@@ -318,6 +323,9 @@ int xts_init(int device) {
     g_ctx.device = -1;
     if (g_ctx.stream) { cudaStreamDestroy(g_ctx.stream); g_ctx.stream = nullptr; }
     if (g_ctx.copy_stream) { cudaStreamDestroy(g_ctx.copy_stream); g_ctx.copy_stream = nullptr; }
+    if (g_ctx.geo_stream) { cudaStreamDestroy(g_ctx.geo_stream); g_ctx.geo_stream = nullptr; }
+    if (g_ctx.fork_ev) { cudaEventDestroy(g_ctx.fork_ev); g_ctx.fork_ev = nullptr; }
+    if (g_ctx.join_ev) { cudaEventDestroy(g_ctx.join_ev); g_ctx.join_ev = nullptr; }
     for (int i = 0; i < N_CHUNK_EV; ++i)
         if (g_ctx.chunk_ev[i]) { cudaEventDestroy(g_ctx.chunk_ev[i]); g_ctx.chunk_ev[i] = nullptr; }
     return ensure_device();
@@ -632,13 +640,23 @@ int xts_point_source_maps(const xts_expcube* cube, const xts_expcube* wcube, con
     const int C = cube->nbrbins;
     const long long nhp = 12LL * cube->nside * cube->nside;
     Stager sg{(flags & XTS_DEVICE_PTRS) != 0, stream ? (cudaStream_t)stream : g_ctx.stream};
+    // The map geometry (pixel grids, solid angles, source boundaries, the window
+    // pass) needs only the source list and the WCS: it runs on the geometry
+    // stream from here on, beside the livetime-cube upload, the exposure and the
+    // mean PSF, and joins the launching stream before the correction factors.
+    const double* src_d = sg.in(src_sph, (size_t)2 * S);
+    const bool fork = sg.rc == XTS_OK && S > 0;
+    if (fork) {
+        XTS_CUDA(cudaEventRecord(g_ctx.fork_ev, sg.st));
+        XTS_CUDA(cudaStreamWaitEvent(g_ctx.geo_stream, g_ctx.fork_ev, 0));
+    }
     // (a) exposure; its outputs stay in device memory
     ExposureDev ea;
     ea.cube = sg.in(cube->cosbins, (size_t)nhp * C);
     ea.wcube = sg.in(wcube->cosbins, (size_t)nhp * C);
     ea.nside = cube->nside; ea.C = C; ea.cosmin = cube->cosmin; ea.thetabin = cube->thetabin;
     ea.logEs = sg.in(logEs, (size_t)E); ea.E = E;
-    ea.src_sph = sg.in(src_sph, (size_t)2 * S); ea.S = S;
+    ea.src_sph = src_d; ea.S = S;
     ea.af = stage_grid(sg, aeff_front);
     ea.ab = stage_grid(sg, aeff_back);
     ea.ltf = sg.in(front_ltf, (size_t)2 * E);
@@ -672,10 +690,14 @@ int xts_point_source_maps(const xts_expcube* cube, const xts_expcube* wcube, con
     ma.radius = info ? sg.out(info->psf_radius, (size_t)S) : nullptr;
     ma.in_fov = info ? sg.out(info->in_fov, (size_t)S) : nullptr;
     ma.kernel = srcmap_kernel(flags);
+    if (fork) { ma.geo_stream = g_ctx.geo_stream; ma.join_ev = g_ctx.join_ev; }
     int rc = sg.rc;
     if (rc == XTS_OK) rc = launch_exposure(ea, sg.st);
     if (rc == XTS_OK) rc = launch_psf(pa, sg.st);
-    if (rc != XTS_OK) return sg.finish(rc);
+    if (rc != XTS_OK) {
+        if (fork) StreamJoin{g_ctx.geo_stream, sg.st, g_ctx.join_ev}.join();
+        return sg.finish(rc);
+    }
     return run_srcmap(sg, ma, model_map, npix, f64);
 }
 

@@ -127,6 +127,29 @@ struct SrcmapDev {
     bool adaptive = false;
     double rtol = 1e-4;
     int max_depth = 6;
+    // Optional: a stream for the map geometry (grids, solid angles, boundaries and
+    // the first chunk's window pass), which needs neither the exposure nor uPsf;
+    // it already waits for the source list, and joins the launching stream through
+    // join_ev before the first kernel that reads uPsf.
+    cudaStream_t geo_stream = nullptr;
+    cudaEvent_t join_ev = nullptr;
+};
+
+// The geometry stream joins the launching stream once: at join(), or when it
+// goes out of scope (error paths, so that a stream capture never ends unjoined).
+struct StreamJoin {
+    cudaStream_t from, into;
+    cudaEvent_t ev;
+    bool pending = true;
+    StreamJoin(cudaStream_t f, cudaStream_t i, cudaEvent_t e) : from(f), into(i), ev(e), pending(f != i && e) {}
+    int join() {
+        if (!pending) return XTS_OK;
+        pending = false;
+        cudaError_t e = cudaEventRecord(ev, from);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(into, ev, 0);
+        return e == cudaSuccess ? XTS_OK : cuda_error(e, "geometry stream join");
+    }
+    ~StreamJoin() { join(); }
 };
 enum { SRCMAP_WINDOWS = 0, SRCMAP_ONEPASS = 1, SRCMAP_TCGEN05 = 2 };
 int launch_srcmap(const SrcmapDev& a, cudaStream_t st);
@@ -140,7 +163,7 @@ int srcmap_status(cudaStream_t st);
 int launch_correction(const double* hist, int nch, const SrcInfo* info, int S, const double* upsf,
                       const double* partial, const double* exposure, int E, double* scale,
                       double* inv_integ, double* correction, double* radius, int* in_fov,
-                      cudaStream_t st);
+                      cudaStream_t st, float* lut = nullptr, int Epad = 0);  // lut: scaled FP32 table too
 bool srcmap_win_supported(int E);
 bool exposure_map_supported(int C, int E);
 int launch_exposure_map_tc(const float* cube, const float* wcube, long long npix, int C, const double* front_aeff,
@@ -158,6 +181,7 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
                       double* scale, double* inv_integ, double* correction, double* radius,
                       int* in_fov, int* status, float* out, int chunk_sources,
                       int (*on_chunk)(void*, int, int, cudaStream_t), void* on_chunk_ctx,
+                      StreamJoin& geo,  // the first chunk's window pass runs on geo.from
                       cudaStream_t st);  // 0, or XTS_ERR_TIMEOUT if a bounded device wait gave up
 int launch_srcmap_fast(const double* corners, const double* omega, const SrcInfo* info,
                        const double* upsf, const double* scale, int S, int H, int W, int E,

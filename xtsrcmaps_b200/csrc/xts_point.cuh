@@ -19,16 +19,31 @@
 #pragma once
 
 #include <math.h>
+#include <string.h>
 
 #include "xts_geom.cuh"
 #include "xts_internal.cuh"
 
 namespace xts {
 
+// Bins of the squared chord q by its FP64 exponent and top SB_BITS mantissa bits
+// (32 bins per binade, q from 2^-39 to 8): a bin is narrower in ln q (at most
+// ln(33/32) = 0.031) than any table row (0.0586 at 70 deg, 0.0672 at small
+// angles), so it holds at most one row boundary and its row is k0 or k0 + 1.
+struct SepBin {
+    int k0, pad;  // lower row of the bin's low edge, clamped to [1, 399]
+    double thr;   // q[k0 + 1] (+inf when k0 = 399): q >= thr selects row k0 + 1
+};
+constexpr int SB_EXP0 = 984;  // biased FP64 exponent of the first bin
+constexpr int SB_BITS = 5;
+constexpr int NSB = (1025 - SB_EXP0 + 1) << SB_BITS;
+
 // Separation tables shared by every launch (see build_septab).
 struct SepTab {
     double q[ND + 1];      // squared chord of S[k] (k = 0..400), q[401] = +inf guard
-    float coef[ND][8];     // row k (= idx - 1): {1/q[k], c0..c4 of P_k(z)}, z = (d - DPOLY_C)/DPOLY_H
+    float coef[ND][8];     // row k (= idx - 1): {1/q[k], c0..c4 of P_k(z), q[k] as two words},
+                           // z = (d - DPOLY_C)/DPOLY_H
+    SepBin bins[NSB];
 };
 constexpr float DPOLY_C = 0.035f;  // centre and half-width of the fitted d range
 constexpr float DPOLY_H = 0.037f;
@@ -77,6 +92,17 @@ static int build_septab(cudaStream_t st, const SepTab** out) {
         long double m[N] = {cc[0] - cc[2] + cc[4], cc[1] - 3 * cc[3], 2 * cc[2] - 8 * cc[4], 4 * cc[3], 8 * cc[4]};
         h.coef[k][0] = (float)(1.0L / qk);
         for (int j = 0; j < N; ++j) h.coef[k][1 + j] = (float)m[j];
+        memcpy(&h.coef[k][6], &h.q[k], sizeof(double));
+    }
+    for (int b = 0; b < NSB; ++b) {
+        const double qa = ldexp(1.0 + (double)(b & ((1 << SB_BITS) - 1)) / (1 << SB_BITS),
+                                SB_EXP0 + (b >> SB_BITS) - 1023);
+        int k = 0;
+        while (k < ND - 1 && h.q[k + 1] <= qa) ++k;  // largest k with q[k] <= qa
+        k = k < 1 ? 1 : (k > 399 ? 399 : k);
+        h.bins[b].k0 = k;
+        h.bins[b].pad = 0;
+        h.bins[b].thr = k < 399 ? h.q[k + 1] : INFINITY;
     }
     SepTab* d = nullptr;
     XTS_CUDA(cudaMalloc(&d, sizeof(SepTab)));
@@ -87,8 +113,11 @@ static int build_septab(cudaStream_t st, const SepTab** out) {
     return XTS_OK;
 }
 
-// Rule in the bilinear form: u, v, u*v and 0.25 * weight per point.
+// Rule in the bilinear form: u, v, u*v and 0.25 * weight per point (and that
+// weight rounded to FP32).
 static __constant__ double c_rule_uv[12][4];
+static __constant__ float c_rule_w32[12];
+static __constant__ double c_rule_q[12][3];  // u, u*u, v (biquadratic chord form)
 
 static int upload_rule_uv(cudaStream_t st) {
     static int dev_done = -1;
@@ -115,7 +144,15 @@ static int upload_rule_uv(cudaStream_t st) {
         b[p][0] = R[3 * p]; b[p][1] = R[3 * p + 1]; b[p][2] = R[3 * p] * R[3 * p + 1];
         b[p][3] = 0.25 * R[3 * p + 2];
     }
+    float w32[12];
+    double bq[12][3];
+    for (int p = 0; p < 12; ++p) {
+        w32[p] = (float)b[p][3];
+        bq[p][0] = R[3 * p]; bq[p][1] = R[3 * p] * R[3 * p]; bq[p][2] = R[3 * p + 1];
+    }
     XTS_CUDA(cudaMemcpyToSymbolAsync(c_rule_uv, b, sizeof(b), 0, cudaMemcpyHostToDevice, st));
+    XTS_CUDA(cudaMemcpyToSymbolAsync(c_rule_w32, w32, sizeof(w32), 0, cudaMemcpyHostToDevice, st));
+    XTS_CUDA(cudaMemcpyToSymbolAsync(c_rule_q, bq, sizeof(bq), 0, cudaMemcpyHostToDevice, st));
     XTS_CUDA(cudaStreamSynchronize(st));
     dev_done = dev;
     return XTS_OK;
@@ -204,6 +241,28 @@ __device__ __forceinline__ int point_row(double q, const double* sq, const float
     return idx;
 }
 
+// The same row and weight by the bin table: one 16-byte load of the bin of q
+// (exponent and top mantissa bits), one FP64 compare, and the row's record
+// (1/q_k, t polynomial, q_k).  bins: [NSB]; coef: [ND][2] float4 with q_k in the
+// last two words.
+__device__ __forceinline__ int point_row_bin(double q, const SepBin* bins, const float4* coef, float* t_out) {
+    int b = (__double2hiint(q) >> (20 - SB_BITS)) - (SB_EXP0 << SB_BITS);
+    b = min(max(b, 0), NSB - 1);
+    const SepBin sb = bins[b];
+    const int k = sb.k0 + (q >= sb.thr);
+    const float4 c0 = coef[2 * k], c1 = coef[2 * k + 1];
+    const double qlo = __hiloint2double(__float_as_int(c1.w), __float_as_int(c1.z));
+    const float dl = (float)(q - qlo) * c0.x;  // q / q_lo - 1
+    if (dl >= -0.002f && dl <= 0.072f) {
+        const float zz = fmaf(dl, 1.f / DPOLY_H, -DPOLY_C / DPOLY_H);
+        const float P = fmaf(fmaf(fmaf(fmaf(c1.y, zz, c1.x), zz, c0.w), zz, c0.z), zz, c0.y);
+        *t_out = (float)REDM1 * (dl * P);
+    } else {
+        *t_out = t_exact(q, k + 1);
+    }
+    return k + 1;
+}
+
 // Bilinear form of the rule points of pixel (h, w) relative to the source.
 struct PixGeom { double Ax, Ay, Az, Bx, By, Bz, Cx, Cy, Cz, Dx, Dy, Dz; };
 
@@ -234,6 +293,33 @@ __device__ __forceinline__ double point_q(const PixGeom& g, int p) {
     const double y = fma(g.Dy, uv, fma(g.Cy, v, fma(g.By, u, g.Ay)));
     const double z = fma(g.Dz, uv, fma(g.Cz, v, fma(g.Bz, u, g.Az)));
     return fma(x, x, fma(y, y, z * z));
+}
+
+// q(u, v) = |A + Bu + Cv + Duv|^2 of one pixel as a biquadratic polynomial,
+// evaluated per rule point by Horner in v: q = P0(u) + v (P1(u) + v P2(u)), each
+// P a quadratic in u (8 FP64 FMAs per point, dependency depth 4).
+struct PixQ { double a0, a1, a2, a3, a4, a5, a6, a7, a8; };
+
+__device__ __forceinline__ PixQ pixel_q(const PixGeom& g) {
+    PixQ c;
+    c.a0 = fma(g.Ax, g.Ax, fma(g.Ay, g.Ay, g.Az * g.Az));
+    c.a1 = 2.0 * fma(g.Ax, g.Bx, fma(g.Ay, g.By, g.Az * g.Bz));
+    c.a4 = fma(g.Bx, g.Bx, fma(g.By, g.By, g.Bz * g.Bz));
+    c.a2 = 2.0 * fma(g.Ax, g.Cx, fma(g.Ay, g.Cy, g.Az * g.Cz));
+    c.a3 = 2.0 * (fma(g.Ax, g.Dx, fma(g.Ay, g.Dy, g.Az * g.Dz)) + fma(g.Bx, g.Cx, fma(g.By, g.Cy, g.Bz * g.Cz)));
+    c.a6 = 2.0 * fma(g.Bx, g.Dx, fma(g.By, g.Dy, g.Bz * g.Dz));
+    c.a5 = fma(g.Cx, g.Cx, fma(g.Cy, g.Cy, g.Cz * g.Cz));
+    c.a7 = 2.0 * fma(g.Cx, g.Dx, fma(g.Cy, g.Dy, g.Cz * g.Dz));
+    c.a8 = fma(g.Dx, g.Dx, fma(g.Dy, g.Dy, g.Dz * g.Dz));
+    return c;
+}
+
+__device__ __forceinline__ double point_q2(const PixQ& c, int p) {
+    const double u = c_rule_q[p][0], uu = c_rule_q[p][1], v = c_rule_q[p][2];
+    const double p0 = fma(c.a4, uu, fma(c.a1, u, c.a0));
+    const double p1 = fma(c.a6, uu, fma(c.a3, u, c.a2));
+    const double p2 = fma(c.a8, uu, fma(c.a7, u, c.a5));
+    return fma(fma(p2, v, p1), v, p0);
 }
 
 // Scaled FP32 table Y'[s][d][e] = uPsf * (exposure * correction), energies

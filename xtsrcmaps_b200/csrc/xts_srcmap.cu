@@ -81,18 +81,6 @@ static int upload_rule(cudaStream_t st) {
 // ---------------------------------------------------------------- geometry grids
 // corners[i][j] = pix2dir(i + 0.5, j + 0.5), centres[i][j] = pix2dir(i + 1, j + 1),
 // i in [0, H], j in [0, W] (1-based FITS pixels).
-__global__ void k_grids(WcsDev w, int H, int W, double* corners, double* centers) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    int W1 = W + 1;
-    if (k >= (H + 1) * W1) return;
-    int i = k / W1, j = k - i * W1;
-    double v[3];
-    pix2dir(w, i + 0.5, j + 0.5, v);
-    corners[3 * k] = v[0]; corners[3 * k + 1] = v[1]; corners[3 * k + 2] = v[2];
-    pix2dir(w, i + 1.0, j + 1.0, v);
-    centers[3 * k] = v[0]; centers[3 * k + 1] = v[1]; centers[3 * k + 2] = v[2];
-}
-
 __device__ inline double quad_half(const double* P, const double* Q, const double* R) {
     double u[3] = {P[0] - Q[0], P[1] - Q[1], P[2] - Q[2]};
     double v[3] = {P[0] - R[0], P[1] - R[1], P[2] - R[2]};
@@ -103,44 +91,101 @@ __device__ inline double quad_half(const double* P, const double* Q, const doubl
     return dir_diff(P, Q) * dir_diff(P, R) * sqrt(c0 * c0 + c1 * c1 + c2 * c2);
 }
 
-// d2: solid angle of the quad of pixel centres (h+1,w+1),(h+1,w+2),(h+2,w+2),(h+2,w+1).
-__global__ void k_solid_angle(const double* centers, int H, int W, double* omega) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= H * W) return;
-    int h = k / W, w = k - h * W, W1 = W + 1;
-    const double* A = centers + 3 * (h * W1 + w);
-    const double* B = centers + 3 * (h * W1 + w + 1);
-    const double* C = centers + 3 * ((h + 1) * W1 + w + 1);
-    const double* D = centers + 3 * ((h + 1) * W1 + w);
-    omega[k] = 0.5 * (quad_half(A, B, D) + quad_half(C, B, D));
+// d1 + d2 in one launch, by 16x16 tiles of the (H+1) x (W+1) point grid: the
+// tile's corner points and its centre points with a one-point halo (17x17) are
+// evaluated by one thread each (545 pix2dir per block, one round), then the
+// solid angles of the tile's pixels come from the centres in shared memory.
+constexpr int GT = 16;                                   // grid points per tile side
+constexpr int GEO_THREADS = (GT + 1) * (GT + 1) + GT * GT;  // 545 tasks, one per thread
+
+__global__ void __launch_bounds__(GEO_THREADS) k_map_geometry(WcsDev w, int H, int W, double* corners,
+                                                             double* centers, double* omega) {
+    __shared__ double cen[(GT + 1) * (GT + 1)][3];
+    const int i0 = blockIdx.y * GT, j0 = blockIdx.x * GT, W1 = W + 1, t = threadIdx.x;
+    double v[3];
+    if (t < (GT + 1) * (GT + 1)) {  // centre (i0 + li, j0 + lj) = pix2dir(i + 1, j + 1)
+        const int li = t / (GT + 1), lj = t - li * (GT + 1), i = i0 + li, j = j0 + lj;
+        if (i <= H && j <= W) {
+            pix2dir(w, i + 1.0, j + 1.0, v);
+            cen[t][0] = v[0]; cen[t][1] = v[1]; cen[t][2] = v[2];
+            if (li < GT && lj < GT) {
+                double* c = centers + 3 * ((size_t)i * W1 + j);
+                c[0] = v[0]; c[1] = v[1]; c[2] = v[2];
+            }
+        }
+    } else {  // corner (i0 + li, j0 + lj) = pix2dir(i + 0.5, j + 0.5)
+        const int k = t - (GT + 1) * (GT + 1), li = k / GT, lj = k - li * GT, i = i0 + li, j = j0 + lj;
+        if (i <= H && j <= W) {
+            pix2dir(w, i + 0.5, j + 0.5, v);
+            double* c = corners + 3 * ((size_t)i * W1 + j);
+            c[0] = v[0]; c[1] = v[1]; c[2] = v[2];
+        }
+    }
+    __syncthreads();
+    // d2: solid angle of pixel (h, w) from the quad of 1-based pixel centres
+    // (h+1,w+1), (h+1,w+2), (h+2,w+2), (h+2,w+1), i.e. grid centres (h,w) .. (h+1,w+1)
+    if (t < GT * GT) {
+        const int li = t / GT, lj = t - li * GT, h = i0 + li, wc = j0 + lj;
+        if (h < H && wc < W) {
+            const int a = li * (GT + 1) + lj;
+            omega[(size_t)h * W + wc] = 0.5 * (quad_half(cen[a], cen[a + 1], cen[a + GT + 1]) +
+                                               quad_half(cen[a + GT + 2], cen[a + 1], cen[a + GT + 1]));
+        }
+    }
 }
 
 // c6: in-FOV flag (3.5 pixel buffer) and the minimum distance to the map edge,
-// sampled at the corner grid's border.  One block per source.
-__global__ void k_boundary(WcsDev w, const double* src_sph, int H, int W, const double* corners,
-                           SrcInfo* info) {
-    int s = blockIdx.x;
-    double ra = src_sph[2 * s], dec = src_sph[2 * s + 1];
+// sampled at the corner grid's border.  The separation 2 asin(|a - b| / 2) is
+// monotone in the squared chord, so the block finds the smallest squared chord
+// over the border first and evaluates the separation only for the points within
+// 1e-12 of it (the minimum of those is the minimum over the whole border).  One
+// block per source.
+__device__ __forceinline__ void border_point(int k, int H, int W, int* i, int* j) {
+    if (k < H + 1) { *i = k; *j = 0; }
+    else if (k < 2 * (H + 1)) { *i = k - (H + 1); *j = W; }
+    else if (k < 2 * (H + 1) + W + 1) { *i = 0; *j = k - 2 * (H + 1); }
+    else { *i = H; *j = k - 2 * (H + 1) - (W + 1); }
+}
+
+template <typename Op>
+__device__ __forceinline__ double block_reduce(double x, double* red, Op op) {
+    for (int o = 16; o > 0; o >>= 1) x = op(x, __shfl_xor_sync(0xffffffffu, x, o));
+    __syncthreads();  // red is reused between reductions
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = x;
+    __syncthreads();
+    x = red[0];
+    for (int k = 1; k < (int)(blockDim.x + 31) / 32; ++k) x = op(x, red[k]);
+    return x;
+}
+
+__global__ void __launch_bounds__(256) k_boundary_chord(WcsDev w, const double* src_sph, int H, int W,
+                                                        const double* corners, SrcInfo* info) {
+    __shared__ double red[32];
+    const int s = blockIdx.x, W1 = W + 1, nb = 2 * (H + 1) + 2 * (W + 1);
+    const double ra = src_sph[2 * s], dec = src_sph[2 * s + 1];
     double sd[3];
     sph2dir(ra, dec, sd);
-    int W1 = W + 1;
-    int nb = 2 * (H + 1) + 2 * (W + 1);
-    double mn = 360.;
-    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+    auto chord2 = [&](int k) {
         int i, j;
-        if (k < H + 1) { i = k; j = 0; }
-        else if (k < 2 * (H + 1)) { i = k - (H + 1); j = W; }
-        else if (k < 2 * (H + 1) + W + 1) { i = 0; j = k - 2 * (H + 1); }
-        else { i = H; j = k - 2 * (H + 1) - (W + 1); }
-        double d = R2D * dir_diff(sd, corners + 3 * (i * W1 + j));
-        mn = mn < d ? mn : d;
-    }
-    for (int o = 16; o > 0; o >>= 1) { double t = __shfl_xor_sync(0xffffffffu, mn, o); mn = mn < t ? mn : t; }
-    __shared__ double red[32];
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mn;
-    __syncthreads();
+        border_point(k, H, W, &i, &j);
+        const double* c = corners + 3 * ((size_t)i * W1 + j);
+        const double x = sd[0] - c[0], y = sd[1] - c[1], z = sd[2] - c[2];
+        return x * x + y * y + z * z;
+    };
+    double m = INFINITY;
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) m = fmin(m, chord2(k));
+    m = block_reduce(m, red, [](double a, double b) { return fmin(a, b); });
+    double mn = 360.;
+    const double lim = m * (1.0 + 1e-12);
+    for (int k = threadIdx.x; k < nb; k += blockDim.x)
+        if (chord2(k) <= lim) {
+            int i, j;
+            border_point(k, H, W, &i, &j);
+            const double d = R2D * dir_diff(sd, corners + 3 * ((size_t)i * W1 + j));
+            mn = mn < d ? mn : d;
+        }
+    mn = block_reduce(mn, red, [](double a, double b) { return a < b ? a : b; });
     if (threadIdx.x == 0) {
-        for (int k = 1; k < (int)(blockDim.x + 31) / 32; ++k) mn = mn < red[k] ? mn : red[k];
         double r = ra > 180. ? ra - 360. : (ra < -180. ? ra + 360. : ra), p1, p2;
         sph2pix(w, r, dec, &p1, &p2);
         const double buf = 3.5;
@@ -429,13 +474,15 @@ __device__ double correction_factor(const SrcInfo& si, const double* U, const do
 
 // c7 (1/sum) + c9 (containment factor) + c8/c10 folded into one per-(s,e) scale.
 // Block (s, group of 8 energies): fold the source's chunk histograms, then one
-// warp per energy.
+// warp per energy.  With lut given, the block also writes its 8 energies of the
+// source's scaled FP32 table lut[s][r][e] = uPsf * scale (energies E..Epad-1 zero).
 __global__ void __launch_bounds__(256) k_correction_hist(const double* hist_in, int nch, const SrcInfo* info,
                                                          const double* upsf, const double* partial,
                                                          const double* expo, int E, double* scale,
                                                          double* inv_out, double* fac_out,
-                                                         double* rad_out, int* fov_out) {
+                                                         double* rad_out, int* fov_out, float* lut, int Epad) {
     __shared__ double hsum[ND];
+    __shared__ double ssc[8];
     int s = blockIdx.x;
     SrcInfo si = info[s];
     for (int r = threadIdx.x; r < ND; r += blockDim.x) {
@@ -447,35 +494,45 @@ __global__ void __launch_bounds__(256) k_correction_hist(const double* hist_in, 
     const double* U = upsf + (size_t)s * ND * E;
     // one warp per energy (8 energies per block): lanes split the rows, then a
     // fixed shuffle order
-    const int lane = threadIdx.x & 31;
-    {
-        const int e = blockIdx.y * 8 + (threadIdx.x >> 5);
-        if (e >= E) return;
+    const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+    const int e = blockIdx.y * 8 + wq;
+    if (e < E) {
         int i = s * E + e;
         double sum = 0.;
         if (si.in_fov) {
             for (int r = lane; r < ND; r += 32) sum = fma(hsum[r], U[(size_t)r * E + e], sum);
             for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
         }
-        if (lane != 0) return;
-        const double inv = sum != 0. ? 1.0 / sum : sum;
-        const double factor = correction_factor(si, U, partial + (size_t)s * ND * E, E, e, inv);
-        scale[i] = expo[i] * factor;
-        if (inv_out) inv_out[i] = inv;
-        if (fac_out) fac_out[i] = factor;
-        if (e == 0) {
-            if (rad_out) rad_out[s] = si.radius_deg;
-            if (fov_out) fov_out[s] = si.in_fov;
+        if (lane == 0) {
+            const double inv = sum != 0. ? 1.0 / sum : sum;
+            const double factor = correction_factor(si, U, partial + (size_t)s * ND * E, E, e, inv);
+            scale[i] = expo[i] * factor;
+            ssc[wq] = scale[i];
+            if (inv_out) inv_out[i] = inv;
+            if (fac_out) fac_out[i] = factor;
+            if (e == 0) {
+                if (rad_out) rad_out[s] = si.radius_deg;
+                if (fov_out) fov_out[s] = si.in_fov;
+            }
         }
+    }
+    if (!lut) return;
+    __syncthreads();
+    const int e0 = blockIdx.y * 8, ne = min(8, Epad - e0);
+    for (int k = threadIdx.x; k < ND * ne; k += blockDim.x) {
+        const int r = k / ne, j = k - r * ne, ee = e0 + j;
+        lut[((size_t)s * ND + r) * Epad + ee] = ee < E ? (float)(U[(size_t)r * E + ee] * ssc[j]) : 0.f;
     }
 }
 
 int launch_correction(const double* hist, int nch, const SrcInfo* info, int S, const double* upsf,
                       const double* partial, const double* exposure, int E, double* scale,
                       double* inv_integ, double* correction, double* radius, int* in_fov,
-                      cudaStream_t st) {
-    XTS_LAUNCH("k_correction", st, k_correction_hist<<<dim3(S, (E + 7) / 8), 256, 0, st>>>(hist, nch, info, upsf, partial, exposure, E,
-                                                                        scale, inv_integ, correction, radius, in_fov));
+                      cudaStream_t st, float* lut, int Epad) {
+    const int ny = ((lut && Epad > E ? Epad : E) + 7) / 8;
+    XTS_LAUNCH("k_correction", st, k_correction_hist<<<dim3(S, ny), 256, 0, st>>>(hist, nch, info, upsf, partial, exposure, E,
+                                                                        scale, inv_integ, correction, radius, in_fov,
+                                                                        lut, Epad));
     return XTS_OK;
 }
 
@@ -559,11 +616,15 @@ int launch_srcmap(const SrcmapDev& a, cudaStream_t st) {
     double* hist = (double*)workspace(W_PARTSUM, sizeof(double) * (size_t)S * nch * ND + 8);
     double* scale = (double*)workspace(W_SCALE, sizeof(double) * (size_t)S * E + 8);
     if (!corners || !centers || !omega || !info || !hist || !scale) return XTS_ERR_OOM;
-    XTS_LAUNCH("k_grids", st, k_grids<<<(unsigned)((ng + 127) / 128), 128, 0, st>>>(w, H, W, corners, centers));
-    XTS_LAUNCH("k_solid_angle", st, k_solid_angle<<<(npix + 127) / 128, 128, 0, st>>>(centers, H, W, omega));
+    // map geometry on the geometry stream when one is given (joined before uPsf is read)
+    StreamJoin geo(a.geo_stream && a.join_ev ? a.geo_stream : st, st, a.join_ev);
+    cudaStream_t gs = geo.from;
+    const dim3 gg((unsigned)((W + GT) / GT), (unsigned)((H + GT) / GT));  // tiles over the (H+1) x (W+1) grid
+    XTS_LAUNCH("k_map_geometry", gs, k_map_geometry<<<gg, GEO_THREADS, 0, gs>>>(w, H, W, corners, centers, omega));
     if (S == 0) return XTS_OK;
-    XTS_LAUNCH("k_boundary", st, k_boundary<<<S, 128, 0, st>>>(w, a.src_sph, H, W, corners, info));
+    XTS_LAUNCH("k_boundary", gs, k_boundary_chord<<<S, 256, 0, gs>>>(w, a.src_sph, H, W, corners, info));
     if (a.adaptive) {
+        if ((rc = geo.join())) return rc;
         if (a.out_f64 || !srcmap_adaptive_supported(E))
             return set_error(XTS_ERR_ARG, "adaptive cubature: FP32 maps with E <= 256 only");
         return launch_srcmap_adaptive(a, corners, centers, omega, info, scale, nch, st);
@@ -574,8 +635,9 @@ int launch_srcmap(const SrcmapDev& a, cudaStream_t st) {
         XTS_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
         return launch_srcmap_win(corners, centers, omega, info, S, H, W, E, a.upsf, a.partial,
                                  a.exposure, scale, a.inv_integ, a.correction, a.radius, a.in_fov, status,
-                                 (float*)a.out, a.chunk_sources, a.on_chunk, a.on_chunk_ctx, st);
+                                 (float*)a.out, a.chunk_sources, a.on_chunk, a.on_chunk_ctx, geo, st);
     }
+    if ((rc = geo.join())) return rc;
     if (a.out_f64) {  // the reference's own per-point FP64 arithmetic throughout
         XTS_LAUNCH("k_map_integral_f64", st, k_map_integral_hist<<<dim3(nch, S), 256, 0, st>>>(corners, centers, omega, info, H, W, nch, hist));
     } else {

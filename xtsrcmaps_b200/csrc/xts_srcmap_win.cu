@@ -29,8 +29,8 @@ namespace xts {
 // ============================================================================ pass A
 constexpr int WT = 256;  // pixels per tile == threads per block
 
-constexpr size_t WA_OFF_SQ = 0;
-constexpr size_t WA_OFF_COEF = (8 * (ND + 1) + 15) / 16 * 16;
+constexpr size_t WA_OFF_BINS = 0;
+constexpr size_t WA_OFF_COEF = sizeof(SepBin) * NSB;
 constexpr size_t WA_OFF_HIST = WA_OFF_COEF + sizeof(float4) * 2 * ND;
 constexpr size_t WA_OFF_WTS = WA_OFF_HIST + (8 * ND + 15) / 16 * 16;
 constexpr size_t WA_OFF_BASE = WA_OFF_WTS + sizeof(float) * WT * RW;
@@ -39,21 +39,21 @@ constexpr size_t WA_SMEM = WA_OFF_BASE + sizeof(int) * (WT + 4);
 constexpr int NSP = 24;  // entries of a sparse record: 12 points x 2 rows
 constexpr int META_OVERFLOW = -0x7fffffff - 1;  // wide pixel without a sparse record
 
-__global__ void __launch_bounds__(WT, 3) k_pixel_windows(const double* __restrict__ corners, const double* __restrict__ centers,
+__global__ void __launch_bounds__(WT, 4) k_pixel_windows(const double* __restrict__ corners, const double* __restrict__ centers,
                                                       const double* __restrict__ omega, const SrcInfo* __restrict__ info,
                                                       const SepTab* __restrict__ septab, int H, int W, int nch,
                                                       double* __restrict__ hist_out, float4* __restrict__ win,
                                                       int* __restrict__ wmeta, float2* __restrict__ sparse,
                                                       int sparse_cap, int* __restrict__ sparse_count) {
     extern __shared__ __align__(16) unsigned char smem[];
-    double* sq = (double*)(smem + WA_OFF_SQ);
+    SepBin* sbin = (SepBin*)(smem + WA_OFF_BINS);
     float4* scoef = (float4*)(smem + WA_OFF_COEF);
     double* hist = (double*)(smem + WA_OFF_HIST);
     float* wts = (float*)(smem + WA_OFF_WTS);    // [RW][WT] windows (row-major by window slot)
     int* wbase = (int*)(smem + WA_OFF_BASE);     // [WT] first row (-1: not in radius); [WT..WT+3] row min/max by parity
     const int s = blockIdx.y, t = threadIdx.x;
     const SrcInfo si = info[s];
-    for (int k = t; k < ND + 1; k += WT) sq[k] = septab->q[k];
+    for (int k = t; k < NSB; k += WT) sbin[k] = septab->bins[k];
     for (int k = t; k < 2 * ND; k += WT) scoef[k] = ((const float4*)septab->coef)[k];
     for (int r = t; r < ND; r += WT) hist[r] = 0.;
     if (t < 4) wbase[WT + t] = (t & 1) ? -1 : ND;
@@ -82,10 +82,10 @@ __global__ void __launch_bounds__(WT, 3) k_pixel_windows(const double* __restric
                 else if (d2 > ch2 * (1.0 + 1e-12)) inside = false;
                 else inside = dir_diff(si.dir, c) <= si.radius_rad;
             }
-            const PixGeom g = pixel_geom(corners, W1, h, w, si);
+            const PixQ g = pixel_q(pixel_geom(corners, W1, h, w, si));
             const float om = (float)omega[pix];
             float tc;
-            const int ic = point_row(fma(g.Ax, g.Ax, fma(g.Ay, g.Ay, g.Az * g.Az)), sq, scoef, &tc);
+            const int ic = point_row_bin(g.a0, sbin, scoef, &tc);
             const int base = min(max(ic - 1 - RW / 2, 0), ND - RW);
             float* wd = wts + t;  // slot j at wd[j * WT]: lanes hit consecutive words
 #pragma unroll
@@ -95,9 +95,9 @@ __global__ void __launch_bounds__(WT, 3) k_pixel_windows(const double* __restric
 #pragma unroll
             for (int p = 0; p < 12; ++p) {
                 float tt;
-                const int idx = point_row(point_q(g, p), sq, scoef, &tt);
+                const int idx = point_row_bin(point_q2(g, p), sbin, scoef, &tt);
                 const int r = idx - 1 - base;
-                const float wo = (float)c_rule_uv[p][3] * om;
+                const float wo = c_rule_w32[p] * om;
                 const float wa = (1.f - tt) * wo, wb = tt * wo;
                 if (r >= 0 && r < RW - 1) {
                     wd[r * WT] += wa;
@@ -128,8 +128,8 @@ __global__ void __launch_bounds__(WT, 3) k_pixel_windows(const double* __restric
                     float2* rec = sparse + (size_t)slot * NSP;
                     for (int p = 0; p < 12; ++p) {
                         float tt;
-                        const int idx = point_row(point_q(g, p), sq, scoef, &tt);
-                        const float wo = (float)c_rule_uv[p][3] * om;
+                        const int idx = point_row_bin(point_q2(g, p), sbin, scoef, &tt);
+                        const float wo = c_rule_w32[p] * om;
                         rec[2 * p] = make_float2((1.f - tt) * wo, __int_as_float(idx - 1));
                         rec[2 * p + 1] = make_float2(tt * wo, __int_as_float(idx));
                     }
@@ -434,7 +434,7 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
                       double* scale, double* inv_integ, double* correction, double* radius,
                       int* in_fov, int* status, float* out, int chunk_sources,
                       int (*on_chunk)(void*, int, int, cudaStream_t), void* on_chunk_ctx,
-                      cudaStream_t st) {
+                      StreamJoin& geo, cudaStream_t st) {
     int rc = upload_rule_uv(st);
     if (rc) return rc;
     const SepTab* tab = nullptr;
@@ -459,15 +459,19 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
     int dev = 0, nsm = 148, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    // pass A: about four blocks per SM over the chunk's sources; the row
-    // histograms of a chunk ([Sc][nch][401]) are reused by the next chunk
-    int nch = (4 * nsm + Sc - 1) / Sc;
+    // pass A: as many blocks as fit on the GPU at once (one full wave: a partial
+    // second wave would run at low occupancy); the row histograms of a chunk
+    // ([Sc][nch][401]) are reused by the next chunk
+    int resident = 0;
+    XTS_CUDA(cudaFuncSetAttribute(k_pixel_windows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WA_SMEM));
+    XTS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_pixel_windows, WT, WA_SMEM));
+    resident = (resident < 1 ? 1 : resident) * nsm;
+    int nch = resident / Sc;
     const int maxch = (npix + WT - 1) / WT;
     nch = nch < 1 ? 1 : (nch > maxch ? maxch : nch);
     double* hist = (double*)workspace(W_PARTSUM, sizeof(double) * (size_t)Sc * nch * ND + 8);
     if (!win || !wmeta || !lut || !sparse || !hist) return XTS_ERR_OOM;
     int* sparse_count = status + 1;
-    XTS_CUDA(cudaFuncSetAttribute(k_pixel_windows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WA_SMEM));
     const WritePassFn wp = k_write_pass[(E + 3) / 4 - 1];
     rc = wp(0, L.total, st, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, 0, 0, E, EQ,
             nullptr, nullptr, &per_sm, nsm, true);
@@ -476,18 +480,19 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
     for (int s0 = 0; s0 < S; s0 += Sc) {
         const int n = S - s0 < Sc ? S - s0 : Sc;
         const size_t oE = (size_t)s0 * E;
-        XTS_CUDA(cudaMemsetAsync(sparse_count, 0, sizeof(int), st));
-        XTS_LAUNCH("k_pixel_windows", st, k_pixel_windows<<<dim3(nch, n), WT, WA_SMEM, st>>>(
+        // the first chunk's window pass is geometry only: it may run on the geometry stream
+        const cudaStream_t as = s0 == 0 ? geo.from : st;
+        XTS_CUDA(cudaMemsetAsync(sparse_count, 0, sizeof(int), as));
+        XTS_LAUNCH("k_pixel_windows", as, k_pixel_windows<<<dim3(nch, n), WT, WA_SMEM, as>>>(
                                               corners, centers, omega, info + s0, tab, H, W, nch,
                                               hist, win, wmeta, sparse, (int)cap,
                                               sparse_count));
+        if ((rc = geo.join())) return rc;
         rc = launch_correction(hist, nch, info + s0, n, upsf + oE * ND, partial + oE * ND,
                                exposure + oE, E, scale + oE, inv_integ ? inv_integ + oE : nullptr,
                                correction ? correction + oE : nullptr, radius ? radius + s0 : nullptr,
-                               in_fov ? in_fov + s0 : nullptr, st);
+                               in_fov ? in_fov + s0 : nullptr, st, lut, EQ * 4);
         if (rc) return rc;
-        XTS_LAUNCH("k_lut_scaled", st, k_lut_scaled<<<lut_scaled_grid(n), 256, 0, st>>>(
-                                           upsf + oE * ND, scale + oE, n, E, EQ * 4, lut, nullptr, nullptr));
         const long long T = (long long)n * ((npix + BT - 1) / BT);
         long long G = (long long)nsm * per_sm;
         if (G > T) G = T;
