@@ -38,7 +38,8 @@ enum xts_status {
     XTS_ERR_CUDA = -2,    /* a CUDA runtime call failed */
     XTS_ERR_OOM = -3,     /* device allocation failed */
     XTS_ERR_TIMEOUT = -4, /* a bounded device-side wait gave up */
-    XTS_ERR_NODEV = -5    /* no usable sm_100 device */
+    XTS_ERR_NODEV = -5,   /* no usable sm_100 device */
+    XTS_ERR_IO = -6       /* a file could not be opened or written */
 };
 
 enum xts_flags {
@@ -47,8 +48,9 @@ enum xts_flags {
     /* 1u << 2 is reserved */
     XTS_CUDA_CORES = 1u << 3,    /* FP32 source maps by the single-pass CUDA-core kernel (geometry and
                                     map integral in separate passes; default: the two-pass window path) */
-    XTS_TCGEN05 = 1u << 4        /* FP32 source maps with the window-times-table product on tcgen05
+    XTS_TCGEN05 = 1u << 4,       /* FP32 source maps with the window-times-table product on tcgen05
                                     tensor cores (3xTF32); default: the two-pass window path */
+    XTS_FITS_F32 = 1u << 5       /* xts_write_src_model: BITPIX -32 images (default -64, as the reference) */
 };
 
 /* FITS celestial WCS (sky_geom/sky_geom.hxx:17-25, WcsConfig). */
@@ -229,6 +231,19 @@ int xts_point_source_maps(const xts_expcube* exp_cube, const xts_expcube* wexp_c
                           const xts_grid* psf_front, const xts_grid* psf_back,
                           const double* front_ltf, const xts_wcs* wcs, void* model_map,
                           xts_srcmap_info* info, unsigned flags, void* stream);
+
+/* Fermi::fits::write_src_model (xtsrcmaps/fits/fits.write_src_model.cxx:10-66, the
+ * commented-out call at main.cxx:40): the maps [S, H, W, E] (float, or double with
+ * XTS_OUT_F64) written to a FITS file.  Primary HDU without data, HDUNAME =
+ * 'PRIMARY'; then per source an IMAGE extension, EXTNAME = names[s] (NULL names
+ * or entries: "SRC%05d"), NAXIS1 = H, NAXIS2 = W, NAXIS3 = E holding
+ * img[e][w][h] = map[s][h][w][e] (the reference's SHWE -> SEHW reorder), BITPIX
+ * -64 (XTS_FITS_F32: -32), with CHECKSUM and DATASUM.  The reorder, conversion,
+ * byte order and data sums run on the device; the file is complete when the call
+ * returns.  XTS_DEVICE_PTRS: model_map is a device pointer.  Names: printable
+ * ASCII, at most 68 characters (a quote counts twice). */
+int xts_write_src_model(const char* filename, const void* model_map, int S, int H, int W, int E,
+                        const char* const* names, unsigned flags, void* stream);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,84 @@
+"""FITS output on the GPU (xts_write_src_model): the library's file is
+byte-identical to the oracle's restatement of Fermi::fits::write_src_model for
+the same maps, from device and host maps, float and double, BITPIX -64 and -32,
+in one chunk and in many; every HDU satisfies the checksum convention."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import fits_oracle as F
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def api():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from xtsrcmaps_b200 import api as A
+    from xtsrcmaps_b200 import build
+
+    build.build()
+    A.init(0)
+    return A
+
+
+@pytest.mark.parametrize("dtype,bitpix,device,chunk_mb", [
+    (np.float32, -64, True, None), (np.float32, -32, False, None),
+    (np.float64, -32, True, None), (np.float64, -64, False, "1"), (np.float32, -64, True, "1")])
+def test_fits_bytes_match_oracle(api, tmp_path, monkeypatch, dtype, bitpix, device, chunk_mb):
+    import torch
+
+    if chunk_mb:
+        monkeypatch.setenv("XTS_FITS_CHUNK_MB", chunk_mb)
+    rng = np.random.default_rng(5)
+    S, H, W, E = 9, 67, 45, 37  # ragged tiles in h and e; 9 x 0.9 MB (f64) spans several 1 MiB chunks
+    m = (rng.lognormal(0.0, 3.0, (S, H, W, E)) * rng.choice([-1.0, 1.0], (S, H, W, E))).astype(dtype)
+    names = ["PS J%04d" % s for s in range(S)]
+    names[2] = "it's"
+    ours, ref = str(tmp_path / "gpu.fits"), str(tmp_path / "ref.fits")
+    arg = torch.as_tensor(m, device="cuda") if device else m
+    api.write_src_model(ours, arg, names, bitpix)
+    F.write_src_model(ref, m, names, bitpix)
+    a, b = open(ours, "rb").read(), open(ref, "rb").read()
+    assert len(a) == len(b)
+    assert a == b
+    for hdr, hb, db, _ in F.read_fits(ours)[1:]:
+        assert F.hdu_checksum(hb, db) == 0xffffffff
+
+
+def test_fits_of_computed_maps(api, tmp_path):
+    """The maps of the fused call on c0, straight from device memory to a file
+    whose images are the maps in SEHW order."""
+    import torch
+
+    from xtsrcmaps_b200.synth import make_job
+
+    job = make_job("c0", seed=2)
+    d = torch.device("cuda")
+    ltf = api.livetime_efficiency_factors(job.logEs, job.effic_front)
+    nf = api.normalize_rpsf(job.rpsf_front, job.scale_front)
+    nb = api.normalize_rpsf(job.rpsf_back, job.scale_back)
+    m, _ = api.point_source_maps(job.wcs, job.src_sph, job.exp_cube, job.wexp_cube, job.logEs, job.aeff_front,
+                                 job.aeff_back, nf, nb, ltf, with_info=False)
+    fn = str(tmp_path / "c0.fits")
+    api.write_src_model(fn, torch.as_tensor(m, device=d), ["SRC A"])
+    hdus = F.read_fits(fn)
+    assert len(hdus) == 2 and hdus[1][0]["EXTNAME"] == "SRC A"
+    np.testing.assert_array_equal(hdus[1][3], np.transpose(m[0], (2, 1, 0)).astype(np.float64))
+    assert F.hdu_checksum(hdus[1][1], hdus[1][2]) == 0xffffffff
+
+
+def test_fits_bad_names(api, tmp_path):
+    from xtsrcmaps_b200 import _lib
+
+    m = np.zeros((1, 2, 2, 1), np.float32)
+    with pytest.raises(_lib.XtsError) as ei:
+        api.write_src_model(str(tmp_path / "x.fits"), m, ["x" * 69])
+    assert ei.value.code == _lib.XTS_ERR_ARG
+    with pytest.raises(_lib.XtsError) as ei:
+        api.write_src_model(str(tmp_path / "no_such_dir" / "x.fits"), m)
+    assert ei.value.code == _lib.XTS_ERR_IO

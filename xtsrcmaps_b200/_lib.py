@@ -18,11 +18,13 @@ XTS_ERR_CUDA = -2
 XTS_ERR_OOM = -3
 XTS_ERR_TIMEOUT = -4
 XTS_ERR_NODEV = -5
+XTS_ERR_IO = -6
 
 XTS_DEVICE_PTRS = 1 << 0
 XTS_OUT_F64 = 1 << 1
 XTS_CUDA_CORES = 1 << 3
 XTS_TCGEN05 = 1 << 4
+XTS_FITS_F32 = 1 << 5
 
 ND = 401
 
@@ -102,6 +104,8 @@ SIGNATURES = {
                                                        C.POINTER(XtsSrcmapInfo), C.c_uint, _vp]),
     "xts_point_src_model_map_wcs": (C.c_int, [C.POINTER(XtsWcs), _vp, C.c_int, _vp, _vp, _vp,
                                               C.c_int, _vp, C.POINTER(XtsSrcmapInfo), C.c_uint, _vp]),
+    "xts_write_src_model": (C.c_int, [C.c_char_p, _vp, C.c_int, C.c_int, C.c_int, C.c_int,
+                                      C.POINTER(C.c_char_p), C.c_uint, _vp]),
 }
 
 

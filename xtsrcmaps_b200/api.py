@@ -401,6 +401,47 @@ def point_source_maps(wcs: Wcs, src_sph, exp_cube: ExpCube, wexp_cube: ExpCube, 
     return m, info
 
 
+def write_src_model(filename: str, model_map, names=None, bitpix: int = -64) -> None:
+    """Fermi::fits::write_src_model (fits/fits.write_src_model.cxx:10-66): the maps
+    [S, H, W, E] (float32 or float64, host array or CUDA tensor) written as a FITS
+    file, one IMAGE extension per source named ``names[s]`` (default SRC%05d),
+    data in SEHW order (img[e][w][h] = map[s][h][w][e]), BITPIX -64 as the
+    reference or -32, with CHECKSUM and DATASUM.  The reorder, conversion, byte
+    swap and data sums run on the GPU."""
+    if bitpix not in (-64, -32):
+        raise ValueError("bitpix must be -64 or -32")
+    dev = _is_cuda(model_map)
+    if dev:
+        m = model_map.contiguous()
+        f64 = str(m.dtype) == "torch.float64"
+        if not f64 and str(m.dtype) != "torch.float32":
+            raise ValueError("model_map must be float32 or float64")
+        ptr = C.c_void_p(m.data_ptr())
+        import torch
+
+        handle = torch.cuda.current_stream(m.device).cuda_stream
+        stream = C.c_void_p(handle if handle else 1)
+    else:
+        m = np.asarray(model_map)
+        if m.dtype not in (np.float32, np.float64):
+            raise ValueError("model_map must be float32 or float64")
+        m = np.ascontiguousarray(m)
+        f64 = m.dtype == np.float64
+        ptr = C.c_void_p(m.ctypes.data)
+        stream = None
+    if m.ndim != 4:
+        raise ValueError("model_map must be [S, H, W, E]")
+    S, H, W, E = (int(x) for x in m.shape)
+    cnames = None
+    if names is not None:
+        if len(names) != S:
+            raise ValueError("one name per source")
+        enc = [str(n).encode("ascii") for n in names]
+        cnames = (C.c_char_p * S)(*enc)
+    flags = (L.XTS_DEVICE_PTRS if dev else 0) | (L.XTS_OUT_F64 if f64 else 0) | (L.XTS_FITS_F32 if bitpix == -32 else 0)
+    L.check(L.lib().xts_write_src_model(str(filename).encode(), ptr, S, H, W, E, cnames, flags, stream))
+
+
 def compute_srcmaps(wcs: Wcs, src_sph, exp: XtExp, psf: XtPsf, out_dtype: str = "float32", out=None):
     """ModelMap::compute_srcmaps<PointSource> (model_map/model_map.compute_src_maps.cxx:6-22)."""
     m, _ = point_src_model_map_wcs(wcs, src_sph, exp.exposure, psf.uPsf, psf.partial_psf_integral,

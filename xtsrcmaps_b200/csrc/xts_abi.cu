@@ -701,4 +701,16 @@ int xts_point_source_maps(const xts_expcube* cube, const xts_expcube* wcube, con
     return run_srcmap(sg, ma, model_map, npix, f64);
 }
 
+int xts_write_src_model(const char* filename, const void* model_map, int S, int H, int W, int E,
+                        const char* const* names, unsigned flags, void* stream) {
+    XTS_ENTER();
+    if (!filename || S < 0 || H <= 0 || W <= 0 || E <= 0 || (S > 0 && !model_map))
+        return set_error(XTS_ERR_ARG, "write_src_model: null argument or bad size");
+    if (W > 65535 || S > (1 << 30))
+        return set_error(XTS_ERR_ARG, "write_src_model: W must be at most 65535");
+    return write_src_model(filename, model_map, S, H, W, E, names, (flags & XTS_DEVICE_PTRS) != 0,
+                           (flags & XTS_OUT_F64) != 0, (flags & XTS_FITS_F32) == 0,
+                           stream ? (cudaStream_t)stream : g_ctx.stream);
+}
+
 }  // extern "C"

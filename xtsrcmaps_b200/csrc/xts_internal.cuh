@@ -64,6 +64,7 @@ enum Slot {
     // internal scratch
     W_CORNERS, W_CENTERS, W_OMEGA, W_LUT, W_PARTSUM, W_SRCINFO, W_SCALE, W_PSFTAB,
     W_KING, W_MISC, W_WIN, W_WMETA, W_SPARSE, W_MISC2, W_EXPMAP,
+    W_FITS_IN, W_FITS_OUT, W_FITS_SUM,
     N_SLOTS
 };
 void* workspace(int slot, size_t bytes);  // nullptr + error set on OOM
@@ -165,6 +166,8 @@ int launch_correction(const double* hist, int nch, const SrcInfo* info, int S, c
                       double* inv_integ, double* correction, double* radius, int* in_fov,
                       cudaStream_t st, float* lut = nullptr, int Epad = 0);  // lut: scaled FP32 table too
 bool srcmap_win_supported(int E);
+int write_src_model(const char* filename, const void* model_map, int S, int H, int W, int E,
+                    const char* const* names, bool dev_ptrs, bool f64in, bool f64out, cudaStream_t st);
 bool exposure_map_supported(int C, int E);
 int launch_exposure_map_tc(const float* cube, const float* wcube, long long npix, int C, const double* front_aeff,
                            const double* back_aeff, const double* ltf, int E, double* out, int* status,
