@@ -53,3 +53,12 @@ def test_checksum_detects_a_flipped_byte(tmp_path):
     bad = bytearray(db)
     bad[5] ^= 0x10
     assert F.hdu_checksum(hb, bytes(bad)) != 0xffffffff
+
+
+def test_cli_help():
+    import subprocess
+    import sys
+
+    r = subprocess.run([sys.executable, "-m", "xtsrcmaps_b200", "--help"], capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 0 and "--out" in r.stdout

@@ -82,3 +82,19 @@ def test_fits_bad_names(api, tmp_path):
     with pytest.raises(_lib.XtsError) as ei:
         api.write_src_model(str(tmp_path / "no_such_dir" / "x.fits"), m)
     assert ei.value.code == _lib.XTS_ERR_IO
+
+
+def test_cli_end_to_end(api, tmp_path):
+    """python -m xtsrcmaps_b200: the main.cxx flow with the write call, on c0."""
+    from xtsrcmaps_b200.__main__ import main
+
+    src = tmp_path / "src.npz"
+    np.savez(src, src_sph=np.array([[193.98, -5.82], [194.5, -6.3]]), names=np.array(["A", "B"]))
+    fn = str(tmp_path / "cli.fits")
+    assert main(["--config", "c0", "--sources", str(src), "--out", fn, "--bitpix", "-32"]) == 0
+    hdus = F.read_fits(fn)
+    assert [h[0].get("EXTNAME") for h in hdus[1:]] == ["A", "B"]
+    for hdr, hb, db, arr in hdus[1:]:
+        assert hdr["BITPIX"] == -32 and arr.shape == (20, 100, 100)
+        assert F.hdu_checksum(hb, db) == 0xffffffff
+        assert np.isfinite(arr).all() and arr.max() > 0

@@ -81,7 +81,8 @@ __global__ void k_exposure_f64(const double* ecb, const double* wecb, int S, int
     if (i >= S * E) return;
     int s = i / E, e = i - s * E;
     double ef = 0, wf = 0, eb = 0, wb = 0;
-    for (int c = 0; c < C; ++c) {
+#pragma unroll 8
+    for (int c = 0; c < C; ++c) {  // unrolled: eight rows of loads in flight, sums still in c order
         double x = ecb[s * C + c], w = wecb[s * C + c];
         double a = af[c * E + e], b = ab[c * E + e];
         ef = fma(x, a, ef); wf = fma(w, a, wf);

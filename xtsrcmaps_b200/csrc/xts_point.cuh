@@ -263,6 +263,23 @@ __device__ __forceinline__ int point_row_bin(double q, const SepBin* bins, const
     return k + 1;
 }
 
+// point_row_bin without the out-of-range branch: t is NaN for points outside
+// 1e-4 deg .. 70 deg (the caller evaluates those with t_exact), so a run of
+// these lookups has no call in it and the compiler can overlap them.
+__device__ __forceinline__ int point_row_bin_nc(double q, const SepBin* bins, const float4* coef, float* t_out) {
+    int b = (__double2hiint(q) >> (20 - SB_BITS)) - (SB_EXP0 << SB_BITS);
+    b = min(max(b, 0), NSB - 1);
+    const SepBin sb = bins[b];
+    const int k = sb.k0 + (q >= sb.thr);
+    const float4 c0 = coef[2 * k], c1 = coef[2 * k + 1];
+    const double qlo = __hiloint2double(__float_as_int(c1.w), __float_as_int(c1.z));
+    const float dl = (float)(q - qlo) * c0.x;
+    const float zz = fmaf(dl, 1.f / DPOLY_H, -DPOLY_C / DPOLY_H);
+    const float P = fmaf(fmaf(fmaf(fmaf(c1.y, zz, c1.x), zz, c0.w), zz, c0.z), zz, c0.y);
+    *t_out = (dl >= -0.002f && dl <= 0.072f) ? (float)REDM1 * (dl * P) : __int_as_float(0x7fffffff);
+    return k + 1;
+}
+
 // Bilinear form of the rule points of pixel (h, w) relative to the source.
 struct PixGeom { double Ax, Ay, Az, Bx, By, Bz, Cx, Cy, Cz, Dx, Dy, Dz; };
 

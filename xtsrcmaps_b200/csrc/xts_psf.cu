@@ -53,11 +53,36 @@ __device__ inline void lerp_pars2(const double* g, int n, double v, double* wgt,
     *wgt = t; *cmpl = 1. - t; *idx = i;
 }
 
-// b4 + the aeff product of b5, both sides summed: PA[c][d][e].
+// b4 + the aeff product of b5, both sides summed: PA[c][d][e].  The bilinear
+// weights depend on (side, e) and (side, c) only: each block looks them up once
+// for all energies and its (at most two) cos-theta bins into shared memory.
+static size_t psf_aeff_smem(int E) { return sizeof(double) * (4 * (size_t)E + 8) + sizeof(int) * (2 * (size_t)E + 4); }
+
 __global__ void k_psf_aeff(xts_grid pf, xts_grid pb, const double* kf, const double* kb,
                            const double* costh, int C, const double* logEs, int E,
                            const double* af, const double* ab, double* pa) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    extern __shared__ double sh[];
+    double* sew = sh;              // [2][E] energy weight, complement
+    double* sec = sew + 2 * E;
+    double* scw = sec + 2 * E;     // [2 sides][2 bins] cos-theta weight, complement
+    double* scc = scw + 4;
+    int* sei = (int*)(scc + 4);    // [2][E], [2][2] indices
+    int* sci = sei + 2 * E;
+    const int i0 = blockIdx.x * blockDim.x;
+    const int cfirst = i0 / (ND * E);
+    for (int k = threadIdx.x; k < 2 * E + 4; k += blockDim.x) {
+        if (k < 2 * E) {
+            const int side = k / E, e = k - side * E;
+            const xts_grid& g = side ? pb : pf;
+            lerp_pars2(g.logEs, g.n_e, logEs[e], &sew[k], &sec[k], &sei[k]);
+        } else {
+            const int j = k - 2 * E, side = j >> 1, c = cfirst + (j & 1);
+            const xts_grid& g = side ? pb : pf;
+            if (c < C) lerp_pars2(g.cosths, g.n_cos, costh[c], &scw[j], &scc[j], &sci[j]);
+        }
+    }
+    __syncthreads();
+    int i = i0 + threadIdx.x;
     if (i >= C * ND * E) return;
     int e = i % E;
     int cd = i / E;
@@ -66,9 +91,9 @@ __global__ void k_psf_aeff(xts_grid pf, xts_grid pb, const double* kf, const dou
     for (int side = 0; side < 2; ++side) {
         const xts_grid& g = side ? pb : pf;
         const double* K = (side ? kb : kf) + (size_t)d * g.n_cos * g.n_e;
-        double cw, cc, ew, ec; int ci, ei;
-        lerp_pars2(g.cosths, g.n_cos, costh[c], &cw, &cc, &ci);
-        lerp_pars2(g.logEs, g.n_e, logEs[e], &ew, &ec, &ei);
+        const int jc = 2 * side + (c - cfirst), je = side * E + e;
+        const double cw = scw[jc], cc = scc[jc], ew = sew[je], ec = sec[je];
+        const int ci = sci[jc], ei = sei[je];
         int Me = g.n_e;
         double b = cc * ec * K[(ci - 1) * Me + ei - 1] + cc * ew * K[(ci - 1) * Me + ei] +
                    cw * ec * K[ci * Me + ei - 1] + cw * ew * K[ci * Me + ei];
@@ -85,15 +110,13 @@ constexpr int PSF_MAX_C = 64;
 __global__ void __launch_bounds__(128) k_mean_psf(const double* pa, int C, int E, const double* ecb,
                                                   const double* wecb, int S, const double* ltf,
                                                   const double* expo, double* out) {
-    __shared__ double sx[PSF_MAX_C][PSF_TILE_S];
-    __shared__ double sw[PSF_MAX_C][PSF_TILE_S];
+    __shared__ double2 sxw[PSF_MAX_C][PSF_TILE_S];  // (exposure, weighted exposure) cos-theta rows
     int s0 = blockIdx.y * PSF_TILE_S;
     int ns = min(PSF_TILE_S, S - s0);
     for (int k = threadIdx.x; k < PSF_TILE_S * C; k += blockDim.x) {
         int s = k / C, c = k - s * C;
         bool ok = s < ns;
-        sx[c][s] = ok ? ecb[(size_t)(s0 + s) * C + c] : 0.;
-        sw[c][s] = ok ? wecb[(size_t)(s0 + s) * C + c] : 0.;
+        sxw[c][s] = make_double2(ok ? ecb[(size_t)(s0 + s) * C + c] : 0., ok ? wecb[(size_t)(s0 + s) * C + c] : 0.);
     }
     __syncthreads();
     int DE = ND * E;
@@ -103,10 +126,15 @@ __global__ void __launch_bounds__(128) k_mean_psf(const double* pa, int C, int E
     double x[PSF_TILE_S], w[PSF_TILE_S];
 #pragma unroll
     for (int s = 0; s < PSF_TILE_S; ++s) { x[s] = 0.; w[s] = 0.; }
-    for (int c = 0; c < C; ++c) {
+#pragma unroll 8
+    for (int c = 0; c < C; ++c) {  // unrolled: eight column loads in flight
         const double col = pa[(size_t)c * DE + j];
 #pragma unroll
-        for (int s = 0; s < PSF_TILE_S; ++s) { x[s] = fma(sx[c][s], col, x[s]); w[s] = fma(sw[c][s], col, w[s]); }
+        for (int s = 0; s < PSF_TILE_S; ++s) {
+            const double2 xw = sxw[c][s];
+            x[s] = fma(xw.x, col, x[s]);
+            w[s] = fma(xw.y, col, w[s]);
+        }
     }
     double l0 = ltf[e], l1 = ltf[E + e];
 #pragma unroll
@@ -118,15 +146,21 @@ __global__ void __launch_bounds__(128) k_mean_psf(const double* pa, int C, int E
 // over each separation bin (psf.partial_total_integral.cxx:8-52), prefix sum,
 // normalised partials, then uPsf /= total (psf.normalize.cxx:7-24).  One warp per
 // (source, energy): each lane integrates a run of 13 bins, the runs are joined by
-// a shuffle scan, and every lane normalises its own rows.
+// a shuffle scan, and every lane normalises its own rows.  The reference forms
+// the bin integral as 0.5 m (t2^2 - t1^2) + b (t2 - t1) with the slope m and
+// intercept b of the interpolant; that is exactly the trapezoid
+// 0.5 (t2 - t1)(y1 + y2), used here without its division (the two agree to a
+// few ulp), and the normalisation multiplies by 1/total.
 constexpr int PSCAN_ROWS = (ND - 1 + 31) / 32;  // bins per lane
 
 __global__ void __launch_bounds__(256) k_partial_scan(double* upsf, double* partial, int E) {
-    __shared__ double th[ND], st[ND];  // theta (rad) and 2 pi sin(theta) of the separations
+    __shared__ double th[ND], st[ND], hdt[ND];  // theta (rad), 2 pi sin(theta), half bin widths
     for (int d = threadIdx.x; d < ND; d += blockDim.x) {
         th[d] = D2R * sep_deg(d);
         st[d] = TWOPI * sin(th[d]);
     }
+    __syncthreads();
+    for (int d = 1 + threadIdx.x; d < ND; d += blockDim.x) hdt[d] = 0.5 * (th[d] - th[d - 1]);
     __syncthreads();
     const int s = blockIdx.x, lane = threadIdx.x & 31;
     const int e = blockIdx.y * 8 + (threadIdx.x >> 5);
@@ -138,18 +172,13 @@ __global__ void __launch_bounds__(256) k_partial_scan(double* upsf, double* part
     double cum[PSCAN_ROWS];
     double run = 0.0;
     if (d0 < ND) {
-        double t1 = th[d0 - 1];
         double y1 = u[(size_t)(d0 - 1) * E] * st[d0 - 1];
 #pragma unroll
         for (int k = 0; k < PSCAN_ROWS; ++k) {
             const int d = d0 + k;
             if (d < d1) {
-                const double t2 = th[d];
                 const double y2 = u[(size_t)d * E] * st[d];
-                const double m = (y2 - y1) / (t2 - t1);
-                const double b = y1 - t1 * m;
-                run += 0.5 * m * (t2 * t2 - t1 * t1) + b * (t2 - t1);
-                t1 = t2;
+                run = fma(hdt[d], y1 + y2, run);
                 y1 = y2;
             }
             cum[k] = run;
@@ -163,23 +192,25 @@ __global__ void __launch_bounds__(256) k_partial_scan(double* upsf, double* part
     }
     const double base = incl - run;
     const double tot = __shfl_sync(0xffffffffu, incl, 31);
+    const double inv = 1.0 / tot;  // +-inf when the total is 0: u / 0 as in the reference
     if (lane == 0) {
         p[0] = 0.0;
-        u[0] = u[0] / tot;
+        u[0] = u[0] * inv;
     }
 #pragma unroll
     for (int k = 0; k < PSCAN_ROWS; ++k) {
         const int d = d0 + k;
         if (d < d1) {
             const double c = base + cum[k];
-            p[(size_t)d * E] = tot != 0. ? c / tot : c;
-            u[(size_t)d * E] = u[(size_t)d * E] / tot;
+            p[(size_t)d * E] = tot != 0. ? c * inv : c;
+            u[(size_t)d * E] = u[(size_t)d * E] * inv;
         }
     }
 }
 
 int launch_psf(const PsfDev& a, cudaStream_t st) {
     if (a.C > PSF_MAX_C) return set_error(XTS_ERR_ARG, "compute_psf_data: C=%d exceeds %d", a.C, PSF_MAX_C);
+    if (psf_aeff_smem(a.E) > 48 * 1024) return set_error(XTS_ERR_ARG, "compute_psf_data: E=%d exceeds 1200", a.E);
     size_t kf_n = (size_t)ND * a.pf.n_cos * a.pf.n_e, kb_n = (size_t)ND * a.pb.n_cos * a.pb.n_e;
     double* king = (double*)workspace(W_KING, sizeof(double) * (kf_n + kb_n));
     double* pa = (double*)workspace(W_PSFTAB, sizeof(double) * (size_t)a.C * ND * a.E);
@@ -187,8 +218,8 @@ int launch_psf(const PsfDev& a, cudaStream_t st) {
     int mx = (int)(kf_n > kb_n ? kf_n : kb_n);
     XTS_LAUNCH("k_king", st, k_king<<<dim3((mx + 127) / 128, 2), 128, 0, st>>>(a.pf, a.pb, king, king + kf_n));
     int n = a.C * ND * a.E;
-    XTS_LAUNCH("k_psf_aeff", st, k_psf_aeff<<<(n + 127) / 128, 128, 0, st>>>(a.pf, a.pb, king, king + kf_n, a.costh, a.C,
-                                               a.logEs, a.E, a.af, a.ab, pa));
+    XTS_LAUNCH("k_psf_aeff", st, k_psf_aeff<<<(n + 127) / 128, 128, psf_aeff_smem(a.E), st>>>(a.pf, a.pb, king, king + kf_n,
+                                               a.costh, a.C, a.logEs, a.E, a.af, a.ab, pa));
     if (a.S == 0) return XTS_OK;
     int DE = ND * a.E;
     dim3 g((DE + 127) / 128, (a.S + PSF_TILE_S - 1) / PSF_TILE_S);
@@ -202,12 +233,13 @@ int launch_psf(const PsfDev& a, cudaStream_t st) {
 // table (C * 401 * E doubles).  Nothing here allocates.
 int launch_psf_scratch(const PsfDev& a, double* king, double* pa, cudaStream_t st) {
     if (a.C > PSF_MAX_C) return set_error(XTS_ERR_ARG, "compute_psf_data: C=%d exceeds %d", a.C, PSF_MAX_C);
+    if (psf_aeff_smem(a.E) > 48 * 1024) return set_error(XTS_ERR_ARG, "compute_psf_data: E=%d exceeds 1200", a.E);
     size_t kf_n = (size_t)ND * a.pf.n_cos * a.pf.n_e, kb_n = (size_t)ND * a.pb.n_cos * a.pb.n_e;
     int mx = (int)(kf_n > kb_n ? kf_n : kb_n);
     XTS_LAUNCH("k_king", st, k_king<<<dim3((mx + 127) / 128, 2), 128, 0, st>>>(a.pf, a.pb, king, king + kf_n));
     int n = a.C * ND * a.E;
-    XTS_LAUNCH("k_psf_aeff", st, k_psf_aeff<<<(n + 127) / 128, 128, 0, st>>>(a.pf, a.pb, king, king + kf_n, a.costh, a.C,
-                                               a.logEs, a.E, a.af, a.ab, pa));
+    XTS_LAUNCH("k_psf_aeff", st, k_psf_aeff<<<(n + 127) / 128, 128, psf_aeff_smem(a.E), st>>>(a.pf, a.pb, king, king + kf_n,
+                                               a.costh, a.C, a.logEs, a.E, a.af, a.ab, pa));
     if (a.S == 0) return XTS_OK;
     int DE = ND * a.E;
     dim3 g((DE + 127) / 128, (a.S + PSF_TILE_S - 1) / PSF_TILE_S);
