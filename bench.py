@@ -323,7 +323,8 @@ def run_ours(args, rank, world, local_rank):
     ms_max = float(ms_t.item())
     value = n_values * world * args.steps / (ms_max * 1e-3)
 
-    # dominant kernel roofline (k_srcmap), measured inside the timed region
+    # roofline of the write pass (k_srcmap, the kernel that writes the srcmap values), measured
+    # inside the timed region
     kname = "k_srcmap"
     launches, kms = prof.get(kname, (0, 0.0))
     epad = (E + 3) // 4 * 4
@@ -351,6 +352,19 @@ def run_ours(args, rank, world, local_rank):
                 "kernel_timing": "library CUDA events around each kernel, from %d instrumented steps "
                                  "(%.4f ms/step with the timers)" % (args.steps, ms_prof / args.steps)}
     kernels = {k: {"launches": v[0], "ms": round(v[1], 4)} for k, v in prof.items()}
+    # the kernel with the largest share of the instrumented step, and the path as a whole
+    # against HBM (4 B written per value)
+    dom = max(prof.items(), key=lambda kv: kv[1][1]) if prof else None
+    dominant = None
+    if dom:
+        dominant = {"kernel": dom[0], "share": dom[1][1] / ms_prof if ms_prof else None,
+                    "avg_launch_ms": dom[1][1] / dom[1][0] if dom[1][0] else None}
+        if dom[0] == "k_pixel_windows":
+            dominant["bound"] = ("FP64 issue and shared-memory latency (geometry of 12 points per pixel; "
+                                 "~2 % of DRAM bandwidth): not an HBM or tensor kernel")
+    path_gbs = 4.0 * n_values * world / (ms_max / args.steps * 1e-3) / 1e9
+    roofline_path = {"bound": "hbm", "achieved": path_gbs, "peak": peak, "unit": "GB/s", "frac": path_gbs / peak,
+                     "note": "whole step: 4 B written per srcmap value over the step time"}
     gpu_launches = sum(v[0] for v in prof.values())
 
     # end to end through the public API with host (pinned) buffers: the fused
@@ -430,7 +444,8 @@ def run_ours(args, rank, world, local_rank):
                    "l2": "256 MiB buffer written between timed steps (L2 flush); the 296 MB map "
                          "written per step also exceeds the 126 MB L2",
                    "output_dtype": "float32", "launch": graph_note},
-        "roofline": roofline, "kernels": kernels, "gpu_launches": gpu_launches,
+        "roofline": roofline, "dominant_kernel": dominant, "roofline_path": roofline_path,
+        "kernels": kernels, "gpu_launches": gpu_launches,
         "clocks": ck, "e2e": e2e, "cpu_baseline": cpu, "max_rel_err_vs_fp64_oracle": err,
         "adaptive": adaptive,
         "three_calls_device": {"ms_per_step": ms3 / args.steps, "value": n_values * world * args.steps / (ms3 * 1e-3),

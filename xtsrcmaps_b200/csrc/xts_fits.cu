@@ -30,51 +30,57 @@
 
 namespace xts {
 
-constexpr int FT = 32;  // tile side (h x e) of the reorder
+constexpr int FH = 32;  // h values per tile: one per lane
+static_assert(FH == 32, "k_fits_encode maps lanes to h");
+constexpr int FE = 64;  // energies per tile (E is looped over in chunks of FE)
 
 __device__ __forceinline__ unsigned long long bswap64(unsigned long long b) {
     const unsigned lo = (unsigned)b, hi = (unsigned)(b >> 32);
     return ((unsigned long long)__byte_perm(lo, 0, 0x0123) << 32) | __byte_perm(hi, 0, 0x0123);
 }
 
-// Block (h tile x e tile, w, source of the chunk), 256 threads: a 32 x 32 tile of
-// (h, e) at one w read along e, written along h.
+// Block (h tile, w, source of the chunk), 256 threads: the tile of 32 h x all E at
+// one w, read along e (E contiguous values per h) and written along h (32
+// contiguous values per e).
 template <typename Tin, bool F64OUT>
 __global__ void __launch_bounds__(256) k_fits_encode(const Tin* __restrict__ map, int H, int W, int E,
                                                      void* __restrict__ out,
                                                      unsigned long long* __restrict__ datasum) {
-    __shared__ double tile[FT][FT + 1];
+    __shared__ double tile[FH][FE + 1];
     __shared__ unsigned long long red[8];
-    const int nhb = (H + FT - 1) / FT;
-    const int h0 = (blockIdx.x % nhb) * FT, e0 = (blockIdx.x / nhb) * FT;
-    const int w = blockIdx.y, s = blockIdx.z;
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    for (int i = ty; i < FT; i += 8) {
-        const int h = h0 + i, e = e0 + tx;
-        tile[i][tx] = (h < H && e < E) ? (double)map[(((size_t)s * H + h) * W + w) * E + e] : 0.0;
-    }
-    __syncthreads();
+    const int h0 = blockIdx.x * FH, w = blockIdx.y, s = blockIdx.z, t = threadIdx.x;  // FH == 32 lanes
+    const int nh = min(FH, H - h0);
+    const size_t per_src = (size_t)H * W * E;
+    const Tin* src = map + per_src * s + ((size_t)h0 * W + w) * E;  // (h0, w, 0)
+    const size_t hstride = (size_t)W * E;                              // next h
+    const int lane = t & 31, warp = t >> 5;
     unsigned long long sum = 0;
-    for (int i = ty; i < FT; i += 8) {
-        const int e = e0 + i, h = h0 + tx;
-        if (e < E && h < H) {
-            const size_t k = (((size_t)s * E + e) * W + w) * H + h;
-            const double v = tile[tx][i];
-            if (F64OUT) {
-                const unsigned long long b = (unsigned long long)__double_as_longlong(v);
-                sum += (b >> 32) + (b & 0xffffffffull);
-                ((unsigned long long*)out)[k] = bswap64(b);
-            } else {
-                const unsigned b = __float_as_uint((float)v);
-                sum += b;
-                ((unsigned*)out)[k] = __byte_perm(b, 0, 0x0123);
+    for (int e0 = 0; e0 < E; e0 += FE) {
+        const int ne = min(FE, E - e0);
+        if (e0) __syncthreads();
+        for (int h = warp; h < nh; h += 8)  // warp per h row, lanes along e
+            for (int e = lane; e < ne; e += 32) tile[h][e] = (double)src[(size_t)h * hstride + e0 + e];
+        __syncthreads();
+        for (int e = warp; e < ne; e += 8) {  // warp per energy plane, lanes along h
+            const size_t o = per_src * s + ((size_t)(e0 + e) * W + w) * H + h0 + lane;
+            if (lane < nh) {
+                const double v = tile[lane][e];
+                if (F64OUT) {
+                    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+                    sum += (b >> 32) + (b & 0xffffffffull);
+                    ((unsigned long long*)out)[o] = bswap64(b);
+                } else {
+                    const unsigned b = __float_as_uint((float)v);
+                    sum += b;
+                    ((unsigned*)out)[o] = __byte_perm(b, 0, 0x0123);
+                }
             }
         }
     }
     for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-    if (tx == 0) red[ty] = sum;
+    if ((t & 31) == 0) red[t >> 5] = sum;
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (t == 0) {
         unsigned long long b = 0;
         for (int k = 0; k < 8; ++k) b += red[k];
         atomicAdd(datasum + s, b);
@@ -182,8 +188,7 @@ static std::string image_header(int bitpix, int H, int W, int E, const std::stri
 template <typename Tin>
 static int launch_encode(const Tin* map, int n, int H, int W, int E, bool f64out, void* out,
                          unsigned long long* datasum, cudaStream_t st) {
-    const int nhb = (H + FT - 1) / FT, neb = (E + FT - 1) / FT;
-    const dim3 g((unsigned)(nhb * neb), (unsigned)W, (unsigned)n);
+    const dim3 g((unsigned)((H + FH - 1) / FH), (unsigned)W, (unsigned)n);
     if (f64out)
         XTS_LAUNCH("k_fits_encode", st, (k_fits_encode<Tin, true><<<g, 256, 0, st>>>(map, H, W, E, out, datasum)));
     else
