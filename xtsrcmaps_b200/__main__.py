@@ -4,12 +4,14 @@
 
 main.cxx:17-40 collects the configuration, observation, sources and IRFs, runs
 compute_exposure, compute_psf_data and compute_srcmaps (:28-30) and would write
-the maps with fits::write_src_model (:40, commented out there).  Here the inputs
-are a seeded synthetic job of the named configuration (the reference's FITS
-inputs need cfitsio, which this build does not read), optionally with source
-positions and names from an .npz file (arrays ``src_sph`` [S, 2] degrees and
-``names``); the three calls run as one device call and the maps go to the FITS
-file from device memory.
+the maps with fits::write_src_model (:40, commented out there).  Every input
+starts as the seeded synthetic job of the named configuration and can be
+replaced by the reference's own files: --ccube (counts cube: WCS and energies,
+observation/observation.cxx), --ltcube (livetime cube, EXPOSURE and
+WEIGHTED_EXPOSURE tables), --aeff and --psf (Pass-8 IRF files), --xml (point
+sources of a source model), or --sources (an .npz with ``src_sph`` [S, 2] degrees
+and ``names``).  The three calls run as one device call and the maps go to the
+FITS file from device memory.
 """
 from __future__ import annotations
 
@@ -23,6 +25,11 @@ def main(argv=None) -> int:
     ap.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "c4"], help="synthetic job")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--sources", help=".npz with src_sph [S, 2] (deg) and optional names")
+    ap.add_argument("--xml", help="source model XML: its point sources")
+    ap.add_argument("--ccube", help="counts cube FITS: map WCS and energies")
+    ap.add_argument("--ltcube", help="livetime cube FITS (EXPOSURE, WEIGHTED_EXPOSURE tables)")
+    ap.add_argument("--aeff", help="effective-area IRF FITS (EFFECTIVE AREA_*, EFFICIENCY_PARAMS_*)")
+    ap.add_argument("--psf", help="PSF IRF FITS (RPSF_*, PSF_SCALING_PARAMS_*)")
     ap.add_argument("--out", required=True, help="output FITS file")
     ap.add_argument("--bitpix", type=int, default=-64, choices=[-64, -32])
     ap.add_argument("--adaptive", type=float, default=None, metavar="RTOL",
@@ -34,6 +41,7 @@ def main(argv=None) -> int:
     import torch
 
     from . import api as A
+    from . import fits_io, irf
     from .synth import make_job
 
     job = make_job(args.config, seed=args.seed)
@@ -42,6 +50,25 @@ def main(argv=None) -> int:
         z = np.load(args.sources, allow_pickle=False)
         job.src_sph = np.ascontiguousarray(z["src_sph"], dtype=np.float64)
         names = [str(n) for n in z["names"]] if "names" in z.files else ["SRC%05d" % s for s in range(job.S)]
+    if args.xml:
+        from .sources import read_point_sources
+
+        names, job.src_sph = read_point_sources(args.xml)
+    if args.ccube:  # observation/observation.cxx: WCS from the cube, energies from EBOUNDS
+        job.wcs, _ = fits_io.read_image_meta(args.ccube)
+        job.energies = fits_io.read_energies(args.ccube)
+        job.logEs = np.log10(job.energies)
+    if args.ltcube:
+        job.exp_cube = fits_io.read_expcube(args.ltcube, "EXPOSURE")
+        job.wexp_cube = fits_io.read_expcube(args.ltcube, "WEIGHTED_EXPOSURE")
+    if args.aeff:
+        a = irf.load_aeff(args.aeff)
+        job.aeff_front, job.aeff_back = a["front"].grid, a["back"].grid
+        job.effic_front = a["front"].effic
+    if args.psf:
+        p = irf.load_psf(args.psf)
+        job.rpsf_front, job.rpsf_back = p["front"].grid, p["back"].grid
+        job.scale_front, job.scale_back = p["front"].scale, p["back"].scale
     A.init(args.device)
     dev = torch.device("cuda", args.device)
     t0 = time.perf_counter()

@@ -88,3 +88,55 @@ def prepare_scale(row) -> IrfScale:
 def prepare_effic(p0, p1) -> IrfEffic:
     """irf/irf.prepare_effic.cpp:6-22."""
     return IrfEffic(np.asarray(p0, dtype=np.float32), np.asarray(p1, dtype=np.float32))
+
+
+@dataclass
+class IrfSide:
+    """One event class side of an IRF file: the grids the reference keeps in
+    ``aeff::Data`` / ``psf::Data`` (irf/irf_types.hxx)."""
+
+    grid: IrfGrid               # EFFECTIVE AREA or RPSF (raw, not normalised)
+    second: IrfGrid             # PHI_DEPENDENCE or FISHEYE_CORRECTION (loaded, unused on the path)
+    effic: IrfEffic | None = None   # EFFICIENCY_PARAMS (aeff files)
+    scale: IrfScale | None = None   # PSF_SCALING_PARAMS (psf files)
+
+
+def _grid(path: str, table: str) -> IrfGrid:
+    from .fits_io import read_irf_pars
+
+    ext, off, rows = read_irf_pars(path, table)
+    return prepare_grid(ext, off, rows[0])
+
+
+def load_aeff(path: str) -> dict:
+    """Fermi::Irf::load_aeff (irf/irf.cxx:24-46) and prepare_aeff_data
+    (irf/irf.prepare_aeff_data.cpp:7-23): front and back EFFECTIVE AREA and
+    PHI_DEPENDENCE grids and the two EFFICIENCY_PARAMS rows."""
+    from .fits_io import read_irf_pars
+
+    out = {}
+    for side in ("FRONT", "BACK"):
+        ext, _, rows = read_irf_pars(path, f"EFFICIENCY_PARAMS_{side}")
+        if list(ext) != [6] or rows.shape != (2, 6):
+            raise ValueError(f"{path}: EFFICIENCY_PARAMS_{side} must be 2 rows of 6 (irf.prepare_effic.cpp:8-10)")
+        out[side.lower()] = IrfSide(_grid(path, f"EFFECTIVE AREA_{side}"), _grid(path, f"PHI_DEPENDENCE_{side}"),
+                                    effic=prepare_effic(rows[0], rows[1]))
+    return out
+
+
+def load_psf(path: str) -> dict:
+    """Fermi::Irf::load_psf (irf/irf.cxx:48-70) and prepare_psf_data
+    (irf/irf.prepare_psf_data.cpp:6-25) up to the normalisation: front and back
+    RPSF and FISHEYE_CORRECTION grids and the PSF_SCALING_PARAMS row.  The King
+    grids are normalised by the library (``api.normalize_rpsf``, the reference's
+    irf/irf.normalize_rpsf.cpp:11-61)."""
+    from .fits_io import read_irf_pars
+
+    out = {}
+    for side in ("FRONT", "BACK"):
+        _, _, rows = read_irf_pars(path, f"PSF_SCALING_PARAMS_{side}")
+        if rows.shape != (1, 3):
+            raise ValueError(f"{path}: PSF_SCALING_PARAMS_{side} must be 1 row of 3 (irf.prepare_scale.cpp:7-8)")
+        out[side.lower()] = IrfSide(_grid(path, f"RPSF_{side}"), _grid(path, f"FISHEYE_CORRECTION_{side}"),
+                                    scale=prepare_scale(rows[0]))
+    return out
