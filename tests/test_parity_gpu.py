@@ -223,6 +223,34 @@ def test_golden_exposure_and_psf_on_gpu(api, golden):
     assert max_rel(ps.uPsf[:, 0, :], golden("psf")["upsf_peak"]) < 2e-6
 
 
+def test_golden_inputs_model_maps(api, golden):
+    """Model maps on the reference's own inputs end to end: its 3C279 counts-cube
+    WCS (AIT, 100 x 100 @ 0.2 deg), its 263 point sources, livetime rows and P8R3
+    IRFs (as the reference's tests hold them) through exposure, mean PSF and maps
+    on the GPU; in-FOV flags as Fermitools (47), maps against the FP64 oracle."""
+    from test_oracle_golden import _exposure_inputs
+    from oracle import oracle as O
+    from xtsrcmaps_b200.api import XtExp
+    from xtsrcmaps_b200.wcs import Wcs
+
+    z, g, e, cos, loge, af, ab, ltf, ecb, wecb = _exposure_inputs(golden)
+    gm = golden("geom")
+    w = Wcs(int(gm["naxis"][0]), int(gm["naxis"][1]), *gm["crpix"], *gm["crval"], *gm["cdelt"],
+            crota2=float(gm["crota2"]), proj=str(gm["proj"]))
+    src = gm["src_sph"]
+    ex = api.exposure(ecb, wecb, af, ab, ltf)
+    nf = api.normalize_rpsf(g["rpsf_front"], g["scale_front"])
+    nb = api.normalize_rpsf(g["rpsf_back"], g["scale_back"])
+    ps = api.compute_psf_data(nf, nb, XtExp(cos, af, ab, ecb, wecb, ex), loge, ltf)
+    m, info = api.point_src_model_map_wcs(w, src, ex, ps.uPsf, ps.partial_psf_integral)
+    fov = np.asarray(info.in_fov).astype(bool)
+    assert fov.sum() == gm["ft_in_fov"].sum() == 47
+    sample = list(np.flatnonzero(fov)[::12]) + list(np.flatnonzero(~fov)[::60])
+    ref = O.point_src_model_map_wcs(w, src[sample], ex[sample], ps.uPsf[sample], ps.partial_psf_integral[sample])
+    assert max_rel(m[sample], ref["map"]) < 1e-5
+    np.testing.assert_allclose(info.inv_map_integral[sample], ref["inv_integ"], rtol=1e-7)
+
+
 @pytest.mark.parametrize("out_dtype", ["float32", "float64"])
 def test_point_source_maps_fused_call(api, c1_small, out_dtype):
     """xts_point_source_maps (the three calls of main.cxx:28-30 in one) gives the
