@@ -245,6 +245,27 @@ int xts_point_source_maps(const xts_expcube* exp_cube, const xts_expcube* wexp_c
 int xts_write_src_model(const char* filename, const void* model_map, int S, int H, int W, int E,
                         const char* const* names, unsigned flags, void* stream);
 
+/* Psf::make_kernel (psf/psf.make_kernel.cpp:8-90), a step of the reference's
+ * work-in-progress diffuse-source map: the mean PSF of one source (upsf [401, E],
+ * one source's slice of the uPsf table) sampled at the centres (h + 1, w + 1) of an
+ * Nk x Nk grid described by kernel_wcs, by separation from the grid's reference
+ * point (CRVAL), with the row and weight of the point-source cubature's logsep rule;
+ * each energy plane normalised to unit sum.  kernel is [E, Nk, Nk], Nk odd.  The
+ * reference weights the lower row by t and the upper by 1 - t there
+ * (make_kernel.cpp:43-45), the reverse of its cubature; this uses the cubature's
+ * (1 - t, t). */
+int xts_make_psf_kernel(const xts_wcs* kernel_wcs, int Nk, const double* upsf, int E, double* kernel,
+                        unsigned flags, void* stream);
+
+/* FFT::convolve_map_psf (model_map/mm_fft/fft.convolve_map_psf.cpp:7-43, over
+ * fftw_convolve_3d, math/convolve/fft/fft.fftw_convolve_CHW.cpp:7-90): for every
+ * energy plane the full linear 2-D convolution of image [E, H, W] with kernel
+ * [E, K, K], out [E, H + K - 1, W + K - 1], FP64, by cuFFT.  The reference's
+ * transform is 3-D over (energy, h, w) and its scale factor is misparenthesised;
+ * this is the per-plane convolution those lines are written for. */
+int xts_convolve_map_psf(const double* image, int E, int H, int W, const double* kernel, int K, double* out,
+                         unsigned flags, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

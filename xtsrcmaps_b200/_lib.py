@@ -106,6 +106,8 @@ SIGNATURES = {
                                               C.c_int, _vp, C.POINTER(XtsSrcmapInfo), C.c_uint, _vp]),
     "xts_write_src_model": (C.c_int, [C.c_char_p, _vp, C.c_int, C.c_int, C.c_int, C.c_int,
                                       C.POINTER(C.c_char_p), C.c_uint, _vp]),
+    "xts_make_psf_kernel": (C.c_int, [C.POINTER(XtsWcs), C.c_int, _vp, C.c_int, _vp, C.c_uint, _vp]),
+    "xts_convolve_map_psf": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_uint, _vp]),
 }
 
 

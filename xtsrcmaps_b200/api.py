@@ -442,6 +442,38 @@ def write_src_model(filename: str, model_map, names=None, bitpix: int = -64) -> 
     L.check(L.lib().xts_write_src_model(str(filename).encode(), ptr, S, H, W, E, cnames, flags, stream))
 
 
+def make_psf_kernel(kernel_wcs: Wcs, Nk: int, upsf):
+    """Psf::make_kernel (psf/psf.make_kernel.cpp:8-90): one source's mean PSF
+    ``upsf`` [401, E] sampled at the pixel centres of the Nk x Nk grid
+    ``kernel_wcs`` (Nk odd) by separation from its CRVAL, each energy plane
+    normalised to unit sum -> [E, Nk, Nk] (float64)."""
+    like = _device_of(upsf)
+    c = _Call(like is not None, like)
+    up, u = c.inp(upsf)
+    E = int(u.shape[-1])
+    kp, k = c.out((E, int(Nk), int(Nk)))
+    w = _wcs_struct(kernel_wcs)
+    L.check(L.lib().xts_make_psf_kernel(C.byref(w), int(Nk), up, E, kp, c.flags, c.stream))
+    return k
+
+
+def convolve_map_psf(image, kernel):
+    """FFT::convolve_map_psf (model_map/mm_fft/fft.convolve_map_psf.cpp:7-43): per
+    energy plane, the full linear convolution of image [E, H, W] with kernel
+    [E, K, K] -> [E, H + K - 1, W + K - 1] (float64, cuFFT)."""
+    like = _device_of(image, kernel)
+    c = _Call(like is not None, like)
+    ip, im = c.inp(image)
+    kp, ke = c.inp(kernel)
+    E, H, W = (int(x) for x in im.shape)
+    K = int(ke.shape[1])
+    if tuple(ke.shape) != (E, K, K):
+        raise ValueError("kernel must be [E, K, K] with the image's E")
+    op, o = c.out((E, H + K - 1, W + K - 1))
+    L.check(L.lib().xts_convolve_map_psf(ip, E, H, W, kp, K, op, c.flags, c.stream))
+    return o
+
+
 def compute_srcmaps(wcs: Wcs, src_sph, exp: XtExp, psf: XtPsf, out_dtype: str = "float32", out=None):
     """ModelMap::compute_srcmaps<PointSource> (model_map/model_map.compute_src_maps.cxx:6-22)."""
     m, _ = point_src_model_map_wcs(wcs, src_sph, exp.exposure, psf.uPsf, psf.partial_psf_integral,

@@ -43,8 +43,10 @@ def needs_build() -> bool:
 def build(force: bool = False, verbose_ptxas: bool = False) -> str:
     if not force and not needs_build():
         return OUT
+    # cuFFT (the diffuse-map convolution) from the toolkit next to nvcc, found at run time by rpath
+    lib64 = os.path.join(os.path.dirname(os.path.dirname(os.path.realpath(nvcc()))), "lib64")
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-           "-o", OUT + ".tmp", *sources()]
+           "-o", OUT + ".tmp", *sources(), "-L" + lib64, "-lcufft", "-Xlinker", "-rpath=" + lib64]
     if verbose_ptxas:
         cmd.insert(1, "-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -701,6 +701,36 @@ int xts_point_source_maps(const xts_expcube* cube, const xts_expcube* wcube, con
     return run_srcmap(sg, ma, model_map, npix, f64);
 }
 
+int xts_make_psf_kernel(const xts_wcs* kernel_wcs, int Nk, const double* upsf, int E, double* kernel,
+                        unsigned flags, void* stream) {
+    XTS_ENTER();
+    if (!kernel_wcs || Nk <= 0 || !(Nk & 1) || E <= 0 || !upsf || !kernel || (long long)Nk * Nk > (1LL << 30))
+        return set_error(XTS_ERR_ARG, "make_psf_kernel: null argument or bad size (Nk odd and positive)");
+    if ((kernel_wcs->proj != 0 && kernel_wcs->proj != 1) || kernel_wcs->cdelt1 == 0. || kernel_wcs->cdelt2 == 0.)
+        return set_error(XTS_ERR_ARG, "make_psf_kernel: bad WCS (CAR/AIT, nonzero CDELT)");
+    Stager sg{(flags & XTS_DEVICE_PTRS) != 0, stream ? (cudaStream_t)stream : g_ctx.stream};
+    const double* u = sg.in(upsf, (size_t)ND * E);
+    double* k = sg.out(kernel, (size_t)E * Nk * Nk);
+    int rc = sg.rc ? sg.rc : make_psf_kernel(*kernel_wcs, Nk, u, E, k, sg.st);
+    return sg.finish(rc);
+}
+
+int xts_convolve_map_psf(const double* image, int E, int H, int W, const double* kernel, int K, double* out,
+                         unsigned flags, void* stream) {
+    XTS_ENTER();
+    if (!image || !kernel || !out || E <= 0 || H <= 0 || W <= 0 || K <= 0)
+        return set_error(XTS_ERR_ARG, "convolve_map_psf: null argument or bad size");
+    const long long PH = (long long)H + K - 1, PW = (long long)W + K - 1;
+    if (PH > (1 << 20) || PW > (1 << 20) || (long long)E * PH * PW > (1LL << 31))
+        return set_error(XTS_ERR_ARG, "convolve_map_psf: padded cube too large");
+    Stager sg{(flags & XTS_DEVICE_PTRS) != 0, stream ? (cudaStream_t)stream : g_ctx.stream};
+    const double* im = sg.in(image, (size_t)E * H * W);
+    const double* ke = sg.in(kernel, (size_t)E * K * K);
+    double* o = sg.out(out, (size_t)E * PH * PW);
+    int rc = sg.rc ? sg.rc : convolve_map_psf(im, E, H, W, ke, K, o, sg.st);
+    return sg.finish(rc);
+}
+
 int xts_write_src_model(const char* filename, const void* model_map, int S, int H, int W, int E,
                         const char* const* names, unsigned flags, void* stream) {
     XTS_ENTER();

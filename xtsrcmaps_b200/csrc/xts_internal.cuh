@@ -64,7 +64,7 @@ enum Slot {
     // internal scratch
     W_CORNERS, W_CENTERS, W_OMEGA, W_LUT, W_PARTSUM, W_SRCINFO, W_SCALE, W_PSFTAB,
     W_KING, W_MISC, W_WIN, W_WMETA, W_SPARSE, W_MISC2, W_EXPMAP,
-    W_FITS_IN, W_FITS_OUT, W_FITS_SUM,
+    W_FITS_IN, W_FITS_OUT, W_FITS_SUM, W_FFT_A, W_FFT_B, W_FFT_C, W_FFT_WORK,
     N_SLOTS
 };
 void* workspace(int slot, size_t bytes);  // nullptr + error set on OOM
@@ -166,6 +166,9 @@ int launch_correction(const double* hist, int nch, const SrcInfo* info, int S, c
                       double* inv_integ, double* correction, double* radius, int* in_fov,
                       cudaStream_t st, float* lut = nullptr, int Epad = 0);  // lut: scaled FP32 table too
 bool srcmap_win_supported(int E);
+int make_psf_kernel(const xts_wcs& wcs, int Nk, const double* upsf, int E, double* kernel, cudaStream_t st);
+int convolve_map_psf(const double* image, int E, int H, int W, const double* kernel, int K, double* out,
+                     cudaStream_t st);
 int write_src_model(const char* filename, const void* model_map, int S, int H, int W, int E,
                     const char* const* names, bool dev_ptrs, bool f64in, bool f64out, cudaStream_t st);
 bool exposure_map_supported(int C, int E);
