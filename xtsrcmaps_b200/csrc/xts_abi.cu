@@ -34,6 +34,7 @@ struct Ctx {
     cudaStream_t copy_stream = nullptr;    // device-to-host copies of finished map chunks
     cudaStream_t geo_stream = nullptr;     // map geometry of the fused call, beside exposure and PSF
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    cudaEvent_t pipe_a[2] = {}, pipe_b[2] = {};  // chunk pipeline of the window path
     cudaEvent_t chunk_ev[N_CHUNK_EV] = {};
     void* buf[N_SLOTS] = {};
     size_t cap[N_SLOTS] = {};
@@ -63,6 +64,10 @@ int ensure_device() {
     if (!g_ctx.geo_stream) XTS_CUDA(cudaStreamCreateWithFlags(&g_ctx.geo_stream, cudaStreamNonBlocking));
     if (!g_ctx.fork_ev) XTS_CUDA(cudaEventCreateWithFlags(&g_ctx.fork_ev, cudaEventDisableTiming));
     if (!g_ctx.join_ev) XTS_CUDA(cudaEventCreateWithFlags(&g_ctx.join_ev, cudaEventDisableTiming));
+    for (int i = 0; i < 2; ++i) {
+        if (!g_ctx.pipe_a[i]) XTS_CUDA(cudaEventCreateWithFlags(&g_ctx.pipe_a[i], cudaEventDisableTiming));
+        if (!g_ctx.pipe_b[i]) XTS_CUDA(cudaEventCreateWithFlags(&g_ctx.pipe_b[i], cudaEventDisableTiming));
+    }
     for (int i = 0; i < N_CHUNK_EV; ++i)
         if (!g_ctx.chunk_ev[i]) XTS_CUDA(cudaEventCreateWithFlags(&g_ctx.chunk_ev[i], cudaEventDisableTiming));
     g_ctx.device = dev;
@@ -70,6 +75,13 @@ int ensure_device() {
 }
 
 cudaStream_t default_stream() { return g_ctx.stream; }
+
+void pipe_events(cudaEvent_t a[2], cudaEvent_t b[2]) {
+    for (int i = 0; i < 2; ++i) {
+        a[i] = g_ctx.pipe_a[i];
+        b[i] = g_ctx.pipe_b[i];
+    }
+}
 
 void* workspace(int slot, size_t bytes) {
     bytes = align_up(bytes ? bytes : 1, 256);
@@ -326,6 +338,10 @@ int xts_init(int device) {
     if (g_ctx.geo_stream) { cudaStreamDestroy(g_ctx.geo_stream); g_ctx.geo_stream = nullptr; }
     if (g_ctx.fork_ev) { cudaEventDestroy(g_ctx.fork_ev); g_ctx.fork_ev = nullptr; }
     if (g_ctx.join_ev) { cudaEventDestroy(g_ctx.join_ev); g_ctx.join_ev = nullptr; }
+    for (int i = 0; i < 2; ++i) {
+        if (g_ctx.pipe_a[i]) { cudaEventDestroy(g_ctx.pipe_a[i]); g_ctx.pipe_a[i] = nullptr; }
+        if (g_ctx.pipe_b[i]) { cudaEventDestroy(g_ctx.pipe_b[i]); g_ctx.pipe_b[i] = nullptr; }
+    }
     for (int i = 0; i < N_CHUNK_EV; ++i)
         if (g_ctx.chunk_ev[i]) { cudaEventDestroy(g_ctx.chunk_ev[i]); g_ctx.chunk_ev[i] = nullptr; }
     return ensure_device();
@@ -525,6 +541,14 @@ int xts_point_src_model_map_wcs(const xts_wcs* wcs, const double* src_sph, int S
     a.radius = info ? sg.out(info->psf_radius, (size_t)S) : nullptr;
     a.in_fov = info ? sg.out(info->in_fov, (size_t)S) : nullptr;
     a.kernel = srcmap_kernel(flags);
+    // the map geometry and the window passes on the geometry stream (forked here,
+    // after the inputs are staged), so the chunks of the window path pipeline
+    if (sg.rc == XTS_OK && S > 0) {
+        XTS_CUDA(cudaEventRecord(g_ctx.fork_ev, sg.st));
+        XTS_CUDA(cudaStreamWaitEvent(g_ctx.geo_stream, g_ctx.fork_ev, 0));
+        a.geo_stream = g_ctx.geo_stream;
+        a.join_ev = g_ctx.join_ev;
+    }
     return run_srcmap(sg, a, model_map, npix, f64);
 }
 

@@ -136,6 +136,9 @@ struct SrcmapDev {
     cudaEvent_t join_ev = nullptr;
 };
 
+// Two pairs of events for the chunk pipeline of the window path (library-owned).
+void pipe_events(cudaEvent_t a[2], cudaEvent_t b[2]);
+
 // The geometry stream joins the launching stream once: at join(), or when it
 // goes out of scope (error paths, so that a stream capture never ends unjoined).
 struct StreamJoin {

@@ -595,6 +595,10 @@ int srcmap_status(cudaStream_t st) {
 }
 
 int launch_srcmap(const SrcmapDev& a, cudaStream_t st) {
+    // map geometry on the geometry stream when one is given; it joins the launching
+    // stream before uPsf is read, and on every early return
+    StreamJoin geo(a.geo_stream && a.join_ev ? a.geo_stream : st, st, a.join_ev);
+    cudaStream_t gs = geo.from;
     int rc = upload_rule(st);
     if (rc) return rc;
     int H = (int)a.wcs.naxis1, W = (int)a.wcs.naxis2, S = a.S, E = a.E;
@@ -616,9 +620,6 @@ int launch_srcmap(const SrcmapDev& a, cudaStream_t st) {
     double* hist = (double*)workspace(W_PARTSUM, sizeof(double) * (size_t)S * nch * ND + 8);
     double* scale = (double*)workspace(W_SCALE, sizeof(double) * (size_t)S * E + 8);
     if (!corners || !centers || !omega || !info || !hist || !scale) return XTS_ERR_OOM;
-    // map geometry on the geometry stream when one is given (joined before uPsf is read)
-    StreamJoin geo(a.geo_stream && a.join_ev ? a.geo_stream : st, st, a.join_ev);
-    cudaStream_t gs = geo.from;
     const dim3 gg((unsigned)((W + GT) / GT), (unsigned)((H + GT) / GT));  // tiles over the (H+1) x (W+1) grid
     XTS_LAUNCH("k_map_geometry", gs, k_map_geometry<<<gg, GEO_THREADS, 0, gs>>>(w, H, W, corners, centers, omega));
     if (S == 0) return XTS_OK;
