@@ -91,12 +91,12 @@ __device__ inline double quad_half(const double* P, const double* Q, const doubl
     return dir_diff(P, Q) * dir_diff(P, R) * sqrt(c0 * c0 + c1 * c1 + c2 * c2);
 }
 
-// d1 + d2 in one launch, by 16x16 tiles of the (H+1) x (W+1) point grid: the
-// tile's corner points and its centre points with a one-point halo (17x17) are
-// evaluated by one thread each (545 pix2dir per block, one round), then the
+// d1 + d2 in one launch, by 8x8 tiles of the (H+1) x (W+1) point grid: the
+// tile's corner points and its centre points with a one-point halo (9x9) are
+// evaluated by one thread each (145 pix2dir per block, one round), then the
 // solid angles of the tile's pixels come from the centres in shared memory.
-constexpr int GT = 16;                                   // grid points per tile side
-constexpr int GEO_THREADS = (GT + 1) * (GT + 1) + GT * GT;  // 545 tasks, one per thread
+constexpr int GT = 8;                                    // grid points per tile side (one wave of blocks)
+constexpr int GEO_THREADS = (GT + 1) * (GT + 1) + GT * GT;  // 145 tasks, one per thread
 
 __global__ void __launch_bounds__(GEO_THREADS) k_map_geometry(WcsDev w, int H, int W, double* corners,
                                                              double* centers, double* omega) {
@@ -453,9 +453,7 @@ __global__ void __launch_bounds__(256) k_map_integral_hist(const double* corners
 // integral out to the boundary radius over the whole bin at the radius's lower
 // index (fast_separation_lower_index, psf.fast_separation_lower_index.cxx:5-22,
 // with its `v < 1.` rule), capped at 1, times 1/map integral; 1 out of FOV.
-__device__ double correction_factor(const SrcInfo& si, const double* U, const double* partial_s, int E, int e,
-                                    double inv) {
-    if (!si.in_fov) return 1.0;
+__device__ double containment(const SrcInfo& si, const double* U, const double* partial_s, int E, int e) {
     const double v0 = si.radius_deg;
     const int li = v0 < 1. ? 1 : (int)floor(1. + log(1e4 * v0) * RECIPSTEP);
     const int d = li >= ND - 2 ? ND - 2 : li;
@@ -467,9 +465,13 @@ __device__ double correction_factor(const SrcInfo& si, const double* U, const do
     const double m = (y2 - y1) / (t2 - t1);
     const double b = y1 - t1 * m;
     const double v = 0.5 * m * (t2 * t2 - t1 * t1) + b * (t2 - t1);
-    double integ = v + partial_s[(size_t)d * E + e];
-    integ = integ > 1.0 ? 1.0 : integ;
-    return integ * inv;
+    const double integ = v + partial_s[(size_t)d * E + e];
+    return integ > 1.0 ? 1.0 : integ;
+}
+
+__device__ double correction_factor(const SrcInfo& si, const double* U, const double* partial_s, int E, int e,
+                                    double inv) {
+    return si.in_fov ? containment(si, U, partial_s, E, e) * inv : 1.0;
 }
 
 // c7 (1/sum) + c9 (containment factor) + c8/c10 folded into one per-(s,e) scale.
@@ -487,7 +489,8 @@ __global__ void __launch_bounds__(256) k_correction_hist(const double* hist_in, 
     SrcInfo si = info[s];
     for (int r = threadIdx.x; r < ND; r += blockDim.x) {
         double v = 0.;
-        for (int c = 0; c < nch; ++c) v += hist_in[((size_t)s * nch + c) * ND + r];
+#pragma unroll 4
+        for (int c = 0; c < nch; ++c) v += hist_in[((size_t)s * nch + c) * ND + r];  // loads in flight, sum in c order
         hsum[r] = v;
     }
     __syncthreads();
@@ -498,14 +501,18 @@ __global__ void __launch_bounds__(256) k_correction_hist(const double* hist_in, 
     const int e = blockIdx.y * 8 + wq;
     if (e < E) {
         int i = s * E + e;
+        // the containment integral does not depend on the map integral: formed
+        // first, so its transcendental chain overlaps the dot product's loads
+        const double integ = si.in_fov ? containment(si, U, partial + (size_t)s * ND * E, E, e) : 1.0;
         double sum = 0.;
         if (si.in_fov) {
+#pragma unroll 13
             for (int r = lane; r < ND; r += 32) sum = fma(hsum[r], U[(size_t)r * E + e], sum);
             for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
         }
         if (lane == 0) {
             const double inv = sum != 0. ? 1.0 / sum : sum;
-            const double factor = correction_factor(si, U, partial + (size_t)s * ND * E, E, e, inv);
+            const double factor = si.in_fov ? integ * inv : 1.0;
             scale[i] = expo[i] * factor;
             ssc[wq] = scale[i];
             if (inv_out) inv_out[i] = inv;
