@@ -19,13 +19,13 @@
 // is stored, which equals convolve_pixel_psf_searchsep inside [3e-4, 60] deg and
 // keeps logsep's row-400 clamp and its extrapolation below 1e-4 deg.
 //
-// The map is written once: a first pass (k_map_integral) evaluates the
-// cubature only for in-FOV sources and only for pixels whose centre lies within
-// the boundary radius, in FP64, and reduces per tile; k_correction folds the
-// tiles in a fixed order into 1/sum and the containment factor; the write pass
-// (k_srcmap) evaluates every pixel again and stores raw * omega * exposure *
-// factor.  Re-evaluating the disk costs less than writing the raw map and
-// reading it back.
+// The map is written once: a first pass gives the map integral of every in-FOV
+// source from the pixels whose centre lies within the boundary radius (FP64 row
+// histograms: k_map_integral_hist here for the FP64 path, the window pass of
+// xts_srcmap_win.cu for the default FP32 path); k_correction_hist folds them in a
+// fixed order into 1/sum and the containment factor; the write pass then stores
+// value * omega * exposure * factor.  Computing the integral before the write
+// costs less than writing the raw map and reading it back.
 #include <math.h>
 
 #include <type_traits>
@@ -199,16 +199,6 @@ __global__ void __launch_bounds__(256) k_boundary_chord(WcsDev w, const double* 
     }
 }
 
-// FP32 copy of each source's mean-PSF table, energies padded to Epad.
-__global__ void k_lut32(const double* upsf, int S, int E, int Epad, float* lut) {
-    size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    size_t n = (size_t)S * ND * Epad;
-    if (k >= n) return;
-    int e = (int)(k % Epad);
-    size_t sd = k / Epad;
-    lut[k] = e < E ? (float)upsf[sd * E + e] : 0.f;
-}
-
 // ---------------------------------------------------------------- cubature core
 // c2 + c3 for one pixel: the 12 rule points, their LUT columns and the
 // collapsed interpolation weights, in order of first appearance.
@@ -247,100 +237,6 @@ constexpr int TP = 128;  // pixels per tile (flat h*W + w order)
 struct PixCols32 { float va[NPTS], vb[NPTS]; short key[NPTS]; int n; };
 struct PixCols64 { double va[NPTS], vb[NPTS]; short key[NPTS]; int n; };
 
-// c7 pass: per (tile, source) FP64 sums over pixels whose centre lies within
-// the boundary radius of sum_columns (va U[k-1] + vb U[k]) * omega.
-__global__ void __launch_bounds__(TP) k_map_integral(const double* corners, const double* centers,
-                                                     const double* omega, const SrcInfo* info,
-                                                     const double* upsf, int H, int W, int E,
-                                                     int ntiles, double* partsum) {
-    __shared__ PixCols64 cols[TP];
-    __shared__ double som[TP];
-    __shared__ int any;
-    int tile = blockIdx.x, s = blockIdx.y;
-    double* out = partsum + ((size_t)s * ntiles + tile) * E;
-    SrcInfo si = info[s];
-    if (!si.in_fov) {
-        for (int e = threadIdx.x; e < E; e += blockDim.x) out[e] = 0.;
-        return;
-    }
-    if (threadIdx.x == 0) any = 0;
-    __syncthreads();
-    int npix = H * W, W1 = W + 1;
-    int pix = tile * TP + threadIdx.x;
-    int n = 0;
-    if (pix < npix) {
-        int h = pix / W, w = pix - h * W;
-        double rad = dir_diff(si.dir, centers + 3 * (h * W1 + w));
-        if (rad <= si.radius_rad) {
-            int keys[NPTS]; double va[NPTS], vb[NPTS];
-            n = pixel_columns(corners, W1, h, w, si.dir, keys, va, vb);
-            for (int k = 0; k < n; ++k) { cols[threadIdx.x].key[k] = (short)keys[k]; cols[threadIdx.x].va[k] = va[k]; cols[threadIdx.x].vb[k] = vb[k]; }
-            som[threadIdx.x] = omega[pix];
-            any = 1;
-        }
-    }
-    cols[threadIdx.x].n = n;
-    __syncthreads();
-    if (!any) {
-        for (int e = threadIdx.x; e < E; e += blockDim.x) out[e] = 0.;
-        return;
-    }
-    const double* U = upsf + (size_t)s * ND * E;
-    for (int e = threadIdx.x; e < E; e += blockDim.x) {
-        double acc = 0.;
-        for (int p = 0; p < TP; ++p) {
-            int np_ = cols[p].n;
-            if (!np_) continue;
-            double raw = 0.;
-            for (int k = 0; k < np_; ++k) {
-                int key = cols[p].key[k];
-                raw += (cols[p].va[k] * U[(size_t)(key - 1) * E + e]) + (cols[p].vb[k] * U[(size_t)key * E + e]);
-            }
-            acc += raw * som[p];
-        }
-        out[e] = acc;
-    }
-}
-
-// c7 (1/sum) + c9 (containment factor) + c8/c10 folded into one per-(s,e) scale.
-__global__ void k_correction(const double* partsum, int ntiles, const SrcInfo* info,
-                             const double* upsf, const double* partial, const double* expo, int S,
-                             int E, double* scale, double* inv_out, double* fac_out,
-                             double* rad_out, int* fov_out) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= S * E) return;
-    int s = i / E, e = i - s * E;
-    SrcInfo si = info[s];
-    double sum = 0.;
-    for (int t = 0; t < ntiles; ++t) sum += partsum[((size_t)s * ntiles + t) * E + e];
-    double inv = sum != 0. ? 1.0 / sum : sum;
-    double factor;
-    if (!si.in_fov) factor = 1.0;
-    else {
-        double v0 = si.radius_deg;
-        int li = v0 < 1. ? 1 : (int)floor(1. + log(1e4 * v0) * RECIPSTEP);
-        int d = li >= ND - 2 ? ND - 2 : li;
-        const double xstep = log(70. / 1e-4) / (400 - 1.);
-        double t1 = (d == 0 ? 0. : 1e-4 * exp((d - 1) * xstep)) * D2R;
-        double t2 = (1e-4 * exp(d * xstep)) * D2R;
-        const double* U = upsf + (size_t)s * ND * E;
-        double y1 = TWOPI * U[(size_t)d * E + e] * sin(t1);
-        double y2 = TWOPI * U[(size_t)(d + 1) * E + e] * sin(t2);
-        double m = (y2 - y1) / (t2 - t1);
-        double b = y1 - t1 * m;
-        double v = 0.5 * m * (t2 * t2 - t1 * t1) + b * (t2 - t1);
-        double integ = v + partial[(size_t)s * ND * E + (size_t)d * E + e];
-        integ = integ > 1.0 ? 1.0 : integ;
-        factor = integ * inv;
-    }
-    scale[i] = expo[i] * factor;
-    if (inv_out) inv_out[i] = inv;
-    if (fac_out) fac_out[i] = factor;
-    if (e == 0) {
-        if (rad_out) rad_out[s] = si.radius_deg;
-        if (fov_out) fov_out[s] = si.in_fov;
-    }
-}
 
 // d1 + d2 + c8 + c10: evaluate every pixel of a tile and write the scaled map.
 // Phase 1: one thread per pixel computes its columns (FP64 separations).
