@@ -89,11 +89,20 @@ constexpr size_t AO_COEF = (8 * (ND + 1) + 15) / 16 * 16;
 constexpr size_t AO_WIN = AO_COEF + sizeof(float4) * 2 * ND;  // [4][AW][AT] floats
 constexpr size_t A_SMEM = AO_WIN + sizeof(float) * 4 * AW * AT;
 
+__device__ __forceinline__ float4 f4fma(float a, const float4& y, const float4& c) {
+    return make_float4(fmaf(a, y.x, c.x), fmaf(a, y.y, c.y), fmaf(a, y.z, c.z), fmaf(a, y.w, c.w));
+}
+__device__ __forceinline__ float f4c(const float4& v, int c) { return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w; }
+
 // Evaluates one region.  Returns true when it is accepted, after adding
-// area * R7 into mean[e] (atomically when `atomic`); otherwise sets *dim.
+// area * R7 into mean[e] (atomically when `atomic`); otherwise sets *dim.  Y is
+// the source's FP32 mean-PSF table with rows of EP = E rounded up to 4 floats
+// (zeros past E), read four energies at a time.  Without `atomic` (level 0, one
+// region per pixel) the values are written during the acceptance check and the
+// caller clears them when the region is split.
 __device__ __noinline__ bool gm_region(const PixGeom& g, float c0, float c1, float h0, float h1, bool last,
                                           const double* sq, const float4* scoef, float* wk, const float* Y, int E,
-                                          float rtol, float* mean, bool atomic, int* dim) {
+                                          int EP, float rtol, float* mean, bool atomic, int* dim) {
     int ix[17];
     float tt[17];
     int rmin = ND, rmax = 0;
@@ -136,50 +145,68 @@ __device__ __noinline__ bool gm_region(const PixGeom& g, float c0, float c1, flo
             e1[j] = wk[(3 * AW + j) * AT];
         }
     }
-    const float* y0 = Y + (size_t)rmin * E;
-    // R7, R5 - R7 and the two fourth differences at energy e: from the windows,
-    // or point by point when the rows are too far apart
-    auto rule = [&](int e, float& v7, float& vd, float& a0, float& a1) {
-        v7 = vd = a0 = a1 = 0.f;
+    const float* y0 = Y + (size_t)rmin * EP;
+    const int EQ4 = EP >> 2;
+    // R7, R5 - R7 and the two fourth differences at energies 4qd .. 4qd + 3: from
+    // the windows, or point by point when the rows are too far apart
+    auto rule = [&](int qd, float4& v7, float4& vd, float4& a0, float4& a1) {
+        v7 = vd = a0 = a1 = make_float4(0.f, 0.f, 0.f, 0.f);
         if (windowed) {
 #pragma unroll
             for (int j = 0; j < AW; ++j) {
                 if (j < nr) {
-                    const float yv = __ldg(y0 + (size_t)j * E + e);
-                    v7 = fmaf(w7[j], yv, v7);
-                    vd = fmaf(wd[j], yv, vd);
-                    a0 = fmaf(e0[j], yv, a0);
-                    a1 = fmaf(e1[j], yv, a1);
+                    const float4 yv = __ldg((const float4*)(y0 + (size_t)j * EP) + qd);
+                    v7 = f4fma(w7[j], yv, v7);
+                    vd = f4fma(wd[j], yv, vd);
+                    a0 = f4fma(e0[j], yv, a0);
+                    a1 = f4fma(e1[j], yv, a1);
                 }
             }
         } else {
             for (int p = 0; p < 17; ++p) {
-                const float* yl = Y + (size_t)(ix[p] - 1) * E + e;
-                const float f = fmaf(tt[p], __ldg(yl + E) - __ldg(yl), __ldg(yl));
-                v7 = fmaf(c_gm.w7[p], f, v7);
-                vd = fmaf(c_gm.wd[p], f, vd);
-                a0 = fmaf(c_gm.d0[p], f, a0);
-                a1 = fmaf(c_gm.d1[p], f, a1);
+                const float4* yl = (const float4*)(Y + (size_t)(ix[p] - 1) * EP) + qd;
+                const float4 lo = __ldg(yl), hi = __ldg(yl + EQ4);
+                const float4 f = make_float4(fmaf(tt[p], hi.x - lo.x, lo.x), fmaf(tt[p], hi.y - lo.y, lo.y),
+                                             fmaf(tt[p], hi.z - lo.z, lo.z), fmaf(tt[p], hi.w - lo.w, lo.w));
+                v7 = f4fma(c_gm.w7[p], f, v7);
+                vd = f4fma(c_gm.wd[p], f, vd);
+                a0 = f4fma(c_gm.d0[p], f, a0);
+                a1 = f4fma(c_gm.d1[p], f, a1);
             }
         }
     };
     float rel = 0.f, dd0 = 0.f, dd1 = 0.f;
     if (!last) {
-        for (int e = 0; e < E; ++e) {
-            float v7, vd, a0, a1;
-            rule(e, v7, vd, a0, a1);
-            const float r = fabsf(vd) <= rtol * fabsf(v7) ? 0.f : (v7 != 0.f ? fabsf(vd) / fabsf(v7) : 3.4e38f);
-            rel = fmaxf(rel, r);
-            dd0 += fabsf(a0);
-            dd1 += fabsf(a1);
+        for (int qd = 0; qd < EQ4; ++qd) {
+            float4 v7, vd, a0, a1;
+            rule(qd, v7, vd, a0, a1);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int e = 4 * qd + c;
+                if (e < E) {
+                    const float x7 = f4c(v7, c), xd = f4c(vd, c);
+                    const float r = fabsf(xd) <= rtol * fabsf(x7) ? 0.f : (x7 != 0.f ? fabsf(xd) / fabsf(x7) : 3.4e38f);
+                    rel = fmaxf(rel, r);
+                    dd0 += fabsf(f4c(a0, c));
+                    dd1 += fabsf(f4c(a1, c));
+                    if (!atomic) mean[e] = area * x7;  // kept if accepted, cleared by the caller if not
+                }
+            }
         }
+        if (!atomic && rel <= rtol) return true;
     }
     if (last || rel <= rtol) {
-        for (int e = 0; e < E; ++e) {
-            float v7, vd, a0, a1;
-            rule(e, v7, vd, a0, a1);
-            if (atomic) atomicAdd(mean + e, area * v7);
-            else mean[e] = area * v7;
+        for (int qd = 0; qd < EQ4; ++qd) {
+            float4 v7, vd, a0, a1;
+            rule(qd, v7, vd, a0, a1);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int e = 4 * qd + c;
+                if (e < E) {
+                    if (atomic) atomicAdd(mean + e, area * f4c(v7, c));
+                    else mean[e] = area * f4c(v7, c);
+                }
+            }
         }
         return true;
     }
@@ -233,12 +260,13 @@ k_adaptive_level0(const double* __restrict__ corners, const SrcInfo* __restrict_
     const int sp = s * npix + pix;
     float* m = mean + (size_t)sp * E;
     int dim = 0;
-    if (gm_region(g, 0.f, 0.f, 1.f, 1.f, max_depth == 0, sq, scoef, wk, lut + (size_t)s * ND * E, E, rtol, m,
+    const int EP = (E + 3) & ~3;
+    if (gm_region(g, 0.f, 0.f, 1.f, 1.f, max_depth == 0, sq, scoef, wk, lut + (size_t)s * ND * EP, E, EP, rtol, m,
                   false, &dim))
         return;
     for (int e = 0; e < E; ++e) m[e] = 0.f;
     if (!push_halves(q, qcount, qcap, sp, 0.f, 0.f, 1.f, 1.f, dim))  // queue full: keep the estimate
-        gm_region(g, 0.f, 0.f, 1.f, 1.f, true, sq, scoef, wk, lut + (size_t)s * ND * E, E, rtol, m, false, &dim);
+        gm_region(g, 0.f, 0.f, 1.f, 1.f, true, sq, scoef, wk, lut + (size_t)s * ND * EP, E, EP, rtol, m, false, &dim);
 }
 
 // Level >= 1: persistent grid-stride over the previous level's queue.
@@ -261,12 +289,13 @@ k_adaptive_level(const double* __restrict__ corners, const SrcInfo* __restrict__
         const SrcInfo si = info[s];
         const int h = pix / W, w = pix - h * W;
         const PixGeom g = pixel_geom(corners, W + 1, h, w, si);
-        const float* Y = lut + (size_t)s * ND * E;
+        const int EP = (E + 3) & ~3;
+        const float* Y = lut + (size_t)s * ND * EP;
         float* m = mean + (size_t)r.sp * E;
         int dim = 0;
-        if (gm_region(g, r.c0, r.c1, r.h0, r.h1, last, sq, scoef, wk, Y, E, rtol, m, true, &dim)) continue;
+        if (gm_region(g, r.c0, r.c1, r.h0, r.h1, last, sq, scoef, wk, Y, E, EP, rtol, m, true, &dim)) continue;
         if (!push_halves(qout, qout_count, qcap, r.sp, r.c0, r.c1, r.h0, r.h1, dim))
-            gm_region(g, r.c0, r.c1, r.h0, r.h1, true, sq, scoef, wk, Y, E, rtol, m, true, &dim);
+            gm_region(g, r.c0, r.c1, r.h0, r.h1, true, sq, scoef, wk, Y, E, EP, rtol, m, true, &dim);
     }
 }
 
@@ -336,7 +365,8 @@ int launch_adaptive_map(const double* corners, const double* centers, const doub
     if (rc) return rc;
     const int npix = H * W;
     // the mean PSF rows in FP32, [S][401][E]
-    float* lut = (float*)workspace(W_LUT, sizeof(float) * (size_t)S * ND * E + 16);
+    const int EP = (E + 3) & ~3;  // table rows padded to whole float4s
+    float* lut = (float*)workspace(W_LUT, sizeof(float) * (size_t)S * ND * EP + 16);
     // two region queues (ping-pong) and their counters
     long long cap = 4LL * S * npix;
     cap = cap < (1 << 20) ? (1 << 20) : cap;
@@ -344,7 +374,7 @@ int launch_adaptive_map(const double* corners, const double* centers, const doub
     QRegion* q = (QRegion*)workspace(W_SPARSE, sizeof(QRegion) * 2 * (size_t)cap + 16);
     int* counts = (int*)workspace(W_WMETA, sizeof(int) * 64);
     if (!lut || !q || !counts) return XTS_ERR_OOM;
-    XTS_LAUNCH("k_lut_scaled", st, k_lut_scaled<<<lut_scaled_grid(S), 256, 0, st>>>(upsf, nullptr, S, E, E, lut,
+    XTS_LAUNCH("k_lut_scaled", st, k_lut_scaled<<<lut_scaled_grid(S), 256, 0, st>>>(upsf, nullptr, S, E, EP, lut,
                                                                                        nullptr, nullptr));
     XTS_CUDA(cudaFuncSetAttribute(k_adaptive_level0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A_SMEM));
     XTS_CUDA(cudaFuncSetAttribute(k_adaptive_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A_SMEM));
