@@ -381,14 +381,18 @@ def test_adaptive_map_accuracy_gain(api):
     assert e_ad < 0.5 * e_pl
 
 
-@pytest.mark.parametrize("name", ["c0", "c1"])
-def test_exposure_map_tensor_cores(api, name):
+@pytest.mark.parametrize("name,n_e", [("c0", None), ("c1", None), ("c0", 80)])
+def test_exposure_map_tensor_cores(api, name, n_e):
     """The full-sky exposure contraction on tcgen05 (3xTF32, FP32 accumulation)
     against the FP64 oracle applied to every livetime-cube row, and its rows at
-    the sources' NESTED pixels against the FP64 per-source exposures."""
+    the sources' NESTED pixels against the FP64 per-source exposures, for E = 20,
+    37 and 80 (N = 32, 48 and 80 columns of the accumulator)."""
     from oracle import oracle as O
 
     job = _job(name, seed=4)
+    if n_e:
+        job.energies = np.logspace(2.0, 5.0, n_e)
+        job.logEs = np.log10(job.energies)
     ref = oracle_pipeline(job, with_map=False)
     cube, wcube = job.exp_cube, job.wexp_cube
     m = api.exposure_map(cube, wcube, job.logEs, job.aeff_front, job.aeff_back, ref["ltf"])
