@@ -72,3 +72,16 @@ def test_fft_convolution(api, upsf):
     o2 = api.convolve_map_psf(img[:, :30, :20], delta)
     assert np.abs(o2[:, :30, :20] - img[:, :30, :20]).max() <= 1e-12 * img.max()
     assert np.abs(o2[:, 30:, :]).max() <= 1e-12 * img.max()
+
+
+def test_diffuse_argument_errors(api, upsf):
+    """Shape errors come back as XTS_ERR_ARG, before any launch."""
+    from xtsrcmaps_b200 import _lib
+    from xtsrcmaps_b200.wcs import Wcs
+
+    w = Wcs(20, 20, 10.5, 10.5, 193.98, -5.82, -0.1, 0.1, proj="CAR")
+    with pytest.raises(_lib.XtsError) as ei:
+        api.make_psf_kernel(w, 20, upsf)  # even kernel size
+    assert ei.value.code == _lib.XTS_ERR_ARG
+    with pytest.raises(ValueError):
+        api.convolve_map_psf(np.zeros((2, 8, 8)), np.zeros((3, 5, 5)))  # energies differ
