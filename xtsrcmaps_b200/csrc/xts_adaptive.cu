@@ -97,9 +97,11 @@ __device__ __forceinline__ float f4c(const float4& v, int c) { return c == 0 ? v
 // Evaluates one region.  Returns true when it is accepted, after adding
 // area * R7 into mean[e] (atomically when `atomic`); otherwise sets *dim.  Y is
 // the source's FP32 mean-PSF table with rows of EP = E rounded up to 4 floats
-// (zeros past E), read four energies at a time.  Without `atomic` (level 0, one
-// region per pixel) the values are written during the acceptance check and the
-// caller clears them when the region is split.
+// (zeros past E), read four energies at a time.  The values are added during the
+// acceptance check, so an accepted region (most of them) is evaluated once; a
+// split region's values are taken back out (atomically; at level 0, one region
+// per pixel, the caller clears them), which leaves FP32 rounding of the order of
+// one ulp of the pixel mean.
 __device__ __noinline__ bool gm_region(const PixGeom& g, float c0, float c1, float h0, float h1, bool last,
                                           const double* sq, const float4* scoef, float* wk, const float* Y, int E,
                                           int EP, float rtol, float* mean, bool atomic, int* dim) {
@@ -189,13 +191,27 @@ __device__ __noinline__ bool gm_region(const PixGeom& g, float c0, float c1, flo
                     rel = fmaxf(rel, r);
                     dd0 += fabsf(f4c(a0, c));
                     dd1 += fabsf(f4c(a1, c));
-                    if (!atomic) mean[e] = area * x7;  // kept if accepted, cleared by the caller if not
+                    // added now, so an accepted region needs no second pass; a split
+                    // region is taken back out below (level 0: cleared by the caller)
+                    if (atomic) atomicAdd(mean + e, area * x7);
+                    else mean[e] = area * x7;
                 }
             }
         }
-        if (!atomic && rel <= rtol) return true;
+        if (rel <= rtol) return true;
+        if (atomic) {
+            for (int qd = 0; qd < EQ4; ++qd) {
+                float4 v7, vd, a0, a1;
+                rule(qd, v7, vd, a0, a1);
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                    if (4 * qd + c < E) atomicAdd(mean + 4 * qd + c, -(area * f4c(v7, c)));
+            }
+        }
+        *dim = dd0 >= dd1 ? 0 : 1;
+        return false;
     }
-    if (last || rel <= rtol) {
+    {  // the depth limit: accepted without a check
         for (int qd = 0; qd < EQ4; ++qd) {
             float4 v7, vd, a0, a1;
             rule(qd, v7, vd, a0, a1);
@@ -210,8 +226,6 @@ __device__ __noinline__ bool gm_region(const PixGeom& g, float c0, float c1, flo
         }
         return true;
     }
-    *dim = dd0 >= dd1 ? 0 : 1;
-    return false;
 }
 
 // Pushes the two halves of a region (lower half first in the queue), or returns
