@@ -302,8 +302,8 @@ k_srcmap_win(const float4* __restrict__ win, const int* __restrict__ wmeta, cons
         if (kmax <= RW) {  // window records only (warp-uniform)
 #pragma unroll
             for (int j = 0; j < RW; ++j) {
-                if (j < kmax) {  // rows past a pixel's own window carry weight 0
-                    const float4* yr = tab + (rb + j) * EQ;
+                if (j < kmax && j < nent) {  // rows past a pixel's own window carry weight 0: lanes
+                    const float4* yr = tab + (rb + j) * EQ;  // past theirs issue no shared loads
                     const float wj = w[j];
 #pragma unroll
                     for (int q = 0; q < NQ; ++q) {
