@@ -405,14 +405,17 @@ def run_ours(args, rank, world, local_rank):
         te3 = wall(step_three)
         C = int(job.exp_cube.nbrbins)
         grid_b = lambda g: 8 * (g.cosths.size + g.logEs.size + g.params.size)
-        h2d = (2 * job.exp_cube.cosbins.nbytes + 8 * E + 8 * 2 * S + grid_b(job.aeff_front) + grid_b(job.aeff_back)
+        # with host buffers the library uploads only the livetime rows at the sources' pixels
+        # (their indices come back first, 8 B per source)
+        cube_b = 2 * 4 * S * C
+        h2d = (cube_b + 8 * E + 8 * 2 * S + grid_b(job.aeff_front) + grid_b(job.aeff_back)
                + grid_b(nf_h) + grid_b(nb_h) + 8 * 2 * E)
-        d2h = 4 * n_values
-        h2d3 = (2 * job.exp_cube.cosbins.nbytes + 8 * E + 8 * 2 * S + grid_b(job.aeff_front) + grid_b(job.aeff_back)
+        d2h = 4 * n_values + 8 * S
+        h2d3 = (cube_b + 8 * E + 8 * 2 * S + grid_b(job.aeff_front) + grid_b(job.aeff_back)
                 + 8 * 2 * E  # exposure
                 + grid_b(nf_h) + grid_b(nb_h) + 8 * (C + E + 2 * C * E + 2 * S * C + 2 * E + S * E)  # psf
                 + 8 * (2 * S + S * E + 2 * S * 401 * E))  # srcmap
-        d2h3 = (8 * (C + 2 * C * E + 2 * S * C + S * E) + 8 * 2 * S * 401 * E + 4 * n_values)
+        d2h3 = (8 * S + 8 * (C + 2 * C * E + 2 * S * C + S * E) + 8 * 2 * S * 401 * E + 4 * n_values)
         e2e = {"value": n_values * world * ke / te, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "steps": ke,
                "note": "one public call per step (point_source_maps: the three calls of main.cxx:28-30 fused) "

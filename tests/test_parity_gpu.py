@@ -71,6 +71,31 @@ def test_exposure_vs_oracle(api, c1_small):
     assert max_rel(ex.exposure, ref["exposure"]) < 1e-13
 
 
+def test_exposure_host_rows_match_device(api):
+    """With host buffers only the livetime rows at the sources' pixels are uploaded;
+    the result equals the device-pointer call, which reads the whole cubes, also for
+    a repeated source and a non-finite position (whatever row that maps to)."""
+    import torch
+
+    from xtsrcmaps_b200.api import ExpCube
+
+    job = _job("c1", seed=8, n=5)
+    src = np.vstack([job.src_sph, job.src_sph[:1], [[np.nan, 0.0]]])
+    ltf = api.livetime_efficiency_factors(job.logEs, job.effic_front)
+    eh = api.compute_exposure(job.exp_cube, job.wexp_cube, job.logEs, src, job.aeff_front, job.aeff_back, ltf)
+    d = torch.device("cuda")
+    tc = lambda c: ExpCube(torch.as_tensor(c.cosbins, device=d), c.nside, c.nbrbins, c.cosmin, c.thetabin)
+    ed = api.compute_exposure(tc(job.exp_cube), tc(job.wexp_cube), torch.as_tensor(job.logEs, device=d),
+                              torch.as_tensor(src, device=d), job.aeff_front, job.aeff_back,
+                              torch.as_tensor(ltf, device=d))
+    torch.cuda.synchronize()
+    for a, b in ((eh.src_exposure_cosbins, ed.src_exposure_cosbins), (eh.exposure, ed.exposure)):
+        b = b.cpu().numpy()
+        np.testing.assert_array_equal(np.isnan(a), np.isnan(b))
+        np.testing.assert_array_equal(a[:-1], b[:-1])
+    np.testing.assert_array_equal(eh.exposure[0], eh.exposure[5])
+
+
 def test_mean_psf_vs_oracle(api, c1_small):
     job, ref, gpu = c1_small
     assert max_rel(gpu["ps"].uPsf, ref["upsf"]) < 1e-11

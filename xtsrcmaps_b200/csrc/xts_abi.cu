@@ -1,10 +1,12 @@
 // xts_abi.cu -- the extern "C" entry points of include/xtsrcmaps_b200.h: argument
 // checks, host<->device staging, the cached device workspace and error strings.
+#include <math.h>
 #include <stdarg.h>
 #include <stdio.h>
 #include <string.h>
 
 #include <mutex>
+#include <vector>
 
 #include "xts_internal.cuh"
 
@@ -305,6 +307,43 @@ static xts_grid stage_grid(Stager& sg, const xts_grid* g) {
     return d;
 }
 
+// Host mode: the per-source path needs only the livetime rows at the sources'
+// NESTED pixels, so those rows are gathered on the host (pixels computed on the
+// device from the staged positions) and only they are uploaded, instead of the
+// whole cubes ([12 nside^2, C] floats each).  Device mode uploads nothing and
+// reads the cubes in place.  The gathered rows must outlive the call's copies.
+struct CubeRows {
+    std::vector<float> x, w;
+};
+static void stage_cubes(Stager& sg, const xts_expcube* cube, const xts_expcube* wcube, const double* src_d, int S,
+                        ExposureDev& ea, CubeRows& rows) {
+    const int C = cube->nbrbins;
+    const long long nhp = 12LL * cube->nside * cube->nside;
+    if (sg.dev || S <= 0 || sg.rc) {
+        ea.cube = sg.in(cube->cosbins, (size_t)nhp * C);
+        ea.wcube = sg.in(wcube->cosbins, (size_t)nhp * C);
+        return;
+    }
+    long long* pix_d = (long long*)workspace(W_SRCPIX, sizeof(long long) * (size_t)S);
+    if (!pix_d) { sg.rc = XTS_ERR_OOM; return; }
+    std::vector<long long> pix((size_t)S);
+    int rc = launch_src_pixels(src_d, S, cube->nside, pix_d, sg.st);
+    if (rc) { sg.rc = rc; return; }
+    cudaError_t e = cudaMemcpyAsync(pix.data(), pix_d, sizeof(long long) * (size_t)S, cudaMemcpyDeviceToHost, sg.st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(sg.st);
+    if (e != cudaSuccess) { sg.rc = cuda_error(e, "source pixels"); return; }
+    rows.x.assign((size_t)S * C, NAN);
+    rows.w.assign((size_t)S * C, NAN);
+    for (int s = 0; s < S; ++s)
+        if (pix[s] >= 0 && pix[s] < nhp) {
+            memcpy(&rows.x[(size_t)s * C], cube->cosbins + (size_t)pix[s] * C, sizeof(float) * C);
+            memcpy(&rows.w[(size_t)s * C], wcube->cosbins + (size_t)pix[s] * C, sizeof(float) * C);
+        }
+    ea.cube = sg.in(rows.x.data(), (size_t)S * C);
+    ea.wcube = sg.in(rows.w.data(), (size_t)S * C);
+    ea.gathered = true;
+}
+
 }  // namespace xts
 
 using namespace xts;
@@ -442,11 +481,11 @@ int xts_compute_exposure(const xts_expcube* cube, const xts_expcube* wcube, cons
     long long npix = 12LL * cube->nside * cube->nside;
     Stager sg{(flags & XTS_DEVICE_PTRS) != 0, stream ? (cudaStream_t)stream : g_ctx.stream};
     ExposureDev a;
-    a.cube = sg.in(cube->cosbins, (size_t)npix * C);
-    a.wcube = sg.in(wcube->cosbins, (size_t)npix * C);
+    a.src_sph = sg.in(src_sph, (size_t)2 * S); a.S = S;
+    CubeRows rows;
+    stage_cubes(sg, cube, wcube, a.src_sph, S, a, rows);
     a.nside = cube->nside; a.C = C; a.cosmin = cube->cosmin; a.thetabin = cube->thetabin;
     a.logEs = sg.in(logEs, (size_t)E); a.E = E;
-    a.src_sph = sg.in(src_sph, (size_t)2 * S); a.S = S;
     a.af = stage_grid(sg, aeff_front);
     a.ab = stage_grid(sg, aeff_back);
     a.ltf = sg.in(front_ltf, (size_t)2 * E);
@@ -676,11 +715,11 @@ int xts_point_source_maps(const xts_expcube* cube, const xts_expcube* wcube, con
     }
     // (a) exposure; its outputs stay in device memory
     ExposureDev ea;
-    ea.cube = sg.in(cube->cosbins, (size_t)nhp * C);
-    ea.wcube = sg.in(wcube->cosbins, (size_t)nhp * C);
+    ea.src_sph = src_d; ea.S = S;
+    CubeRows rows;
+    stage_cubes(sg, cube, wcube, src_d, S, ea, rows);
     ea.nside = cube->nside; ea.C = C; ea.cosmin = cube->cosmin; ea.thetabin = cube->thetabin;
     ea.logEs = sg.in(logEs, (size_t)E); ea.E = E;
-    ea.src_sph = src_d; ea.S = S;
     ea.af = stage_grid(sg, aeff_front);
     ea.ab = stage_grid(sg, aeff_back);
     ea.ltf = sg.in(front_ltf, (size_t)2 * E);

@@ -56,16 +56,35 @@ __global__ void k_exposure_tables(int C, double cosmin, int thetabin, const doub
     }
 }
 
-// a2: livetime rows of each source's NESTED pixel, float -> double [S, C].
+// The NESTED pixel of each source (exposure/exposure.cxx:42-63), -1 when the
+// position is not finite.
+__device__ __forceinline__ long long src_pixel(const double* src_sph, int s, long long nside) {
+    const double theta = HALFPI - src_sph[2 * s + 1] * D2R;
+    const double phi = D2R * src_sph[2 * s];
+    const long long pix = ang2pix_nest(theta, phi, nside);
+    return pix < 0 || pix >= 12 * nside * nside ? -1 : pix;
+}
+
+__global__ void k_src_pixels(const double* src_sph, int S, long long nside, long long* pix) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < S) pix[s] = src_pixel(src_sph, s, nside);
+}
+
+int launch_src_pixels(const double* src_sph, int S, long long nside, long long* pix, cudaStream_t st) {
+    if (S > 0)
+        XTS_LAUNCH("k_src_pixels", st, k_src_pixels<<<(S + 127) / 128, 128, 0, st>>>(src_sph, S, nside, pix));
+    return XTS_OK;
+}
+
+// a2: livetime rows of each source's NESTED pixel, float -> double [S, C].  With
+// `gathered` the cubes hold only those rows already, [S][C] in source order.
 __global__ void k_src_cosbins(const double* src_sph, int S, const float* cube, const float* wcube,
-                              long long nside, int C, double* ecb, double* wecb) {
+                              long long nside, int C, int gathered, double* ecb, double* wecb) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= S * C) return;
     int s = i / C, c = i - s * C;
-    double theta = HALFPI - src_sph[2 * s + 1] * D2R;
-    double phi = D2R * src_sph[2 * s];
-    long long pix = ang2pix_nest(theta, phi, nside);
-    if (pix < 0 || pix >= 12 * nside * nside) {  // non-finite source position
+    const long long pix = gathered ? s : src_pixel(src_sph, s, nside);
+    if (pix < 0) {  // non-finite source position
         ecb[i] = wecb[i] = __longlong_as_double(0x7ff8000000000000ll);
         return;
     }
@@ -109,7 +128,7 @@ int launch_exposure(const ExposureDev& a, cudaStream_t st) {
     n = a.S * a.C;
     if (n > 0) {
         XTS_LAUNCH("k_src_cosbins", st, k_src_cosbins<<<(n + 127) / 128, 128, 0, st>>>(a.src_sph, a.S, a.cube, a.wcube, a.nside,
-                                                      a.C, a.ecb, a.wecb));
+                                                      a.C, a.gathered ? 1 : 0, a.ecb, a.wecb));
     }
     return launch_exposure_contract(a.ecb, a.wecb, a.S, a.C, a.front_aeff, a.back_aeff, a.ltf, a.E,
                                     a.exposure, st);

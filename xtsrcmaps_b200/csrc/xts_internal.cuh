@@ -64,7 +64,7 @@ enum Slot {
     // internal scratch
     W_CORNERS, W_CENTERS, W_OMEGA, W_LUT, W_PARTSUM, W_SRCINFO, W_SCALE, W_PSFTAB,
     W_KING, W_MISC, W_WIN, W_WMETA, W_SPARSE, W_MISC2, W_EXPMAP,
-    W_FITS_IN, W_FITS_OUT, W_FITS_SUM, W_FFT_A, W_FFT_B, W_FFT_C, W_FFT_WORK,
+    W_FITS_IN, W_FITS_OUT, W_FITS_SUM, W_FFT_A, W_FFT_B, W_FFT_C, W_FFT_WORK, W_SRCPIX,
     N_SLOTS
 };
 void* workspace(int slot, size_t bytes);  // nullptr + error set on OOM
@@ -91,8 +91,10 @@ struct ExposureDev {
     const double* ltf;
     double* exp_costhetas; double* front_aeff; double* back_aeff;
     double* ecb; double* wecb; double* exposure;
+    bool gathered = false;  // cube, wcube hold only the sources' rows, [S][C] in source order
 };
 int launch_exposure(const ExposureDev& a, cudaStream_t st);
+int launch_src_pixels(const double* src_sph, int S, long long nside, long long* pix, cudaStream_t st);
 int launch_exposure_contract(const double* ecb, const double* wecb, int S, int C, const double* af,
                              const double* ab, const double* ltf, int E, double* out, cudaStream_t st);
 
