@@ -131,7 +131,9 @@ int xts_normalize_rpsf(double* params, int Mc, int Me, const double* grid_logEs,
                        unsigned flags, void* stream);
 
 /* Exposure::compute_exposure<T> (exposure/exposure.hxx:44-88): steps a1-a5.
- * front_ltf is Irf::XtIrf::front_LTF [2, E]; C = exp_cube->nbrbins. */
+ * front_ltf is Irf::XtIrf::front_LTF [2, E]; C = exp_cube->nbrbins.  With host
+ * pointers only the cube rows at the sources' NESTED pixels are copied to the
+ * device (as in xts_point_source_maps); device-pointer cubes are read in place. */
 int xts_compute_exposure(const xts_expcube* exp_cube, const xts_expcube* wexp_cube,
                          const double* logEs, int E, const double* src_sph, int S,
                          const xts_grid* aeff_front, const xts_grid* aeff_back,
