@@ -336,6 +336,10 @@ def run_ours(args, rank, world, local_rank):
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    # the write pass runs once per chunk of sources; its algorithmic bytes per launch are
+    # the step's bytes divided by the launches per step
+    per_step = launches / args.steps if launches else 1
+    alg_bytes = alg_bytes / per_step
     achieved = alg_bytes / (kms / launches * 1e-3) / 1e9 if launches else None
     traffic = None
     try:
@@ -346,7 +350,7 @@ def run_ours(args, rank, world, local_rank):
         pass
     roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "peak_source": peak_src,
-                "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
+                "traffic": traffic, "alg_bytes_per_launch": int(alg_bytes), "launches_per_step": per_step,
                 "avg_launch_ms": kms / launches if launches else None,
                 "kernel_share": kms / ms_prof if ms_prof else None,
                 "kernel_timing": "library CUDA events around each kernel, from %d instrumented steps "
