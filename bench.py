@@ -531,8 +531,11 @@ def run_reference(args, rank, world):
     run, threads, desc = _reference_runner(job)
     if run is not None:
         kind = "reference"
-        for _ in range(max(1, min(args.warmup, 2))):
+        warm = 0
+        t_w = time.perf_counter()
+        while warm < max(3, args.warmup) and (warm < 3 or time.perf_counter() - t_w < 30.0):
             run()
+            warm += 1
         times = []
         t_all = time.perf_counter()
         for _ in range(args.steps):  # each step is the whole workload; stop after ~60 s
@@ -553,7 +556,9 @@ def run_reference(args, rank, world):
         threads = len(chunks)
         ctx = mp.get_context("spawn")
         with ctx.Pool(len(chunks)) as pool:
-            pool.map(_oracle_worker, chunks)
+            warm = max(3, min(args.warmup, 5))
+            for _ in range(warm):
+                pool.map(_oracle_worker, chunks)
             times = []
             for _ in range(max(1, min(args.steps, 5))):
                 t0 = time.perf_counter()
@@ -564,7 +569,7 @@ def run_reference(args, rank, world):
     value = job.n_values / (ms * 1e-3)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-        "steps": len(times), "warmup": max(1, min(args.warmup, 2)), "ms_per_step": ms, "higher_is_better": True,
+        "steps": len(times), "warmup": warm, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
         "config": {"workload": args.config + ": " + DESCRIPTIONS[args.config]},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
