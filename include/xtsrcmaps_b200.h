@@ -268,6 +268,96 @@ int xts_make_psf_kernel(const xts_wcs* kernel_wcs, int Nk, const double* upsf, i
 int xts_convolve_map_psf(const double* image, int E, int H, int W, const double* kernel, int K, double* out,
                          unsigned flags, void* stream);
 
+/* Learned surrogate of the pixel cubature ---------------------------------------
+ * No counterpart in the reference.  A multilayer perceptron 5 -> 128 -> 128 ->
+ * 128 -> 1 with tanh-form GELU after each hidden layer maps five features of a
+ * (source, pixel, energy) value to y = ln(m / u_c) * rho^2, where m is the
+ * 12-point rule mean of the mean PSF over the pixel (the quantity of
+ * cubature_convolve_map_psf, model_map/mm_cubature/cubature.implementation.cxx:21-55,
+ * before the solid angle), u_c the mean PSF at the pixel centre and rho the
+ * centre's separation in pixel sizes.  Features, in order: log10 rho; the
+ * centre's offset between the two rows of the 401-row separation table that
+ * bracket it (its logsep interpolation weight); log10 of the pixel's solid angle
+ * in deg^2; log10 of the energy in MeV; the log slope ln(U[i] / U[i-1]) / step
+ * of the mean PSF's table segment holding the centre.  The hidden layers run on tcgen05 tensor
+ * cores with BF16 operands and FP32 accumulators in tensor memory; the input and
+ * output layers and the GELUs on CUDA cores in FP32 (weights rounded to BF16).
+ * All pointers are device pointers on the library's current device. */
+#define XTS_MLP_IN 5
+#define XTS_MLP_HID 128
+#define XTS_MLP_W1 0                                     /* [128][5] */
+#define XTS_MLP_B1 (XTS_MLP_W1 + XTS_MLP_HID * XTS_MLP_IN)  /* [128] */
+#define XTS_MLP_W2 (XTS_MLP_B1 + XTS_MLP_HID)                /* [128 out][128 in] */
+#define XTS_MLP_B2 (XTS_MLP_W2 + XTS_MLP_HID * XTS_MLP_HID)
+#define XTS_MLP_W3 (XTS_MLP_B2 + XTS_MLP_HID)
+#define XTS_MLP_B3 (XTS_MLP_W3 + XTS_MLP_HID * XTS_MLP_HID)
+#define XTS_MLP_W4 (XTS_MLP_B3 + XTS_MLP_HID)                /* [128] */
+#define XTS_MLP_B4 (XTS_MLP_W4 + XTS_MLP_HID)                /* [1] */
+#define XTS_MLP_NPARAM (XTS_MLP_B4 + 1)
+
+typedef struct xts_mlp {
+    float* params;          /* [XTS_MLP_NPARAM] FP32 master parameters (device) */
+    unsigned short* wbf16;  /* [2][128][128] BF16 copies of W2 and W3 (device), kept by the update */
+    float in_mu[XTS_MLP_IN], in_sd[XTS_MLP_IN];  /* feature standardisation x' = (x - mu) / sd */
+    float out_mu, out_sd;                       /* target standardisation */
+    float lo[XTS_MLP_IN], hi[XTS_MLP_IN];       /* accepted feature range (the training range) */
+    float rho_min;          /* centres closer than rho_min pixel sizes take the 12-point rule */
+} xts_mlp;
+
+/* C = A B^T in FP32 from BF16 operands on tcgen05: A [M][K] (a_trans: stored
+ * [K][M]), B [128][K] (b_trans: stored [K][128]), C [M][128] (c_trans: stored
+ * [128][M]); M a multiple of 128, K of 64.  accumulate: C += A B^T (atomic
+ * adds, K split over the blocks), else C = A B^T. */
+int xts_gemm_bf16(const unsigned short* A, int a_trans, const unsigned short* B, int b_trans, int M, int K,
+                  float* C, int c_trans, int accumulate, void* stream);
+
+/* Network output y (de-standardised) for n feature rows X [n][5]. */
+int xts_mlp_forward(const xts_mlp* net, const float* X, long long n, float* y, void* stream);
+
+/* Gradient of the loss L = (1/n) sum (y' - (Y - out_mu) / out_sd)^2 (y' the
+ * standardised output) with respect to the FP32 parameters, grads
+ * [XTS_MLP_NPARAM] (overwritten); loss [1] (may be NULL).  n a multiple of 128. */
+int xts_mlp_grads(const xts_mlp* net, const float* X, const float* Y, long long n, float* grads, float* loss,
+                  void* stream);
+
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on a batch: grads, adam_m,
+ * adam_v [XTS_MLP_NPARAM] (grads zero on entry, left zero), step >= 1; the BF16
+ * copies are refreshed.  loss [1] accumulates the batch loss (may be NULL). */
+int xts_mlp_train_step(const xts_mlp* net, const float* X, const float* Y, long long n, float* grads,
+                       float* adam_m, float* adam_v, int step, float lr, float* loss, void* stream);
+
+/* Training samples from mean-PSF tables upsf [S][401][E] and energies logEs [E]:
+ * per sample a source, an energy, a separation log-uniform in
+ * [max(0.001, rho_min * size), 30] deg, a pixel of size uniform in [0.025, 0.2]
+ * deg with aspect ratio in [0.8, 1.25] and a uniform orientation, placed on the
+ * sphere; X [n][5] its features and Y [n] its target, both from the FP64 rule
+ * the model map uses (a hash of seed and sample index drives every draw). */
+int xts_surrogate_samples(const double* upsf, const double* logEs, int S, int E, long long n,
+                          unsigned long long seed, double rho_min, float* X, float* Y, void* stream);
+
+/* Counts of a surrogate model map. */
+typedef struct xts_surrogate_stats {
+    long long values;        /* S * H * W * E */
+    long long accepted;      /* values taken from the network */
+    long long checked;       /* accepted values also evaluated by the 12-point rule */
+    int maps_fallback;       /* sources whose check failed: all their values by the rule */
+    float max_check_err;     /* largest relative difference seen by the check */
+} xts_surrogate_stats;
+
+/* The model map of xts_point_src_model_map_wcs with the pixel means taken from
+ * the network wherever the centre lies at least rho_min pixel sizes from the
+ * source and every feature is inside [lo, hi]; the other values take the FP64
+ * 12-point rule.  Every 61st pixel's accepted values are also evaluated by the
+ * rule; a source whose largest relative difference exceeds check_tol is redone
+ * entirely by the rule.  Map integral, correction and scalings as
+ * xts_point_src_model_map_wcs.  Device pointers; model_map float [S, H, W, E]. */
+int xts_point_src_model_map_wcs_surrogate(const xts_wcs* wcs, const double* src_sph, int S,
+                                          const double* exposure, const double* upsf,
+                                          const double* partial, const double* logEs, int E,
+                                          const xts_mlp* net,
+                                          double check_tol, float* model_map, xts_srcmap_info* info,
+                                          xts_surrogate_stats* stats, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

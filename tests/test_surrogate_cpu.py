@@ -1,0 +1,96 @@
+"""CPU checks of the surrogate network's host side: the numpy oracle's gradient
+against finite differences (this pins the oracle the GPU gradients are checked
+against), its BF16 rounding, the ctypes layout of xts_mlp and
+xts_surrogate_stats against the C header, and the sample oracle's geometry."""
+import math
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as MO
+from oracle import surrogate_oracle as SO
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _net(seed=3):
+    rng = np.random.default_rng(seed)
+    p = rng.normal(0.0, 0.15, MO.NPARAM)
+    X = rng.normal(0.0, 1.0, (16, MO.IN))
+    Y = rng.normal(0.0, 1.0, 16)
+    return p, X, Y
+
+
+def test_oracle_gradient_matches_finite_differences():
+    p, X, Y = _net()
+    mu, sd = np.zeros(MO.IN), np.ones(MO.IN)
+    loss, g = MO.loss_and_grads(p, X, Y, mu, sd, 0.0, 1.0, use_bf16=False)
+    rng = np.random.default_rng(0)
+    idx = np.concatenate([rng.choice(np.arange(lo, hi), 6, replace=False)
+                          for lo, hi in ((MO.W1, MO.B1), (MO.B1, MO.W2), (MO.W2, MO.B2), (MO.B2, MO.W3),
+                                         (MO.W3, MO.B3), (MO.B3, MO.W4), (MO.W4, MO.B4))] + [[MO.B4]])
+    h = 1e-6
+    for i in idx:
+        q = p.copy()
+        q[i] += h
+        lp, _ = MO.loss_and_grads(q, X, Y, mu, sd, 0.0, 1.0, use_bf16=False)
+        q[i] -= 2 * h
+        lm, _ = MO.loss_and_grads(q, X, Y, mu, sd, 0.0, 1.0, use_bf16=False)
+        fd = (lp - lm) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(fd)), (i, fd, g[i])
+    assert loss > 0
+
+
+def test_bf16_rounding_ties_to_even():
+    # 1 + 2^-8 lies halfway between BF16 neighbours 1 and 1 + 2^-7: even mantissa (1) wins
+    assert MO.bf16(np.float32(1.0 + 2.0 ** -8))[()] == 1.0
+    assert MO.bf16(np.float32(1.0 + 3 * 2.0 ** -8))[()] == 1.0 + 2.0 ** -6
+    assert MO.bf16(np.float32(-2.5))[()] == -2.5
+
+
+def test_struct_layouts_match_the_header():
+    from xtsrcmaps_b200 import _lib as L
+    import ctypes as C
+
+    src = r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "xtsrcmaps_b200.h"
+int main(void) {
+    printf("%zu %zu %zu %zu %zu %zu\n", sizeof(xts_mlp), offsetof(xts_mlp, in_mu), offsetof(xts_mlp, out_mu),
+           offsetof(xts_mlp, lo), offsetof(xts_mlp, rho_min), sizeof(xts_surrogate_stats));
+    printf("%d %d %d %d\n", XTS_MLP_W2, XTS_MLP_W3, XTS_MLP_B4, XTS_MLP_NPARAM);
+    return 0;
+}
+'''
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        exe = os.path.join(d, "t")
+        open(c, "w").write(src)
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe], check=True)
+        out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split("\n")
+    sizes = [int(v) for v in out[0].split()]
+    assert sizes == [C.sizeof(L.XtsMlp), L.XtsMlp.in_mu.offset, L.XtsMlp.out_mu.offset, L.XtsMlp.lo.offset,
+                     L.XtsMlp.rho_min.offset, C.sizeof(L.XtsSurrogateStats)]
+    consts = [int(v) for v in out[1].split()]
+    assert consts == [L.MLP_W2, L.MLP_W3, L.MLP_B4, L.MLP_NPARAM] == [MO.W2, MO.W3, MO.B4, MO.NPARAM]
+
+
+def test_sample_oracle_geometry():
+    assert abs(SO.RULE[:, 2].sum() - 4.0) < 1e-12
+    # a smooth table (u = exp(-theta / 2 deg)) and a sample far from the source:
+    # the rule mean approaches the centre value
+    seps = np.array([0.0] + [1e-4 * math.exp(k * SO.SEP_STEP) for k in range(400)])
+    U = np.exp(-seps / 2.0)[:, None] * np.ones((1, 3))
+    upsf = U[None]
+    logEs = np.array([2.0, 3.0, 4.0])
+    for i in range(20):
+        x, y = SO.sample(upsf, logEs, i, seed=5, rho_min=20.0)
+        assert 10 ** x[0] >= 20.0 * 0.999  # rho >= rho_min
+        assert 0.0 <= x[1] <= 1.0  # offset between table rows
+        assert math.log10(0.025 ** 2 * 0.99) <= x[2] <= math.log10(0.2 ** 2 * 1.01)
+        assert x[3] in logEs
+        assert np.isfinite(y)

@@ -1,0 +1,183 @@
+"""GPU checks of the learned surrogate: the tcgen05 BF16 GEMM against FP64
+products of the same BF16 values, the network's forward pass and gradient
+against the CPU oracle (oracle/mlp_oracle.py, itself pinned to finite
+differences), the training samples against oracle/surrogate_oracle.py, the
+model map's fallback path, and what the trained network gains over the centre
+value alone.
+
+Tolerances:
+  * GEMM: relative 1e-5 of the output scale (FP32 accumulation of BF16 products);
+  * forward output: relative L2 2e-2; gradient blocks: relative L2 5e-2 -- the
+    kernels use tanh.approx (relative error ~5e-4) where the oracle uses tanh,
+    which flips some BF16 roundings of activations;
+  * samples: features 1e-5, targets 1e-4 relative (FP64 math, FP32 storage);
+  * the model map with every map redone by the rule: 1e-5 relative against the
+    plain FP32 map (both the FP64 12-point rule, stored in FP32).
+"""
+import numpy as np
+import pytest
+
+from helpers import max_rel
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def api():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from xtsrcmaps_b200 import api as A
+    from xtsrcmaps_b200 import build
+
+    build.build()
+    A.init(0)
+    return A
+
+
+def _psf_tables(A, name, seed, n=None):
+    """Device uPsf / partial / exposure of a synthetic job."""
+    import torch
+
+    from xtsrcmaps_b200.synth import make_job
+
+    job = make_job(name, seed=seed, n_sources=n)
+    ltf = A.livetime_efficiency_factors(job.logEs, job.effic_front)
+    nf = A.normalize_rpsf(job.rpsf_front, job.scale_front)
+    nb = A.normalize_rpsf(job.rpsf_back, job.scale_back)
+    ex = A.compute_exposure(job.exp_cube, job.wexp_cube, job.logEs, job.src_sph, job.aeff_front,
+                            job.aeff_back, ltf)
+    ps = A.compute_psf_data(nf, nb, ex, job.logEs, ltf)
+    d = torch.device("cuda")
+    t = lambda x: torch.as_tensor(np.ascontiguousarray(x), device=d)
+    return job, t(ps.uPsf), t(ps.partial_psf_integral), t(ex.exposure)
+
+
+def _bf16(rng, shape):
+    import torch
+
+    return torch.as_tensor(rng.normal(0.0, 1.0, shape).astype(np.float32)).to(torch.bfloat16)
+
+
+@pytest.mark.parametrize("M,K,at,bt,ct,acc", [(256, 128, 0, 0, 0, 0), (384, 128, 1, 1, 1, 0),
+                                             (128, 4096, 0, 0, 0, 1), (256, 192, 1, 0, 1, 0),
+                                             (128, 1024, 1, 1, 0, 1)])
+def test_gemm_bf16_layouts(api, M, K, at, bt, ct, acc):
+    import torch
+
+    from xtsrcmaps_b200.surrogate import gemm_bf16
+
+    rng = np.random.default_rng(M + K)
+    A = _bf16(rng, (K, M) if at else (M, K))
+    B = _bf16(rng, (K, 128) if bt else (128, K))
+    Amk = (A.T if at else A).double().numpy()
+    Bnk = (B.T if bt else B).double().numpy()
+    ref = Amk @ Bnk.T
+    d = torch.device("cuda")
+    out = gemm_bf16(A.to(d), B.to(d), M, K, bool(at), bool(bt), bool(ct), accumulate=bool(acc))
+    got = out.cpu().double().numpy()
+    got = got.T if ct else got
+    assert np.abs(got - ref).max() <= 1e-5 * np.abs(ref).max()
+
+
+def _rel_l2(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def test_forward_and_gradient_match_oracle(api):
+    import torch
+
+    from oracle import mlp_oracle as MO
+    from xtsrcmaps_b200.surrogate import Surrogate
+
+    d = torch.device("cuda")
+    net = Surrogate(device=d, seed=1)
+    rng = np.random.default_rng(2)
+    n = 1024
+    X = rng.normal(0.5, 2.0, (n, 5)).astype(np.float32)
+    Y = rng.normal(0.0, 1.5, n).astype(np.float32)
+    net.in_mu = np.full(5, 0.5, np.float32)
+    net.in_sd = np.full(5, 2.0, np.float32)
+    net.out_mu, net.out_sd = 0.25, 1.5
+    p = net.params.cpu().numpy()
+    y = net.predict(torch.as_tensor(X, device=d)).cpu().numpy()
+    y_ref = MO.predict(p, X, net.in_mu, net.in_sd, net.out_mu, net.out_sd)
+    assert _rel_l2(y, y_ref) < 2e-2
+    g, loss = net.gradient(torch.as_tensor(X, device=d), torch.as_tensor(Y, device=d))
+    loss_ref, g_ref = MO.loss_and_grads(p, X, Y, net.in_mu, net.in_sd, net.out_mu, net.out_sd)
+    assert abs(loss - loss_ref) <= 1e-2 * loss_ref
+    g = g.cpu().numpy()
+    for name, lo, hi in (("W1", MO.W1, MO.B1), ("b1", MO.B1, MO.W2), ("W2", MO.W2, MO.B2), ("b2", MO.B2, MO.W3),
+                         ("W3", MO.W3, MO.B3), ("b3", MO.B3, MO.W4), ("W4", MO.W4, MO.B4), ("b4", MO.B4, MO.NPARAM)):
+        assert _rel_l2(g[lo:hi], g_ref[lo:hi]) < 5e-2, name
+
+
+def test_samples_match_oracle(api):
+    import torch
+
+    from oracle import surrogate_oracle as SO
+    from xtsrcmaps_b200.surrogate import samples
+
+    job, upsf, _, _ = _psf_tables(api, "c1", seed=4, n=5)
+    X, Y = samples(upsf, job.logEs, 300, seed=12345, rho_min=20.0)
+    X, Y = X.cpu().numpy(), Y.cpu().numpy()
+    U = upsf.cpu().numpy()
+    for i in range(300):
+        x, y = SO.sample(U, job.logEs, i, 12345, 20.0)
+        np.testing.assert_allclose(X[i], x, rtol=1e-5, atol=1e-5)
+        assert abs(Y[i] - y) <= 1e-4 * abs(y) + 1e-5, (i, Y[i], y)
+
+
+def test_map_fallback_equals_rule(api):
+    """With a check tolerance no network meets, every map is redone by the FP64
+    12-point rule: the plain path's values."""
+    import torch
+
+    from xtsrcmaps_b200.surrogate import Surrogate, model_map, samples
+
+    job, upsf, partial, expo = _psf_tables(api, "c1", seed=6, n=4)
+    net = Surrogate(device=torch.device("cuda"), seed=0)
+    X, Y = samples(upsf, job.logEs, 128 * 64, seed=3)
+    net.fit_standardisation(X, Y)
+    src = torch.as_tensor(job.src_sph, device=upsf.device)
+    m, info, st = model_map(job.wcs, src, expo, upsf, partial, job.logEs, net, check_tol=1e-12)
+    plain, pinfo = api.point_src_model_map_wcs(job.wcs, src, expo, upsf, partial)
+    assert st["values"] == m.numel() and st["maps_fallback"] >= 1 and st["accepted"] == 0
+    assert st["checked"] > 0
+    assert max_rel(m.cpu().numpy(), plain.cpu().numpy()) < 1e-5
+    assert max_rel(info.inv_map_integral.cpu().numpy(), pinfo.inv_map_integral.cpu().numpy()) < 1e-7
+
+
+def test_trained_network_gains_over_centre_value(api):
+    """Trained on the GPU on samples of one job's mean PSFs, the network's error on
+    fresh samples is compared with the centre value alone (y = 0, the method
+    without the network); then the model map of another job."""
+    import torch
+
+    from xtsrcmaps_b200.surrogate import Surrogate, model_map, samples
+
+    job, upsf, _, _ = _psf_tables(api, "c1", seed=7, n=50)
+    X, Y = samples(upsf, job.logEs, 4_000_000, seed=11)
+    net = Surrogate(device=upsf.device, seed=0)
+    losses = net.train(X, Y, epochs=12)
+    assert losses[-1] < 0.1 * losses[0]
+    Xh, Yh = samples(upsf, job.logEs, 400_000, seed=99)
+    yp = net.predict(Xh)
+    rho2 = (10.0 ** Xh[:, 0].double()) ** 2
+    err_net = ((yp.double() - Yh.double()).abs() / rho2).cpu().numpy()
+    err_c = (Yh.double().abs() / rho2).cpu().numpy()
+    gain = float(np.sqrt(np.mean(err_c ** 2)) / np.sqrt(np.mean(err_net ** 2)))
+    print(f"\nsurrogate: rms rel error {np.sqrt(np.mean(err_net**2)):.2e} vs centre value "
+          f"{np.sqrt(np.mean(err_c**2)):.2e} (gain {gain:.1f}x); within 1e-4: {np.mean(err_net <= 1e-4):.4f}")
+    assert gain > 5.0
+    job2, upsf2, partial2, expo2 = _psf_tables(api, "c1", seed=8, n=6)
+    src = torch.as_tensor(job2.src_sph, device=upsf2.device)
+    m, _, st = model_map(job2.wcs, src, expo2, upsf2, partial2, job2.logEs, net, check_tol=1e-4)
+    plain, _ = api.point_src_model_map_wcs(job2.wcs, src, expo2, upsf2, partial2)
+    m, plain = m.cpu().numpy(), plain.cpu().numpy()
+    err = np.abs(m.astype(np.float64) - plain) / np.maximum(np.abs(plain), 1e-300)
+    print(f"surrogate map: {st}; max rel err vs plain {err.max():.2e}, "
+          f"fraction within 1e-4 {np.mean(err <= 1e-4):.4f}")
+    assert 0 <= st["accepted"] <= st["values"] == m.size
+    assert np.isfinite(m).all()

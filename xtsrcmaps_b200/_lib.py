@@ -71,6 +71,36 @@ class XtsSrcmapInfo(C.Structure):
     ]
 
 
+MLP_IN = 5
+MLP_HID = 128
+MLP_W1 = 0
+MLP_B1 = MLP_W1 + MLP_HID * MLP_IN
+MLP_W2 = MLP_B1 + MLP_HID
+MLP_B2 = MLP_W2 + MLP_HID * MLP_HID
+MLP_W3 = MLP_B2 + MLP_HID
+MLP_B3 = MLP_W3 + MLP_HID * MLP_HID
+MLP_W4 = MLP_B3 + MLP_HID
+MLP_B4 = MLP_W4 + MLP_HID
+MLP_NPARAM = MLP_B4 + 1
+
+
+class XtsMlp(C.Structure):
+    _fields_ = [
+        ("params", _vp), ("wbf16", _vp),
+        ("in_mu", C.c_float * MLP_IN), ("in_sd", C.c_float * MLP_IN),
+        ("out_mu", C.c_float), ("out_sd", C.c_float),
+        ("lo", C.c_float * MLP_IN), ("hi", C.c_float * MLP_IN),
+        ("rho_min", C.c_float),
+    ]
+
+
+class XtsSurrogateStats(C.Structure):
+    _fields_ = [
+        ("values", C.c_longlong), ("accepted", C.c_longlong), ("checked", C.c_longlong),
+        ("maps_fallback", C.c_int), ("max_check_err", C.c_float),
+    ]
+
+
 # Every symbol the header declares, with its signature.
 SIGNATURES = {
     "xts_init": (C.c_int, [C.c_int]),
@@ -108,6 +138,17 @@ SIGNATURES = {
                                       C.POINTER(C.c_char_p), C.c_uint, _vp]),
     "xts_make_psf_kernel": (C.c_int, [C.POINTER(XtsWcs), C.c_int, _vp, C.c_int, _vp, C.c_uint, _vp]),
     "xts_convolve_map_psf": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_uint, _vp]),
+    "xts_gemm_bf16": (C.c_int, [_vp, C.c_int, _vp, C.c_int, C.c_int, C.c_int, _vp, C.c_int, C.c_int, _vp]),
+    "xts_mlp_forward": (C.c_int, [C.POINTER(XtsMlp), _vp, C.c_longlong, _vp, _vp]),
+    "xts_mlp_grads": (C.c_int, [C.POINTER(XtsMlp), _vp, _vp, C.c_longlong, _vp, _vp, _vp]),
+    "xts_mlp_train_step": (C.c_int, [C.POINTER(XtsMlp), _vp, _vp, C.c_longlong, _vp, _vp, _vp, C.c_int,
+                                     C.c_float, _vp, _vp]),
+    "xts_surrogate_samples": (C.c_int, [_vp, _vp, C.c_int, C.c_int, C.c_longlong, C.c_ulonglong, C.c_double,
+                                        _vp, _vp, _vp]),
+    "xts_point_src_model_map_wcs_surrogate": (C.c_int, [C.POINTER(XtsWcs), _vp, C.c_int, _vp, _vp, _vp, _vp,
+                                                        C.c_int, C.POINTER(XtsMlp), C.c_double, _vp,
+                                                        C.POINTER(XtsSrcmapInfo),
+                                                        C.POINTER(XtsSurrogateStats), _vp]),
 }
 
 

@@ -505,3 +505,13 @@ def profile_read() -> dict:
 
 def release() -> None:
     L.lib().xts_release()
+
+
+def point_src_model_map_wcs_surrogate(wcs: Wcs, src_sph, exposure, uPsf, partial_integrals, logEs, net,
+                                      check_tol: float = 1e-4, with_info: bool = True):
+    """point_src_model_map_wcs with the pixel means from the learned surrogate
+    (xtsrcmaps_b200.surrogate.Surrogate) where it applies and the FP64 12-point
+    rule elsewhere; CUDA tensors.  Returns (maps, SrcmapInfo or None, stats)."""
+    from .surrogate import model_map
+
+    return model_map(wcs, src_sph, exposure, uPsf, partial_integrals, logEs, net, check_tol, with_info)

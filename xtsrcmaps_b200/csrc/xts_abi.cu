@@ -675,6 +675,124 @@ int xts_point_src_model_map_wcs_adaptive(const xts_wcs* wcs, const double* src_s
     return run_srcmap(sg, a, model_map, npix, false);
 }
 
+// ------------------------------------------------------------------ surrogate network
+static int mlp_ok(const xts_mlp* net, const char* who) {
+    if (!net || !net->params || !net->wbf16) return set_error(XTS_ERR_ARG, "%s: network parameters missing", who);
+    for (int k = 0; k < XTS_MLP_IN; ++k)
+        if (!(net->in_sd[k] > 0.f) || !std::isfinite(net->in_mu[k]))
+            return set_error(XTS_ERR_ARG, "%s: feature standardisation %d must be finite with sd > 0", who, k);
+    if (!(net->out_sd > 0.f) || !std::isfinite(net->out_mu))
+        return set_error(XTS_ERR_ARG, "%s: target standardisation must be finite with sd > 0", who);
+    return XTS_OK;
+}
+
+static int* mlp_status_word(cudaStream_t st) {
+    int* status = (int*)workspace(W_MISC2, 64);
+    if (status && cudaMemsetAsync(status, 0, sizeof(int), st) != cudaSuccess) return nullptr;
+    return status;
+}
+
+int xts_gemm_bf16(const unsigned short* A, int a_trans, const unsigned short* B, int b_trans, int M, int K,
+                  float* C, int c_trans, int accumulate, void* stream) {
+    XTS_ENTER();
+    if (!A || !B || !C) return set_error(XTS_ERR_ARG, "gemm_bf16: null operand");
+    cudaStream_t st = stream ? (cudaStream_t)stream : g_ctx.stream;
+    int* status = mlp_status_word(st);
+    if (!status) return XTS_ERR_OOM;
+    int rc = launch_gemm_bf16(A, a_trans, B, b_trans, M, K, C, c_trans, accumulate, status, st);
+    if (rc) return rc;
+    return mlp_check_status(status, st);
+}
+
+int xts_mlp_forward(const xts_mlp* net, const float* X, long long n, float* y, void* stream) {
+    XTS_ENTER();
+    int rc = mlp_ok(net, "mlp_forward");
+    if (rc) return rc;
+    if (n < 0 || (n > 0 && (!X || !y))) return set_error(XTS_ERR_ARG, "mlp_forward: null argument or n < 0");
+    cudaStream_t st = stream ? (cudaStream_t)stream : g_ctx.stream;
+    int* status = mlp_status_word(st);
+    if (!status) return XTS_ERR_OOM;
+    if ((rc = launch_mlp_forward(net, X, n, y, status, st))) return rc;
+    return mlp_check_status(status, st);
+}
+
+int xts_mlp_grads(const xts_mlp* net, const float* X, const float* Y, long long n, float* grads, float* loss,
+                  void* stream) {
+    XTS_ENTER();
+    int rc = mlp_ok(net, "mlp_grads");
+    if (rc) return rc;
+    if (!X || !Y || !grads) return set_error(XTS_ERR_ARG, "mlp_grads: null argument");
+    cudaStream_t st = stream ? (cudaStream_t)stream : g_ctx.stream;
+    int* status = mlp_status_word(st);
+    if (!status) return XTS_ERR_OOM;
+    return launch_mlp_grads(net, X, Y, n, grads, loss, status, st);
+}
+
+int xts_mlp_train_step(const xts_mlp* net, const float* X, const float* Y, long long n, float* grads,
+                       float* adam_m, float* adam_v, int step, float lr, float* loss, void* stream) {
+    XTS_ENTER();
+    int rc = mlp_ok(net, "mlp_train_step");
+    if (rc) return rc;
+    if (!X || !Y || !grads || !adam_m || !adam_v) return set_error(XTS_ERR_ARG, "mlp_train_step: null argument");
+    if (!(lr > 0.f) || !std::isfinite(lr)) return set_error(XTS_ERR_ARG, "mlp_train_step: lr must be > 0");
+    cudaStream_t st = stream ? (cudaStream_t)stream : g_ctx.stream;
+    int* status = mlp_status_word(st);
+    if (!status) return XTS_ERR_OOM;
+    if ((rc = launch_mlp_train_step(net, X, Y, n, grads, adam_m, adam_v, step, lr, loss, status, st))) return rc;
+    return mlp_check_status(status, st);
+}
+
+int xts_surrogate_samples(const double* upsf, const double* logEs, int S, int E, long long n,
+                          unsigned long long seed, double rho_min, float* X, float* Y, void* stream) {
+    XTS_ENTER();
+    if (n > 0 && (!upsf || !logEs || !X || !Y)) return set_error(XTS_ERR_ARG, "surrogate_samples: null argument");
+    cudaStream_t st = stream ? (cudaStream_t)stream : g_ctx.stream;
+    int rc = launch_surrogate_samples(upsf, logEs, S, E, n, seed, rho_min, X, Y, st);
+    if (rc) return rc;
+    XTS_CUDA(cudaStreamSynchronize(st));
+    return XTS_OK;
+}
+
+int xts_point_src_model_map_wcs_surrogate(const xts_wcs* wcs, const double* src_sph, int S,
+                                          const double* exposure, const double* upsf,
+                                          const double* partial, const double* logEs, int E,
+                                          const xts_mlp* net, double check_tol, float* model_map,
+                                          xts_srcmap_info* info, xts_surrogate_stats* stats, void* stream) {
+    XTS_ENTER();
+    int rc = mlp_ok(net, "point_src_model_map_wcs_surrogate");
+    if (rc) return rc;
+    if (!wcs || wcs->naxis1 <= 0 || wcs->naxis2 <= 0 || (wcs->proj != 0 && wcs->proj != 1) ||
+        wcs->cdelt1 == 0. || wcs->cdelt2 == 0.)
+        return set_error(XTS_ERR_ARG, "point_src_model_map_wcs_surrogate: bad WCS (CAR/AIT, nonzero CDELT)");
+    if (S < 0 || E <= 0 || E > 256 ||
+        (S > 0 && (!src_sph || !exposure || !upsf || !partial || !logEs || !model_map)))
+        return set_error(XTS_ERR_ARG, "point_src_model_map_wcs_surrogate: null argument or bad size (E <= 256)");
+    if ((long long)wcs->naxis1 * wcs->naxis2 * E > 0xffffffffLL || S > 65535)
+        return set_error(XTS_ERR_ARG, "point_src_model_map_wcs_surrogate: map or source count too large");
+    if (!(check_tol > 0.)) return set_error(XTS_ERR_ARG, "point_src_model_map_wcs_surrogate: check_tol must be > 0");
+    const size_t npix = (size_t)wcs->naxis1 * wcs->naxis2;
+    Stager sg{true, stream ? (cudaStream_t)stream : g_ctx.stream};
+    SrcmapDev a;
+    a.wcs = *wcs;
+    a.src_sph = src_sph; a.S = S;
+    a.exposure = exposure;
+    a.upsf = upsf;
+    a.partial = partial; a.E = E;
+    a.out_f64 = false;
+    a.out = model_map;
+    a.inv_integ = info ? info->inv_map_integral : nullptr;
+    a.correction = info ? info->correction : nullptr;
+    a.radius = info ? info->psf_radius : nullptr;
+    a.in_fov = info ? info->in_fov : nullptr;
+    a.kernel = SRCMAP_WINDOWS;
+    a.surrogate = net;
+    a.logEs = logEs;
+    a.check_tol = check_tol;
+    a.sur_stats = stats;
+    if (stats) memset(stats, 0, sizeof(*stats));
+    return run_srcmap(sg, a, model_map, npix, false);
+}
+
 int xts_point_source_maps(const xts_expcube* cube, const xts_expcube* wcube, const double* logEs,
                           int E, const double* src_sph, int S, const xts_grid* aeff_front,
                           const xts_grid* aeff_back, const xts_grid* psf_front,

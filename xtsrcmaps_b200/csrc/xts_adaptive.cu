@@ -408,8 +408,15 @@ int launch_adaptive_map(const double* corners, const double* centers, const doub
                                              corners, info, tab, lut, H, W, E, (float)rtol, level, max_depth, out,
                                              qin, counts + level - 1, qout, counts + level, (int)cap));
     }
+    (void)centers; (void)omega; (void)nch; (void)sums;  // the c7 sums: launch_mean_integral, by the caller
+    return XTS_OK;
+}
+
+int launch_mean_integral(const double* centers, const double* omega, const SrcInfo* info, const float* mean, int S,
+                         int H, int W, int E, int nch, double* sums, cudaStream_t st) {
+    if (E < 1 || E > AT) return set_error(XTS_ERR_ARG, "map integral of pixel means: E (%d) above %d", E, AT);
     XTS_LAUNCH("k_adaptive_integral", st, k_adaptive_integral<<<dim3(nch, S), AT, 0, st>>>(centers, omega, info,
-                                                                                          out, H, W, E, nch, sums));
+                                                                                          mean, H, W, E, nch, sums));
     return XTS_OK;
 }
 

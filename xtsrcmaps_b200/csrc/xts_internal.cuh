@@ -65,6 +65,7 @@ enum Slot {
     W_CORNERS, W_CENTERS, W_OMEGA, W_LUT, W_PARTSUM, W_SRCINFO, W_SCALE, W_PSFTAB,
     W_KING, W_MISC, W_WIN, W_WMETA, W_SPARSE, W_MISC2, W_EXPMAP,
     W_FITS_IN, W_FITS_OUT, W_FITS_SUM, W_FFT_A, W_FFT_B, W_FFT_C, W_FFT_WORK, W_SRCPIX,
+    W_MLP_Z, W_MLP_H, W_MLP_DZ, W_MLP_DH, W_MLP_Y, W_SUR_X, W_SUR_AUX, W_SUR_Y, W_SUR_ERR,
     N_SLOTS
 };
 void* workspace(int slot, size_t bytes);  // nullptr + error set on OOM
@@ -136,6 +137,11 @@ struct SrcmapDev {
     // join_ev before the first kernel that reads uPsf.
     cudaStream_t geo_stream = nullptr;
     cudaEvent_t join_ev = nullptr;
+    // pixel means from the surrogate network (with the 12-point rule as fallback)
+    const xts_mlp* surrogate = nullptr;
+    const double* logEs = nullptr;  // [E] log10 energies (the network's fourth feature)
+    double check_tol = 1e-4;
+    xts_surrogate_stats* sur_stats = nullptr;
 };
 
 // Two pairs of events for the chunk pipeline of the window path (library-owned).
@@ -186,6 +192,26 @@ int launch_adaptive_map(const double* corners, const double* centers, const doub
                         double* sums, float* out, cudaStream_t st);
 int launch_scale_map(float* out, const double* omega, const double* scale, int S, int npix, int E,
                      cudaStream_t st);
+// c7 sums [S][nch][E] of pixel means [S][H*W][E] times solid angle over the pixels
+// inside each source's boundary radius (E <= 256)
+int launch_mean_integral(const double* centers, const double* omega, const SrcInfo* info, const float* mean, int S,
+                         int H, int W, int E, int nch, double* sums, cudaStream_t st);
+// map of pixel means -> model map: c7 sums, c9 correction, c8/c10 scalings with the solid angle
+int finish_mean_map(const SrcmapDev& a, const double* centers, const double* omega, const SrcInfo* info,
+                    double* scale, int nch, cudaStream_t st);
+// the surrogate network (xts_mlp.cu) and the surrogate model map (xts_surrogate.cu)
+int launch_gemm_bf16(const void* A, int a_trans, const void* B, int b_trans, int M, int K, float* C, int c_trans,
+                     int accumulate, int* status, cudaStream_t st);
+int launch_mlp_forward(const xts_mlp* net, const float* X, long long n, float* y, int* status, cudaStream_t st);
+int launch_mlp_grads(const xts_mlp* net, const float* X, const float* Y, long long n, float* grads, float* loss,
+                     int* status, cudaStream_t st);
+int launch_mlp_train_step(const xts_mlp* net, const float* X, const float* Y, long long n, float* grads,
+                          float* m, float* v, int step, float lr, float* loss, int* status, cudaStream_t st);
+int mlp_check_status(int* status, cudaStream_t st);
+int launch_surrogate_samples(const double* upsf, const double* logEs, int S, int E, long long n,
+                             unsigned long long seed, double rho_min, float* X, float* Y, cudaStream_t st);
+int launch_srcmap_surrogate(const SrcmapDev& a, const double* corners, const double* centers, const double* omega,
+                            const SrcInfo* info, double* scale, int nch, cudaStream_t st);
 int launch_srcmap_win(const double* corners, const double* centers, const double* omega,
                       const SrcInfo* info, int S, int H, int W, int E,
                       const double* upsf, const double* partial, const double* exposure,

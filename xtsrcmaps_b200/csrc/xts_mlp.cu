@@ -1,0 +1,598 @@
+// xts_mlp.cu -- the surrogate network of the pixel cubature: a 5 -> 128 -> 128 ->
+// 128 -> 1 perceptron with tanh-form GELU (Hendrycks & Gimpel, "Gaussian Error
+// Linear Units", 2016: gelu(z) = z/2 (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3)))),
+// its forward pass, its gradient and an Adam update (Kingma & Ba, 2015).
+//
+// The two 128 x 128 layers run on tcgen05 tensor cores: BF16 operands in shared
+// memory (K-major, 128-byte swizzle: a [128 rows][64] BF16 atom is 16 KB, rows
+// of 128 bytes whose 16-byte chunks are permuted by row & 7, 8-row groups 1024
+// bytes apart), one thread issuing tcgen05.mma.kind::f16 (M = N = 128, K = 16)
+// into an FP32 accumulator of 128 tensor-memory columns, the four warps reading
+// it back with tcgen05.ld (warp w owns lanes 32w..32w+31 = rows of the tile).
+//
+//   * k_mlp_forward: one tile of 128 rows per step of a persistent loop.  Layer 1
+//     (K = 5) and the GELUs on CUDA cores; each hidden layer's BF16 activations
+//     are written by their row's thread straight into the swizzled A operand of
+//     the next MMA; the output layer is a per-row dot product.  For training it
+//     also writes the pre-activations z1..z3 and the activations h1, h2,
+//     transposed ([128][n], coalesced across the threads of a warp).
+//   * k_gemm_bf16: C = A B^T for the backward pass (dW = dZ^T H, dH = dZ W), with
+//     either operand given transposed (gathered into the swizzled layout by the
+//     loading threads), a two-stage shared-memory ring and split-K with atomic
+//     FP32 accumulation.
+//   * k_mlp_bwd_elem: dZ = dH * gelu'(Z) per layer in the [unit][row] layout, with
+//     the bias (and output-layer and first-layer weight) gradients reduced per
+//     block and added atomically.
+//   * k_mlp_adam: the update of the FP32 master parameters and the BF16 copies.
+//
+// Every mbarrier wait is bounded (WAIT_LIMIT polls); a timeout sets the status
+// word, stops issuing work, lets issued MMAs complete (bounded) and frees the
+// tensor memory.
+#include <cuda_bf16.h>
+
+#include "xts_point.cuh"
+
+namespace xts {
+
+constexpr int MH = XTS_MLP_HID;  // hidden width == MMA N
+constexpr int MI = XTS_MLP_IN;
+constexpr int MT = 128;          // rows per tile == MMA M == threads per block
+constexpr int ATOM = 16384;      // bytes of a [128][64] BF16 swizzled atom
+
+static_assert(MH == 128 && MT == 128, "the MMA shapes below assume 128 x 128 tiles");
+
+struct MlpNorm {
+    float mu[MI], sd[MI], out_mu, out_sd;
+};
+
+static MlpNorm mlp_norm(const xts_mlp* net) {
+    MlpNorm m;
+    for (int k = 0; k < MI; ++k) { m.mu[k] = net->in_mu[k]; m.sd[k] = net->in_sd[k]; }
+    m.out_mu = net->out_mu;
+    m.out_sd = net->out_sd;
+    return m;
+}
+
+__device__ __forceinline__ float tanh_fast(float x) {
+    float r;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+constexpr float GK0 = 0.7978845608028654f;  // sqrt(2 / pi)
+constexpr float GK1 = 0.044715f;
+__device__ __forceinline__ float gelu(float z) {
+    return 0.5f * z * (1.f + tanh_fast(GK0 * fmaf(GK1 * z * z, z, z)));
+}
+__device__ __forceinline__ float gelu_grad(float z) {
+    const float z2 = z * z, th = tanh_fast(GK0 * fmaf(GK1 * z2, z, z));
+    return 0.5f * (1.f + th) + 0.5f * z * (1.f - th * th) * GK0 * fmaf(3.f * GK1, z2, 1.f);
+}
+
+// byte offset of element (r, k) of a [128][K] BF16 operand made of [128][64] atoms
+__device__ __forceinline__ unsigned sw_off(int r, int k) {
+    return (unsigned)((k >> 6) * ATOM + r * 128 + ((((k & 63) >> 3) ^ (r & 7)) << 4) + (k & 7) * 2);
+}
+
+static __device__ __forceinline__ unsigned long long m_desc(unsigned addr) {
+    // K-major, 128-byte swizzle: start >> 4, LBO 16 >> 4, SBO 1024 >> 4 (8-row groups), version 1
+    return (unsigned long long)((addr >> 4) & 0x3FFF) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
+}
+
+// D f32, A and B bf16, both K-major, M = 128, N = 128.
+constexpr unsigned M_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(MH >> 3) << 17) |
+                             ((unsigned)(MT >> 4) << 24);
+
+// K = 16 * nk of one MMA chain; a, b: shared addresses of the operands (atoms
+// 16 KB apart); acc0: accumulate onto D from the first step.
+__device__ __forceinline__ void mma_chain(unsigned tmem, unsigned a, unsigned b, int nk, bool acc0) {
+    for (int ks = 0; ks < nk; ++ks) {
+        const unsigned off = (unsigned)((ks >> 2) * ATOM + (ks & 3) * 32);
+        const unsigned long long da = m_desc(a + off), db = m_desc(b + off);
+        const unsigned acc = (acc0 || ks > 0) ? 1u : 0u;
+        asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n"
+                     :: "r"(tmem), "l"(da), "l"(db), "r"(M_IDESC), "r"(acc), "r"(0u));
+    }
+}
+
+__device__ __forceinline__ void mma_commit(unsigned bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" :: "r"(bar) : "memory");
+}
+
+// 16 accumulator columns c0..c0+15 of this thread's row
+__device__ __forceinline__ void tmem_ld16(unsigned taddr, float* v) {
+    unsigned r[16];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+__device__ __forceinline__ unsigned pack_bf16(float a, float b) {
+    const __nv_bfloat162 p = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const unsigned*>(&p);
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ unsigned tmem_alloc(unsigned slot_addr, unsigned ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" :: "r"(slot_addr), "r"(ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    return 0;
+}
+__device__ __forceinline__ void tmem_free(unsigned tmem, unsigned ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(ncols));
+}
+
+// ====================================================================== forward
+struct FwdLayout {
+    static constexpr size_t w2 = 0, w3 = 2 * ATOM, act = 4 * ATOM;
+    static constexpr size_t f32 = 6 * ATOM;  // W1 [128][5], b1, b2, b3, w4 [128], b4
+    static constexpr size_t bars = f32 + 4 * (MH * MI + 4 * MH + 4);
+    static constexpr size_t total = bars + 64;
+};
+constexpr size_t FWD_SMEM = FwdLayout::total + 1024;
+
+struct FwdSaves {  // training only; all NULL for inference
+    float* z1; float* z2; float* z3;  // [128][n]
+    __nv_bfloat16* h1; __nv_bfloat16* h2;  // [128][n]
+    float* yn;  // [n] standardised output
+};
+
+__global__ void __launch_bounds__(MT, 1)
+k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict__ wbf, MlpNorm nm,
+              const float* __restrict__ X, long long n, float* __restrict__ y, FwdSaves sv,
+              int* __restrict__ status) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
+    const int t = threadIdx.x, warp = t >> 5;
+    float* w1 = (float*)(smem + FwdLayout::f32);
+    float* b1 = w1 + MH * MI;
+    float* b2 = b1 + MH;
+    float* b3 = b2 + MH;
+    float* w4 = b3 + MH;
+    float* b4 = w4 + MH;
+    unsigned long long* bars = (unsigned long long*)(smem + FwdLayout::bars);
+    unsigned* tmem_slot = (unsigned*)(smem + FwdLayout::bars + 32);
+    int* abort_flag = (int*)(smem + FwdLayout::bars + 48);
+    const unsigned bar = smem_u32(&bars[0]);
+    const unsigned s_w2 = smem_u32(smem + FwdLayout::w2), s_w3 = smem_u32(smem + FwdLayout::w3);
+    const unsigned s_act = smem_u32(smem + FwdLayout::act);
+
+    // weights: W2, W3 [out][in] BF16 -> swizzled B operands (row = out, K = in)
+    for (int idx = t; idx < 2 * MH * (MH / 8); idx += MT) {
+        const int l = idx / (MH * (MH / 8)), rem = idx - l * (MH * (MH / 8));
+        const int r = rem >> 4, ch = rem & 15;
+        const uint4 v = *reinterpret_cast<const uint4*>(wbf + (size_t)l * MH * MH + r * MH + ch * 8);
+        *reinterpret_cast<uint4*>(smem + (l ? FwdLayout::w3 : FwdLayout::w2) + sw_off(r, ch * 8)) = v;
+    }
+    for (int k = t; k < MH * MI; k += MT) w1[k] = __bfloat162float(__float2bfloat16_rn(params[XTS_MLP_W1 + k]));
+    for (int k = t; k < MH; k += MT) {
+        b1[k] = params[XTS_MLP_B1 + k];
+        b2[k] = params[XTS_MLP_B2 + k];
+        b3[k] = params[XTS_MLP_B3 + k];
+        w4[k] = __bfloat162float(__float2bfloat16_rn(params[XTS_MLP_W4 + k]));
+    }
+    if (t == 0) {
+        b4[0] = params[XTS_MLP_B4];
+        mbar_init(bar, 1);
+        *abort_flag = 0;
+    }
+    if (warp == 0) tmem_alloc(smem_u32(tmem_slot), 128);
+    fence_async_shared();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tmem = *tmem_slot;
+    const unsigned trow = tmem + ((unsigned)(warp * 32) << 16);
+    unsigned ph = 0;
+    bool ok = true;
+    const long long ntiles = (n + MT - 1) / MT;
+    for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const long long row = tile * MT + t;
+        const bool live = row < n;
+        float x[MI];
+#pragma unroll
+        for (int k = 0; k < MI; ++k) x[k] = live ? (X[row * MI + k] - nm.mu[k]) / nm.sd[k] : 0.f;
+        // layer 1 on CUDA cores -> A operand of layer 2
+        for (int j0 = 0; j0 < MH; j0 += 8) {
+            float h[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const float* w = w1 + (j0 + j) * MI;
+                float z = b1[j0 + j];
+#pragma unroll
+                for (int k = 0; k < MI; ++k) z = fmaf(w[k], x[k], z);
+                h[j] = gelu(z);
+                if (sv.z1 && live) sv.z1[(size_t)(j0 + j) * n + row] = z;
+            }
+            uint4 pk = make_uint4(pack_bf16(h[0], h[1]), pack_bf16(h[2], h[3]), pack_bf16(h[4], h[5]),
+                                  pack_bf16(h[6], h[7]));
+            if (sv.h1 && live) {
+                const __nv_bfloat16* hb = reinterpret_cast<const __nv_bfloat16*>(&pk);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) sv.h1[(size_t)(j0 + j) * n + row] = hb[j];
+            }
+            *reinterpret_cast<uint4*>(smem + FwdLayout::act + sw_off(t, j0)) = pk;
+        }
+        float yacc = 0.f;
+        for (int layer = 2; layer <= 3 && ok; ++layer) {
+            fence_async_shared();
+            tc_fence_before();
+            __syncthreads();
+            if (t == 0) {
+                tc_fence_after();
+                mma_chain(tmem, s_act, layer == 2 ? s_w2 : s_w3, MH / 16, false);
+                mma_commit(bar);
+            }
+            const bool got = mbar_wait(bar, ph);
+            if (!__syncthreads_and(got)) { ok = false; break; }  // ph stays: the exit path waits on it
+            ph ^= 1;
+            tc_fence_after();
+            const float* bias = layer == 2 ? b2 : b3;
+            float* zs = layer == 2 ? sv.z2 : sv.z3;
+            for (int c0 = 0; c0 < MH; c0 += 16) {
+                float v[16];
+                tmem_ld16(trow + (unsigned)c0, v);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    v[j] += bias[c0 + j];
+                    if (zs && live) zs[(size_t)(c0 + j) * n + row] = v[j];
+                    v[j] = gelu(v[j]);
+                }
+                if (layer == 2) {
+#pragma unroll
+                    for (int hlf = 0; hlf < 2; ++hlf) {
+                        const float* u = v + 8 * hlf;
+                        uint4 pk = make_uint4(pack_bf16(u[0], u[1]), pack_bf16(u[2], u[3]), pack_bf16(u[4], u[5]),
+                                              pack_bf16(u[6], u[7]));
+                        if (sv.h2 && live) {
+                            const __nv_bfloat16* hb = reinterpret_cast<const __nv_bfloat16*>(&pk);
+#pragma unroll
+                            for (int j = 0; j < 8; ++j) sv.h2[(size_t)(c0 + 8 * hlf + j) * n + row] = hb[j];
+                        }
+                        *reinterpret_cast<uint4*>(smem + FwdLayout::act + sw_off(t, c0 + 8 * hlf)) = pk;
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) yacc = fmaf(v[j], w4[c0 + j], yacc);
+                }
+            }
+        }
+        if (!ok) break;
+        const float yn = yacc + b4[0];
+        if (live) {
+            if (sv.yn) sv.yn[row] = yn;
+            if (y) y[row] = fmaf(yn, nm.out_sd, nm.out_mu);
+        }
+        tc_fence_before();  // the next tile's MMA overwrites the accumulator read above
+    }
+    if (!ok && t == 0) {
+        atomicExch(status, 1);
+        mbar_wait(bar, ph);  // bounded: let an issued MMA land
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) tmem_free(tmem, 128);
+}
+
+// ====================================================================== GEMM
+constexpr size_t GEMM_SMEM = 4 * ATOM / 2 * 2 + 64 + 1024;  // two stages of A and B chunks ([128][64] each)
+
+// Stage the [128 rows][64] chunk (rows r0.., K columns k0..) of an operand into
+// one swizzled atom.  trans: the operand is stored [K][ld] (row index fastest).
+__device__ __forceinline__ void load_chunk(unsigned char* dst, const __nv_bfloat16* src, int trans, long long ld,
+                                           long long r0, long long k0, int t) {
+    if (!trans) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int idx = t + MT * i, r = idx >> 3, ch = idx & 7;
+            const uint4 v = *reinterpret_cast<const uint4*>(src + (r0 + r) * ld + k0 + ch * 8);
+            *reinterpret_cast<uint4*>(dst + sw_off(r, ch * 8)) = v;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int idx = t + MT * i, kk = idx >> 4, rg = idx & 15;
+            const uint4 v = *reinterpret_cast<const uint4*>(src + (k0 + kk) * ld + r0 + rg * 8);
+            const unsigned short* e = reinterpret_cast<const unsigned short*>(&v);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) *reinterpret_cast<unsigned short*>(dst + sw_off(rg * 8 + j, kk)) = e[j];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(MT, 1)
+k_gemm_bf16(const __nv_bfloat16* __restrict__ A, int a_trans, const __nv_bfloat16* __restrict__ B, int b_trans,
+            int M, int K, int cps, float* __restrict__ C, int c_trans, int atomic, int* __restrict__ status) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
+    const int t = threadIdx.x, warp = t >> 5;
+    const int nkc = K / 64;
+    const int kc0 = blockIdx.y * cps, kc1 = min(kc0 + cps, nkc);
+    if (kc0 >= kc1) return;  // uniform over the block, before any tensor memory is held
+    const long long m0 = (long long)blockIdx.x * MT;
+    unsigned long long* bars = (unsigned long long*)(smem + 4 * ATOM);
+    unsigned* tmem_slot = (unsigned*)(smem + 4 * ATOM + 32);
+    if (t == 0) {
+        mbar_init(smem_u32(&bars[0]), 1);
+        mbar_init(smem_u32(&bars[1]), 1);
+    }
+    if (warp == 0) tmem_alloc(smem_u32(tmem_slot), 128);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tmem = *tmem_slot;
+    unsigned ph[2] = {0, 0};
+    int pending[2] = {0, 0};
+    bool ok = true;
+    for (int c = kc0; c < kc1; ++c) {
+        const int st = (c - kc0) & 1;
+        unsigned char* sa = smem + st * 2 * ATOM;
+        unsigned char* sb = sa + ATOM;
+        if (pending[st]) {  // the MMAs issued two chunks ago read this stage
+            const bool got = mbar_wait(smem_u32(&bars[st]), ph[st]);
+            if (!__syncthreads_and(got)) { ok = false; break; }  // still pending: the exit path waits
+            ph[st] ^= 1;
+            pending[st] = 0;
+        }
+        load_chunk(sa, A, a_trans, a_trans ? (long long)M : (long long)K, m0, (long long)c * 64, t);
+        load_chunk(sb, B, b_trans, b_trans ? (long long)MH : (long long)K, 0, (long long)c * 64, t);
+        fence_async_shared();
+        tc_fence_before();
+        __syncthreads();
+        if (t == 0) {
+            tc_fence_after();
+            mma_chain(tmem, smem_u32(sa), smem_u32(sb), 4, c > kc0);
+            mma_commit(smem_u32(&bars[st]));
+        }
+        pending[st] = 1;
+    }
+    // the last commit covers every MMA issued before it
+    const int last = (kc1 - 1 - kc0) & 1;
+    if (ok) {
+        const bool got = mbar_wait(smem_u32(&bars[last]), ph[last]);
+        ok = __syncthreads_and(got);
+        if (ok) {
+            ph[last] ^= 1;
+            pending[last] = 0;
+        }
+    }
+    if (ok) {
+        tc_fence_after();
+        const long long m = m0 + t;
+        const unsigned trow = tmem + ((unsigned)(warp * 32) << 16);
+        for (int c0 = 0; c0 < MH; c0 += 16) {
+            float v[16];
+            tmem_ld16(trow + (unsigned)c0, v);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                float* dst = c_trans ? C + (size_t)(c0 + j) * M + m : C + (size_t)m * MH + c0 + j;
+                if (atomic) atomicAdd(dst, v[j]);
+                else *dst = v[j];
+            }
+        }
+    } else if (t == 0) {
+        atomicExch(status, 1);
+        for (int s = 0; s < 2; ++s)
+            if (pending[s]) mbar_wait(smem_u32(&bars[s]), ph[s]);  // bounded
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) tmem_free(tmem, 128);
+}
+
+// ====================================================================== backward
+// Per layer, in the [unit][row] layout: dz = dh * gelu'(z) (head: dh = dy * w4).
+// Block (row range, unit j): bias gradient, and for the head the output-layer
+// weight, for layer 1 the first-layer weights, reduced per block.
+enum { BW_HEAD = 0, BW_HIDDEN = 1, BW_FIRST = 2 };
+constexpr int BW_ROWS = 1024;  // rows per block (256 threads x 4)
+
+__global__ void __launch_bounds__(256) k_mlp_bwd_elem(int mode, const float* __restrict__ params, MlpNorm nm,
+                                                      const float* __restrict__ zT, const float* __restrict__ dhT,
+                                                      const float* __restrict__ yn, const float* __restrict__ Y,
+                                                      const float* __restrict__ X, long long n,
+                                                      __nv_bfloat16* __restrict__ dzT, float* __restrict__ grads,
+                                                      float* __restrict__ loss) {
+    __shared__ float red[8][8];
+    const int j = blockIdx.y, t = threadIdx.x, lane = t & 31, wp = t >> 5;
+    const float w4 = __bfloat162float(__float2bfloat16_rn(params[XTS_MLP_W4 + j]));
+    const float inv_n = 1.f / (float)n;
+    // accumulators: 0 bias, 1 w4 (head) / dy (head, unit 0), 2 loss, 3..7 first-layer weights
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const long long r0 = (long long)blockIdx.x * BW_ROWS;
+    for (int i = 0; i < BW_ROWS / 256; ++i) {
+        const long long r = r0 + t + 256 * i;
+        if (r >= n) break;
+        const size_t k = (size_t)j * n + r;
+        const float z = zT[k];
+        float dh;
+        if (mode == BW_HEAD) {
+            const float tgt = (Y[r] - nm.out_mu) / nm.out_sd;
+            const float d = yn[r] - tgt;
+            const float dy = 2.f * d * inv_n;
+            dh = dy * w4;
+            acc[1] = fmaf(dy, gelu(z), acc[1]);
+            if (j == 0) { acc[2] = fmaf(d, d, acc[2]); acc[3] += dy; }
+        } else {
+            dh = dhT[k];
+        }
+        const float dz = dh * gelu_grad(z);
+        acc[0] += dz;
+        if (mode == BW_FIRST) {
+#pragma unroll
+            for (int q = 0; q < MI; ++q) acc[3 + q] = fmaf(dz, (X[r * MI + q] - nm.mu[q]) / nm.sd[q], acc[3 + q]);
+        } else {
+            dzT[k] = __float2bfloat16_rn(dz);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        float v = acc[q];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) red[wp][q] = v;
+    }
+    __syncthreads();
+    if (t < 8) {
+        float v = 0.f;
+        for (int w = 0; w < 8; ++w) v += red[w][t];
+        const int q = t;
+        if (mode == BW_HEAD) {
+            if (q == 0) atomicAdd(grads + XTS_MLP_B3 + j, v);
+            if (q == 1) atomicAdd(grads + XTS_MLP_W4 + j, v);
+            if (j == 0 && q == 2 && loss) atomicAdd(loss, v * inv_n);
+            if (j == 0 && q == 3) atomicAdd(grads + XTS_MLP_B4, v);
+        } else if (mode == BW_HIDDEN) {
+            if (q == 0) atomicAdd(grads + XTS_MLP_B2 + j, v);
+        } else {
+            if (q == 0) atomicAdd(grads + XTS_MLP_B1 + j, v);
+            if (q >= 3) atomicAdd(grads + XTS_MLP_W1 + j * MI + (q - 3), v);
+        }
+    }
+}
+
+// Adam on the FP32 master parameters; the BF16 copies of W2 and W3 follow.
+__global__ void k_mlp_adam(float* __restrict__ p, float* __restrict__ g, float* __restrict__ m,
+                           float* __restrict__ v, __nv_bfloat16* __restrict__ wbf, float lr, float c1, float c2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= XTS_MLP_NPARAM) return;
+    const float gi = g[i];
+    const float mi = fmaf(0.9f, m[i], 0.1f * gi);
+    const float vi = fmaf(0.999f, v[i], 0.001f * gi * gi);
+    m[i] = mi;
+    v[i] = vi;
+    g[i] = 0.f;
+    const float pi = p[i] - lr * (mi * c1) / (sqrtf(vi * c2) + 1e-8f);
+    p[i] = pi;
+    if (i >= XTS_MLP_W2 && i < XTS_MLP_B2) wbf[i - XTS_MLP_W2] = __float2bfloat16_rn(pi);
+    if (i >= XTS_MLP_W3 && i < XTS_MLP_B3) wbf[MH * MH + (i - XTS_MLP_W3)] = __float2bfloat16_rn(pi);
+}
+
+// ====================================================================== launchers
+static int sm_count() {
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    return nsm;
+}
+
+static int mlp_status(int* status, cudaStream_t st) {
+    int v = 0;
+    XTS_CUDA(cudaMemcpyAsync(&v, status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    XTS_CUDA(cudaStreamSynchronize(st));
+    if (v) {
+        cudaMemsetAsync(status, 0, sizeof(int), st);
+        return set_error(XTS_ERR_TIMEOUT, "a bounded tensor-core wait gave up (surrogate network)");
+    }
+    return XTS_OK;
+}
+
+int launch_gemm_bf16(const void* A, int a_trans, const void* B, int b_trans, int M, int K, float* C, int c_trans,
+                     int accumulate, int* status, cudaStream_t st) {
+    if (M <= 0 || K <= 0 || M % MT || K % 64)
+        return set_error(XTS_ERR_ARG, "gemm_bf16: M (%d) must be a multiple of 128 and K (%d) of 64", M, K);
+    static bool attr = false;
+    if (!attr) {
+        XTS_CUDA(cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM));
+        attr = true;
+    }
+    const int mt = M / MT, nkc = K / 64;
+    int nsplit = 1;
+    if (accumulate) {  // spread the K chunks over about one wave of blocks
+        nsplit = (sm_count() + mt - 1) / mt;
+        nsplit = nsplit < 1 ? 1 : (nsplit > nkc ? nkc : nsplit);
+    }
+    const int cps = (nkc + nsplit - 1) / nsplit;
+    nsplit = (nkc + cps - 1) / cps;
+    if (!accumulate && nsplit != 1) return set_error(XTS_ERR_ARG, "gemm_bf16: internal split");
+    XTS_LAUNCH("k_gemm_bf16", st, k_gemm_bf16<<<dim3(mt, nsplit), MT, GEMM_SMEM, st>>>(
+                                      (const __nv_bfloat16*)A, a_trans, (const __nv_bfloat16*)B, b_trans, M, K, cps,
+                                      C, c_trans, accumulate, status));
+    return XTS_OK;
+}
+
+static int forward(const xts_mlp* net, const float* X, long long n, float* y, FwdSaves sv, int* status,
+                   cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+        XTS_CUDA(cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM));
+        attr = true;
+    }
+    const long long ntiles = (n + MT - 1) / MT;
+    const long long g = ntiles < sm_count() ? ntiles : sm_count();
+    XTS_LAUNCH("k_mlp_forward", st, k_mlp_forward<<<(unsigned)g, MT, FWD_SMEM, st>>>(
+                                        net->params, (const __nv_bfloat16*)net->wbf16, mlp_norm(net), X, n, y, sv,
+                                        status));
+    return XTS_OK;
+}
+
+int launch_mlp_forward(const xts_mlp* net, const float* X, long long n, float* y, int* status, cudaStream_t st) {
+    if (n <= 0) return XTS_OK;
+    return forward(net, X, n, y, FwdSaves{}, status, st);
+}
+
+// forward with saves, then the gradient accumulated into grads (zero on entry)
+static int mlp_backprop(const xts_mlp* net, const float* X, const float* Y, long long n, float* grads,
+                        float* loss, int* status, cudaStream_t st) {
+    if (n <= 0 || n % MT) return set_error(XTS_ERR_ARG, "surrogate training: n (%lld) must be a positive multiple of 128", n);
+    if (n > (1ll << 24)) return set_error(XTS_ERR_ARG, "surrogate training: n (%lld) above 2^24 rows per batch", n);
+    const size_t hn = (size_t)MH * n;
+    float* z = (float*)workspace(W_MLP_Z, sizeof(float) * 3 * hn);
+    __nv_bfloat16* h = (__nv_bfloat16*)workspace(W_MLP_H, sizeof(__nv_bfloat16) * 2 * hn);
+    __nv_bfloat16* dz = (__nv_bfloat16*)workspace(W_MLP_DZ, sizeof(__nv_bfloat16) * hn);
+    float* dh = (float*)workspace(W_MLP_DH, sizeof(float) * hn);
+    float* yn = (float*)workspace(W_MLP_Y, sizeof(float) * n);
+    if (!z || !h || !dz || !dh || !yn) return XTS_ERR_OOM;
+    FwdSaves sv{z, z + hn, z + 2 * hn, h, h + hn, yn};
+    int rc = forward(net, X, n, nullptr, sv, status, st);
+    if (rc) return rc;
+    const MlpNorm nm = mlp_norm(net);
+    const dim3 eg((unsigned)((n + BW_ROWS - 1) / BW_ROWS), MH);
+    const __nv_bfloat16* w2 = (const __nv_bfloat16*)net->wbf16;
+    const __nv_bfloat16* w3 = w2 + MH * MH;
+    // head: dz3 = dy w4 gelu'(z3); dW3 = dz3^T h2; dh2 = dz3 W3
+    XTS_LAUNCH("k_mlp_bwd", st, k_mlp_bwd_elem<<<eg, 256, 0, st>>>(BW_HEAD, net->params, nm, sv.z3, nullptr, yn, Y,
+                                                                     X, n, dz, grads, loss));
+    if ((rc = launch_gemm_bf16(dz, 0, sv.h2, 0, MH, (int)n, grads + XTS_MLP_W3, 0, 1, status, st))) return rc;
+    if ((rc = launch_gemm_bf16(dz, 1, w3, 1, (int)n, MH, dh, 1, 0, status, st))) return rc;
+    // layer 2: dz2 = dh2 gelu'(z2); dW2 = dz2^T h1; dh1 = dz2 W2
+    XTS_LAUNCH("k_mlp_bwd", st, k_mlp_bwd_elem<<<eg, 256, 0, st>>>(BW_HIDDEN, net->params, nm, sv.z2, dh, yn, Y, X,
+                                                                     n, dz, grads, loss));
+    if ((rc = launch_gemm_bf16(dz, 0, sv.h1, 0, MH, (int)n, grads + XTS_MLP_W2, 0, 1, status, st))) return rc;
+    if ((rc = launch_gemm_bf16(dz, 1, w2, 1, (int)n, MH, dh, 1, 0, status, st))) return rc;
+    // layer 1: dz1 = dh1 gelu'(z1); dW1 = dz1^T x
+    XTS_LAUNCH("k_mlp_bwd", st, k_mlp_bwd_elem<<<eg, 256, 0, st>>>(BW_FIRST, net->params, nm, sv.z1, dh, yn, Y, X,
+                                                                     n, dz, grads, loss));
+    return XTS_OK;
+}
+
+int launch_mlp_grads(const xts_mlp* net, const float* X, const float* Y, long long n, float* grads, float* loss,
+                     int* status, cudaStream_t st) {
+    XTS_CUDA(cudaMemsetAsync(grads, 0, sizeof(float) * XTS_MLP_NPARAM, st));
+    if (loss) XTS_CUDA(cudaMemsetAsync(loss, 0, sizeof(float), st));
+    int rc = mlp_backprop(net, X, Y, n, grads, loss, status, st);
+    if (rc) return rc;
+    return mlp_status(status, st);
+}
+
+int launch_mlp_train_step(const xts_mlp* net, const float* X, const float* Y, long long n, float* grads,
+                          float* m, float* v, int step, float lr, float* loss, int* status, cudaStream_t st) {
+    if (step < 1) return set_error(XTS_ERR_ARG, "surrogate training: step must be >= 1");
+    int rc = mlp_backprop(net, X, Y, n, grads, loss, status, st);
+    if (rc) return rc;
+    const float c1 = (float)(1.0 / (1.0 - pow(0.9, step))), c2 = (float)(1.0 / (1.0 - pow(0.999, step)));
+    XTS_LAUNCH("k_mlp_adam", st, k_mlp_adam<<<(XTS_MLP_NPARAM + 255) / 256, 256, 0, st>>>(
+                                     net->params, grads, m, v, (__nv_bfloat16*)net->wbf16, lr, c1, c2));
+    return XTS_OK;
+}
+
+int mlp_check_status(int* status, cudaStream_t st) { return mlp_status(status, st); }
+
+}  // namespace xts

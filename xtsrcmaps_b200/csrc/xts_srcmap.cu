@@ -478,10 +478,23 @@ static int launch_srcmap_adaptive(const SrcmapDev& a, const double* corners, con
     int rc = launch_adaptive_map(corners, centers, omega, info, a.upsf, S, H, W, E, a.rtol, a.max_depth, nch,
                                  sums, (float*)a.out, st);
     if (rc) return rc;
+    return finish_mean_map(a, centers, omega, info, scale, nch, st);
+}
+
+// A map of pixel means [S][H*W][E] (a.out, FP32) -> the model map: the map
+// integral sums over the pixels inside the boundary radius, the correction, and
+// value = mean * solid angle * exposure * correction.
+int finish_mean_map(const SrcmapDev& a, const double* centers, const double* omega, const SrcInfo* info,
+                    double* scale, int nch, cudaStream_t st) {
+    const int H = (int)a.wcs.naxis1, W = (int)a.wcs.naxis2, S = a.S, E = a.E;
+    double* sums = (double*)workspace(W_PARTSUM, sizeof(double) * (size_t)S * nch * E + 8);
+    if (!sums) return XTS_ERR_OOM;
+    int rc = launch_mean_integral(centers, omega, info, (const float*)a.out, S, H, W, E, nch, sums, st);
+    if (rc) return rc;
     XTS_LAUNCH("k_correction", st, k_correction_sums<<<S, 128, 0, st>>>(sums, nch, info, a.upsf, a.partial,
                                                                         a.exposure, E, scale, a.inv_integ,
                                                                         a.correction, a.radius, a.in_fov));
-    return launch_scale_map((float*)a.out, omega, scale, S, npix, E, st);
+    return launch_scale_map((float*)a.out, omega, scale, S, H * W, E, st);
 }
 
 int srcmap_status(cudaStream_t st) {
@@ -527,6 +540,12 @@ int launch_srcmap(const SrcmapDev& a, cudaStream_t st) {
     XTS_LAUNCH("k_map_geometry", gs, k_map_geometry<<<gg, GEO_THREADS, 0, gs>>>(w, H, W, corners, centers, omega));
     if (S == 0) return XTS_OK;
     XTS_LAUNCH("k_boundary", gs, k_boundary_chord<<<S, 256, 0, gs>>>(w, a.src_sph, H, W, corners, info));
+    if (a.surrogate) {
+        if ((rc = geo.join())) return rc;
+        if (a.out_f64 || !srcmap_adaptive_supported(E))
+            return set_error(XTS_ERR_ARG, "surrogate map: FP32 maps with E <= 256 only");
+        return launch_srcmap_surrogate(a, corners, centers, omega, info, scale, nch, st);
+    }
     if (a.adaptive) {
         if ((rc = geo.join())) return rc;
         if (a.out_f64 || !srcmap_adaptive_supported(E))

@@ -1,0 +1,341 @@
+// xts_surrogate.cu -- the surrogate model map: pixel means of the mean PSF from
+// the network of xts_mlp.cu, with the 12-point rule of the plain path as the
+// fallback and as the check; and the training samples the network learns from.
+//
+// For a source and a pixel in bilinear form p(u, v) = src + A + B u + C v + D uv
+// (the corners' unit vectors blended as square_ptswts, points_weights.hpp:5-56):
+//   * centre separation theta_c = 2 asin(|A| / 2), cell solid angle 4 |B x C|,
+//     size delta = sqrt(solid angle), rho = theta_c / delta;
+//   * the centre's offset t_c in the separation table: its logsep interpolation
+//     weight between the bracketing rows (the mean PSF is the piecewise-linear
+//     interpolant of 401 rows, whose curvature error, up to ~4e-3 of u between
+//     rows, depends on where the pixel falls between them);
+//   * per energy: u_c = the mean PSF at theta_c, the log slope
+//     ln(U[i] / U[i-1]) / step of the table segment holding theta_c, and the
+//     rule mean m = sum_p w_p u(theta_p) over the 12 points (the plain path's
+//     cubature, cubature.implementation.cxx:21-55, with the logsep row and weight
+//     of convolve_pixel_psf_logsep.hpp:39-55, keys fixed).
+// The network's target is y = ln(m / u_c) rho^2; a value is m = u_c exp(y / rho^2).
+// All of this is FP64 up to the network's FP32 input.
+#include <vector>
+
+#include "xts_point.cuh"
+
+namespace xts {
+
+constexpr int SUR_CHECK_EVERY = 61;         // every 61st pixel's values are also taken by the rule
+constexpr long long SUR_CHUNK_VALUES = 1ll << 26;  // values per pass of the network (sources chunked)
+
+__device__ __forceinline__ int sur_row(double sdeg, double* t) {
+    const double j = sdeg < 1e-4 ? 1. : 1. + RECIPSTEP * (LN_1E4 + log(sdeg));
+    int idx = 1 + (int)j;
+    idx = idx > 400 ? 400 : (idx < 2 ? 2 : idx);
+    *t = REDM1 * (sdeg * 1e4 * exp(SEP_STEP * (2. - idx)) - 1.);
+    return idx;
+}
+
+__device__ __forceinline__ double sur_lerp(const double* U, int E, int e, int idx, double t) {
+    return (1.0 - t) * U[(size_t)(idx - 1) * E + e] + t * U[(size_t)idx * E + e];
+}
+
+struct SurPix {
+    int idx[12];
+    double tt[12];
+    int ic;
+    double tc;
+    float f0, f1, f2;
+    double rho;
+};
+
+__device__ __forceinline__ void sur_pixel(const PixGeom& g, SurPix& sp) {
+    const PixQ c = pixel_q(g);
+#pragma unroll
+    for (int p = 0; p < 12; ++p) sp.idx[p] = sur_row(2.0 * R2D * asin(0.5 * sqrt(point_q2(c, p))), &sp.tt[p]);
+    const double alen = sqrt(c.a0);
+    const double thc = 2.0 * asin(0.5 * alen);  // radians
+    const double cx = g.By * g.Cz - g.Bz * g.Cy, cy = g.Bz * g.Cx - g.Bx * g.Cz, cz = g.Bx * g.Cy - g.By * g.Cx;
+    const double om = 4.0 * sqrt(cx * cx + cy * cy + cz * cz);
+    const double delta = sqrt(om);
+    sp.rho = thc / delta;
+    sp.ic = sur_row(R2D * thc, &sp.tc);
+    sp.f0 = (float)log10(sp.rho);
+    sp.f1 = (float)sp.tc;
+    sp.f2 = (float)log10(om * R2D * R2D);
+}
+
+__device__ __forceinline__ double sur_rule(const SurPix& sp, const double* U, int E, int e) {
+    double m = 0.;
+#pragma unroll
+    for (int p = 0; p < 12; ++p) m += c_rule_uv[p][3] * sur_lerp(U, E, e, sp.idx[p], sp.tt[p]);
+    return m;
+}
+
+// centre value and the log slope of its table segment at energy e
+__device__ __forceinline__ double sur_centre(const SurPix& sp, const double* U, int E, int e, double* slope) {
+    const double lo = U[(size_t)(sp.ic - 1) * E + e], hi = U[(size_t)sp.ic * E + e];
+    *slope = (lo > 0. && hi > 0.) ? log(hi / lo) * (1.0 / SEP_STEP) : 0.;
+    return (1.0 - sp.tc) * lo + sp.tc * hi;
+}
+
+// ------------------------------------------------------------------ samples
+__device__ __forceinline__ unsigned long long splitmix(unsigned long long& s) {
+    unsigned long long z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+__device__ __forceinline__ double uni(unsigned long long& s) { return (double)(splitmix(s) >> 11) * 0x1.0p-53; }
+
+__global__ void k_sur_samples(const double* __restrict__ upsf, const double* __restrict__ logEs, int S, int E,
+                              long long n, unsigned long long seed, double rho_min, float* __restrict__ X,
+                              float* __restrict__ Y) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    unsigned long long st = seed ^ ((unsigned long long)i * 0xD1B54A32D192ED03ull);
+    splitmix(st);
+    const int s = min((int)(uni(st) * S), S - 1);
+    const int e = min((int)(uni(st) * E), E - 1);
+    const double size = 0.025 + 0.175 * uni(st);             // degrees
+    const double asp = exp(log(1.25) * (2.0 * uni(st) - 1.0));
+    const double lo = fmax(0.001, rho_min * size);
+    const double th = lo * exp(uni(st) * log(30.0 / lo)) * D2R;
+    const double al = uni(st) * HALFPI;
+    const double ha = 0.5 * size * sqrt(asp) * D2R, hb = 0.5 * size / sqrt(asp) * D2R;
+    // source at the pole; the pixel centre at polar angle th, axes rotated by al
+    const double c[3] = {sin(th), 0.0, cos(th)};
+    const double e1[3] = {cos(th), 0.0, -sin(th)}, e2[3] = {0.0, 1.0, 0.0};
+    const double ca = cos(al), sa = sin(al);
+    double U[3], V[3], k[4][3];
+    for (int q = 0; q < 3; ++q) { U[q] = ca * e1[q] + sa * e2[q]; V[q] = -sa * e1[q] + ca * e2[q]; }
+    const double su[4] = {-1, 1, 1, -1}, sv[4] = {-1, -1, 1, 1};  // LL, LR, UR, UL
+    for (int j = 0; j < 4; ++j) {
+        double nn = 0.;
+        for (int q = 0; q < 3; ++q) {
+            k[j][q] = c[q] + su[j] * ha * U[q] + sv[j] * hb * V[q];
+            nn += k[j][q] * k[j][q];
+        }
+        nn = 1.0 / sqrt(nn);
+        for (int q = 0; q < 3; ++q) k[j][q] *= nn;
+    }
+    const double src[3] = {0.0, 0.0, 1.0};
+    PixGeom g;
+    const double *a = k[0], *b = k[1], *cc = k[2], *d = k[3];
+    g.Ax = 0.25 * ((a[0] + b[0]) + (cc[0] + d[0])) - src[0];
+    g.Ay = 0.25 * ((a[1] + b[1]) + (cc[1] + d[1])) - src[1];
+    g.Az = 0.25 * ((a[2] + b[2]) + (cc[2] + d[2])) - src[2];
+    g.Bx = 0.25 * ((b[0] + cc[0]) - (a[0] + d[0]));
+    g.By = 0.25 * ((b[1] + cc[1]) - (a[1] + d[1]));
+    g.Bz = 0.25 * ((b[2] + cc[2]) - (a[2] + d[2]));
+    g.Cx = 0.25 * ((cc[0] + d[0]) - (a[0] + b[0]));
+    g.Cy = 0.25 * ((cc[1] + d[1]) - (a[1] + b[1]));
+    g.Cz = 0.25 * ((cc[2] + d[2]) - (a[2] + b[2]));
+    g.Dx = 0.25 * ((a[0] + cc[0]) - (b[0] + d[0]));
+    g.Dy = 0.25 * ((a[1] + cc[1]) - (b[1] + d[1]));
+    g.Dz = 0.25 * ((a[2] + cc[2]) - (b[2] + d[2]));
+    SurPix sp;
+    sur_pixel(g, sp);
+    const double* Us = upsf + (size_t)s * ND * E;
+    double slope;
+    const double uc = sur_centre(sp, Us, E, e, &slope);
+    const double m = sur_rule(sp, Us, E, e);
+    X[i * 5 + 0] = sp.f0;
+    X[i * 5 + 1] = sp.f1;
+    X[i * 5 + 2] = sp.f2;
+    X[i * 5 + 3] = (float)logEs[e];
+    X[i * 5 + 4] = (float)slope;
+    Y[i] = (float)(log(m / uc) * sp.rho * sp.rho);
+}
+
+int launch_surrogate_samples(const double* upsf, const double* logEs, int S, int E, long long n,
+                             unsigned long long seed, double rho_min, float* X, float* Y, cudaStream_t st) {
+    if (S < 1 || E < 1 || n < 0 || !(rho_min >= 0.))
+        return set_error(XTS_ERR_ARG, "surrogate samples: S %d, E %d, n %lld, rho_min %g", S, E, n, rho_min);
+    if (n == 0) return XTS_OK;
+    int rc = upload_rule_uv(st);
+    if (rc) return rc;
+    XTS_LAUNCH("k_sur_samples", st, k_sur_samples<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(
+                                        upsf, logEs, S, E, n, seed, rho_min, X, Y));
+    return XTS_OK;
+}
+
+// ------------------------------------------------------------------ model map
+struct SurRange { float lo[5], hi[5], rho_min; };
+
+// Per (source, pixel) of a chunk of sources: features of every energy, or the
+// rule's mean where the value is not the network's.  aux = (u_c, 1 / rho^2), or
+// (0, -1) for a value taken by the rule.
+__global__ void __launch_bounds__(128) k_sur_features(const double* __restrict__ corners, const SrcInfo* __restrict__ info,
+                                                      const double* __restrict__ upsf, const double* __restrict__ logEs,
+                                                      int s0, int H, int W, int E, SurRange rg, float* __restrict__ X,
+                                                      float2* __restrict__ aux, float* __restrict__ mean,
+                                                      unsigned long long* __restrict__ accepted) {
+    const int s = s0 + blockIdx.y, pix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int npix = H * W;
+    unsigned acc = 0;
+    if (pix < npix) {
+        const int h = pix / W, w = pix - h * W;
+        SurPix sp;
+        sur_pixel(pixel_geom(corners, W + 1, h, w, info[s]), sp);
+        const double* U = upsf + (size_t)s * ND * E;
+        const bool geo_ok = sp.rho >= rg.rho_min && sp.f0 >= rg.lo[0] && sp.f0 <= rg.hi[0] && sp.f1 >= rg.lo[1] &&
+                            sp.f1 <= rg.hi[1] && sp.f2 >= rg.lo[2] && sp.f2 <= rg.hi[2];
+        const float eps = (float)(1.0 / (sp.rho * sp.rho));
+        const size_t v0 = ((size_t)blockIdx.y * npix + pix) * E;
+        for (int e = 0; e < E; ++e) {
+            double slope;
+            const double uc = sur_centre(sp, U, E, e, &slope);
+            const float le = (float)logEs[e], sl = (float)slope;
+            const bool ok = geo_ok && uc > 0. && le >= rg.lo[3] && le <= rg.hi[3] && sl >= rg.lo[4] && sl <= rg.hi[4];
+            const size_t v = v0 + e;
+            float* x = X + v * 5;
+            x[0] = sp.f0; x[1] = sp.f1; x[2] = sp.f2; x[3] = le; x[4] = sl;
+            if (ok) {
+                aux[v] = make_float2((float)uc, eps);
+                ++acc;
+            } else {
+                aux[v] = make_float2(0.f, -1.f);
+                mean[((size_t)s * npix + pix) * E + e] = (float)sur_rule(sp, U, E, e);
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0 && acc) atomicAdd(accepted + s, (unsigned long long)acc);
+}
+
+__global__ void k_sur_assemble(const float2* __restrict__ aux, const float* __restrict__ y, long long n,
+                               float* __restrict__ mean) {
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const float2 a = aux[v];
+    if (a.y >= 0.f) mean[v] = a.x * expf(y[v] * a.y);
+}
+
+// The check: every SUR_CHECK_EVERY-th pixel of the chunk, all energies taken by
+// the network, against the rule; the largest relative difference per source.
+__global__ void __launch_bounds__(128) k_sur_check(const double* __restrict__ corners, const SrcInfo* __restrict__ info,
+                                                   const double* __restrict__ upsf, int s0, int H, int W, int E,
+                                                   const float2* __restrict__ aux, const float* __restrict__ mean,
+                                                   float* __restrict__ err, unsigned long long* __restrict__ counts) {
+    const int s = s0 + blockIdx.y, npix = H * W;
+    const int pix = (blockIdx.x * blockDim.x + threadIdx.x) * SUR_CHECK_EVERY;
+    float worst = 0.f;
+    unsigned nchk = 0;
+    if (pix < npix) {
+        const int h = pix / W, w = pix - h * W;
+        SurPix sp;
+        sur_pixel(pixel_geom(corners, W + 1, h, w, info[s]), sp);
+        const double* U = upsf + (size_t)s * ND * E;
+        const size_t v0 = ((size_t)blockIdx.y * npix + pix) * E;
+        for (int e = 0; e < E; ++e) {
+            if (aux[v0 + e].y < 0.f) continue;
+            const double m = sur_rule(sp, U, E, e);
+            const double got = mean[((size_t)s * npix + pix) * E + e];
+            const float r = (float)(m != 0. ? fabs(got - m) / fabs(m) : fabs(got));
+            worst = fmaxf(worst, r != r ? 3.4e38f : r);
+            ++nchk;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        worst = fmaxf(worst, __shfl_xor_sync(0xffffffffu, worst, o));
+        nchk += __shfl_xor_sync(0xffffffffu, nchk, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (worst > 0.f) atomicMax((int*)(err + s), __float_as_int(worst));  // non-negative floats order as ints
+        if (nchk) atomicAdd(counts, (unsigned long long)nchk);
+    }
+}
+
+// Every value of the listed sources by the rule.
+__global__ void __launch_bounds__(128) k_sur_fallback(const double* __restrict__ corners, const SrcInfo* __restrict__ info,
+                                                      const double* __restrict__ upsf, const int* __restrict__ list,
+                                                      int H, int W, int E, float* __restrict__ mean) {
+    const int s = list[blockIdx.y], npix = H * W;
+    const int pix = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pix >= npix) return;
+    const int h = pix / W, w = pix - h * W;
+    SurPix sp;
+    sur_pixel(pixel_geom(corners, W + 1, h, w, info[s]), sp);
+    const double* U = upsf + (size_t)s * ND * E;
+    for (int e = 0; e < E; ++e) mean[((size_t)s * npix + pix) * E + e] = (float)sur_rule(sp, U, E, e);
+}
+
+int launch_srcmap_surrogate(const SrcmapDev& a, const double* corners, const double* centers, const double* omega,
+                            const SrcInfo* info, double* scale, int nch, cudaStream_t st) {
+    const xts_mlp* net = a.surrogate;
+    const int H = (int)a.wcs.naxis1, W = (int)a.wcs.naxis2, S = a.S, E = a.E;
+    const long long npix = (long long)H * W;
+    if (!net->params || !net->wbf16) return set_error(XTS_ERR_ARG, "surrogate map: network parameters missing");
+    for (int k = 0; k < XTS_MLP_IN; ++k)
+        if (!(net->in_sd[k] > 0.f)) return set_error(XTS_ERR_ARG, "surrogate map: in_sd[%d] must be > 0", k);
+    if (!(net->out_sd > 0.f)) return set_error(XTS_ERR_ARG, "surrogate map: out_sd must be > 0");
+    int rc = upload_rule_uv(st);
+    if (rc) return rc;
+    const long long per_src = npix * E;
+    int sc = (int)(SUR_CHUNK_VALUES / (per_src > 0 ? per_src : 1));
+    sc = sc < 1 ? 1 : (sc > S ? S : sc);
+    const long long nmax = per_src * sc;
+    float* X = (float*)workspace(W_SUR_X, sizeof(float) * 5 * (size_t)nmax + 16);
+    float2* aux = (float2*)workspace(W_SUR_AUX, sizeof(float2) * (size_t)nmax + 16);
+    float* yv = (float*)workspace(W_SUR_Y, sizeof(float) * (size_t)nmax + 16);
+    // per source: largest check difference, values accepted; then the checked count,
+    // the status word, and the list of sources redone by the rule
+    const size_t o_cnt = align_up(sizeof(float) * S, 16), o_ctr = o_cnt + align_up(8 * (size_t)S, 16);
+    const size_t o_list = o_ctr + 64;
+    char* misc = (char*)workspace(W_SUR_ERR, o_list + sizeof(int) * (size_t)S + 16);
+    if (!X || !aux || !yv || !misc) return XTS_ERR_OOM;
+    float* err = (float*)misc;
+    unsigned long long* acc_d = (unsigned long long*)(misc + o_cnt);
+    unsigned long long* counts = (unsigned long long*)(misc + o_ctr);
+    int* status = (int*)(counts + 4);
+    int* list_d = (int*)(misc + o_list);
+    XTS_CUDA(cudaMemsetAsync(misc, 0, o_list, st));
+    SurRange rg;
+    for (int k = 0; k < 5; ++k) { rg.lo[k] = net->lo[k]; rg.hi[k] = net->hi[k]; }
+    rg.rho_min = net->rho_min;
+    float* mean = (float*)a.out;
+    for (int s0 = 0; s0 < S; s0 += sc) {
+        const int ns = S - s0 < sc ? S - s0 : sc;
+        const long long n = per_src * ns;
+        const dim3 gf((unsigned)((npix + 127) / 128), (unsigned)ns);
+        XTS_LAUNCH("k_sur_features", st, k_sur_features<<<gf, 128, 0, st>>>(corners, info, a.upsf, a.logEs, s0, H, W, E, rg,
+                                                                            X, aux, mean, acc_d));
+        if ((rc = launch_mlp_forward(net, X, n, yv, status, st))) return rc;
+        float* m0 = mean + (size_t)s0 * per_src;
+        XTS_LAUNCH("k_sur_assemble", st, k_sur_assemble<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(aux, yv, n, m0));
+        const long long nck = (npix + SUR_CHECK_EVERY - 1) / SUR_CHECK_EVERY;
+        const dim3 gc((unsigned)((nck + 127) / 128), (unsigned)ns);
+        XTS_LAUNCH("k_sur_check", st, k_sur_check<<<gc, 128, 0, st>>>(corners, info, a.upsf, s0, H, W, E, aux, mean,
+                                                                      err, counts));
+    }
+    if ((rc = mlp_check_status(status, st))) return rc;
+    std::vector<float> herr(S > 0 ? S : 1);
+    std::vector<unsigned long long> hacc(S > 0 ? S : 1);
+    unsigned long long hc = 0;
+    XTS_CUDA(cudaMemcpyAsync(herr.data(), err, sizeof(float) * S, cudaMemcpyDeviceToHost, st));
+    XTS_CUDA(cudaMemcpyAsync(hacc.data(), acc_d, sizeof(unsigned long long) * S, cudaMemcpyDeviceToHost, st));
+    XTS_CUDA(cudaMemcpyAsync(&hc, counts, sizeof(hc), cudaMemcpyDeviceToHost, st));
+    XTS_CUDA(cudaStreamSynchronize(st));
+    std::vector<int> list;
+    float worst = 0.f;
+    long long accepted = 0;
+    for (int s = 0; s < S; ++s) {
+        worst = herr[s] > worst ? herr[s] : worst;
+        if (!(herr[s] <= (float)a.check_tol)) list.push_back(s);
+        else accepted += (long long)hacc[s];
+    }
+    if (!list.empty()) {
+        XTS_CUDA(cudaMemcpyAsync(list_d, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, st));
+        const dim3 gb((unsigned)((npix + 127) / 128), (unsigned)list.size());
+        XTS_LAUNCH("k_sur_fallback", st, k_sur_fallback<<<gb, 128, 0, st>>>(corners, info, a.upsf, list_d, H, W, E, mean));
+    }
+    if (a.sur_stats) {
+        a.sur_stats->values = (long long)S * per_src;
+        a.sur_stats->accepted = accepted;  // the redone maps' values are the rule's
+        a.sur_stats->checked = (long long)hc;
+        a.sur_stats->maps_fallback = (int)list.size();
+        a.sur_stats->max_check_err = worst;
+    }
+    return finish_mean_map(a, centers, omega, info, scale, nch, st);
+}
+
+}  // namespace xts
