@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="time eager launches instead of a CUDA graph")
     ap.add_argument("--no-adaptive", action="store_true", help="skip the adaptive-cubature measurement")
+    ap.add_argument("--no-surrogate", action="store_true", help="skip training and timing the learned surrogate")
+    ap.add_argument("--surrogate-samples", type=int, default=10_000_000)
+    ap.add_argument("--surrogate-epochs", type=int, default=20)
     ap.add_argument("--exposure-map-nside", type=int, default=0,
                     help="time only the full-sky exposure map at this nside and exit")
     ap.add_argument("--kernel", default="windows", choices=["windows", "cuda_cores", "tcgen05"],
@@ -317,6 +320,9 @@ def run_ours(args, rank, world, local_rank):
                     "rtol": 1e-4, "max_depth": 6,
                     "note": "point_src_model_map_wcs_adaptive (Genz-Malik 7/5 per pixel) in place of the 12-point "
                             "rule; eager launches; accuracy vs the converged pixel integral is in the tests"}
+    surrogate = None
+    if not args.no_surrogate:
+        surrogate = bench_surrogate(args, A, job, d, nf, nb, ltf, out, flush, stream, dev, n_values, world)
     ms_t = torch.tensor([ms], dtype=torch.float64, device=dev)
     if dist:
         dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
@@ -454,12 +460,104 @@ def run_ours(args, rank, world, local_rank):
         "roofline": roofline, "dominant_kernel": dominant, "roofline_path": roofline_path,
         "kernels": kernels, "gpu_launches": gpu_launches,
         "clocks": ck, "e2e": e2e, "cpu_baseline": cpu, "max_rel_err_vs_fp64_oracle": err,
-        "adaptive": adaptive,
+        "adaptive": adaptive, "surrogate": surrogate,
         "three_calls_device": {"ms_per_step": ms3 / args.steps, "value": n_values * world * args.steps / (ms3 * 1e-3),
                                "note": "compute_exposure, compute_psf_data, point_src_model_map_wcs as three "
                                        "device-pointer calls on one stream (no geometry overlap)"},
     }
     print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- surrogate
+def bench_surrogate(args, A, job, d, nf, nb, ltf, out, flush, stream, dev, n_values, world):
+    """The learned surrogate on the bench job: trained on the GPU (untimed) on
+    samples of the 12-point rule around the mean PSFs of a 500-source job of
+    another seed, its error on fresh samples of a third seed against the centre
+    value alone, then the same step as the plain path (exposure, mean PSF, model
+    map) with the surrogate's model map, timed with the same rules."""
+    import numpy as np
+    import torch
+
+    from xtsrcmaps_b200.surrogate import Surrogate, samples
+    from xtsrcmaps_b200.synth import make_job
+
+    def tables(seed):
+        j = make_job("c2", seed=seed)
+        lt = A.livetime_efficiency_factors(j.logEs, j.effic_front)
+        f = A.normalize_rpsf(j.rpsf_front, j.scale_front)
+        b = A.normalize_rpsf(j.rpsf_back, j.scale_back)
+        ex = A.compute_exposure(j.exp_cube, j.wexp_cube, j.logEs, j.src_sph, j.aeff_front, j.aeff_back, lt)
+        ps = A.compute_psf_data(f, b, ex, j.logEs, lt)
+        return j, torch.as_tensor(np.ascontiguousarray(ps.uPsf), device=dev)
+
+    tj, tu = tables(args.seed + 100)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    X, Y = samples(tu, tj.logEs, args.surrogate_samples, seed=args.seed + 1)
+    net = Surrogate(device=dev, seed=args.seed)
+    losses = net.train(X, Y, epochs=args.surrogate_epochs)
+    torch.cuda.synchronize(dev)
+    t_train = time.perf_counter() - t0
+    del X, Y
+    hj, hu = tables(args.seed + 200)
+    Xh, Yh = samples(hu, hj.logEs, 1_000_000, seed=args.seed + 2)
+    yp = net.predict(Xh)
+    rho2 = (10.0 ** Xh[:, 0].double()) ** 2
+    err_net = ((yp.double() - Yh.double()).abs() / rho2)
+    err_c = Yh.double().abs() / rho2
+    held = {"samples": int(Xh.shape[0]), "rms_rel_err": float(err_net.pow(2).mean().sqrt()),
+            "max_rel_err": float(err_net.max()), "frac_within_1e-4": float((err_net <= 1e-4).double().mean()),
+            "centre_value_rms_rel_err": float(err_c.pow(2).mean().sqrt()),
+            "centre_value_max_rel_err": float(err_c.max())}
+    held["gain_rms"] = held["centre_value_rms_rel_err"] / held["rms_rel_err"]
+    del Xh, Yh, yp
+    out_s = torch.empty_like(out)
+    stats = {}
+
+    def step_sur():
+        with torch.cuda.stream(stream):
+            ex = A.compute_exposure(d["cube"], d["wcube"], d["logEs"], d["src"], d["af"], d["ab"], ltf)
+            ps = A.compute_psf_data(nf, nb, ex, d["logEs"], ltf)
+            m, _, st = A.point_src_model_map_wcs_surrogate(job.wcs, d["src"], ex.exposure, ps.uPsf,
+                                                           ps.partial_psf_integral, d["logEs"], net,
+                                                           check_tol=1e-4, with_info=False)
+            out_s.copy_(m)
+            stats.update(st)
+
+    for _ in range(max(3, args.warmup)):
+        step_sur()
+    ks = max(3, min(args.steps, 5))
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(ks)]
+    torch.cuda.synchronize(dev)
+    for k in range(ks):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        ev[k][0].record(stream)
+        step_sur()
+        ev[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    ms_s = sum(a_.elapsed_time(b_) for a_, b_ in ev) / ks
+    A.profile_enable(True)
+    step_sur()
+    prof = A.profile_read()
+    A.profile_enable(False)
+    rel = ((out_s.double() - out.double()).abs() / out.double().abs().clamp_min(1e-300))
+    fwd_ms = prof.get("k_mlp_forward", (0, 0.0))[1]
+    flop = 2 * (5 * 128 + 2 * 128 * 128 + 128) * n_values
+    return {"value": n_values * world / (ms_s * 1e-3), "unit": UNIT, "ms_per_step": ms_s, "steps": ks,
+            "check_tol": 1e-4, "rho_min": net.rho_min, "stats": stats,
+            "accepted_frac": stats.get("accepted", 0) / max(1, stats.get("values", 1)),
+            "max_rel_err_vs_plain_map": float(rel.max()), "frac_within_1e-4_vs_plain_map": float((rel <= 1e-4).double().mean()),
+            "network_forward": {"ms": fwd_ms, "rows": n_values, "tflops": flop / (fwd_ms * 1e-3) / 1e12 if fwd_ms else None,
+                                "note": "67,072 FLOP per row (5-128-128-128-1); the two hidden layers on tcgen05"},
+            "train": {"samples": args.surrogate_samples, "epochs": args.surrogate_epochs, "seconds": t_train,
+                      "first_epoch_loss": losses[0], "final_loss": losses[-1],
+                      "psf_tables": "c2-style job (500 sources) of another seed"},
+            "held_out": held,
+            "note": "pixel means from the network where the centre is >= rho_min pixel sizes from the source and "
+                    "the features lie in the training range, the FP64 12-point rule elsewhere; every 61st pixel "
+                    "checked against the rule and a map whose check exceeds check_tol redone by the rule; "
+                    "step = exposure + mean PSF + surrogate model map, eager launches"}
 
 
 # ----------------------------------------------------------------------------- CPU legs

@@ -10,10 +10,12 @@
 // into an FP32 accumulator of 128 tensor-memory columns, the four warps reading
 // it back with tcgen05.ld (warp w owns lanes 32w..32w+31 = rows of the tile).
 //
-//   * k_mlp_forward: one tile of 128 rows per step of a persistent loop.  Layer 1
-//     (K = 5) and the GELUs on CUDA cores; each hidden layer's BF16 activations
-//     are written by their row's thread straight into the swizzled A operand of
-//     the next MMA; the output layer is a per-row dot product.  For training it
+//   * k_mlp_forward: one tile of 128 rows per step of a persistent loop, two
+//     blocks of two warpgroups per SM (each row's 128 columns split between two
+//     threads).  Layer 1 (K = 5) and the GELUs on CUDA cores; each hidden layer's
+//     BF16 activations are written by their row's threads straight into the
+//     swizzled A operand of the next MMA; the output layer is a per-row dot
+//     product.  For training it
 //     also writes the pre-activations z1..z3 and the activations h1, h2,
 //     transposed ([128][n], coalesced across the threads of a warp).
 //   * k_gemm_bf16: C = A B^T for the backward pass (dW = dZ^T H, dH = dZ W), with
@@ -129,10 +131,12 @@ __device__ __forceinline__ void tmem_free(unsigned tmem, unsigned ncols) {
 }
 
 // ====================================================================== forward
+constexpr int FT = 2 * MT;  // forward threads: two warpgroups, each row's 128 columns split in halves
+
 struct FwdLayout {
     static constexpr size_t w2 = 0, w3 = 2 * ATOM, act = 4 * ATOM;
-    static constexpr size_t f32 = 6 * ATOM;  // W1 [128][5], b1, b2, b3, w4 [128], b4
-    static constexpr size_t bars = f32 + 4 * (MH * MI + 4 * MH + 4);
+    static constexpr size_t f32 = 6 * ATOM;  // W1 [128][5], b1, b2, b3, w4 [128], b4 (+3), partial y [128]
+    static constexpr size_t bars = f32 + 4 * (MH * MI + 4 * MH + 4 + MT);
     static constexpr size_t total = bars + 64;
 };
 constexpr size_t FWD_SMEM = FwdLayout::total + 1024;
@@ -143,35 +147,38 @@ struct FwdSaves {  // training only; all NULL for inference
     float* yn;  // [n] standardised output
 };
 
-__global__ void __launch_bounds__(MT, 1)
+// Thread t works on row r = t & 127 of the tile and hidden columns [64 hf, 64 hf + 64),
+// hf = t >> 7: warp w reads tensor-memory lanes 32 (w & 3).. and, in the A operand,
+// writes the [128][64] atom hf of its rows.
+__global__ void __launch_bounds__(FT, 2)
 k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict__ wbf, MlpNorm nm,
               const float* __restrict__ X, long long n, float* __restrict__ y, FwdSaves sv,
               int* __restrict__ status) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
-    const int t = threadIdx.x, warp = t >> 5;
+    const int t = threadIdx.x, warp = t >> 5, r = t & (MT - 1), hf = t >> 7, cb = 64 * hf;
     float* w1 = (float*)(smem + FwdLayout::f32);
     float* b1 = w1 + MH * MI;
     float* b2 = b1 + MH;
     float* b3 = b2 + MH;
     float* w4 = b3 + MH;
     float* b4 = w4 + MH;
+    float* ypart = b4 + 4;
     unsigned long long* bars = (unsigned long long*)(smem + FwdLayout::bars);
     unsigned* tmem_slot = (unsigned*)(smem + FwdLayout::bars + 32);
-    int* abort_flag = (int*)(smem + FwdLayout::bars + 48);
     const unsigned bar = smem_u32(&bars[0]);
     const unsigned s_w2 = smem_u32(smem + FwdLayout::w2), s_w3 = smem_u32(smem + FwdLayout::w3);
     const unsigned s_act = smem_u32(smem + FwdLayout::act);
 
     // weights: W2, W3 [out][in] BF16 -> swizzled B operands (row = out, K = in)
-    for (int idx = t; idx < 2 * MH * (MH / 8); idx += MT) {
+    for (int idx = t; idx < 2 * MH * (MH / 8); idx += FT) {
         const int l = idx / (MH * (MH / 8)), rem = idx - l * (MH * (MH / 8));
-        const int r = rem >> 4, ch = rem & 15;
-        const uint4 v = *reinterpret_cast<const uint4*>(wbf + (size_t)l * MH * MH + r * MH + ch * 8);
-        *reinterpret_cast<uint4*>(smem + (l ? FwdLayout::w3 : FwdLayout::w2) + sw_off(r, ch * 8)) = v;
+        const int row = rem >> 4, ch = rem & 15;
+        const uint4 v = *reinterpret_cast<const uint4*>(wbf + (size_t)l * MH * MH + row * MH + ch * 8);
+        *reinterpret_cast<uint4*>(smem + (l ? FwdLayout::w3 : FwdLayout::w2) + sw_off(row, ch * 8)) = v;
     }
-    for (int k = t; k < MH * MI; k += MT) w1[k] = __bfloat162float(__float2bfloat16_rn(params[XTS_MLP_W1 + k]));
-    for (int k = t; k < MH; k += MT) {
+    for (int k = t; k < MH * MI; k += FT) w1[k] = __bfloat162float(__float2bfloat16_rn(params[XTS_MLP_W1 + k]));
+    for (int k = t; k < MH; k += FT) {
         b1[k] = params[XTS_MLP_B1 + k];
         b2[k] = params[XTS_MLP_B2 + k];
         b3[k] = params[XTS_MLP_B3 + k];
@@ -180,7 +187,6 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
     if (t == 0) {
         b4[0] = params[XTS_MLP_B4];
         mbar_init(bar, 1);
-        *abort_flag = 0;
     }
     if (warp == 0) tmem_alloc(smem_u32(tmem_slot), 128);
     fence_async_shared();
@@ -188,18 +194,18 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
     __syncthreads();
     tc_fence_after();
     const unsigned tmem = *tmem_slot;
-    const unsigned trow = tmem + ((unsigned)(warp * 32) << 16);
+    const unsigned trow = tmem + ((unsigned)((warp & 3) * 32) << 16) + (unsigned)cb;
     unsigned ph = 0;
     bool ok = true;
     const long long ntiles = (n + MT - 1) / MT;
     for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-        const long long row = tile * MT + t;
+        const long long row = tile * MT + r;
         const bool live = row < n;
         float x[MI];
 #pragma unroll
         for (int k = 0; k < MI; ++k) x[k] = live ? (X[row * MI + k] - nm.mu[k]) / nm.sd[k] : 0.f;
-        // layer 1 on CUDA cores -> A operand of layer 2
-        for (int j0 = 0; j0 < MH; j0 += 8) {
+        // layer 1 on CUDA cores -> this thread's half of the A operand of layer 2
+        for (int j0 = cb; j0 < cb + 64; j0 += 8) {
             float h[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
@@ -217,7 +223,7 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
 #pragma unroll
                 for (int j = 0; j < 8; ++j) sv.h1[(size_t)(j0 + j) * n + row] = hb[j];
             }
-            *reinterpret_cast<uint4*>(smem + FwdLayout::act + sw_off(t, j0)) = pk;
+            *reinterpret_cast<uint4*>(smem + FwdLayout::act + sw_off(r, j0)) = pk;
         }
         float yacc = 0.f;
         for (int layer = 2; layer <= 3 && ok; ++layer) {
@@ -235,41 +241,44 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
             tc_fence_after();
             const float* bias = layer == 2 ? b2 : b3;
             float* zs = layer == 2 ? sv.z2 : sv.z3;
-            for (int c0 = 0; c0 < MH; c0 += 16) {
+            for (int c0 = 0; c0 < 64; c0 += 16) {
                 float v[16];
                 tmem_ld16(trow + (unsigned)c0, v);
+                const int cc = cb + c0;
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
-                    v[j] += bias[c0 + j];
-                    if (zs && live) zs[(size_t)(c0 + j) * n + row] = v[j];
+                    v[j] += bias[cc + j];
+                    if (zs && live) zs[(size_t)(cc + j) * n + row] = v[j];
                     v[j] = gelu(v[j]);
                 }
                 if (layer == 2) {
 #pragma unroll
-                    for (int hlf = 0; hlf < 2; ++hlf) {
-                        const float* u = v + 8 * hlf;
+                    for (int q = 0; q < 2; ++q) {
+                        const float* u = v + 8 * q;
                         uint4 pk = make_uint4(pack_bf16(u[0], u[1]), pack_bf16(u[2], u[3]), pack_bf16(u[4], u[5]),
                                               pack_bf16(u[6], u[7]));
                         if (sv.h2 && live) {
                             const __nv_bfloat16* hb = reinterpret_cast<const __nv_bfloat16*>(&pk);
 #pragma unroll
-                            for (int j = 0; j < 8; ++j) sv.h2[(size_t)(c0 + 8 * hlf + j) * n + row] = hb[j];
+                            for (int j = 0; j < 8; ++j) sv.h2[(size_t)(cc + 8 * q + j) * n + row] = hb[j];
                         }
-                        *reinterpret_cast<uint4*>(smem + FwdLayout::act + sw_off(t, c0 + 8 * hlf)) = pk;
+                        *reinterpret_cast<uint4*>(smem + FwdLayout::act + sw_off(r, cc + 8 * q)) = pk;
                     }
                 } else {
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) yacc = fmaf(v[j], w4[c0 + j], yacc);
+                    for (int j = 0; j < 16; ++j) yacc = fmaf(v[j], w4[cc + j], yacc);
                 }
             }
         }
         if (!ok) break;
-        const float yn = yacc + b4[0];
-        if (live) {
+        if (hf) ypart[r] = yacc;
+        tc_fence_before();  // the next tile's MMA overwrites the accumulator read above
+        __syncthreads();
+        if (!hf && live) {
+            const float yn = (yacc + ypart[r]) + b4[0];
             if (sv.yn) sv.yn[row] = yn;
             if (y) y[row] = fmaf(yn, nm.out_sd, nm.out_mu);
         }
-        tc_fence_before();  // the next tile's MMA overwrites the accumulator read above
     }
     if (!ok && t == 0) {
         atomicExch(status, 1);
@@ -526,8 +535,8 @@ static int forward(const xts_mlp* net, const float* X, long long n, float* y, Fw
         attr = true;
     }
     const long long ntiles = (n + MT - 1) / MT;
-    const long long g = ntiles < sm_count() ? ntiles : sm_count();
-    XTS_LAUNCH("k_mlp_forward", st, k_mlp_forward<<<(unsigned)g, MT, FWD_SMEM, st>>>(
+    const long long g = ntiles < 2 * sm_count() ? ntiles : 2 * sm_count();  // two blocks per SM
+    XTS_LAUNCH("k_mlp_forward", st, k_mlp_forward<<<(unsigned)g, FT, FWD_SMEM, st>>>(
                                         net->params, (const __nv_bfloat16*)net->wbf16, mlp_norm(net), X, n, y, sv,
                                         status));
     return XTS_OK;
