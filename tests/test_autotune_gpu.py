@@ -1,0 +1,51 @@
+"""GPU check of the autotuner: the write-pass choice is one of the parity-tested
+kernels and the adaptive cubature's (rtol, depth) choice meets its error target
+against the converged map it was measured on."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def api():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from xtsrcmaps_b200 import api as A
+    from xtsrcmaps_b200 import build
+
+    build.build()
+    A.init(0)
+    return A
+
+
+def test_autotune_choices(api):
+    import torch
+
+    from xtsrcmaps_b200 import autotune as T
+    from xtsrcmaps_b200.synth import make_job
+
+    job = make_job("c1", seed=9, n_sources=4)
+    ltf = api.livetime_efficiency_factors(job.logEs, job.effic_front)
+    nf = api.normalize_rpsf(job.rpsf_front, job.scale_front)
+    nb = api.normalize_rpsf(job.rpsf_back, job.scale_back)
+    ex = api.compute_exposure(job.exp_cube, job.wexp_cube, job.logEs, job.src_sph, job.aeff_front,
+                              job.aeff_back, ltf)
+    ps = api.compute_psf_data(nf, nb, ex, job.logEs, ltf)
+    d = torch.device("cuda")
+    t = lambda x: torch.as_tensor(np.ascontiguousarray(x), device=d)
+    src, expo, upsf, part = t(job.src_sph), t(ex.exposure), t(ps.uPsf), t(ps.partial_psf_integral)
+    w = T.tune_write_pass(job.wcs, src, expo, upsf, part)
+    assert w["kernel"] in ("windows", "cuda_cores", "tcgen05")
+    assert all(v > 0 for v in w["ms"].values()) and w["ms"][w["kernel"]] == min(w["ms"].values())
+    assert T.tune_write_pass(job.wcs, src, expo, upsf, part) is w  # cached per shape
+    a = T.tune_adaptive(job.wcs, src, expo, upsf, part, target=1e-3, rtols=(1e-3, 1e-4), depths=(4, 6, 8),
+                        n_sources=2)
+    assert a is not None, "no adaptive setting met 1e-3"
+    assert a["err"] <= 1e-3 and (a["rtol"], a["max_depth"]) in [(r, dd) for r in (1e-3, 1e-4) for dd in (4, 6, 8)]
+    ok = [v["ms"] for v in a["table"].values() if v["err"] <= 1e-3]
+    assert a["ms"] == min(ok)
+    print(f"\nwrite pass: {w}\nadaptive: rtol {a['rtol']:g}, depth {a['max_depth']}, {a['ms']:.3f} ms, "
+          f"err {a['err']:.2e}")

@@ -43,7 +43,7 @@ def _stream(dev) -> C.c_void_p:
     return C.c_void_p(h if h else 1)  # 0 would mean the library's own stream
 
 
-def samples(upsf, logEs, n: int, seed: int = 1, rho_min: float = 20.0):
+def samples(upsf, logEs, n: int, seed: int = 1, rho_min: float = 100.0):
     """Training samples from mean-PSF tables upsf [S, 401, E] (float64, CUDA) and
     log10 energies [E]: features X [n, 5] and targets Y [n] (float32, CUDA)."""
     torch = _torch()
@@ -77,7 +77,7 @@ class Surrogate:
     """Parameters (FP32 master copy, BF16 copies of the hidden layers), Adam
     state and standardisation of one surrogate network."""
 
-    def __init__(self, device=None, seed: int = 0, rho_min: float = 20.0):
+    def __init__(self, device=None, seed: int = 0, rho_min: float = 100.0):
         torch = _torch()
         self.device = torch.device(device) if device is not None else torch.device("cuda")
         rng = np.random.default_rng(seed)
