@@ -320,6 +320,13 @@ def run_ours(args, rank, world, local_rank):
                     "rtol": 1e-4, "max_depth": 6,
                     "note": "point_src_model_map_wcs_adaptive (Genz-Malik 7/5 per pixel) in place of the 12-point "
                             "rule; eager launches; accuracy vs the converged pixel integral is in the tests"}
+    # the autotuner's write-pass choice on this job (each kernel timed on the job's own geometry)
+    from xtsrcmaps_b200.autotune import tune_write_pass
+
+    with torch.cuda.stream(stream):
+        ex_t = A.compute_exposure(d["cube"], d["wcube"], d["logEs"], d["src"], d["af"], d["ab"], ltf)
+        ps_t = A.compute_psf_data(nf, nb, ex_t, d["logEs"], ltf)
+        autotune = tune_write_pass(job.wcs, d["src"], ex_t.exposure, ps_t.uPsf, ps_t.partial_psf_integral)
     surrogate = None
     if not args.no_surrogate:
         surrogate = bench_surrogate(args, A, job, d, nf, nb, ltf, out, flush, stream, dev, n_values, world)
@@ -460,7 +467,7 @@ def run_ours(args, rank, world, local_rank):
         "roofline": roofline, "dominant_kernel": dominant, "roofline_path": roofline_path,
         "kernels": kernels, "gpu_launches": gpu_launches,
         "clocks": ck, "e2e": e2e, "cpu_baseline": cpu, "max_rel_err_vs_fp64_oracle": err,
-        "adaptive": adaptive, "surrogate": surrogate,
+        "adaptive": adaptive, "surrogate": surrogate, "autotune_write_pass": autotune,
         "three_calls_device": {"ms_per_step": ms3 / args.steps, "value": n_values * world * args.steps / (ms3 * 1e-3),
                                "note": "compute_exposure, compute_psf_data, point_src_model_map_wcs as three "
                                        "device-pointer calls on one stream (no geometry overlap)"},
