@@ -150,6 +150,9 @@ struct FwdSaves {  // training only; all NULL for inference
 // Thread t works on row r = t & 127 of the tile and hidden columns [64 hf, 64 hf + 64),
 // hf = t >> 7: warp w reads tensor-memory lanes 32 (w & 3).. and, in the A operand,
 // writes the [128][64] atom hf of its rows.
+// SAVE: training (pre-activations, activations and the standardised output saved;
+// y unused); else inference (y only).
+template <bool SAVE>
 __global__ void __launch_bounds__(FT, 2)
 k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict__ wbf, MlpNorm nm,
               const float* __restrict__ X, long long n, float* __restrict__ y, FwdSaves sv,
@@ -214,11 +217,11 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
 #pragma unroll
                 for (int k = 0; k < MI; ++k) z = fmaf(w[k], x[k], z);
                 h[j] = gelu(z);
-                if (sv.z1 && live) sv.z1[(size_t)(j0 + j) * n + row] = z;
+                if (SAVE && live) sv.z1[(size_t)(j0 + j) * n + row] = z;
             }
             uint4 pk = make_uint4(pack_bf16(h[0], h[1]), pack_bf16(h[2], h[3]), pack_bf16(h[4], h[5]),
                                   pack_bf16(h[6], h[7]));
-            if (sv.h1 && live) {
+            if (SAVE && live) {
                 const __nv_bfloat16* hb = reinterpret_cast<const __nv_bfloat16*>(&pk);
 #pragma unroll
                 for (int j = 0; j < 8; ++j) sv.h1[(size_t)(j0 + j) * n + row] = hb[j];
@@ -240,7 +243,7 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
             ph ^= 1;
             tc_fence_after();
             const float* bias = layer == 2 ? b2 : b3;
-            float* zs = layer == 2 ? sv.z2 : sv.z3;
+            float* zs = SAVE ? (layer == 2 ? sv.z2 : sv.z3) : nullptr;
             for (int c0 = 0; c0 < 64; c0 += 16) {
                 float v[16];
                 tmem_ld16(trow + (unsigned)c0, v);
@@ -248,7 +251,7 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
                     v[j] += bias[cc + j];
-                    if (zs && live) zs[(size_t)(cc + j) * n + row] = v[j];
+                    if (SAVE && live) zs[(size_t)(cc + j) * n + row] = v[j];
                     v[j] = gelu(v[j]);
                 }
                 if (layer == 2) {
@@ -257,7 +260,7 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
                         const float* u = v + 8 * q;
                         uint4 pk = make_uint4(pack_bf16(u[0], u[1]), pack_bf16(u[2], u[3]), pack_bf16(u[4], u[5]),
                                               pack_bf16(u[6], u[7]));
-                        if (sv.h2 && live) {
+                        if (SAVE && live) {
                             const __nv_bfloat16* hb = reinterpret_cast<const __nv_bfloat16*>(&pk);
 #pragma unroll
                             for (int j = 0; j < 8; ++j) sv.h2[(size_t)(cc + 8 * q + j) * n + row] = hb[j];
@@ -276,8 +279,8 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
         __syncthreads();
         if (!hf && live) {
             const float yn = (yacc + ypart[r]) + b4[0];
-            if (sv.yn) sv.yn[row] = yn;
-            if (y) y[row] = fmaf(yn, nm.out_sd, nm.out_mu);
+            if (SAVE) sv.yn[row] = yn;
+            else y[row] = fmaf(yn, nm.out_sd, nm.out_mu);
         }
     }
     if (!ok && t == 0) {
@@ -531,14 +534,23 @@ static int forward(const xts_mlp* net, const float* X, long long n, float* y, Fw
                    cudaStream_t st) {
     static bool attr = false;
     if (!attr) {
-        XTS_CUDA(cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM));
+        XTS_CUDA(cudaFuncSetAttribute(k_mlp_forward<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM));
+        XTS_CUDA(cudaFuncSetAttribute(k_mlp_forward<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM));
         attr = true;
     }
+    const bool save = sv.z1 != nullptr;
+    if (save && !(sv.z2 && sv.z3 && sv.h1 && sv.h2 && sv.yn)) return set_error(XTS_ERR_ARG, "mlp forward: saves");
+    if (!save && !y) return set_error(XTS_ERR_ARG, "mlp forward: output");
     const long long ntiles = (n + MT - 1) / MT;
     const long long g = ntiles < 2 * sm_count() ? ntiles : 2 * sm_count();  // two blocks per SM
-    XTS_LAUNCH("k_mlp_forward", st, k_mlp_forward<<<(unsigned)g, FT, FWD_SMEM, st>>>(
-                                        net->params, (const __nv_bfloat16*)net->wbf16, mlp_norm(net), X, n, y, sv,
-                                        status));
+    if (save)
+        XTS_LAUNCH("k_mlp_forward", st, k_mlp_forward<true><<<(unsigned)g, FT, FWD_SMEM, st>>>(
+                                            net->params, (const __nv_bfloat16*)net->wbf16, mlp_norm(net), X, n, y,
+                                            sv, status));
+    else
+        XTS_LAUNCH("k_mlp_forward", st, k_mlp_forward<false><<<(unsigned)g, FT, FWD_SMEM, st>>>(
+                                            net->params, (const __nv_bfloat16*)net->wbf16, mlp_norm(net), X, n, y,
+                                            sv, status));
     return XTS_OK;
 }
 
