@@ -47,11 +47,16 @@ struct SurPix {
     double rho;
 };
 
-__device__ __forceinline__ void sur_pixel(const PixGeom& g, SurPix& sp) {
+// the 12 rule points' rows and weights
+__device__ __forceinline__ void sur_points(const PixGeom& g, SurPix& sp) {
     const PixQ c = pixel_q(g);
 #pragma unroll
     for (int p = 0; p < 12; ++p) sp.idx[p] = sur_row(2.0 * R2D * asin(0.5 * sqrt(point_q2(c, p))), &sp.tt[p]);
-    const double alen = sqrt(c.a0);
+}
+
+// the centre's separation, row and offset, and the pixel features
+__device__ __forceinline__ void sur_centre_geom(const PixGeom& g, SurPix& sp) {
+    const double alen = sqrt(fma(g.Ax, g.Ax, fma(g.Ay, g.Ay, g.Az * g.Az)));
     const double thc = 2.0 * asin(0.5 * alen);  // radians
     const double cx = g.By * g.Cz - g.Bz * g.Cy, cy = g.Bz * g.Cx - g.Bx * g.Cz, cz = g.Bx * g.Cy - g.By * g.Cx;
     const double om = 4.0 * sqrt(cx * cx + cy * cy + cz * cz);
@@ -61,6 +66,11 @@ __device__ __forceinline__ void sur_pixel(const PixGeom& g, SurPix& sp) {
     sp.f0 = (float)log10(sp.rho);
     sp.f1 = (float)sp.tc;
     sp.f2 = (float)log10(om * R2D * R2D);
+}
+
+__device__ __forceinline__ void sur_pixel(const PixGeom& g, SurPix& sp) {
+    sur_points(g, sp);
+    sur_centre_geom(g, sp);
 }
 
 __device__ __forceinline__ double sur_rule(const SurPix& sp, const double* U, int E, int e) {
@@ -175,7 +185,9 @@ __global__ void __launch_bounds__(128) k_sur_features(const double* __restrict__
     if (pix < npix) {
         const int h = pix / W, w = pix - h * W;
         SurPix sp;
-        sur_pixel(pixel_geom(corners, W + 1, h, w, info[s]), sp);
+        const PixGeom g = pixel_geom(corners, W + 1, h, w, info[s]);
+        sur_centre_geom(g, sp);
+        bool have_points = false;  // the rule points, once a value needs them
         const double* U = upsf + (size_t)s * ND * E;
         const bool geo_ok = sp.rho >= rg.rho_min && sp.f0 >= rg.lo[0] && sp.f0 <= rg.hi[0] && sp.f1 >= rg.lo[1] &&
                             sp.f1 <= rg.hi[1] && sp.f2 >= rg.lo[2] && sp.f2 <= rg.hi[2];
@@ -194,6 +206,10 @@ __global__ void __launch_bounds__(128) k_sur_features(const double* __restrict__
                 ++acc;
             } else {
                 aux[v] = make_float2(0.f, -1.f);
+                if (!have_points) {
+                    sur_points(g, sp);
+                    have_points = true;
+                }
                 mean[((size_t)s * npix + pix) * E + e] = (float)sur_rule(sp, U, E, e);
             }
         }
