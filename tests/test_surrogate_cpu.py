@@ -94,3 +94,37 @@ def test_sample_oracle_geometry():
         assert math.log10(0.025 ** 2 * 0.99) <= x[2] <= math.log10(0.2 ** 2 * 1.01)
         assert x[3] in logEs
         assert np.isfinite(y)
+
+
+def test_surrogate_state_round_trip(tmp_path):
+    """Host side of xtsrcmaps_b200.surrogate without a GPU: initialisation, the
+    BF16 copies (round to nearest even), standardisation from a training set, and
+    save/load of the parameters and standardisation."""
+    import torch
+
+    from xtsrcmaps_b200 import _lib as L
+    from xtsrcmaps_b200.surrogate import Surrogate
+
+    net = Surrogate(device="cpu", seed=4, rho_min=50.0)
+    p = net.params.numpy()
+    assert p.shape == (L.MLP_NPARAM,) and np.all(p[L.MLP_B1:L.MLP_W2] == 0)
+    w23 = np.concatenate([p[L.MLP_W2:L.MLP_B2], p[L.MLP_W3:L.MLP_B3]])
+    bits = net.wbf16.numpy().astype(np.uint16).astype(np.uint32) << 16
+    np.testing.assert_array_equal(bits.view(np.float32), MO.bf16(w23).astype(np.float32))
+    rng = np.random.default_rng(0)
+    X = torch.as_tensor(rng.normal(2.0, 3.0, (4096, 5)).astype(np.float32))
+    Y = torch.as_tensor(rng.normal(-1.0, 0.5, 4096).astype(np.float32))
+    net.fit_standardisation(X, Y)
+    assert np.allclose(net.in_mu, 2.0, atol=0.2) and np.allclose(net.in_sd, 3.0, atol=0.2)
+    assert np.all(net.lo <= X.numpy().min(0)) and np.all(net.hi >= X.numpy().max(0))
+    assert abs(net.out_mu + 1.0) < 0.05 and abs(net.out_sd - 0.5) < 0.05
+    f = str(tmp_path / "net.npz")
+    net.save(f)
+    back = Surrogate.load(f, device="cpu")
+    np.testing.assert_array_equal(back.params.numpy(), p)
+    np.testing.assert_array_equal(back.wbf16.numpy(), net.wbf16.numpy())
+    for a in ("in_mu", "in_sd", "lo", "hi"):
+        np.testing.assert_array_equal(getattr(back, a), getattr(net, a))
+    assert (back.out_mu, back.out_sd, back.rho_min) == (net.out_mu, net.out_sd, 50.0)
+    s = back.struct()
+    assert abs(s.rho_min - 50.0) < 1e-6 and list(s.in_sd) == pytest.approx(list(net.in_sd))
