@@ -307,7 +307,7 @@ def convolve_pixel_logsep(pw48, lut, src3) -> np.ndarray:
 
 
 def adaptive_cubature_map(wcs, src_sph, upsf, rtol: float, max_depth: int = 6):
-    """Pixel-mean PSF [S, H, W, E] by adaptive Genz-Malik cubature (SURVEY row d3;
+    """Pixel-mean PSF [S, H, W, E] by adaptive Genz-Malik cubature (the reference's
     math/genz_malik.hxx:18-85 design, published rule with rectangular sub-regions)
     and the number of regions evaluated per (source, pixel)."""
     w = _wcs(wcs)

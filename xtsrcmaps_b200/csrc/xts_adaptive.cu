@@ -1,4 +1,5 @@
-// xts_adaptive.cu -- adaptive cubature of the pixel-mean PSF:
+// xts_adaptive.cu -- adaptive cubature of the pixel-mean PSF (the design of the
+// reference's uncompiled math/genz_malik.hxx:18-195):
 // the published Genz-Malik degree-7/5 rule for two dimensions (A.C. Genz,
 // A.A. Malik, J. Comput. Appl. Math. 6 (1980) 295-302; weights as updated by
 // Bernstein, Espelid and Genz), the design the reference lays out in
