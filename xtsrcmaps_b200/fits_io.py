@@ -2,7 +2,7 @@
 
 The reference reads its inputs through cfitsio (fits/fits.read_irf_pars.cxx:12-126 for
 the IRF parameter tables, observation/observation.cxx for the counts cube); cfitsio is
-not available to this build, so the few structures the path needs are parsed here
+not a dependency of this package, so the few structures the path needs are parsed here
 from the FITS standard 4.0: 80-byte header cards in 2880-byte blocks, IMAGE and
 BINTABLE extensions, big-endian data.  Only fixed-length columns are read (the IRF
 tables have no variable-length arrays).
