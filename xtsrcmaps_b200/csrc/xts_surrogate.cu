@@ -171,51 +171,78 @@ int launch_surrogate_samples(const double* upsf, const double* logEs, int S, int
 // ------------------------------------------------------------------ model map
 struct SurRange { float lo[5], hi[5], rho_min; };
 
-// Per (source, pixel) of a chunk of sources: features of every energy, or the
-// rule's mean where the value is not the network's.  aux = (u_c, 1 / rho^2), or
-// (0, -1) for a value taken by the rule.
-__global__ void __launch_bounds__(128) k_sur_features(const double* __restrict__ corners, const SrcInfo* __restrict__ info,
-                                                      const double* __restrict__ upsf, const double* __restrict__ logEs,
-                                                      int s0, int H, int W, int E, SurRange rg, float* __restrict__ X,
-                                                      float2* __restrict__ aux, float* __restrict__ mean,
-                                                      unsigned long long* __restrict__ accepted) {
-    const int s = s0 + blockIdx.y, pix = blockIdx.x * blockDim.x + threadIdx.x;
-    const int npix = H * W;
-    unsigned acc = 0;
-    if (pix < npix) {
-        const int h = pix / W, w = pix - h * W;
-        SurPix sp;
+// Per block: SF_PIX pixels of one source of a chunk.  Phase 1, one thread per
+// pixel: the centre, the features that do not depend on energy and the 12 rule
+// points, into shared memory.  Phase 2, one thread per (pixel, energy) value in the
+// maps' order, so that the feature rows [v][5], aux [v] and fallback values are
+// written coalesced: the centre value and segment slope, the five features, and
+// either aux = (u_c, 1 / rho^2) or, for a value the network does not take,
+// aux = (0, -1) and the rule's mean.
+constexpr int SF_PIX = 128;
+constexpr int SF_THREADS = 256;
+
+struct SurPixS {
+    float f0, f1, f2, eps;
+    double tc;
+    int ic, geo_ok;
+    short idx[12];
+    double tt[12];
+};
+
+__global__ void __launch_bounds__(SF_THREADS) k_sur_features(const double* __restrict__ corners,
+                                                             const SrcInfo* __restrict__ info,
+                                                             const double* __restrict__ upsf,
+                                                             const double* __restrict__ logEs, int s0, int H, int W,
+                                                             int E, SurRange rg, float* __restrict__ X,
+                                                             float2* __restrict__ aux, float* __restrict__ mean,
+                                                             unsigned long long* __restrict__ accepted) {
+    __shared__ SurPixS sp[SF_PIX];
+    const int s = s0 + blockIdx.y, t = threadIdx.x;
+    const int npix = H * W, p0 = blockIdx.x * SF_PIX;
+    const int np = min(SF_PIX, npix - p0);
+    if (t < np) {
+        const int pix = p0 + t, h = pix / W, w = pix - h * W;
+        SurPix q;
         const PixGeom g = pixel_geom(corners, W + 1, h, w, info[s]);
-        sur_centre_geom(g, sp);
-        bool have_points = false;  // the rule points, once a value needs them
-        const double* U = upsf + (size_t)s * ND * E;
-        const bool geo_ok = sp.rho >= rg.rho_min && sp.f0 >= rg.lo[0] && sp.f0 <= rg.hi[0] && sp.f1 >= rg.lo[1] &&
-                            sp.f1 <= rg.hi[1] && sp.f2 >= rg.lo[2] && sp.f2 <= rg.hi[2];
-        const float eps = (float)(1.0 / (sp.rho * sp.rho));
-        const size_t v0 = ((size_t)blockIdx.y * npix + pix) * E;
-        for (int e = 0; e < E; ++e) {
-            double slope;
-            const double uc = sur_centre(sp, U, E, e, &slope);
-            const float le = (float)logEs[e], sl = (float)slope;
-            const bool ok = geo_ok && uc > 0. && le >= rg.lo[3] && le <= rg.hi[3] && sl >= rg.lo[4] && sl <= rg.hi[4];
-            const size_t v = v0 + e;
-            float* x = X + v * 5;
-            x[0] = sp.f0; x[1] = sp.f1; x[2] = sp.f2; x[3] = le; x[4] = sl;
-            if (ok) {
-                aux[v] = make_float2((float)uc, eps);
-                ++acc;
-            } else {
-                aux[v] = make_float2(0.f, -1.f);
-                if (!have_points) {
-                    sur_points(g, sp);
-                    have_points = true;
-                }
-                mean[((size_t)s * npix + pix) * E + e] = (float)sur_rule(sp, U, E, e);
-            }
+        sur_pixel(g, q);
+        SurPixS& o = sp[t];
+        o.f0 = q.f0; o.f1 = q.f1; o.f2 = q.f2;
+        o.eps = (float)(1.0 / (q.rho * q.rho));
+        o.tc = q.tc;
+        o.ic = q.ic;
+        o.geo_ok = q.rho >= rg.rho_min && q.f0 >= rg.lo[0] && q.f0 <= rg.hi[0] && q.f1 >= rg.lo[1] &&
+                   q.f1 <= rg.hi[1] && q.f2 >= rg.lo[2] && q.f2 <= rg.hi[2];
+#pragma unroll
+        for (int p = 0; p < 12; ++p) { o.idx[p] = (short)q.idx[p]; o.tt[p] = q.tt[p]; }
+    }
+    __syncthreads();
+    const double* U = upsf + (size_t)s * ND * E;
+    const size_t vb = ((size_t)blockIdx.y * npix + p0) * E;  // first value of the block (chunk-relative)
+    const size_t mb = ((size_t)s * npix + p0) * E;           // the same value in the map
+    unsigned acc = 0;
+    for (int k = t; k < np * E; k += SF_THREADS) {
+        const int lp = k / E, e = k - lp * E;
+        const SurPixS& o = sp[lp];
+        const double lo = U[(size_t)(o.ic - 1) * E + e], hi = U[(size_t)o.ic * E + e];
+        const double slope = (lo > 0. && hi > 0.) ? log(hi / lo) * (1.0 / SEP_STEP) : 0.;
+        const double uc = (1.0 - o.tc) * lo + o.tc * hi;
+        const float le = (float)logEs[e], sl = (float)slope;
+        const bool ok = o.geo_ok && uc > 0. && le >= rg.lo[3] && le <= rg.hi[3] && sl >= rg.lo[4] && sl <= rg.hi[4];
+        float* x = X + (vb + k) * 5;
+        x[0] = o.f0; x[1] = o.f1; x[2] = o.f2; x[3] = le; x[4] = sl;
+        if (ok) {
+            aux[vb + k] = make_float2((float)uc, o.eps);
+            ++acc;
+        } else {
+            aux[vb + k] = make_float2(0.f, -1.f);
+            double m = 0.;
+#pragma unroll
+            for (int p = 0; p < 12; ++p) m += c_rule_uv[p][3] * sur_lerp(U, E, e, o.idx[p], o.tt[p]);
+            mean[mb + k] = (float)m;
         }
     }
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0 && acc) atomicAdd(accepted + s, (unsigned long long)acc);
+    if ((t & 31) == 0 && acc) atomicAdd(accepted + s, (unsigned long long)acc);
 }
 
 __global__ void k_sur_assemble(const float2* __restrict__ aux, const float* __restrict__ y, long long n,
@@ -312,8 +339,8 @@ int launch_srcmap_surrogate(const SrcmapDev& a, const double* corners, const dou
     for (int s0 = 0; s0 < S; s0 += sc) {
         const int ns = S - s0 < sc ? S - s0 : sc;
         const long long n = per_src * ns;
-        const dim3 gf((unsigned)((npix + 127) / 128), (unsigned)ns);
-        XTS_LAUNCH("k_sur_features", st, k_sur_features<<<gf, 128, 0, st>>>(corners, info, a.upsf, a.logEs, s0, H, W, E, rg,
+        const dim3 gf((unsigned)((npix + SF_PIX - 1) / SF_PIX), (unsigned)ns);
+        XTS_LAUNCH("k_sur_features", st, k_sur_features<<<gf, SF_THREADS, 0, st>>>(corners, info, a.upsf, a.logEs, s0, H, W, E, rg,
                                                                             X, aux, mean, acc_d));
         if ((rc = launch_mlp_forward(net, X, n, yv, status, st))) return rc;
         float* m0 = mean + (size_t)s0 * per_src;
