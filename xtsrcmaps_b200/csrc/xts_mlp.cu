@@ -135,8 +135,9 @@ constexpr int FT = 2 * MT;  // forward threads: two warpgroups, each row's 128 c
 
 struct FwdLayout {
     static constexpr size_t w2 = 0, w3 = 2 * ATOM, act = 4 * ATOM;
-    static constexpr size_t f32 = 6 * ATOM;  // W1 [128][5], b1, b2, b3, w4 [128], b4 (+3), partial y [128]
-    static constexpr size_t bars = f32 + 4 * (MH * MI + 4 * MH + 4 + MT);
+    // [128][8] rows (W1 row, b1, 0, 0), then b2, b3, w4 [128], b4 (+3), partial y [128]
+    static constexpr size_t f32 = 6 * ATOM;
+    static constexpr size_t bars = f32 + 4 * (MH * 8 + 3 * MH + 4 + MT);
     static constexpr size_t total = bars + 64;
 };
 constexpr size_t FWD_SMEM = FwdLayout::total + 1024;
@@ -160,9 +161,8 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
     const int t = threadIdx.x, warp = t >> 5, r = t & (MT - 1), hf = t >> 7, cb = 64 * hf;
-    float* w1 = (float*)(smem + FwdLayout::f32);
-    float* b1 = w1 + MH * MI;
-    float* b2 = b1 + MH;
+    float* w1 = (float*)(smem + FwdLayout::f32);  // [128][8]: W1 row, b1, 0, 0
+    float* b2 = w1 + MH * 8;
     float* b3 = b2 + MH;
     float* w4 = b3 + MH;
     float* b4 = w4 + MH;
@@ -180,9 +180,12 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
         const uint4 v = *reinterpret_cast<const uint4*>(wbf + (size_t)l * MH * MH + row * MH + ch * 8);
         *reinterpret_cast<uint4*>(smem + (l ? FwdLayout::w3 : FwdLayout::w2) + sw_off(row, ch * 8)) = v;
     }
-    for (int k = t; k < MH * MI; k += FT) w1[k] = __bfloat162float(__float2bfloat16_rn(params[XTS_MLP_W1 + k]));
+    for (int k = t; k < MH * 8; k += FT) {
+        const int j = k >> 3, q = k & 7;
+        w1[k] = q < MI ? __bfloat162float(__float2bfloat16_rn(params[XTS_MLP_W1 + j * MI + q]))
+                       : (q == MI ? params[XTS_MLP_B1 + j] : 0.f);
+    }
     for (int k = t; k < MH; k += FT) {
-        b1[k] = params[XTS_MLP_B1 + k];
         b2[k] = params[XTS_MLP_B2 + k];
         b3[k] = params[XTS_MLP_B3 + k];
         w4[k] = __bfloat162float(__float2bfloat16_rn(params[XTS_MLP_W4 + k]));
@@ -212,10 +215,9 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
             float h[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-                const float* w = w1 + (j0 + j) * MI;
-                float z = b1[j0 + j];
-#pragma unroll
-                for (int k = 0; k < MI; ++k) z = fmaf(w[k], x[k], z);
+                const float4 wa = reinterpret_cast<const float4*>(w1)[2 * (j0 + j)];
+                const float4 wb = reinterpret_cast<const float4*>(w1)[2 * (j0 + j) + 1];
+                const float z = fmaf(wb.x, x[4], fmaf(wa.w, x[3], fmaf(wa.z, x[2], fmaf(wa.y, x[1], fmaf(wa.x, x[0], wb.y)))));
                 h[j] = gelu(z);
                 if (SAVE && live) sv.z1[(size_t)(j0 + j) * n + row] = z;
             }
@@ -245,12 +247,17 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
             const float* bias = layer == 2 ? b2 : b3;
             float* zs = SAVE ? (layer == 2 ? sv.z2 : sv.z3) : nullptr;
             for (int c0 = 0; c0 < 64; c0 += 16) {
-                float v[16];
+                float v[16], bv[16];
                 tmem_ld16(trow + (unsigned)c0, v);
                 const int cc = cb + c0;
 #pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float4 b = reinterpret_cast<const float4*>(bias + cc)[q];
+                    bv[4 * q] = b.x; bv[4 * q + 1] = b.y; bv[4 * q + 2] = b.z; bv[4 * q + 3] = b.w;
+                }
+#pragma unroll
                 for (int j = 0; j < 16; ++j) {
-                    v[j] += bias[cc + j];
+                    v[j] += bv[j];
                     if (SAVE && live) zs[(size_t)(cc + j) * n + row] = v[j];
                     v[j] = gelu(v[j]);
                 }
@@ -269,7 +276,11 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
                     }
                 } else {
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) yacc = fmaf(v[j], w4[cc + j], yacc);
+                    for (int q = 0; q < 4; ++q) {
+                        const float4 wv = reinterpret_cast<const float4*>(w4 + cc)[q];
+                        yacc = fmaf(v[4 * q], wv.x, fmaf(v[4 * q + 1], wv.y, fmaf(v[4 * q + 2], wv.z,
+                                                                                   fmaf(v[4 * q + 3], wv.w, yacc))));
+                    }
                 }
             }
         }
