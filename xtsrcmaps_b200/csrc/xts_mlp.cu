@@ -65,6 +65,13 @@ constexpr float GK1 = 0.044715f;
 __device__ __forceinline__ float gelu(float z) {
     return 0.5f * z * (1.f + tanh_fast(GK0 * fmaf(GK1 * z * z, z, z)));
 }
+// two GELUs with packed FP32 arithmetic (same formula as gelu, rounding order differs)
+__device__ __forceinline__ float2 gelu2(float2 z) {
+    const float2 t = __ffma2_rn(make_float2(GK1, GK1), __fmul2_rn(z, z), make_float2(1.f, 1.f));
+    const float2 u = __fmul2_rn(__fmul2_rn(make_float2(GK0, GK0), z), t);
+    const float2 hz = __fmul2_rn(make_float2(0.5f, 0.5f), z);
+    return __ffma2_rn(hz, make_float2(tanh_fast(u.x), tanh_fast(u.y)), hz);
+}
 __device__ __forceinline__ float gelu_grad(float z) {
     const float z2 = z * z, th = tanh_fast(GK0 * fmaf(GK1 * z2, z, z));
     return 0.5f * (1.f + th) + 0.5f * z * (1.f - th * th) * GK0 * fmaf(3.f * GK1, z2, 1.f);
@@ -135,7 +142,8 @@ constexpr int FT = 2 * MT;  // forward threads: two warpgroups, each row's 128 c
 
 struct FwdLayout {
     static constexpr size_t w2 = 0, w3 = 2 * ATOM, act = 4 * ATOM;
-    // [128][8] rows (W1 row, b1, 0, 0), then b2, b3, w4 [128], b4 (+3), partial y [128]
+    // W1 transposed [5][128] and b1 [128] (six rows of 128), then 2 rows of padding, b2, b3,
+    // w4 [128], b4 (+3), partial y [128]
     static constexpr size_t f32 = 6 * ATOM;
     static constexpr size_t bars = f32 + 4 * (MH * 8 + 3 * MH + 4 + MT);
     static constexpr size_t total = bars + 64;
@@ -161,7 +169,7 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
     const int t = threadIdx.x, warp = t >> 5, r = t & (MT - 1), hf = t >> 7, cb = 64 * hf;
-    float* w1 = (float*)(smem + FwdLayout::f32);  // [128][8]: W1 row, b1, 0, 0
+    float* w1 = (float*)(smem + FwdLayout::f32);  // [6][128]: W1^T rows, then b1
     float* b2 = w1 + MH * 8;
     float* b3 = b2 + MH;
     float* w4 = b3 + MH;
@@ -181,7 +189,7 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
         *reinterpret_cast<uint4*>(smem + (l ? FwdLayout::w3 : FwdLayout::w2) + sw_off(row, ch * 8)) = v;
     }
     for (int k = t; k < MH * 8; k += FT) {
-        const int j = k >> 3, q = k & 7;
+        const int q = k >> 7, j = k & (MH - 1);
         w1[k] = q < MI ? __bfloat162float(__float2bfloat16_rn(params[XTS_MLP_W1 + j * MI + q]))
                        : (q == MI ? params[XTS_MLP_B1 + j] : 0.f);
     }
@@ -204,32 +212,50 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
     unsigned ph = 0;
     bool ok = true;
     const long long ntiles = (n + MT - 1) / MT;
+    // layer 1 of tile tl on CUDA cores: this thread's 64 BF16 activations of its row
+    auto layer1 = [&](long long tl, uint4* hq) {
+        const long long rw = tl * MT + r;
+        const bool lv = rw < n;
+        float x[MI];
+#pragma unroll
+        for (int k = 0; k < MI; ++k) x[k] = lv ? (X[rw * MI + k] - nm.mu[k]) / nm.sd[k] : 0.f;
+#pragma unroll
+        for (int g = 0; g < 8; ++g) {
+            const int j0 = cb + 8 * g;
+            float h[8];
+#pragma unroll
+            for (int j = 0; j < 8; j += 2) {
+                const float2* wp = reinterpret_cast<const float2*>(w1 + j0 + j);  // units j0 + j, j0 + j + 1
+                float2 z = wp[MI * MH / 2];  // b1
+#pragma unroll
+                for (int k = 0; k < MI; ++k) z = __ffma2_rn(wp[k * MH / 2], make_float2(x[k], x[k]), z);
+                const float2 g2 = gelu2(z);
+                h[j] = g2.x;
+                h[j + 1] = g2.y;
+                if (SAVE && lv) {
+                    sv.z1[(size_t)(j0 + j) * n + rw] = z.x;
+                    sv.z1[(size_t)(j0 + j + 1) * n + rw] = z.y;
+                }
+            }
+            hq[g] = make_uint4(pack_bf16(h[0], h[1]), pack_bf16(h[2], h[3]), pack_bf16(h[4], h[5]),
+                               pack_bf16(h[6], h[7]));
+            if (SAVE && lv) {
+                const __nv_bfloat16* hb = reinterpret_cast<const __nv_bfloat16*>(&hq[g]);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) sv.h1[(size_t)(j0 + j) * n + rw] = hb[j];
+            }
+        }
+    };
+    uint4 hq[8];
+    if (!SAVE && (long long)blockIdx.x < ntiles) layer1(blockIdx.x, hq);
     for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
         const long long row = tile * MT + r;
         const bool live = row < n;
-        float x[MI];
+        // the A operand of layer 2: this tile's layer 1 (for inference computed while the
+        // previous tile's last MMA ran; the MMA that read the buffer has completed)
+        if (SAVE) layer1(tile, hq);
 #pragma unroll
-        for (int k = 0; k < MI; ++k) x[k] = live ? (X[row * MI + k] - nm.mu[k]) / nm.sd[k] : 0.f;
-        // layer 1 on CUDA cores -> this thread's half of the A operand of layer 2
-        for (int j0 = cb; j0 < cb + 64; j0 += 8) {
-            float h[8];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const float4 wa = reinterpret_cast<const float4*>(w1)[2 * (j0 + j)];
-                const float4 wb = reinterpret_cast<const float4*>(w1)[2 * (j0 + j) + 1];
-                const float z = fmaf(wb.x, x[4], fmaf(wa.w, x[3], fmaf(wa.z, x[2], fmaf(wa.y, x[1], fmaf(wa.x, x[0], wb.y)))));
-                h[j] = gelu(z);
-                if (SAVE && live) sv.z1[(size_t)(j0 + j) * n + row] = z;
-            }
-            uint4 pk = make_uint4(pack_bf16(h[0], h[1]), pack_bf16(h[2], h[3]), pack_bf16(h[4], h[5]),
-                                  pack_bf16(h[6], h[7]));
-            if (SAVE && live) {
-                const __nv_bfloat16* hb = reinterpret_cast<const __nv_bfloat16*>(&pk);
-#pragma unroll
-                for (int j = 0; j < 8; ++j) sv.h1[(size_t)(j0 + j) * n + row] = hb[j];
-            }
-            *reinterpret_cast<uint4*>(smem + FwdLayout::act + sw_off(r, j0)) = pk;
-        }
+        for (int g = 0; g < 8; ++g) *reinterpret_cast<uint4*>(smem + FwdLayout::act + sw_off(r, cb + 8 * g)) = hq[g];
         float yacc = 0.f;
         for (int layer = 2; layer <= 3 && ok; ++layer) {
             fence_async_shared();
@@ -240,6 +266,8 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
                 mma_chain(tmem, s_act, layer == 2 ? s_w2 : s_w3, MH / 16, false);
                 mma_commit(bar);
             }
+            // inference: layer 1 of the next tile in registers while the last MMA of this one runs
+            if (!SAVE && layer == 3 && tile + gridDim.x < ntiles) layer1(tile + gridDim.x, hq);
             const bool got = mbar_wait(bar, ph);
             if (!__syncthreads_and(got)) { ok = false; break; }  // ph stays: the exit path waits on it
             ph ^= 1;
@@ -256,10 +284,15 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
                     bv[4 * q] = b.x; bv[4 * q + 1] = b.y; bv[4 * q + 2] = b.z; bv[4 * q + 3] = b.w;
                 }
 #pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    v[j] += bv[j];
-                    if (SAVE && live) zs[(size_t)(cc + j) * n + row] = v[j];
-                    v[j] = gelu(v[j]);
+                for (int j = 0; j < 16; j += 2) {
+                    const float2 z = __fadd2_rn(make_float2(v[j], v[j + 1]), make_float2(bv[j], bv[j + 1]));
+                    if (SAVE && live) {
+                        zs[(size_t)(cc + j) * n + row] = z.x;
+                        zs[(size_t)(cc + j + 1) * n + row] = z.y;
+                    }
+                    const float2 g2 = gelu2(z);
+                    v[j] = g2.x;
+                    v[j + 1] = g2.y;
                 }
                 if (layer == 2) {
 #pragma unroll
