@@ -98,3 +98,20 @@ def test_cli_end_to_end(api, tmp_path):
         assert hdr["BITPIX"] == -32 and arr.shape == (20, 100, 100)
         assert F.hdu_checksum(hb, db) == 0xffffffff
         assert np.isfinite(arr).all() and arr.max() > 0
+
+
+def test_cli_surrogate(api, tmp_path):
+    """python -m xtsrcmaps_b200 --train-surrogate, then --surrogate with the saved network."""
+    from xtsrcmaps_b200.__main__ import main
+
+    net = str(tmp_path / "net.npz")
+    fn1, fn2, fn0 = (str(tmp_path / f) for f in ("s1.fits", "s2.fits", "plain.fits"))
+    base = ["--config", "c0", "--bitpix", "-32"]
+    assert main(base + ["--out", fn0]) == 0
+    assert main(base + ["--out", fn1, "--train-surrogate", net, "--surrogate-samples", "400000",
+                        "--surrogate-epochs", "4"]) == 0
+    assert main(base + ["--out", fn2, "--surrogate", net]) == 0
+    a0, a1, a2 = (F.read_fits(f)[1][3] for f in (fn0, fn1, fn2))
+    np.testing.assert_array_equal(a1, a2)  # the saved network reproduces the maps
+    assert np.isfinite(a1).all() and a1.shape == a0.shape
+    assert np.max(np.abs(a1.astype(np.float64) - a0) / np.maximum(np.abs(a0), 1e-30)) < 1e-3

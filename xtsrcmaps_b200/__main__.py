@@ -11,7 +11,9 @@ observation/observation.cxx), --ltcube (livetime cube, EXPOSURE and
 WEIGHTED_EXPOSURE tables), --aeff and --psf (Pass-8 IRF files), --xml (point
 sources of a source model), or --sources (an .npz with ``src_sph`` [S, 2] degrees
 and ``names``).  The three calls run as one device call and the maps go to the
-FITS file from device memory.
+FITS file from device memory.  --adaptive RTOL uses the adaptive cubature, and
+--surrogate / --train-surrogate the learned surrogate of the pixel cubature (with
+the 12-point rule where it does not apply).
 """
 from __future__ import annotations
 
@@ -34,6 +36,14 @@ def main(argv=None) -> int:
     ap.add_argument("--bitpix", type=int, default=-64, choices=[-64, -32])
     ap.add_argument("--adaptive", type=float, default=None, metavar="RTOL",
                     help="adaptive Genz-Malik cubature at this relative tolerance instead of the 12-point rule")
+    ap.add_argument("--surrogate", metavar="NET.npz", help="pixel means from this trained surrogate network "
+                    "(the 12-point rule where it does not apply)")
+    ap.add_argument("--train-surrogate", metavar="NET.npz", help="train a surrogate network on samples of this "
+                    "job's mean PSFs, save it here and use it")
+    ap.add_argument("--surrogate-samples", type=int, default=10_000_000)
+    ap.add_argument("--surrogate-epochs", type=int, default=20)
+    ap.add_argument("--check-tol", type=float, default=1e-4,
+                    help="surrogate maps whose check against the rule exceeds this are redone by the rule")
     ap.add_argument("--device", type=int, default=0)
     args = ap.parse_args(argv)
 
@@ -76,7 +86,10 @@ def main(argv=None) -> int:
     nf = A.normalize_rpsf(job.rpsf_front, job.scale_front)
     nb = A.normalize_rpsf(job.rpsf_back, job.scale_back)
     src = torch.as_tensor(job.src_sph, device=dev)
-    if args.adaptive is None:
+    use_sur = args.surrogate or args.train_surrogate
+    if args.adaptive is not None and use_sur:
+        ap.error("--adaptive and the surrogate options exclude each other")
+    if args.adaptive is None and not use_sur:
         cube = A.ExpCube(torch.as_tensor(job.exp_cube.cosbins, device=dev), job.exp_cube.nside,
                          job.exp_cube.nbrbins, job.exp_cube.cosmin, job.exp_cube.thetabin)
         wcube = A.ExpCube(torch.as_tensor(job.wexp_cube.cosbins, device=dev), job.wexp_cube.nside,
@@ -89,9 +102,29 @@ def main(argv=None) -> int:
                                 job.aeff_back, ltf)
         ps = A.compute_psf_data(nf, nb, ex, job.logEs, ltf)
         t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
-        maps, _ = A.point_src_model_map_wcs_adaptive(job.wcs, src, t(ex.exposure), t(ps.uPsf),
-                                                     t(ps.partial_psf_integral), rtol=args.adaptive,
-                                                     with_info=False)
+        if args.adaptive is not None:
+            maps, _ = A.point_src_model_map_wcs_adaptive(job.wcs, src, t(ex.exposure), t(ps.uPsf),
+                                                         t(ps.partial_psf_integral), rtol=args.adaptive,
+                                                         with_info=False)
+        else:
+            from .surrogate import Surrogate, samples
+
+            if args.train_surrogate:
+                X, Y = samples(t(ps.uPsf), job.logEs, args.surrogate_samples, seed=args.seed)
+                net = Surrogate(device=dev, seed=args.seed)
+                losses = net.train(X, Y, epochs=args.surrogate_epochs)
+                del X, Y
+                net.save(args.train_surrogate)
+                print(f"surrogate trained: {args.surrogate_samples} samples, {args.surrogate_epochs} epochs, "
+                      f"loss {losses[0]:.3e} -> {losses[-1]:.3e}, saved to {args.train_surrogate}")
+            else:
+                net = Surrogate.load(args.surrogate, device=dev)
+            maps, _, st = A.point_src_model_map_wcs_surrogate(job.wcs, src, t(ex.exposure), t(ps.uPsf),
+                                                              t(ps.partial_psf_integral), t(job.logEs), net,
+                                                              check_tol=args.check_tol, with_info=False)
+            print(f"surrogate: {st['accepted']} of {st['values']} values from the network, "
+                  f"{st['maps_fallback']} maps redone by the rule (largest check difference "
+                  f"{st['max_check_err']:.2e})")
     t1 = time.perf_counter()
     A.write_src_model(args.out, maps, names, args.bitpix)
     torch.cuda.synchronize(dev)
