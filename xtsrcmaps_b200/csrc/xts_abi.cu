@@ -687,7 +687,7 @@ static int mlp_ok(const xts_mlp* net, const char* who) {
 }
 
 static int* mlp_status_word(cudaStream_t st) {
-    int* status = (int*)workspace(W_MISC2, 64);
+    int* status = (int*)workspace(W_MLP_ST, 64);
     if (status && cudaMemsetAsync(status, 0, sizeof(int), st) != cudaSuccess) return nullptr;
     return status;
 }

@@ -554,11 +554,7 @@ int launch_gemm_bf16(const void* A, int a_trans, const void* B, int b_trans, int
                      int accumulate, int* status, cudaStream_t st) {
     if (M <= 0 || K <= 0 || M % MT || K % 64)
         return set_error(XTS_ERR_ARG, "gemm_bf16: M (%d) must be a multiple of 128 and K (%d) of 64", M, K);
-    static bool attr = false;
-    if (!attr) {
-        XTS_CUDA(cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM));
-        attr = true;
-    }
+    XTS_CUDA(cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM));
     const int mt = M / MT, nkc = K / 64;
     int nsplit = 1;
     if (accumulate) {  // spread the K chunks over about one wave of blocks
@@ -576,12 +572,9 @@ int launch_gemm_bf16(const void* A, int a_trans, const void* B, int b_trans, int
 
 static int forward(const xts_mlp* net, const float* X, long long n, float* y, FwdSaves sv, int* status,
                    cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        XTS_CUDA(cudaFuncSetAttribute(k_mlp_forward<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM));
-        XTS_CUDA(cudaFuncSetAttribute(k_mlp_forward<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM));
-        attr = true;
-    }
+    // per call: the attribute belongs to the current device's context
+    XTS_CUDA(cudaFuncSetAttribute(k_mlp_forward<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM));
+    XTS_CUDA(cudaFuncSetAttribute(k_mlp_forward<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM));
     const bool save = sv.z1 != nullptr;
     if (save && !(sv.z2 && sv.z3 && sv.h1 && sv.h2 && sv.yn)) return set_error(XTS_ERR_ARG, "mlp forward: saves");
     if (!save && !y) return set_error(XTS_ERR_ARG, "mlp forward: output");
