@@ -316,13 +316,15 @@ int xts_mlp_forward(const xts_mlp* net, const float* X, long long n, float* y, v
 
 /* Gradient of the loss L = (1/n) sum (y' - (Y - out_mu) / out_sd)^2 (y' the
  * standardised output) with respect to the FP32 parameters, grads
- * [XTS_MLP_NPARAM] (overwritten); loss [1] (may be NULL).  n a multiple of 128. */
+ * [XTS_MLP_NPARAM] (overwritten); loss [1] (may be NULL).  n a multiple of 128, at most
+ * 2^24 rows per call. */
 int xts_mlp_grads(const xts_mlp* net, const float* X, const float* Y, long long n, float* grads, float* loss,
                   void* stream);
 
 /* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on a batch: grads, adam_m,
  * adam_v [XTS_MLP_NPARAM] (grads zero on entry, left zero), step >= 1; the BF16
- * copies are refreshed.  loss [1] accumulates the batch loss (may be NULL). */
+ * copies are refreshed.  loss [1] accumulates the batch loss (may be NULL).  n as for
+ * xts_mlp_grads. */
 int xts_mlp_train_step(const xts_mlp* net, const float* X, const float* Y, long long n, float* grads,
                        float* adam_m, float* adam_v, int step, float lr, float* loss, void* stream);
 
