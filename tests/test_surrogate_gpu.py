@@ -181,3 +181,31 @@ def test_trained_network_gains_over_centre_value(api):
           f"fraction within 1e-4 {np.mean(err <= 1e-4):.4f}")
     assert 0 <= st["accepted"] <= st["values"] == m.size
     assert np.isfinite(m).all()
+
+
+def test_surrogate_argument_errors(api):
+    """Shapes and parameters the entry points reject with XTS_ERR_ARG (no launch)."""
+    import torch
+
+    from xtsrcmaps_b200 import _lib as L
+    from xtsrcmaps_b200.surrogate import Surrogate, gemm_bf16
+
+    d = torch.device("cuda")
+    a = torch.zeros((100, 128), dtype=torch.bfloat16, device=d)
+    b = torch.zeros((128, 128), dtype=torch.bfloat16, device=d)
+    with pytest.raises(L.XtsError) as ei:
+        gemm_bf16(a, b, 100, 128)  # M not a multiple of 128
+    assert ei.value.code == L.XTS_ERR_ARG
+    with pytest.raises(L.XtsError) as ei:
+        gemm_bf16(torch.zeros((128, 96), dtype=torch.bfloat16, device=d), b[:, :96], 128, 96)  # K % 64
+    assert ei.value.code == L.XTS_ERR_ARG
+    net = Surrogate(device=d, seed=0)
+    X = torch.zeros((200, 5), dtype=torch.float32, device=d)
+    Y = torch.zeros((200,), dtype=torch.float32, device=d)
+    with pytest.raises(L.XtsError) as ei:
+        net.gradient(X, Y)  # 200 rows: not a multiple of 128
+    assert ei.value.code == L.XTS_ERR_ARG
+    net.in_sd[2] = 0.0
+    with pytest.raises(L.XtsError) as ei:
+        net.predict(X)
+    assert ei.value.code == L.XTS_ERR_ARG
