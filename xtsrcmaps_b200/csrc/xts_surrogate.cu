@@ -189,29 +189,57 @@ struct SurPixS {
     double tt[12];
 };
 
+__device__ __forceinline__ bool sur_geo_ok(const SurPix& q, const SurRange& rg) {
+    return q.rho >= rg.rho_min && q.f0 >= rg.lo[0] && q.f0 <= rg.hi[0] && q.f1 >= rg.lo[1] && q.f1 <= rg.hi[1] &&
+           q.f2 >= rg.lo[2] && q.f2 <= rg.hi[2];
+}
+
+// Centre value and segment slope of one energy, and whether the network takes the value.
+__device__ __forceinline__ bool sur_value(const double* U, int E, int e, int ic, double tc, bool geo_ok,
+                                          float le, const SurRange& rg, double* uc, float* sl) {
+    const double lo = U[(size_t)(ic - 1) * E + e], hi = U[(size_t)ic * E + e];
+    const double slope = (lo > 0. && hi > 0.) ? log(hi / lo) * (1.0 / SEP_STEP) : 0.;
+    *uc = (1.0 - tc) * lo + tc * hi;
+    *sl = (float)slope;
+    return geo_ok && *uc > 0. && le >= rg.lo[3] && le <= rg.hi[3] && *sl >= rg.lo[4] && *sl <= rg.hi[4];
+}
+
+// Per block: SF_PIX pixels of one source of a chunk.  Phase 1, one thread per
+// pixel: the centre, the features that do not depend on energy and the 12 rule
+// points, into shared memory.  Pass 1, one thread per (pixel, energy) value in
+// the maps' order: whether the network takes the value (a bit in shared memory),
+// and for a value it does not, the rule's mean written to the map.  The block then
+// reserves room for its accepted values in the compacted network input with one
+// atomic, and pass 2 writes each accepted value's five features, aux = (u_c,
+// 1 / rho^2) and its chunk-relative value index there.
 __global__ void __launch_bounds__(SF_THREADS) k_sur_features(const double* __restrict__ corners,
                                                              const SrcInfo* __restrict__ info,
                                                              const double* __restrict__ upsf,
                                                              const double* __restrict__ logEs, int s0, int H, int W,
                                                              int E, SurRange rg, float* __restrict__ X,
-                                                             float2* __restrict__ aux, float* __restrict__ mean,
+                                                             float2* __restrict__ aux, unsigned* __restrict__ vidx,
+                                                             unsigned long long* __restrict__ n_acc,
+                                                             float* __restrict__ mean,
                                                              unsigned long long* __restrict__ accepted) {
     __shared__ SurPixS sp[SF_PIX];
-    const int s = s0 + blockIdx.y, t = threadIdx.x;
+    __shared__ unsigned okbits[SF_PIX * 256 / 32];  // one bit per (pixel, energy) value, E <= 256
+    __shared__ unsigned wsum[SF_THREADS / 32];
+    __shared__ unsigned long long base_s;
+    const int s = s0 + blockIdx.y, t = threadIdx.x, lane = t & 31, wp = t >> 5;
     const int npix = H * W, p0 = blockIdx.x * SF_PIX;
     const int np = min(SF_PIX, npix - p0);
+    const int nv = np * E;
+    for (int k = t; k < (nv + 31) / 32; k += SF_THREADS) okbits[k] = 0u;
     if (t < np) {
         const int pix = p0 + t, h = pix / W, w = pix - h * W;
         SurPix q;
-        const PixGeom g = pixel_geom(corners, W + 1, h, w, info[s]);
-        sur_pixel(g, q);
+        sur_pixel(pixel_geom(corners, W + 1, h, w, info[s]), q);
         SurPixS& o = sp[t];
         o.f0 = q.f0; o.f1 = q.f1; o.f2 = q.f2;
         o.eps = (float)(1.0 / (q.rho * q.rho));
         o.tc = q.tc;
         o.ic = q.ic;
-        o.geo_ok = q.rho >= rg.rho_min && q.f0 >= rg.lo[0] && q.f0 <= rg.hi[0] && q.f1 >= rg.lo[1] &&
-                   q.f1 <= rg.hi[1] && q.f2 >= rg.lo[2] && q.f2 <= rg.hi[2];
+        o.geo_ok = sur_geo_ok(q, rg);
 #pragma unroll
         for (int p = 0; p < 12; ++p) { o.idx[p] = (short)q.idx[p]; o.tt[p] = q.tt[p]; }
     }
@@ -219,46 +247,73 @@ __global__ void __launch_bounds__(SF_THREADS) k_sur_features(const double* __res
     const double* U = upsf + (size_t)s * ND * E;
     const size_t vb = ((size_t)blockIdx.y * npix + p0) * E;  // first value of the block (chunk-relative)
     const size_t mb = ((size_t)s * npix + p0) * E;           // the same value in the map
-    unsigned acc = 0;
-    for (int k = t; k < np * E; k += SF_THREADS) {
+    unsigned cnt = 0;
+    for (int k = t; k < nv; k += SF_THREADS) {
         const int lp = k / E, e = k - lp * E;
         const SurPixS& o = sp[lp];
-        const double lo = U[(size_t)(o.ic - 1) * E + e], hi = U[(size_t)o.ic * E + e];
-        const double slope = (lo > 0. && hi > 0.) ? log(hi / lo) * (1.0 / SEP_STEP) : 0.;
-        const double uc = (1.0 - o.tc) * lo + o.tc * hi;
-        const float le = (float)logEs[e], sl = (float)slope;
-        const bool ok = o.geo_ok && uc > 0. && le >= rg.lo[3] && le <= rg.hi[3] && sl >= rg.lo[4] && sl <= rg.hi[4];
-        float* x = X + (vb + k) * 5;
-        x[0] = o.f0; x[1] = o.f1; x[2] = o.f2; x[3] = le; x[4] = sl;
-        if (ok) {
-            aux[vb + k] = make_float2((float)uc, o.eps);
-            ++acc;
+        double uc;
+        float sl;
+        if (sur_value(U, E, e, o.ic, o.tc, o.geo_ok, (float)logEs[e], rg, &uc, &sl)) {
+            atomicOr(&okbits[k >> 5], 1u << (k & 31));
+            ++cnt;
         } else {
-            aux[vb + k] = make_float2(0.f, -1.f);
             double m = 0.;
 #pragma unroll
             for (int p = 0; p < 12; ++p) m += c_rule_uv[p][3] * sur_lerp(U, E, e, o.idx[p], o.tt[p]);
             mean[mb + k] = (float)m;
         }
     }
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if ((t & 31) == 0 && acc) atomicAdd(accepted + s, (unsigned long long)acc);
+    // exclusive scan of the per-thread counts; one reservation per block
+    unsigned inc = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned v = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += v;
+    }
+    if (lane == 31) wsum[wp] = inc;
+    __syncthreads();
+    unsigned before = 0, total = 0;
+    for (int w = 0; w < SF_THREADS / 32; ++w) {
+        before += w < wp ? wsum[w] : 0u;
+        total += wsum[w];
+    }
+    if (t == 0) {
+        base_s = total ? atomicAdd(n_acc, (unsigned long long)total) : 0ull;
+        if (total) atomicAdd(accepted + s, (unsigned long long)total);
+    }
+    __syncthreads();
+    unsigned long long j = base_s + before + (inc - cnt);
+    for (int k = t; k < nv; k += SF_THREADS) {
+        if (!((okbits[k >> 5] >> (k & 31)) & 1u)) continue;
+        const int lp = k / E, e = k - lp * E;
+        const SurPixS& o = sp[lp];
+        double uc;
+        float sl;
+        const float le = (float)logEs[e];
+        sur_value(U, E, e, o.ic, o.tc, o.geo_ok, le, rg, &uc, &sl);
+        float* x = X + j * 5;
+        x[0] = o.f0; x[1] = o.f1; x[2] = o.f2; x[3] = le; x[4] = sl;
+        aux[j] = make_float2((float)uc, o.eps);
+        vidx[j] = (unsigned)(vb + k);
+        ++j;
+    }
 }
 
-__global__ void k_sur_assemble(const float2* __restrict__ aux, const float* __restrict__ y, long long n,
-                               float* __restrict__ mean) {
-    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= n) return;
-    const float2 a = aux[v];
-    if (a.y >= 0.f) mean[v] = a.x * expf(y[v] * a.y);
+// The network's values into the map: row i of the compacted input is value vidx[i].
+__global__ void k_sur_assemble(const float2* __restrict__ aux, const unsigned* __restrict__ vidx,
+                               const float* __restrict__ y, long long n, float* __restrict__ mean) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float2 a = aux[i];
+    mean[vidx[i]] = a.x * expf(y[i] * a.y);
 }
 
 // The check: every SUR_CHECK_EVERY-th pixel of the chunk, all energies taken by
 // the network, against the rule; the largest relative difference per source.
 __global__ void __launch_bounds__(128) k_sur_check(const double* __restrict__ corners, const SrcInfo* __restrict__ info,
-                                                   const double* __restrict__ upsf, int s0, int H, int W, int E,
-                                                   const float2* __restrict__ aux, const float* __restrict__ mean,
-                                                   float* __restrict__ err, unsigned long long* __restrict__ counts) {
+                                                   const double* __restrict__ upsf, const double* __restrict__ logEs,
+                                                   int s0, int H, int W, int E, SurRange rg,
+                                                   const float* __restrict__ mean, float* __restrict__ err,
+                                                   unsigned long long* __restrict__ counts) {
     const int s = s0 + blockIdx.y, npix = H * W;
     const int pix = (blockIdx.x * blockDim.x + threadIdx.x) * SUR_CHECK_EVERY;
     float worst = 0.f;
@@ -267,10 +322,12 @@ __global__ void __launch_bounds__(128) k_sur_check(const double* __restrict__ co
         const int h = pix / W, w = pix - h * W;
         SurPix sp;
         sur_pixel(pixel_geom(corners, W + 1, h, w, info[s]), sp);
+        const bool geo_ok = sur_geo_ok(sp, rg);
         const double* U = upsf + (size_t)s * ND * E;
-        const size_t v0 = ((size_t)blockIdx.y * npix + pix) * E;
-        for (int e = 0; e < E; ++e) {
-            if (aux[v0 + e].y < 0.f) continue;
+        for (int e = 0; geo_ok && e < E; ++e) {
+            double uc;
+            float sl;
+            if (!sur_value(U, E, e, sp.ic, sp.tc, true, (float)logEs[e], rg, &uc, &sl)) continue;
             const double m = sur_rule(sp, U, E, e);
             const double got = mean[((size_t)s * npix + pix) * E + e];
             const float r = (float)(m != 0. ? fabs(got - m) / fabs(m) : fabs(got));
@@ -320,6 +377,8 @@ int launch_srcmap_surrogate(const SrcmapDev& a, const double* corners, const dou
     float* X = (float*)workspace(W_SUR_X, sizeof(float) * 5 * (size_t)nmax + 16);
     float2* aux = (float2*)workspace(W_SUR_AUX, sizeof(float2) * (size_t)nmax + 16);
     float* yv = (float*)workspace(W_SUR_Y, sizeof(float) * (size_t)nmax + 16);
+    unsigned* vidx = (unsigned*)workspace(W_SUR_IDX, sizeof(unsigned) * (size_t)nmax + 16);
+    if (!vidx) return XTS_ERR_OOM;
     // per source: largest check difference, values accepted; then the checked count,
     // the status word, and the list of sources redone by the rule
     const size_t o_cnt = align_up(sizeof(float) * S, 16), o_ctr = o_cnt + align_up(8 * (size_t)S, 16);
@@ -328,7 +387,7 @@ int launch_srcmap_surrogate(const SrcmapDev& a, const double* corners, const dou
     if (!X || !aux || !yv || !misc) return XTS_ERR_OOM;
     float* err = (float*)misc;
     unsigned long long* acc_d = (unsigned long long*)(misc + o_cnt);
-    unsigned long long* counts = (unsigned long long*)(misc + o_ctr);
+    unsigned long long* counts = (unsigned long long*)(misc + o_ctr);  // [0] checked, [1] compacted rows
     int* status = (int*)(counts + 4);
     int* list_d = (int*)(misc + o_list);
     XTS_CUDA(cudaMemsetAsync(misc, 0, o_list, st));
@@ -340,15 +399,24 @@ int launch_srcmap_surrogate(const SrcmapDev& a, const double* corners, const dou
         const int ns = S - s0 < sc ? S - s0 : sc;
         const long long n = per_src * ns;
         const dim3 gf((unsigned)((npix + SF_PIX - 1) / SF_PIX), (unsigned)ns);
-        XTS_LAUNCH("k_sur_features", st, k_sur_features<<<gf, SF_THREADS, 0, st>>>(corners, info, a.upsf, a.logEs, s0, H, W, E, rg,
-                                                                            X, aux, mean, acc_d));
-        if ((rc = launch_mlp_forward(net, X, n, yv, status, st))) return rc;
-        float* m0 = mean + (size_t)s0 * per_src;
-        XTS_LAUNCH("k_sur_assemble", st, k_sur_assemble<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(aux, yv, n, m0));
+        XTS_CUDA(cudaMemsetAsync(counts + 1, 0, sizeof(unsigned long long), st));
+        XTS_LAUNCH("k_sur_features", st, k_sur_features<<<gf, SF_THREADS, 0, st>>>(
+                                             corners, info, a.upsf, a.logEs, s0, H, W, E, rg, X, aux, vidx,
+                                             counts + 1, mean, acc_d));
+        unsigned long long n_acc = 0;  // rows of the compacted network input
+        XTS_CUDA(cudaMemcpyAsync(&n_acc, counts + 1, sizeof(n_acc), cudaMemcpyDeviceToHost, st));
+        XTS_CUDA(cudaStreamSynchronize(st));
+        if (n_acc > (unsigned long long)n) return set_error(XTS_ERR_CUDA, "surrogate map: compaction overflow");
+        if (n_acc) {
+            if ((rc = launch_mlp_forward(net, X, (long long)n_acc, yv, status, st))) return rc;
+            float* m0 = mean + (size_t)s0 * per_src;
+            XTS_LAUNCH("k_sur_assemble", st, k_sur_assemble<<<(unsigned)((n_acc + 255) / 256), 256, 0, st>>>(
+                                                 aux, vidx, yv, (long long)n_acc, m0));
+        }
         const long long nck = (npix + SUR_CHECK_EVERY - 1) / SUR_CHECK_EVERY;
         const dim3 gc((unsigned)((nck + 127) / 128), (unsigned)ns);
-        XTS_LAUNCH("k_sur_check", st, k_sur_check<<<gc, 128, 0, st>>>(corners, info, a.upsf, s0, H, W, E, aux, mean,
-                                                                      err, counts));
+        XTS_LAUNCH("k_sur_check", st, k_sur_check<<<gc, 128, 0, st>>>(corners, info, a.upsf, a.logEs, s0, H, W, E,
+                                                                      rg, mean, err, counts));
     }
     if ((rc = mlp_check_status(status, st))) return rc;
     std::vector<float> herr(S > 0 ? S : 1);
