@@ -550,12 +550,13 @@ def bench_surrogate(args, A, job, d, nf, nb, ltf, out, flush, stream, dev, n_val
     A.profile_enable(False)
     rel = ((out_s.double() - out.double()).abs() / out.double().abs().clamp_min(1e-300))
     fwd_ms = prof.get("k_mlp_forward", (0, 0.0))[1]
-    flop = 2 * (5 * 128 + 2 * 128 * 128 + 128) * n_values
+    rows = int(stats.get("evaluated", n_values))  # the network runs only on the values it may take
+    flop = 2 * (5 * 128 + 2 * 128 * 128 + 128) * rows
     return {"value": n_values * world / (ms_s * 1e-3), "unit": UNIT, "ms_per_step": ms_s, "steps": ks,
             "check_tol": 1e-4, "rho_min": net.rho_min, "stats": stats,
             "accepted_frac": stats.get("accepted", 0) / max(1, stats.get("values", 1)),
             "max_rel_err_vs_plain_map": float(rel.max()), "frac_within_1e-4_vs_plain_map": float((rel <= 1e-4).double().mean()),
-            "network_forward": {"ms": fwd_ms, "rows": n_values, "tflops": flop / (fwd_ms * 1e-3) / 1e12 if fwd_ms else None,
+            "network_forward": {"ms": fwd_ms, "rows": rows, "tflops": flop / (fwd_ms * 1e-3) / 1e12 if fwd_ms else None,
                                 "note": "67,072 FLOP per row (5-128-128-128-1); the two hidden layers on tcgen05"},
             "train": {"samples": args.surrogate_samples, "epochs": args.surrogate_epochs, "seconds": t_train,
                       "first_epoch_loss": losses[0], "final_loss": losses[-1],

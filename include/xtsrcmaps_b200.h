@@ -344,6 +344,7 @@ typedef struct xts_surrogate_stats {
     long long checked;       /* accepted values also evaluated by the 12-point rule */
     int maps_fallback;       /* sources whose check failed: all their values by the rule */
     float max_check_err;     /* largest relative difference seen by the check */
+    long long evaluated;     /* rows the network evaluated (before the check) */
 } xts_surrogate_stats;
 
 /* The model map of xts_point_src_model_map_wcs with the pixel means taken from

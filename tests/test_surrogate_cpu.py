@@ -60,8 +60,9 @@ def test_struct_layouts_match_the_header():
 #include <stddef.h>
 #include "xtsrcmaps_b200.h"
 int main(void) {
-    printf("%zu %zu %zu %zu %zu %zu\n", sizeof(xts_mlp), offsetof(xts_mlp, in_mu), offsetof(xts_mlp, out_mu),
-           offsetof(xts_mlp, lo), offsetof(xts_mlp, rho_min), sizeof(xts_surrogate_stats));
+    printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(xts_mlp), offsetof(xts_mlp, in_mu), offsetof(xts_mlp, out_mu),
+           offsetof(xts_mlp, lo), offsetof(xts_mlp, rho_min), sizeof(xts_surrogate_stats),
+           offsetof(xts_surrogate_stats, evaluated));
     printf("%d %d %d %d\n", XTS_MLP_W2, XTS_MLP_W3, XTS_MLP_B4, XTS_MLP_NPARAM);
     return 0;
 }
@@ -74,7 +75,7 @@ int main(void) {
         out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split("\n")
     sizes = [int(v) for v in out[0].split()]
     assert sizes == [C.sizeof(L.XtsMlp), L.XtsMlp.in_mu.offset, L.XtsMlp.out_mu.offset, L.XtsMlp.lo.offset,
-                     L.XtsMlp.rho_min.offset, C.sizeof(L.XtsSurrogateStats)]
+                     L.XtsMlp.rho_min.offset, C.sizeof(L.XtsSurrogateStats), L.XtsSurrogateStats.evaluated.offset]
     consts = [int(v) for v in out[1].split()]
     assert consts == [L.MLP_W2, L.MLP_W3, L.MLP_B4, L.MLP_NPARAM] == [MO.W2, MO.W3, MO.B4, MO.NPARAM]
 

@@ -97,7 +97,7 @@ class XtsMlp(C.Structure):
 class XtsSurrogateStats(C.Structure):
     _fields_ = [
         ("values", C.c_longlong), ("accepted", C.c_longlong), ("checked", C.c_longlong),
-        ("maps_fallback", C.c_int), ("max_check_err", C.c_float),
+        ("maps_fallback", C.c_int), ("max_check_err", C.c_float), ("evaluated", C.c_longlong),
     ]
 
 

@@ -428,9 +428,10 @@ int launch_srcmap_surrogate(const SrcmapDev& a, const double* corners, const dou
     XTS_CUDA(cudaStreamSynchronize(st));
     std::vector<int> list;
     float worst = 0.f;
-    long long accepted = 0;
+    long long accepted = 0, evaluated = 0;
     for (int s = 0; s < S; ++s) {
         worst = herr[s] > worst ? herr[s] : worst;
+        evaluated += (long long)hacc[s];
         if (!(herr[s] <= (float)a.check_tol)) list.push_back(s);
         else accepted += (long long)hacc[s];
     }
@@ -445,6 +446,7 @@ int launch_srcmap_surrogate(const SrcmapDev& a, const double* corners, const dou
         a.sur_stats->checked = (long long)hc;
         a.sur_stats->maps_fallback = (int)list.size();
         a.sur_stats->max_check_err = worst;
+        a.sur_stats->evaluated = evaluated;
     }
     return finish_mean_map(a, centers, omega, info, scale, nch, st);
 }

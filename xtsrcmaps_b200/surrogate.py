@@ -240,5 +240,5 @@ def model_map(wcs, src_sph, exposure, uPsf, partial_integrals, logEs, net: Surro
         C.byref(w), _ptr(src), S, _ptr(ex), _ptr(up), _ptr(pp), _ptr(le), E, C.byref(s), float(check_tol),
         _ptr(maps), C.byref(info_s) if info_s is not None else None, C.byref(st), _stream(dev)))
     stats = {"values": st.values, "accepted": st.accepted, "checked": st.checked,
-             "maps_fallback": st.maps_fallback, "max_check_err": st.max_check_err}
+             "maps_fallback": st.maps_fallback, "max_check_err": st.max_check_err, "evaluated": st.evaluated}
     return maps, info, stats
