@@ -17,6 +17,14 @@
 //     of convolve_pixel_psf_logsep.hpp:39-55, keys fixed).
 // The network's target is y = ln(m / u_c) rho^2; a value is m = u_c exp(y / rho^2).
 // All of this is FP64 up to the network's FP32 input.
+//
+// The map, per chunk of sources: k_sur_features writes the rule's mean for every
+// value the network may not take (rho < rho_min or a feature outside the training
+// range) and the features of the others, compacted; the network runs on the
+// compacted rows only; k_sur_assemble scatters its values into the map; k_sur_check
+// re-evaluates every 61st pixel by the rule.  Sources whose check fails are redone
+// by k_sur_fallback, and the map integral, correction and scalings follow as for
+// the adaptive map.
 #include <vector>
 
 #include "xts_point.cuh"
