@@ -209,3 +209,22 @@ def test_surrogate_argument_errors(api):
     with pytest.raises(L.XtsError) as ei:
         net.predict(X)
     assert ei.value.code == L.XTS_ERR_ARG
+
+
+def test_training_is_reproducible(api):
+    """Gradient sums run in a fixed order (split-K partials and per-block partials
+    reduced in order, no atomics), so two trainings from the same start agree bit
+    for bit."""
+    import torch
+
+    from xtsrcmaps_b200.surrogate import Surrogate, samples
+
+    job, upsf, _, _ = _psf_tables(api, "c1", seed=10, n=3)
+    X, Y = samples(upsf, job.logEs, 128 * 148 * 2 * 3, seed=5)
+    out = []
+    for _ in range(2):
+        net = Surrogate(device=upsf.device, seed=3)
+        net.train(X, Y, epochs=2, seed=1)
+        torch.cuda.synchronize()
+        out.append(net.params.cpu().numpy())
+    np.testing.assert_array_equal(out[0], out[1])

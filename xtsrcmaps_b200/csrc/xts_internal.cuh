@@ -65,7 +65,7 @@ enum Slot {
     W_CORNERS, W_CENTERS, W_OMEGA, W_LUT, W_PARTSUM, W_SRCINFO, W_SCALE, W_PSFTAB,
     W_KING, W_MISC, W_WIN, W_WMETA, W_SPARSE, W_MISC2, W_EXPMAP,
     W_FITS_IN, W_FITS_OUT, W_FITS_SUM, W_FFT_A, W_FFT_B, W_FFT_C, W_FFT_WORK, W_SRCPIX,
-    W_MLP_Z, W_MLP_H, W_MLP_DZ, W_MLP_DH, W_MLP_Y, W_MLP_ST, W_SUR_X, W_SUR_AUX, W_SUR_Y, W_SUR_IDX, W_SUR_ERR,
+    W_MLP_Z, W_MLP_H, W_MLP_DZ, W_MLP_DH, W_MLP_Y, W_MLP_ST, W_MLP_PART, W_MLP_PART2, W_SUR_X, W_SUR_AUX, W_SUR_Y, W_SUR_IDX, W_SUR_ERR,
     N_SLOTS
 };
 void* workspace(int slot, size_t bytes);  // nullptr + error set on OOM

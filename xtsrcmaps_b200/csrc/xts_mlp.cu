@@ -20,11 +20,12 @@
 //     transposed ([128][n], coalesced across the threads of a warp).
 //   * k_gemm_bf16: C = A B^T for the backward pass (dW = dZ^T H, dH = dZ W), with
 //     either operand given transposed (gathered into the swizzled layout by the
-//     loading threads), a two-stage shared-memory ring and split-K with atomic
-//     FP32 accumulation.
+//     loading threads), a two-stage shared-memory ring and split-K whose partial
+//     tiles are summed in a fixed order (k_sum_splits), so training is
+//     reproducible.
 //   * k_mlp_bwd_elem: dZ = dH * gelu'(Z) per layer in the [unit][row] layout, with
 //     the bias (and output-layer and first-layer weight) gradients reduced per
-//     block and added atomically.
+//     block into partials that k_bwd_reduce sums in a fixed order.
 //   * k_mlp_adam: the update of the FP32 master parameters and the BF16 copies.
 //
 // Every mbarrier wait is bounded (WAIT_LIMIT polls); a timeout sets the status
@@ -426,12 +427,10 @@ k_gemm_bf16(const __nv_bfloat16* __restrict__ A, int a_trans, const __nv_bfloat1
         for (int c0 = 0; c0 < MH; c0 += 16) {
             float v[16];
             tmem_ld16(trow + (unsigned)c0, v);
+            float* Cs = atomic ? C + (size_t)blockIdx.y * M * MH : C;  // split-K: this split's partial tile
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                float* dst = c_trans ? C + (size_t)(c0 + j) * M + m : C + (size_t)m * MH + c0 + j;
-                if (atomic) atomicAdd(dst, v[j]);
-                else *dst = v[j];
-            }
+            for (int j = 0; j < 16; ++j)
+                *(c_trans ? Cs + (size_t)(c0 + j) * M + m : Cs + (size_t)m * MH + c0 + j) = v[j];
         }
     } else if (t == 0) {
         atomicExch(status, 1);
@@ -455,8 +454,8 @@ __global__ void __launch_bounds__(256) k_mlp_bwd_elem(int mode, const float* __r
                                                       const float* __restrict__ zT, const float* __restrict__ dhT,
                                                       const float* __restrict__ yn, const float* __restrict__ Y,
                                                       const float* __restrict__ X, long long n,
-                                                      __nv_bfloat16* __restrict__ dzT, float* __restrict__ grads,
-                                                      float* __restrict__ loss) {
+                                                      __nv_bfloat16* __restrict__ dzT,
+                                                      float* __restrict__ part) {
     __shared__ float red[8][8];
     const int j = blockIdx.y, t = threadIdx.x, lane = t & 31, wp = t >> 5;
     const float w4 = __bfloat162float(__float2bfloat16_rn(params[XTS_MLP_W4 + j]));
@@ -499,19 +498,39 @@ __global__ void __launch_bounds__(256) k_mlp_bwd_elem(int mode, const float* __r
     if (t < 8) {
         float v = 0.f;
         for (int w = 0; w < 8; ++w) v += red[w][t];
-        const int q = t;
-        if (mode == BW_HEAD) {
-            if (q == 0) atomicAdd(grads + XTS_MLP_B3 + j, v);
-            if (q == 1) atomicAdd(grads + XTS_MLP_W4 + j, v);
-            if (j == 0 && q == 2 && loss) atomicAdd(loss, v * inv_n);
-            if (j == 0 && q == 3) atomicAdd(grads + XTS_MLP_B4, v);
-        } else if (mode == BW_HIDDEN) {
-            if (q == 0) atomicAdd(grads + XTS_MLP_B2 + j, v);
-        } else {
-            if (q == 0) atomicAdd(grads + XTS_MLP_B1 + j, v);
-            if (q >= 3) atomicAdd(grads + XTS_MLP_W1 + j * MI + (q - 3), v);
-        }
+        part[((size_t)blockIdx.x * MH + j) * 8 + t] = v;
     }
+}
+
+// The per-block partials of k_mlp_bwd_elem summed over the row blocks in order and
+// added to the gradient (and the loss); one thread per (unit, quantity).
+__global__ void k_bwd_reduce(int mode, const float* __restrict__ part, int nbx, float inv_n,
+                             float* __restrict__ grads, float* __restrict__ loss) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= MH * 8) return;
+    const int j = i >> 3, q = i & 7;
+    float v = 0.f;
+    for (int b = 0; b < nbx; ++b) v += part[((size_t)b * MH + j) * 8 + q];
+    if (mode == BW_HEAD) {
+        if (q == 0) grads[XTS_MLP_B3 + j] += v;
+        if (q == 1) grads[XTS_MLP_W4 + j] += v;
+        if (j == 0 && q == 2 && loss) *loss += v * inv_n;
+        if (j == 0 && q == 3) grads[XTS_MLP_B4] += v;
+    } else if (mode == BW_HIDDEN) {
+        if (q == 0) grads[XTS_MLP_B2 + j] += v;
+    } else {
+        if (q == 0) grads[XTS_MLP_B1 + j] += v;
+        if (q >= 3 && q < 3 + MI) grads[XTS_MLP_W1 + j * MI + (q - 3)] += v;
+    }
+}
+
+// C[i] += sum over the splits s (in order) of part[s][i]
+__global__ void k_sum_splits(const float* __restrict__ part, int nsplit, long long n, float* __restrict__ C) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float v = 0.f;
+    for (int s = 0; s < nsplit; ++s) v += part[(size_t)s * n + i];
+    C[i] += v;
 }
 
 // Adam on the FP32 master parameters; the BF16 copies of W2 and W3 follow.
@@ -564,9 +583,17 @@ int launch_gemm_bf16(const void* A, int a_trans, const void* B, int b_trans, int
     const int cps = (nkc + nsplit - 1) / nsplit;
     nsplit = (nkc + cps - 1) / cps;
     if (!accumulate && nsplit != 1) return set_error(XTS_ERR_ARG, "gemm_bf16: internal split");
+    float* dst = C;
+    const long long nc = (long long)M * MH;
+    if (accumulate) {  // partial tiles per split, summed in a fixed order below
+        dst = (float*)workspace(W_MLP_PART, sizeof(float) * (size_t)nsplit * nc);
+        if (!dst) return XTS_ERR_OOM;
+    }
     XTS_LAUNCH("k_gemm_bf16", st, k_gemm_bf16<<<dim3(mt, nsplit), MT, GEMM_SMEM, st>>>(
                                       (const __nv_bfloat16*)A, a_trans, (const __nv_bfloat16*)B, b_trans, M, K, cps,
-                                      C, c_trans, accumulate, status));
+                                      dst, c_trans, accumulate, status));
+    if (accumulate)
+        XTS_LAUNCH("k_sum_splits", st, k_sum_splits<<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(dst, nsplit, nc, C));
     return XTS_OK;
 }
 
@@ -612,22 +639,32 @@ static int mlp_backprop(const xts_mlp* net, const float* X, const float* Y, long
     int rc = forward(net, X, n, nullptr, sv, status, st);
     if (rc) return rc;
     const MlpNorm nm = mlp_norm(net);
-    const dim3 eg((unsigned)((n + BW_ROWS - 1) / BW_ROWS), MH);
+    const int nbx = (int)((n + BW_ROWS - 1) / BW_ROWS);
+    const dim3 eg((unsigned)nbx, MH);
+    const float inv_n = 1.f / (float)n;
+    float* part = (float*)workspace(W_MLP_PART2, sizeof(float) * (size_t)nbx * MH * 8);
+    if (!part) return XTS_ERR_OOM;
     const __nv_bfloat16* w2 = (const __nv_bfloat16*)net->wbf16;
     const __nv_bfloat16* w3 = w2 + MH * MH;
     // head: dz3 = dy w4 gelu'(z3); dW3 = dz3^T h2; dh2 = dz3 W3
     XTS_LAUNCH("k_mlp_bwd", st, k_mlp_bwd_elem<<<eg, 256, 0, st>>>(BW_HEAD, net->params, nm, sv.z3, nullptr, yn, Y,
-                                                                     X, n, dz, grads, loss));
+                                                                     X, n, dz, part));
+    XTS_LAUNCH("k_bwd_reduce", st, k_bwd_reduce<<<(MH * 8 + 255) / 256, 256, 0, st>>>(BW_HEAD, part, nbx, inv_n,
+                                                                                      grads, loss));
     if ((rc = launch_gemm_bf16(dz, 0, sv.h2, 0, MH, (int)n, grads + XTS_MLP_W3, 0, 1, status, st))) return rc;
     if ((rc = launch_gemm_bf16(dz, 1, w3, 1, (int)n, MH, dh, 1, 0, status, st))) return rc;
     // layer 2: dz2 = dh2 gelu'(z2); dW2 = dz2^T h1; dh1 = dz2 W2
     XTS_LAUNCH("k_mlp_bwd", st, k_mlp_bwd_elem<<<eg, 256, 0, st>>>(BW_HIDDEN, net->params, nm, sv.z2, dh, yn, Y, X,
-                                                                     n, dz, grads, loss));
+                                                                     n, dz, part));
+    XTS_LAUNCH("k_bwd_reduce", st, k_bwd_reduce<<<(MH * 8 + 255) / 256, 256, 0, st>>>(BW_HIDDEN, part, nbx, inv_n,
+                                                                                      grads, loss));
     if ((rc = launch_gemm_bf16(dz, 0, sv.h1, 0, MH, (int)n, grads + XTS_MLP_W2, 0, 1, status, st))) return rc;
     if ((rc = launch_gemm_bf16(dz, 1, w2, 1, (int)n, MH, dh, 1, 0, status, st))) return rc;
     // layer 1: dz1 = dh1 gelu'(z1); dW1 = dz1^T x
     XTS_LAUNCH("k_mlp_bwd", st, k_mlp_bwd_elem<<<eg, 256, 0, st>>>(BW_FIRST, net->params, nm, sv.z1, dh, yn, Y, X,
-                                                                     n, dz, grads, loss));
+                                                                     n, dz, part));
+    XTS_LAUNCH("k_bwd_reduce", st, k_bwd_reduce<<<(MH * 8 + 255) / 256, 256, 0, st>>>(BW_FIRST, part, nbx, inv_n,
+                                                                                      grads, loss));
     return XTS_OK;
 }
 
