@@ -88,10 +88,15 @@ __device__ __forceinline__ double sur_rule(const SurPix& sp, const double* U, in
     return m;
 }
 
+// log slope ln(hi / lo) / step of a table segment, in FP32 (a network input)
+__device__ __forceinline__ float sur_slope(double lo, double hi) {
+    return (lo > 0. && hi > 0.) ? logf((float)hi / (float)lo) * (float)(1.0 / SEP_STEP) : 0.f;
+}
+
 // centre value and the log slope of its table segment at energy e
 __device__ __forceinline__ double sur_centre(const SurPix& sp, const double* U, int E, int e, double* slope) {
     const double lo = U[(size_t)(sp.ic - 1) * E + e], hi = U[(size_t)sp.ic * E + e];
-    *slope = (lo > 0. && hi > 0.) ? log(hi / lo) * (1.0 / SEP_STEP) : 0.;
+    *slope = sur_slope(lo, hi);
     return (1.0 - sp.tc) * lo + sp.tc * hi;
 }
 
@@ -206,9 +211,8 @@ __device__ __forceinline__ bool sur_geo_ok(const SurPix& q, const SurRange& rg) 
 __device__ __forceinline__ bool sur_value(const double* U, int E, int e, int ic, double tc, bool geo_ok,
                                           float le, const SurRange& rg, double* uc, float* sl) {
     const double lo = U[(size_t)(ic - 1) * E + e], hi = U[(size_t)ic * E + e];
-    const double slope = (lo > 0. && hi > 0.) ? log(hi / lo) * (1.0 / SEP_STEP) : 0.;
     *uc = (1.0 - tc) * lo + tc * hi;
-    *sl = (float)slope;
+    *sl = sur_slope(lo, hi);
     return geo_ok && *uc > 0. && le >= rg.lo[3] && le <= rg.hi[3] && *sl >= rg.lo[4] && *sl <= rg.hi[4];
 }
 
