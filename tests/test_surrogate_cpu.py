@@ -129,3 +129,18 @@ def test_surrogate_state_round_trip(tmp_path):
     assert (back.out_mu, back.out_sd, back.rho_min) == (net.out_mu, net.out_sd, 50.0)
     s = back.struct()
     assert abs(s.rho_min - 50.0) < 1e-6 and list(s.in_sd) == pytest.approx(list(net.in_sd))
+
+
+def test_cli_and_bench_expose_the_surrogate():
+    """The command line and the bench carry the surrogate's options (host side only)."""
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-m", "xtsrcmaps_b200", "--help"], cwd=root, capture_output=True,
+                         text=True, check=True).stdout
+    for opt in ("--surrogate", "--train-surrogate", "--surrogate-samples", "--check-tol"):
+        assert opt in out, opt
+    out = subprocess.run([sys.executable, "bench.py", "--help"], cwd=root, capture_output=True, text=True,
+                         check=True).stdout
+    for opt in ("--no-surrogate", "--surrogate-samples", "--surrogate-epochs"):
+        assert opt in out, opt
