@@ -182,11 +182,13 @@ int xts_compute_psf_data(const xts_grid* psf_front, const xts_grid* psf_back,
  * device, without xts_init.  The King and psf*aeff scratch tables live in one
  * fixed 8 MiB device array that the library holds on every GPU that loads it
  * until the process exits: shapes needing more than XTS_NOALLOC_SCRATCH_DOUBLES
- * doubles, 401 * (Mc*Me front + Mc*Me back) + C * 401 * E (+ up to 31 of
- * padding), fail with XTS_ERR_ARG and launch nothing.  All calls share that
+ * doubles, 401 * (Mc*Me front + Mc*Me back) rounded up to a multiple of 32, plus
+ * C * 401 * E, fail with XTS_ERR_ARG and launch nothing.  All calls share that
  * array and the last call's contents stay in it; calls that overlap on the GPU
  * race on it, so order them on one stream.  The first call on a device looks the
- * array up (cudaGetSymbolAddress) and must come before any stream capture. */
+ * array up (cudaGetSymbolAddress) and must come before any stream capture (on a
+ * capturing stream it is refused with XTS_ERR_ARG); the looked-up address is not
+ * valid after cudaDeviceReset. */
 #define XTS_NOALLOC_SCRATCH_DOUBLES (1u << 20)
 int xts_compute_psf_data_noalloc(const xts_grid* psf_front, const xts_grid* psf_back,
                                  const double* exp_costhetas, int C, const double* logEs,
@@ -268,6 +270,48 @@ int xts_make_psf_kernel(const xts_wcs* kernel_wcs, int Nk, const double* upsf, i
 int xts_convolve_map_psf(const double* image, int E, int H, int W, const double* kernel, int K, double* out,
                          unsigned flags, void* stream);
 
+/* rebin_wcs_config (sky_geom/sky_geom.hxx:352-371, through rebin_skygeom :373-377), a
+ * step of the diffuse-source map: the WCS of the same region at pixel size
+ * target_pix_size (deg): CDELTn = +-target with the input's signs, NAXISn =
+ * round(NAXISn * |CDELTn_in| / target), CRPIXn scaled by the same factor, the
+ * rest unchanged.  The reference stores CRPIX2 into CDELT2 (:367); this writes the
+ * rebinned CDELT2.  Host function (no device work). */
+int xts_rebin_wcs(const xts_wcs* in, double target_pix_size, xts_wcs* out);
+
+/* The all-sky pixel range of fits::read_allsky_cropped
+ * (fits/fits.read_allsky_cropped.cpp:150-194): the ROI pixels (1, 1) and (NAXIS1,
+ * NAXIS2) through the ROI WCS, longitude wrapped into [0, 360) and latitude clamped,
+ * then through the all-sky WCS, rounded and bounded to [1, NAXISn].  range =
+ * {x_first, x_last, y_first, y_last}, 1-based and inclusive (first = min, last =
+ * max, as the reference).  Host function. */
+int xts_allsky_crop_range(const xts_wcs* allsky_wcs, const xts_wcs* roi_wcs, long range[4]);
+
+/* The block of an all-sky cube allsky [E0][NY][NX] (NAXIS1 = NX fastest) inside
+ * range: out [E0][ny][nx], ny = y_last - y_first + 1, nx = x_last - x_first + 1, or,
+ * for x_first > x_last, the columns x_first..NX then 1..x_last across the image's
+ * longitude seam (what readSegmentsAcrossBoundary, fits.read_allsky_cropped.cpp:119-147,
+ * is written for).  FP32 as the FITS image. */
+int xts_crop_allsky(const float* allsky, int E0, long NY, long NX, const long range[4], float* out,
+                    unsigned flags, void* stream);
+
+/* Fermi::math::trilerpEHW (math/trilerp.hpp:7-59): trilinear resampling of src
+ * [E0][H0][W0] onto dst [E1][H1][W1] with corner-aligned axes (scale (n0 - 1) /
+ * (n1 - 1); 0 where n1 = 1, which the reference divides by), FP32 arithmetic in the
+ * reference's order (h, then w, then e). */
+int xts_trilerp_ehw(const float* src, int E0, int H0, int W0, float* dst, int E1, int H1, int W1,
+                    unsigned flags, void* stream);
+
+/* The final scalings of ModelMap::diffuse_src_model_map_wcs
+ * (model_map/model_map.diffuse_src_model_map_wcs.cxx:76-95), which are those of
+ * point_src_model_map_wcs after its cubature (model_map.point_src_model_map_wcs.cxx:24-42):
+ * model_map [S, H, W, E] float holds pixel means on entry; on return
+ * mean * solid angle * exposure * correction, with the map integral over the
+ * pixels whose centre lies within each source's boundary radius (c6, c7) and the
+ * containment correction (c9) as the point-source path computes them. */
+int xts_scale_model_map(const xts_wcs* wcs, const double* src_sph, int S, const double* exposure,
+                        const double* upsf, const double* partial, int E, float* model_map,
+                        xts_srcmap_info* info, unsigned flags, void* stream);
+
 /* Learned surrogate of the pixel cubature ---------------------------------------
  * No counterpart in the reference.  A multilayer perceptron 5 -> 128 -> 128 ->
  * 128 -> 1 with tanh-form GELU after each hidden layer maps five features of a
@@ -294,6 +338,8 @@ int xts_convolve_map_psf(const double* image, int E, int H, int W, const double*
 #define XTS_MLP_W4 (XTS_MLP_B3 + XTS_MLP_HID)                /* [128] */
 #define XTS_MLP_B4 (XTS_MLP_W4 + XTS_MLP_HID)                /* [1] */
 #define XTS_MLP_NPARAM (XTS_MLP_B4 + 1)
+#define XTS_MLP_CELL_NR 32
+#define XTS_MLP_CELL_NS 16
 
 typedef struct xts_mlp {
     float* params;          /* [XTS_MLP_NPARAM] FP32 master parameters (device) */
@@ -302,6 +348,14 @@ typedef struct xts_mlp {
     float out_mu, out_sd;                       /* target standardisation */
     float lo[XTS_MLP_IN], hi[XTS_MLP_IN];       /* accepted feature range (the training range) */
     float rho_min;          /* centres closer than rho_min pixel sizes take the 12-point rule */
+    /* Error cells: feature 0 (log10 rho) in XTS_MLP_CELL_NR bins over [cell_lo[0], cell_hi[0]]
+     * times feature 4 (segment log slope) in XTS_MLP_CELL_NS bins over [cell_lo[1], cell_hi[1]].
+     * cell_ok (device, [XTS_MLP_CELL_NR * XTS_MLP_CELL_NS]) holds 1 in cell i * XTS_MLP_CELL_NS + j
+     * where the network's largest relative error on held-out samples of that cell stayed
+     * within the bound it was calibrated for; the network takes a value only in such a
+     * cell.  NULL: no cell restriction. */
+    float cell_lo[2], cell_hi[2];
+    const unsigned char* cell_ok;
 } xts_mlp;
 
 /* C = A B^T in FP32 from BF16 operands on tcgen05: A [M][K] (a_trans: stored
@@ -340,8 +394,8 @@ int xts_surrogate_samples(const double* upsf, const double* logEs, int S, int E,
 /* Counts of a surrogate model map. */
 typedef struct xts_surrogate_stats {
     long long values;        /* S * H * W * E */
-    long long accepted;      /* values taken from the network */
-    long long checked;       /* accepted values also evaluated by the 12-point rule */
+    long long accepted;      /* values served by the network (maps that passed the check, checked pixels excluded) */
+    long long checked;       /* values the network took in the checked pixels, replaced there by the 12-point rule */
     int maps_fallback;       /* sources whose check failed: all their values by the rule */
     float max_check_err;     /* largest relative difference seen by the check */
     long long evaluated;     /* rows the network evaluated (before the check) */
@@ -349,17 +403,27 @@ typedef struct xts_surrogate_stats {
 
 /* The model map of xts_point_src_model_map_wcs with the pixel means taken from
  * the network wherever the centre lies at least rho_min pixel sizes from the
- * source and every feature is inside [lo, hi]; the other values take the FP64
- * 12-point rule.  Every 61st pixel's accepted values are also evaluated by the
- * rule; a source whose largest relative difference exceeds check_tol is redone
- * entirely by the rule.  Map integral, correction and scalings as
- * xts_point_src_model_map_wcs.  Device pointers; model_map float [S, H, W, E]. */
+ * source, every feature is inside [lo, hi] and the value's error cell is marked
+ * cell_ok; the other values take the FP64 12-point rule.  Every 16th pixel is
+ * also evaluated by the rule, which replaces the network's values there; a
+ * source whose largest relative difference on those pixels exceeds check_tol is
+ * redone entirely by the rule.  Map integral, correction and scalings as
+ * xts_point_src_model_map_wcs.  Device pointers; model_map float [S, H, W, E].
+ * With stats NULL the call neither synchronises nor allocates once its buffers
+ * have grown (it can be captured into a CUDA graph); xts_surrogate_last_stats
+ * then gives the counts of the latest call, and with stats given they are
+ * filled before the call returns. */
 int xts_point_src_model_map_wcs_surrogate(const xts_wcs* wcs, const double* src_sph, int S,
                                           const double* exposure, const double* upsf,
                                           const double* partial, const double* logEs, int E,
                                           const xts_mlp* net,
                                           double check_tol, float* model_map, xts_srcmap_info* info,
                                           xts_surrogate_stats* stats, void* stream);
+
+/* Counts of the latest xts_point_src_model_map_wcs_surrogate call on the
+ * library's device (waits for that call's work on `stream`); XTS_ERR_TIMEOUT if
+ * one of its bounded tensor-core waits gave up. */
+int xts_surrogate_last_stats(xts_surrogate_stats* stats, void* stream);
 
 #ifdef __cplusplus
 }

@@ -3,7 +3,7 @@
 # units, compiled in place from the reference tree, plus oracle/ref_driver.cxx.
 # TEST INFRASTRUCTURE ONLY (CPU checker and timed CPU reference arm).
 #
-#   oracle/build_ref.sh [REFERENCE_ROOT]      (default /root/reference)
+#   oracle/build_ref.sh [REFERENCE_ROOT]      (default $XTS_REFERENCE, else /root/reference)
 #
 # Include order: oracle/ref_overlay (SkyGeom stand-in, cblas.h), then
 # oracle/_ref/patched (a build-time copy of
@@ -11,7 +11,7 @@
 # statement `keys[index] = psfidx;` added after the weight accumulation), then
 # the reference tree.  Outputs go to oracle/_ref only.
 set -e
-REF=${1:-/root/reference}
+REF=${1:-${XTS_REFERENCE:-/root/reference}}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT=$HERE/_ref
 LOGSEP=xtsrcmaps/model_map/mm_cubature/convolve_pixel_psf_logsep.hpp

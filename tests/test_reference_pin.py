@@ -19,7 +19,7 @@ def ref_lib():
     from oracle import oracle_ref as R
 
     if not R.available():
-        src = "/root/reference"
+        src = os.environ.get("XTS_REFERENCE", "/root/reference")
         if not os.path.isdir(src):
             pytest.skip("oracle/_ref not built and the reference tree is absent")
         import subprocess

@@ -60,10 +60,12 @@ def test_struct_layouts_match_the_header():
 #include <stddef.h>
 #include "xtsrcmaps_b200.h"
 int main(void) {
-    printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(xts_mlp), offsetof(xts_mlp, in_mu), offsetof(xts_mlp, out_mu),
-           offsetof(xts_mlp, lo), offsetof(xts_mlp, rho_min), sizeof(xts_surrogate_stats),
-           offsetof(xts_surrogate_stats, evaluated));
-    printf("%d %d %d %d\n", XTS_MLP_W2, XTS_MLP_W3, XTS_MLP_B4, XTS_MLP_NPARAM);
+    printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(xts_mlp), offsetof(xts_mlp, in_mu),
+           offsetof(xts_mlp, out_mu), offsetof(xts_mlp, lo), offsetof(xts_mlp, rho_min),
+           offsetof(xts_mlp, cell_lo), offsetof(xts_mlp, cell_hi), offsetof(xts_mlp, cell_ok),
+           sizeof(xts_surrogate_stats), offsetof(xts_surrogate_stats, evaluated));
+    printf("%d %d %d %d %d %d\n", XTS_MLP_W2, XTS_MLP_W3, XTS_MLP_B4, XTS_MLP_NPARAM, XTS_MLP_CELL_NR,
+           XTS_MLP_CELL_NS);
     return 0;
 }
 '''
@@ -75,9 +77,11 @@ int main(void) {
         out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split("\n")
     sizes = [int(v) for v in out[0].split()]
     assert sizes == [C.sizeof(L.XtsMlp), L.XtsMlp.in_mu.offset, L.XtsMlp.out_mu.offset, L.XtsMlp.lo.offset,
-                     L.XtsMlp.rho_min.offset, C.sizeof(L.XtsSurrogateStats), L.XtsSurrogateStats.evaluated.offset]
+                     L.XtsMlp.rho_min.offset, L.XtsMlp.cell_lo.offset, L.XtsMlp.cell_hi.offset,
+                     L.XtsMlp.cell_ok.offset, C.sizeof(L.XtsSurrogateStats), L.XtsSurrogateStats.evaluated.offset]
     consts = [int(v) for v in out[1].split()]
-    assert consts == [L.MLP_W2, L.MLP_W3, L.MLP_B4, L.MLP_NPARAM] == [MO.W2, MO.W3, MO.B4, MO.NPARAM]
+    assert consts[:4] == [L.MLP_W2, L.MLP_W3, L.MLP_B4, L.MLP_NPARAM] == [MO.W2, MO.W3, MO.B4, MO.NPARAM]
+    assert consts[4:] == [L.MLP_CELL_NR, L.MLP_CELL_NS]
 
 
 def test_sample_oracle_geometry():
@@ -129,6 +133,16 @@ def test_surrogate_state_round_trip(tmp_path):
     assert (back.out_mu, back.out_sd, back.rho_min) == (net.out_mu, net.out_sd, 50.0)
     s = back.struct()
     assert abs(s.rho_min - 50.0) < 1e-6 and list(s.in_sd) == pytest.approx(list(net.in_sd))
+    assert not s.cell_ok  # uncalibrated: no cell restriction (NULL)
+    # calibrated error cells travel with the state
+    net.cell_lo = np.array([-1.0, -30.0], np.float32)
+    net.cell_hi = np.array([3.0, 2.0], np.float32)
+    net.cell_ok = torch.as_tensor(rng.integers(0, 2, L.MLP_CELL_NR * L.MLP_CELL_NS).astype(np.uint8))
+    net.save(f)
+    back = Surrogate.load(f, device="cpu")
+    np.testing.assert_array_equal(back.cell_ok.numpy(), net.cell_ok.numpy())
+    s = back.struct()
+    assert list(s.cell_lo) == [-1.0, -30.0] and list(s.cell_hi) == [3.0, 2.0] and s.cell_ok
 
 
 def test_cli_and_bench_expose_the_surrogate():
@@ -142,5 +156,22 @@ def test_cli_and_bench_expose_the_surrogate():
         assert opt in out, opt
     out = subprocess.run([sys.executable, "bench.py", "--help"], cwd=root, capture_output=True, text=True,
                          check=True).stdout
-    for opt in ("--no-surrogate", "--surrogate-samples", "--surrogate-epochs"):
+    for opt in ("--no-surrogate", "--surrogate-samples", "--surrogate-epochs", "--no-c4", "--no-f64"):
         assert opt in out, opt
+
+
+def test_bench_gpus_launch_refuses_without_gpus():
+    """bench.py --gpus N starts N ranks itself when no launcher did; on a machine
+    with fewer CUDA devices it fails loudly instead of running one rank."""
+    import sys
+
+    import torch
+
+    if torch.cuda.is_available() and torch.cuda.device_count() >= 2:
+        pytest.skip("this machine has the GPUs: the launch would run")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK")}
+    r = subprocess.run([sys.executable, "bench.py", "--gpus", "2", "--steps", "3"], cwd=root, capture_output=True,
+                       text=True, env=env, timeout=300)
+    assert r.returncode == 2
+    assert "one rank per GPU needs 2" in r.stderr

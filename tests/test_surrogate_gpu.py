@@ -150,12 +150,15 @@ def test_map_fallback_equals_rule(api):
 
 
 def test_trained_network_gains_over_centre_value(api):
-    """Trained on the GPU on samples of one job's mean PSFs, the network's error on
-    fresh samples is compared with the centre value alone (y = 0, the method
-    without the network); then the model map of another job."""
+    """Trained on the GPU on samples of one job's mean PSFs (separations 0.001-30
+    deg, pixel sizes 0.025-0.2 deg), the network's error on fresh samples is
+    compared with the centre value alone (y = 0, the method without the network);
+    its error cells are calibrated on a third sample; then the model map of
+    another job must stay within 1e-4 of the plain map everywhere, while the
+    network serves a share of its values."""
     import torch
 
-    from xtsrcmaps_b200.surrogate import Surrogate, model_map, samples
+    from xtsrcmaps_b200.surrogate import Surrogate, last_stats, model_map, samples
 
     job, upsf, _, _ = _psf_tables(api, "c1", seed=7, n=50)
     X, Y = samples(upsf, job.logEs, 4_000_000, seed=11)
@@ -171,6 +174,11 @@ def test_trained_network_gains_over_centre_value(api):
     print(f"\nsurrogate: rms rel error {np.sqrt(np.mean(err_net**2)):.2e} vs centre value "
           f"{np.sqrt(np.mean(err_c**2)):.2e} (gain {gain:.1f}x); within 1e-4: {np.mean(err_net <= 1e-4):.4f}")
     assert gain > 5.0
+    Xc, Yc = samples(upsf, job.logEs, 2_000_000, seed=123)
+    cal = net.calibrate(Xc, Yc, tol=1e-4, margin=0.5)
+    print(f"calibration: {cal}")
+    assert cal["max_rel_err_in_accepted_cells"] <= 0.5e-4
+    assert cal["share_in_accepted_cells"] > 0.2
     job2, upsf2, partial2, expo2 = _psf_tables(api, "c1", seed=8, n=6)
     src = torch.as_tensor(job2.src_sph, device=upsf2.device)
     m, _, st = model_map(job2.wcs, src, expo2, upsf2, partial2, job2.logEs, net, check_tol=1e-4)
@@ -181,6 +189,13 @@ def test_trained_network_gains_over_centre_value(api):
           f"fraction within 1e-4 {np.mean(err <= 1e-4):.4f}")
     assert 0 <= st["accepted"] <= st["values"] == m.size
     assert np.isfinite(m).all()
+    assert st["maps_fallback"] == 0 and st["accepted"] > 0.2 * st["values"]
+    assert err.max() <= 1e-4
+    # the same call without the stats (no synchronisation): identical map, same counts
+    m2, _, none = model_map(job2.wcs, src, expo2, upsf2, partial2, job2.logEs, net, check_tol=1e-4, stats=False)
+    assert none is None
+    assert last_stats(upsf2.device) == st
+    np.testing.assert_array_equal(m2.cpu().numpy(), m)
 
 
 def test_surrogate_argument_errors(api):

@@ -27,6 +27,7 @@ XTS_TCGEN05 = 1 << 4
 XTS_FITS_F32 = 1 << 5
 
 ND = 401
+NOALLOC_SCRATCH_DOUBLES = 1 << 20  # XTS_NOALLOC_SCRATCH_DOUBLES
 
 _vp = C.c_void_p
 
@@ -82,6 +83,8 @@ MLP_B3 = MLP_W3 + MLP_HID * MLP_HID
 MLP_W4 = MLP_B3 + MLP_HID
 MLP_B4 = MLP_W4 + MLP_HID
 MLP_NPARAM = MLP_B4 + 1
+MLP_CELL_NR = 32  # XTS_MLP_CELL_NR
+MLP_CELL_NS = 16  # XTS_MLP_CELL_NS
 
 
 class XtsMlp(C.Structure):
@@ -91,6 +94,8 @@ class XtsMlp(C.Structure):
         ("out_mu", C.c_float), ("out_sd", C.c_float),
         ("lo", C.c_float * MLP_IN), ("hi", C.c_float * MLP_IN),
         ("rho_min", C.c_float),
+        ("cell_lo", C.c_float * 2), ("cell_hi", C.c_float * 2),
+        ("cell_ok", _vp),
     ]
 
 
@@ -149,6 +154,13 @@ SIGNATURES = {
                                                         C.c_int, C.POINTER(XtsMlp), C.c_double, _vp,
                                                         C.POINTER(XtsSrcmapInfo),
                                                         C.POINTER(XtsSurrogateStats), _vp]),
+    "xts_surrogate_last_stats": (C.c_int, [C.POINTER(XtsSurrogateStats), _vp]),
+    "xts_rebin_wcs": (C.c_int, [C.POINTER(XtsWcs), C.c_double, C.POINTER(XtsWcs)]),
+    "xts_allsky_crop_range": (C.c_int, [C.POINTER(XtsWcs), C.POINTER(XtsWcs), C.POINTER(C.c_long)]),
+    "xts_crop_allsky": (C.c_int, [_vp, C.c_int, C.c_long, C.c_long, C.POINTER(C.c_long), _vp, C.c_uint, _vp]),
+    "xts_trilerp_ehw": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _vp, C.c_int, C.c_int, C.c_int, C.c_uint, _vp]),
+    "xts_scale_model_map": (C.c_int, [C.POINTER(XtsWcs), _vp, C.c_int, _vp, _vp, _vp, C.c_int, _vp,
+                                      C.POINTER(XtsSrcmapInfo), C.c_uint, _vp]),
 }
 
 

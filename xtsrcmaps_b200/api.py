@@ -401,6 +401,50 @@ def point_source_maps(wcs: Wcs, src_sph, exp_cube: ExpCube, wexp_cube: ExpCube, 
     return m, info
 
 
+def point_source_maps_surrogate(wcs: Wcs, src_sph, exp_cube: ExpCube, wexp_cube: ExpCube, logEs,
+                                aeff_front: IrfGrid, aeff_back: IrfGrid, psf_front: IrfGrid, psf_back: IrfGrid,
+                                front_ltf, net, check_tol: float = 1e-4, out=None, with_info: bool = False,
+                                stats: bool = True):
+    """The three calls of main.cxx:28-30 with the model map of the learned
+    surrogate (point_src_model_map_wcs_surrogate) in place of the plain cubature.
+    Inputs may be host arrays (numpy, or CPU torch tensors, pinned for
+    asynchronous copies) or CUDA tensors; host inputs are copied to the network's
+    device and the map is copied back into ``out`` (a CPU tensor or numpy array;
+    allocated when None).  Returns (model_map, SrcmapInfo or None, stats or
+    None)."""
+    import torch
+
+    dev = net.device
+    host = not _is_cuda(src_sph)
+
+    def t(a, dt=torch.float64):
+        a = a if isinstance(a, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(a))
+        return a.to(device=dev, dtype=dt, non_blocking=True)
+
+    def grid(g):
+        return IrfGrid(t(g.cosths), t(g.logEs), t(g.params), g.min_cos_theta)
+
+    cube = ExpCube(t(exp_cube.cosbins, torch.float32), exp_cube.nside, exp_cube.nbrbins, exp_cube.cosmin,
+                   exp_cube.thetabin)
+    wcube = ExpCube(t(wexp_cube.cosbins, torch.float32), wexp_cube.nside, wexp_cube.nbrbins, wexp_cube.cosmin,
+                    wexp_cube.thetabin)
+    le, src, ltf = t(logEs), t(src_sph), t(front_ltf)
+    ex = compute_exposure(cube, wcube, le, src, grid(aeff_front), grid(aeff_back), ltf)
+    ps = compute_psf_data(grid(psf_front), grid(psf_back), ex, le, ltf)
+    from .surrogate import model_map
+
+    m, info, st = model_map(wcs, src, ex.exposure, ps.uPsf, ps.partial_psf_integral, le, net, check_tol,
+                            with_info, out=None if host else out, stats=stats)
+    if host:
+        if out is None:
+            out = torch.empty(tuple(m.shape), dtype=torch.float32, pin_memory=True)
+        dst = out if isinstance(out, torch.Tensor) else torch.from_numpy(out)
+        dst.copy_(m, non_blocking=True)
+        torch.cuda.current_stream(dev).synchronize()
+        m = out
+    return m, info, st
+
+
 def write_src_model(filename: str, model_map, names=None, bitpix: int = -64) -> None:
     """Fermi::fits::write_src_model (fits/fits.write_src_model.cxx:10-66): the maps
     [S, H, W, E] (float32 or float64, host array or CUDA tensor) written as a FITS
@@ -474,6 +518,89 @@ def convolve_map_psf(image, kernel):
     return o
 
 
+def rebin_wcs(wcs: Wcs, target_pix_size: float) -> Wcs:
+    """rebin_wcs_config (sky_geom/sky_geom.hxx:352-371): the WCS of the same region at
+    pixel size ``target_pix_size`` degrees (CDELT2 rebinned, where the reference
+    stores CRPIX2)."""
+    w = _wcs_struct(wcs)
+    o = L.XtsWcs()
+    L.check(L.lib().xts_rebin_wcs(C.byref(w), float(target_pix_size), C.byref(o)))
+    return Wcs(int(o.naxis1), int(o.naxis2), o.crpix1, o.crpix2, o.crval1, o.crval2, o.cdelt1, o.cdelt2, o.crota2,
+               wcs.proj, wcs.galactic)
+
+
+def allsky_crop_range(allsky_wcs: Wcs, roi_wcs: Wcs) -> tuple:
+    """The all-sky pixel range under the ROI of fits::read_allsky_cropped
+    (fits/fits.read_allsky_cropped.cpp:150-194): (x_first, x_last, y_first, y_last),
+    1-based and inclusive."""
+    r = (C.c_long * 4)()
+    a, b = _wcs_struct(allsky_wcs), _wcs_struct(roi_wcs)
+    L.check(L.lib().xts_allsky_crop_range(C.byref(a), C.byref(b), r))
+    return tuple(int(v) for v in r)
+
+
+def crop_allsky(allsky, crop_range):
+    """The block of an all-sky cube [E0, NY, NX] (float32) inside ``crop_range``
+    (x_first, x_last, y_first, y_last; x_first > x_last wraps across the image's
+    longitude seam) -> [E0, ny, nx]."""
+    like = _device_of(allsky)
+    c = _Call(like is not None, like)
+    ap, a = c.inp(allsky, "f32")
+    E0, NY, NX = (int(v) for v in a.shape)
+    x0, x1, y0, y1 = (int(v) for v in crop_range)
+    nx = x1 - x0 + 1 if x1 >= x0 else NX - x0 + 1 + x1
+    op, o = c.out((E0, y1 - y0 + 1, nx), "f32")
+    r = (C.c_long * 4)(x0, x1, y0, y1)
+    L.check(L.lib().xts_crop_allsky(ap, E0, NY, NX, r, op, c.flags, c.stream))
+    return o
+
+
+def trilerp_ehw(src, shape):
+    """Fermi::math::trilerpEHW (math/trilerp.hpp:7-59): src [E0, H0, W0] (float32)
+    resampled trilinearly onto ``shape`` = (E1, H1, W1), corner-aligned axes."""
+    like = _device_of(src)
+    c = _Call(like is not None, like)
+    sp, sa = c.inp(src, "f32")
+    E0, H0, W0 = (int(v) for v in sa.shape)
+    E1, H1, W1 = (int(v) for v in shape)
+    dp, d = c.out((E1, H1, W1), "f32")
+    L.check(L.lib().xts_trilerp_ehw(sp, E0, H0, W0, dp, E1, H1, W1, c.flags, c.stream))
+    return d
+
+
+def scale_model_map(wcs: Wcs, src_sph, exposure, uPsf, partial_integrals, means, with_info: bool = True):
+    """The final scalings of the diffuse-source map (model_map.diffuse_src_model_map_wcs.cxx:76-95),
+    those of point_src_model_map_wcs after its cubature: pixel means [S, H, W, E]
+    (float32) -> mean * solid angle * exposure * correction, with the map
+    integral and containment correction of the point-source path.  Returns
+    (model_map, SrcmapInfo or None); a CUDA ``means`` is scaled in place."""
+    like = _device_of(means, exposure, uPsf)
+    c = _Call(like is not None, like)
+    sp, sa = c.inp(src_sph)
+    S = int(sa.shape[0]) if sa.ndim == 2 else 0
+    ep, ea = c.inp(exposure)
+    E = int(ea.shape[1])
+    up, _ = c.inp(uPsf)
+    pp, _ = c.inp(partial_integrals)
+    if c.device:
+        m = means
+        if str(m.dtype) != "torch.float32" or not m.is_contiguous():
+            raise ValueError("means must be a contiguous float32 tensor")
+        mp = C.c_void_p(m.data_ptr())
+    else:
+        m = np.array(means, dtype=np.float32, copy=True, order="C")
+        mp = C.c_void_p(m.ctypes.data)
+    info = info_s = None
+    if with_info:
+        o = [c.out((S, E)), c.out((S, E)), c.out((S,)), c.out((S,), "i32")]
+        info_s = L.XtsSrcmapInfo(*[x[0] for x in o])
+        info = SrcmapInfo(*[x[1] for x in o])
+    w = _wcs_struct(wcs)
+    L.check(L.lib().xts_scale_model_map(C.byref(w), sp, S, ep, up, pp, E, mp,
+                                        C.byref(info_s) if info_s is not None else None, c.flags, c.stream))
+    return m, info
+
+
 def compute_srcmaps(wcs: Wcs, src_sph, exp: XtExp, psf: XtPsf, out_dtype: str = "float32", out=None):
     """ModelMap::compute_srcmaps<PointSource> (model_map/model_map.compute_src_maps.cxx:6-22)."""
     m, _ = point_src_model_map_wcs(wcs, src_sph, exp.exposure, psf.uPsf, psf.partial_psf_integral,
@@ -508,10 +635,13 @@ def release() -> None:
 
 
 def point_src_model_map_wcs_surrogate(wcs: Wcs, src_sph, exposure, uPsf, partial_integrals, logEs, net,
-                                      check_tol: float = 1e-4, with_info: bool = True):
+                                      check_tol: float = 1e-4, with_info: bool = True, out=None,
+                                      stats: bool = True):
     """point_src_model_map_wcs with the pixel means from the learned surrogate
     (xtsrcmaps_b200.surrogate.Surrogate) where it applies and the FP64 12-point
-    rule elsewhere; CUDA tensors.  Returns (maps, SrcmapInfo or None, stats)."""
+    rule elsewhere; CUDA tensors.  Returns (maps, SrcmapInfo or None, stats or
+    None); with stats=False the call does not synchronise."""
     from .surrogate import model_map
 
-    return model_map(wcs, src_sph, exposure, uPsf, partial_integrals, logEs, net, check_tol, with_info)
+    return model_map(wcs, src_sph, exposure, uPsf, partial_integrals, logEs, net, check_tol, with_info, out=out,
+                     stats=stats)

@@ -793,6 +793,11 @@ int xts_point_src_model_map_wcs_surrogate(const xts_wcs* wcs, const double* src_
     return run_srcmap(sg, a, model_map, npix, false);
 }
 
+int xts_surrogate_last_stats(xts_surrogate_stats* stats, void* stream) {
+    XTS_ENTER();
+    return surrogate_last_stats(stats, stream ? (cudaStream_t)stream : g_ctx.stream);
+}
+
 int xts_point_source_maps(const xts_expcube* cube, const xts_expcube* wcube, const double* logEs,
                           int E, const double* src_sph, int S, const xts_grid* aeff_front,
                           const xts_grid* aeff_back, const xts_grid* psf_front,
@@ -909,6 +914,89 @@ int xts_convolve_map_psf(const double* image, int E, int H, int W, const double*
     const double* ke = sg.in(kernel, (size_t)E * K * K);
     double* o = sg.out(out, (size_t)E * PH * PW);
     int rc = sg.rc ? sg.rc : convolve_map_psf(im, E, H, W, ke, K, o, sg.st);
+    return sg.finish(rc);
+}
+
+static bool wcs_ok(const xts_wcs* w) {
+    return w && w->naxis1 > 0 && w->naxis2 > 0 && (w->proj == 0 || w->proj == 1) && w->cdelt1 != 0. &&
+           w->cdelt2 != 0.;
+}
+
+int xts_rebin_wcs(const xts_wcs* in, double target_pix_size, xts_wcs* out) {
+    if (!wcs_ok(in) || !out || !(target_pix_size > 0.) || !std::isfinite(target_pix_size))
+        return set_error(XTS_ERR_ARG, "rebin_wcs: bad WCS or target pixel size");
+    return rebin_wcs(*in, target_pix_size, out);
+}
+
+int xts_allsky_crop_range(const xts_wcs* allsky_wcs, const xts_wcs* roi_wcs, long range[4]) {
+    if (!wcs_ok(allsky_wcs) || !wcs_ok(roi_wcs) || !range)
+        return set_error(XTS_ERR_ARG, "allsky_crop_range: bad WCS (CAR/AIT, nonzero CDELT) or null range");
+    return allsky_crop_range(*allsky_wcs, *roi_wcs, range);
+}
+
+int xts_crop_allsky(const float* allsky, int E0, long NY, long NX, const long range[4], float* out, unsigned flags,
+                    void* stream) {
+    XTS_ENTER();
+    if (!allsky || !out || !range || E0 <= 0 || NY <= 0 || NX <= 0)
+        return set_error(XTS_ERR_ARG, "crop_allsky: null argument or bad size");
+    if (range[0] < 1 || range[0] > NX || range[1] < 1 || range[1] > NX || range[2] < 1 || range[3] > NY ||
+        range[2] > range[3])
+        return set_error(XTS_ERR_ARG, "crop_allsky: range outside the all-sky image");
+    const long nx = range[1] >= range[0] ? range[1] - range[0] + 1 : NX - range[0] + 1 + range[1];
+    const long ny = range[3] - range[2] + 1;
+    Stager sg{(flags & XTS_DEVICE_PTRS) != 0, stream ? (cudaStream_t)stream : g_ctx.stream};
+    const float* sky = sg.in(allsky, (size_t)E0 * NY * NX);
+    float* o = sg.out(out, (size_t)E0 * ny * nx);
+    int rc = sg.rc ? sg.rc : crop_allsky(sky, E0, NY, NX, range, o, sg.st);
+    return sg.finish(rc);
+}
+
+int xts_trilerp_ehw(const float* src, int E0, int H0, int W0, float* dst, int E1, int H1, int W1, unsigned flags,
+                    void* stream) {
+    XTS_ENTER();
+    if (!src || !dst || E0 <= 0 || H0 <= 0 || W0 <= 0 || E1 <= 0 || H1 <= 0 || W1 <= 0 ||
+        (long long)E1 * H1 * W1 > (1LL << 40))
+        return set_error(XTS_ERR_ARG, "trilerp_ehw: null argument or bad size");
+    Stager sg{(flags & XTS_DEVICE_PTRS) != 0, stream ? (cudaStream_t)stream : g_ctx.stream};
+    const float* sp = sg.in(src, (size_t)E0 * H0 * W0);
+    float* dp = sg.out(dst, (size_t)E1 * H1 * W1);
+    int rc = sg.rc ? sg.rc : trilerp_ehw(sp, E0, H0, W0, dp, E1, H1, W1, sg.st);
+    return sg.finish(rc);
+}
+
+int xts_scale_model_map(const xts_wcs* wcs, const double* src_sph, int S, const double* exposure, const double* upsf,
+                        const double* partial, int E, float* model_map, xts_srcmap_info* info, unsigned flags,
+                        void* stream) {
+    XTS_ENTER();
+    if (!wcs_ok(wcs))
+        return set_error(XTS_ERR_ARG, "scale_model_map: bad WCS (CAR/AIT, nonzero CDELT)");
+    if (S < 0 || E <= 0 || E > 256 || (S > 0 && (!src_sph || !exposure || !upsf || !partial || !model_map)))
+        return set_error(XTS_ERR_ARG, "scale_model_map: null argument or bad size (E <= 256)");
+    if ((long long)wcs->naxis1 * wcs->naxis2 * E > 0xffffffffLL || S > 65535)
+        return set_error(XTS_ERR_ARG, "scale_model_map: map or source count too large");
+    if (flags & ~(unsigned)XTS_DEVICE_PTRS)
+        return set_error(XTS_ERR_ARG, "scale_model_map: only XTS_DEVICE_PTRS applies");
+    const size_t npix = (size_t)wcs->naxis1 * wcs->naxis2;
+    Stager sg{(flags & XTS_DEVICE_PTRS) != 0, stream ? (cudaStream_t)stream : g_ctx.stream};
+    SrcmapDev a;
+    a.wcs = *wcs;
+    a.src_sph = sg.in(src_sph, (size_t)2 * S); a.S = S;
+    a.exposure = sg.in(exposure, (size_t)S * E);
+    a.upsf = sg.in(upsf, (size_t)S * ND * E);
+    a.partial = sg.in(partial, (size_t)S * ND * E); a.E = E;
+    a.out_f64 = false;
+    float* m = sg.out(model_map, (size_t)S * npix * E);  // pixel means in, model map out
+    if (!sg.dev && !sg.rc && m && S > 0) {
+        cudaError_t e = cudaMemcpyAsync(m, model_map, sizeof(float) * S * npix * E, cudaMemcpyHostToDevice, sg.st);
+        if (e != cudaSuccess) return cuda_error(e, "cudaMemcpyAsync H2D");
+    }
+    a.out = m;
+    a.inv_integ = info ? sg.out(info->inv_map_integral, (size_t)S * E) : nullptr;
+    a.correction = info ? sg.out(info->correction, (size_t)S * E) : nullptr;
+    a.radius = info ? sg.out(info->psf_radius, (size_t)S) : nullptr;
+    a.in_fov = info ? sg.out(info->in_fov, (size_t)S) : nullptr;
+    a.means_given = true;
+    int rc = sg.rc ? sg.rc : launch_srcmap(a, sg.st);
     return sg.finish(rc);
 }
 

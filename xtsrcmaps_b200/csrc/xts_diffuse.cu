@@ -20,6 +20,14 @@
 // code are not reproduced: its transform is 3-D over (energy, h, w), which mixes
 // energy planes, and its normalisation `1.0 / paddedH * paddedW * C` multiplies
 // where it means to divide.
+//
+// The steps before them: the all-sky cube's block under the ROI
+// (fits::read_allsky_cropped, fits/fits.read_allsky_cropped.cpp:150-230: the
+// pixel range on the host, the block gathered on the device, wrapped at the
+// image's longitude seam as readSegmentsAcrossBoundary :119-147 intends), the
+// WCS at the target pixel size (rebin_wcs_config, sky_geom/sky_geom.hxx:352-371)
+// and the trilinear resampling onto it (Fermi::math::trilerpEHW,
+// math/trilerp.hpp:7-59, in FP32 as the reference's float tensors).
 #include <cufft.h>
 #include <math.h>
 
@@ -183,6 +191,110 @@ int convolve_map_psf(const double* image, int E, int H, int W, const double* ker
                                      C, (const double2*)A, cn, 1.0 / ((double)NH * NW)));
     if (cufftExecZ2D(g_fft.inv, C, B) != CUFFT_SUCCESS) return set_error(XTS_ERR_CUDA, "cufftExecZ2D");
     XTS_LAUNCH("k_fft_crop", st, k_fft_crop<<<(unsigned)((on + 255) / 256), 256, 0, st>>>(B, NH, NW, PH, PW, out, on));
+    return XTS_OK;
+}
+
+// -------------------------------------------------------------- all-sky crop
+// fits.read_allsky_cropped.cpp:155-194: the ROI's pixels (1, 1) and (NAXIS1,
+// NAXIS2) to (lon, lat), longitude wrapped into [0, 360) and latitude clamped,
+// to all-sky pixels, rounded and bounded to [1, NAXISn]; first = min, last = max.
+int allsky_crop_range(const xts_wcs& sky, const xts_wcs& roi, long range[4]) {
+    const WcsDev ws = make_wcs(sky), wr = make_wcs(roi);
+    double lon[2], lat[2], px[2], py[2];
+    pix2sph(wr, 1.0, 1.0, &lon[0], &lat[0]);
+    pix2sph(wr, (double)roi.naxis1, (double)roi.naxis2, &lon[1], &lat[1]);
+    for (int k = 0; k < 2; ++k) {
+        lon[k] = fmod(lon[k] + 360.0, 360.0);
+        lat[k] = lat[k] > 90.0 ? 90.0 : (lat[k] < -90.0 ? -90.0 : lat[k]);
+        sph2pix(ws, lon[k], lat[k], &px[k], &py[k]);
+    }
+    auto bound = [](double v, long mx) {
+        const long r = lround(v);
+        return r < 1 ? 1L : (r > mx ? mx : r);
+    };
+    range[0] = bound(px[0] < px[1] ? px[0] : px[1], sky.naxis1);
+    range[1] = bound(px[0] < px[1] ? px[1] : px[0], sky.naxis1);
+    range[2] = bound(py[0] < py[1] ? py[0] : py[1], sky.naxis2);
+    range[3] = bound(py[0] < py[1] ? py[1] : py[0], sky.naxis2);
+    return XTS_OK;
+}
+
+// out[e][y][x] = allsky[e][y0 + y][(x0 + x) mod NX] (0-based x0 = range[0] - 1):
+// columns past the image's last column continue at its first (the seam).
+__global__ void k_crop_allsky(const float* __restrict__ sky, long NY, long NX, long x0, long y0, long nx, long ny,
+                              long long total, float* __restrict__ out) {
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= total) return;
+    const long long plane = (long long)nx * ny;
+    const long long e = k / plane;
+    const long long r = k - e * plane;
+    const long y = (long)(r / nx), x = (long)(r - (long long)y * nx);
+    long xs = x0 + x;
+    if (xs >= NX) xs -= NX;
+    out[k] = sky[((size_t)e * NY + (y0 + y)) * NX + xs];
+}
+
+int crop_allsky(const float* sky, int E0, long NY, long NX, const long range[4], float* out, cudaStream_t st) {
+    const long x0 = range[0] - 1, y0 = range[2] - 1;
+    const long nx = range[1] >= range[0] ? range[1] - range[0] + 1 : NX - range[0] + 1 + range[1];
+    const long ny = range[3] - range[2] + 1;
+    const long long total = (long long)E0 * nx * ny;
+    if (total == 0) return XTS_OK;
+    XTS_LAUNCH("k_crop_allsky", st, k_crop_allsky<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(
+                                        sky, NY, NX, x0, y0, nx, ny, total, out));
+    return XTS_OK;
+}
+
+// -------------------------------------------------------------- trilinear resampling
+// math/trilerp.hpp:7-59 in FP32: corner-aligned scales (src - 1) / (dst - 1) per
+// axis (0 when dst is 1, where the reference divides by zero), lower index
+// floor(k * scale), upper index min(lower + 1, src - 1); h, then w, then e.
+__global__ void k_trilerp_ehw(const float* __restrict__ src, int E0, int H0, int W0, float* __restrict__ dst,
+                              int E1, int H1, int W1, float se, float sh, float sw) {
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long total = (long long)E1 * H1 * W1;
+    if (k >= total) return;
+    const int j = (int)(k % W1);
+    const int i = (int)((k / W1) % H1);
+    const int kk = (int)(k / ((long long)W1 * H1));
+    const float e = (float)kk * se, h = (float)i * sh, w = (float)j * sw;
+    const int e0 = (int)e, h0 = (int)h, w0 = (int)w;
+    const int e1 = min(e0 + 1, E0 - 1), h1 = min(h0 + 1, H0 - 1), w1 = min(w0 + 1, W0 - 1);
+    const float fe = e - (float)e0, fh = h - (float)h0, fw = w - (float)w0;
+    const float ce = 1.f - fe, ch = 1.f - fh, cw = 1.f - fw;
+    auto at = [&](int a, int b, int c) { return src[((size_t)a * H0 + b) * W0 + c]; };
+    const float c00 = ch * at(e0, h0, w0) + fh * at(e0, h1, w0);
+    const float c01 = ch * at(e1, h0, w0) + fh * at(e1, h1, w0);
+    const float c10 = ch * at(e0, h0, w1) + fh * at(e0, h1, w1);
+    const float c11 = ch * at(e1, h0, w1) + fh * at(e1, h1, w1);
+    const float c0 = cw * c00 + fw * c10;
+    const float c1 = cw * c01 + fw * c11;
+    dst[k] = ce * c0 + fe * c1;
+}
+
+int trilerp_ehw(const float* src, int E0, int H0, int W0, float* dst, int E1, int H1, int W1, cudaStream_t st) {
+    auto scale = [](int a, int b) { return b > 1 ? (float)(a - 1) / (float)(b - 1) : 0.f; };
+    const long long total = (long long)E1 * H1 * W1;
+    if (total == 0) return XTS_OK;
+    XTS_LAUNCH("k_trilerp_ehw", st, k_trilerp_ehw<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(
+                                        src, E0, H0, W0, dst, E1, H1, W1, scale(E0, E1), scale(H0, H1), scale(W0, W1)));
+    return XTS_OK;
+}
+
+// -------------------------------------------------------------- rebinned WCS
+// sky_geom.hxx:352-371: CDELTn = +-target (the input's sign), scale_n = |CDELTn_in /
+// CDELTn|, NAXISn = round(NAXISn_in * scale_n), CRPIXn = CRPIXn_in * scale_n; the
+// reference writes CRPIX2 into CDELT2 (:367), the rebinned CDELT2 is written here.
+int rebin_wcs(const xts_wcs& in, double target, xts_wcs* out) {
+    *out = in;
+    const double c1 = in.cdelt1 < 0. ? -target : target, c2 = in.cdelt2 < 0. ? -target : target;
+    const double s1 = fabs(in.cdelt1 / c1), s2 = fabs(in.cdelt2 / c2);
+    out->cdelt1 = c1;
+    out->cdelt2 = c2;
+    out->naxis1 = lround((double)in.naxis1 * s1);
+    out->naxis2 = lround((double)in.naxis2 * s2);
+    out->crpix1 = in.crpix1 * s1;
+    out->crpix2 = in.crpix2 * s2;
     return XTS_OK;
 }
 

@@ -137,6 +137,9 @@ struct SrcmapDev {
     // join_ev before the first kernel that reads uPsf.
     cudaStream_t geo_stream = nullptr;
     cudaEvent_t join_ev = nullptr;
+    // a.out holds FP32 pixel means on entry: only the scalings of c7-c10 and d2 are
+    // applied (the diffuse map's final steps)
+    bool means_given = false;
     // pixel means from the surrogate network (with the 12-point rule as fallback)
     const xts_mlp* surrogate = nullptr;
     const double* logEs = nullptr;  // [E] log10 energies (the network's fourth feature)
@@ -180,6 +183,10 @@ bool srcmap_win_supported(int E);
 int make_psf_kernel(const xts_wcs& wcs, int Nk, const double* upsf, int E, double* kernel, cudaStream_t st);
 int convolve_map_psf(const double* image, int E, int H, int W, const double* kernel, int K, double* out,
                      cudaStream_t st);
+int allsky_crop_range(const xts_wcs& sky, const xts_wcs& roi, long range[4]);
+int crop_allsky(const float* sky, int E0, long NY, long NX, const long range[4], float* out, cudaStream_t st);
+int trilerp_ehw(const float* src, int E0, int H0, int W0, float* dst, int E1, int H1, int W1, cudaStream_t st);
+int rebin_wcs(const xts_wcs& in, double target, xts_wcs* out);
 int write_src_model(const char* filename, const void* model_map, int S, int H, int W, int E,
                     const char* const* names, bool dev_ptrs, bool f64in, bool f64out, cudaStream_t st);
 bool exposure_map_supported(int C, int E);
@@ -203,6 +210,9 @@ int finish_mean_map(const SrcmapDev& a, const double* centers, const double* ome
 int launch_gemm_bf16(const void* A, int a_trans, const void* B, int b_trans, int M, int K, float* C, int c_trans,
                      int accumulate, int* status, cudaStream_t st);
 int launch_mlp_forward(const xts_mlp* net, const float* X, long long n, float* y, int* status, cudaStream_t st);
+// the same with the row count read on the device (at most n_max rows; no host sync)
+int launch_mlp_forward_dev(const xts_mlp* net, const float* X, const unsigned long long* n_dev, long long n_max,
+                           float* y, int* status, cudaStream_t st);
 int launch_mlp_grads(const xts_mlp* net, const float* X, const float* Y, long long n, float* grads, float* loss,
                      int* status, cudaStream_t st);
 int launch_mlp_train_step(const xts_mlp* net, const float* X, const float* Y, long long n, float* grads,
@@ -212,6 +222,7 @@ int launch_surrogate_samples(const double* upsf, const double* logEs, int S, int
                              unsigned long long seed, double rho_min, float* X, float* Y, cudaStream_t st);
 int launch_srcmap_surrogate(const SrcmapDev& a, const double* corners, const double* centers, const double* omega,
                             const SrcInfo* info, double* scale, int nch, cudaStream_t st);
+int surrogate_last_stats(xts_surrogate_stats* stats, cudaStream_t st);
 int launch_srcmap_win(const double* corners, const double* centers, const double* omega,
                       const SrcInfo* info, int S, int H, int W, int E,
                       const double* upsf, const double* partial, const double* exposure,

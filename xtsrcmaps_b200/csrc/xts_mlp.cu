@@ -165,8 +165,9 @@ struct FwdSaves {  // training only; all NULL for inference
 template <bool SAVE>
 __global__ void __launch_bounds__(FT, 2)
 k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict__ wbf, MlpNorm nm,
-              const float* __restrict__ X, long long n, float* __restrict__ y, FwdSaves sv,
-              int* __restrict__ status) {
+              const float* __restrict__ X, long long n, const unsigned long long* __restrict__ n_dev,
+              float* __restrict__ y, FwdSaves sv, int* __restrict__ status) {
+    if (n_dev) n = min(n, (long long)*n_dev);  // rows counted on the device (at most n)
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
     const int t = threadIdx.x, warp = t >> 5, r = t & (MT - 1), hf = t >> 7, cb = 64 * hf;
@@ -597,8 +598,8 @@ int launch_gemm_bf16(const void* A, int a_trans, const void* B, int b_trans, int
     return XTS_OK;
 }
 
-static int forward(const xts_mlp* net, const float* X, long long n, float* y, FwdSaves sv, int* status,
-                   cudaStream_t st) {
+static int forward(const xts_mlp* net, const float* X, long long n, const unsigned long long* n_dev, float* y,
+                   FwdSaves sv, int* status, cudaStream_t st) {
     // per call: the attribute belongs to the current device's context
     XTS_CUDA(cudaFuncSetAttribute(k_mlp_forward<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM));
     XTS_CUDA(cudaFuncSetAttribute(k_mlp_forward<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM));
@@ -609,18 +610,24 @@ static int forward(const xts_mlp* net, const float* X, long long n, float* y, Fw
     const long long g = ntiles < 2 * sm_count() ? ntiles : 2 * sm_count();  // two blocks per SM
     if (save)
         XTS_LAUNCH("k_mlp_forward", st, k_mlp_forward<true><<<(unsigned)g, FT, FWD_SMEM, st>>>(
-                                            net->params, (const __nv_bfloat16*)net->wbf16, mlp_norm(net), X, n, y,
-                                            sv, status));
+                                            net->params, (const __nv_bfloat16*)net->wbf16, mlp_norm(net), X, n, n_dev,
+                                            y, sv, status));
     else
         XTS_LAUNCH("k_mlp_forward", st, k_mlp_forward<false><<<(unsigned)g, FT, FWD_SMEM, st>>>(
-                                            net->params, (const __nv_bfloat16*)net->wbf16, mlp_norm(net), X, n, y,
-                                            sv, status));
+                                            net->params, (const __nv_bfloat16*)net->wbf16, mlp_norm(net), X, n, n_dev,
+                                            y, sv, status));
     return XTS_OK;
 }
 
 int launch_mlp_forward(const xts_mlp* net, const float* X, long long n, float* y, int* status, cudaStream_t st) {
     if (n <= 0) return XTS_OK;
-    return forward(net, X, n, y, FwdSaves{}, status, st);
+    return forward(net, X, n, nullptr, y, FwdSaves{}, status, st);
+}
+
+int launch_mlp_forward_dev(const xts_mlp* net, const float* X, const unsigned long long* n_dev, long long n_max,
+                           float* y, int* status, cudaStream_t st) {
+    if (n_max <= 0) return XTS_OK;
+    return forward(net, X, n_max, n_dev, y, FwdSaves{}, status, st);
 }
 
 // forward with saves, then the gradient accumulated into grads (zero on entry)
@@ -636,7 +643,7 @@ static int mlp_backprop(const xts_mlp* net, const float* X, const float* Y, long
     float* yn = (float*)workspace(W_MLP_Y, sizeof(float) * n);
     if (!z || !h || !dz || !dh || !yn) return XTS_ERR_OOM;
     FwdSaves sv{z, z + hn, z + 2 * hn, h, h + hn, yn};
-    int rc = forward(net, X, n, nullptr, sv, status, st);
+    int rc = forward(net, X, n, nullptr, nullptr, sv, status, st);
     if (rc) return rc;
     const MlpNorm nm = mlp_norm(net);
     const int nbx = (int)((n + BW_ROWS - 1) / BW_ROWS);

@@ -118,6 +118,7 @@ static int build_septab(cudaStream_t st, const SepTab** out) {
 static __constant__ double c_rule_uv[12][4];
 static __constant__ float c_rule_w32[12];
 static __constant__ double c_rule_q[12][3];  // u, u*u, v (biquadratic chord form)
+static __constant__ float c_rule_f[12][4];   // u, u*u, v in FP32 (chord offsets from the centre), pad
 
 static int upload_rule_uv(cudaStream_t st) {
     static int dev_done = -1;
@@ -144,12 +145,14 @@ static int upload_rule_uv(cudaStream_t st) {
         b[p][0] = R[3 * p]; b[p][1] = R[3 * p + 1]; b[p][2] = R[3 * p] * R[3 * p + 1];
         b[p][3] = 0.25 * R[3 * p + 2];
     }
-    float w32[12];
+    float w32[12], bf[12][4];
     double bq[12][3];
     for (int p = 0; p < 12; ++p) {
         w32[p] = (float)b[p][3];
         bq[p][0] = R[3 * p]; bq[p][1] = R[3 * p] * R[3 * p]; bq[p][2] = R[3 * p + 1];
+        bf[p][0] = (float)bq[p][0]; bf[p][1] = (float)bq[p][1]; bf[p][2] = (float)bq[p][2]; bf[p][3] = 0.f;
     }
+    XTS_CUDA(cudaMemcpyToSymbolAsync(c_rule_f, bf, sizeof(bf), 0, cudaMemcpyHostToDevice, st));
     XTS_CUDA(cudaMemcpyToSymbolAsync(c_rule_uv, b, sizeof(b), 0, cudaMemcpyHostToDevice, st));
     XTS_CUDA(cudaMemcpyToSymbolAsync(c_rule_w32, w32, sizeof(w32), 0, cudaMemcpyHostToDevice, st));
     XTS_CUDA(cudaMemcpyToSymbolAsync(c_rule_q, bq, sizeof(bq), 0, cudaMemcpyHostToDevice, st));

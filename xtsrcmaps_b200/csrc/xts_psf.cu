@@ -102,44 +102,65 @@ __global__ void k_psf_aeff(xts_grid pf, xts_grid pb, const double* kf, const dou
     pa[i] = v;
 }
 
-// b5 + b6: mean[s, de] for a tile of sources; each thread keeps the C values of
-// its (d, e) column in registers and reuses them across the tile's sources.
-constexpr int PSF_TILE_S = 16;
+// b5 + b6: mean[s, de] by a register-tiled FP64 contraction over cos-theta:
+// each block takes MP_TS sources and MP_CPT * 128 columns (d, e); each thread
+// keeps MP_TS x MP_CPT pairs of accumulators (exposure and weighted exposure
+// sides), reads its MP_CPT columns of psf*aeff once per cos-theta bin (coalesced,
+// from L2) and the sources' cos-theta rows from shared memory (broadcast), so
+// every shared load feeds 2 * MP_CPT FMAs and every column load 2 * MP_TS.
+constexpr int PSF_TILE_S = 8;   // sources per block
+constexpr int PSF_CPT = 4;      // columns per thread
 constexpr int PSF_MAX_C = 64;
 
-__global__ void __launch_bounds__(128) k_mean_psf(const double* pa, int C, int E, const double* ecb,
-                                                  const double* wecb, int S, const double* ltf,
-                                                  const double* expo, double* out) {
+__global__ void __launch_bounds__(128) k_mean_psf(const double* __restrict__ pa, int C, int E,
+                                                  const double* __restrict__ ecb, const double* __restrict__ wecb,
+                                                  int S, const double* __restrict__ ltf,
+                                                  const double* __restrict__ expo, double* __restrict__ out) {
     __shared__ double2 sxw[PSF_MAX_C][PSF_TILE_S];  // (exposure, weighted exposure) cos-theta rows
-    int s0 = blockIdx.y * PSF_TILE_S;
-    int ns = min(PSF_TILE_S, S - s0);
+    const int s0 = blockIdx.y * PSF_TILE_S;
+    const int ns = min(PSF_TILE_S, S - s0);
     for (int k = threadIdx.x; k < PSF_TILE_S * C; k += blockDim.x) {
-        int s = k / C, c = k - s * C;
-        bool ok = s < ns;
+        const int s = k / C, c = k - s * C;
+        const bool ok = s < ns;
         sxw[c][s] = make_double2(ok ? ecb[(size_t)(s0 + s) * C + c] : 0., ok ? wecb[(size_t)(s0 + s) * C + c] : 0.);
     }
     __syncthreads();
-    int DE = ND * E;
-    int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= DE) return;
-    int e = j % E;
-    double x[PSF_TILE_S], w[PSF_TILE_S];
+    const int DE = ND * E;
+    const int j0 = blockIdx.x * (128 * PSF_CPT) + threadIdx.x;
+    double x[PSF_TILE_S][PSF_CPT], w[PSF_TILE_S][PSF_CPT];
 #pragma unroll
-    for (int s = 0; s < PSF_TILE_S; ++s) { x[s] = 0.; w[s] = 0.; }
-#pragma unroll 8
-    for (int c = 0; c < C; ++c) {  // unrolled: eight column loads in flight
-        const double col = pa[(size_t)c * DE + j];
+    for (int s = 0; s < PSF_TILE_S; ++s)
+#pragma unroll
+        for (int q = 0; q < PSF_CPT; ++q) { x[s][q] = 0.; w[s][q] = 0.; }
+#pragma unroll 2
+    for (int c = 0; c < C; ++c) {
+        double col[PSF_CPT];
+#pragma unroll
+        for (int q = 0; q < PSF_CPT; ++q) {
+            const int j = j0 + 128 * q;
+            col[q] = j < DE ? __ldg(pa + (size_t)c * DE + j) : 0.;
+        }
 #pragma unroll
         for (int s = 0; s < PSF_TILE_S; ++s) {
             const double2 xw = sxw[c][s];
-            x[s] = fma(xw.x, col, x[s]);
-            w[s] = fma(xw.y, col, w[s]);
+#pragma unroll
+            for (int q = 0; q < PSF_CPT; ++q) {
+                x[s][q] = fma(xw.x, col[q], x[s][q]);
+                w[s][q] = fma(xw.y, col[q], w[s][q]);
+            }
         }
     }
-    double l0 = ltf[e], l1 = ltf[E + e];
 #pragma unroll
-    for (int s = 0; s < PSF_TILE_S; ++s)
-        if (s < ns) out[(size_t)(s0 + s) * DE + j] = (x[s] * l0 + w[s] * l1) / expo[(size_t)(s0 + s) * E + e];
+    for (int q = 0; q < PSF_CPT; ++q) {
+        const int j = j0 + 128 * q;
+        if (j >= DE) continue;
+        const int e = j % E;
+        const double l0 = ltf[e], l1 = ltf[E + e];
+#pragma unroll
+        for (int s = 0; s < PSF_TILE_S; ++s)
+            if (s < ns)
+                out[(size_t)(s0 + s) * DE + j] = (x[s][q] * l0 + w[s][q] * l1) / expo[(size_t)(s0 + s) * E + e];
+    }
 }
 
 // b7: per (s, e) exact integral of the linear interpolant of 2 pi u(theta) sin(theta)
@@ -222,7 +243,7 @@ int launch_psf(const PsfDev& a, cudaStream_t st) {
                                                a.costh, a.C, a.logEs, a.E, a.af, a.ab, pa));
     if (a.S == 0) return XTS_OK;
     int DE = ND * a.E;
-    dim3 g((DE + 127) / 128, (a.S + PSF_TILE_S - 1) / PSF_TILE_S);
+    dim3 g((DE + 128 * PSF_CPT - 1) / (128 * PSF_CPT), (a.S + PSF_TILE_S - 1) / PSF_TILE_S);
     XTS_LAUNCH("k_mean_psf", st, k_mean_psf<<<g, 128, 0, st>>>(pa, a.C, a.E, a.ecb, a.wecb, a.S, a.ltf, a.exposure, a.upsf));
     XTS_LAUNCH("k_partial_integral", st, k_partial_scan<<<dim3(a.S, (a.E + 7) / 8), 256, 0, st>>>(a.upsf, a.partial, a.E));
     return XTS_OK;
@@ -242,7 +263,7 @@ int launch_psf_scratch(const PsfDev& a, double* king, double* pa, cudaStream_t s
                                                a.costh, a.C, a.logEs, a.E, a.af, a.ab, pa));
     if (a.S == 0) return XTS_OK;
     int DE = ND * a.E;
-    dim3 g((DE + 127) / 128, (a.S + PSF_TILE_S - 1) / PSF_TILE_S);
+    dim3 g((DE + 128 * PSF_CPT - 1) / (128 * PSF_CPT), (a.S + PSF_TILE_S - 1) / PSF_TILE_S);
     XTS_LAUNCH("k_mean_psf", st, k_mean_psf<<<g, 128, 0, st>>>(pa, a.C, a.E, a.ecb, a.wecb, a.S, a.ltf, a.exposure, a.upsf));
     XTS_LAUNCH("k_partial_integral", st, k_partial_scan<<<dim3(a.S, (a.E + 7) / 8), 256, 0, st>>>(a.upsf, a.partial, a.E));
     return XTS_OK;

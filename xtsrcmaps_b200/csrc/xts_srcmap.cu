@@ -540,6 +540,12 @@ int launch_srcmap(const SrcmapDev& a, cudaStream_t st) {
     XTS_LAUNCH("k_map_geometry", gs, k_map_geometry<<<gg, GEO_THREADS, 0, gs>>>(w, H, W, corners, centers, omega));
     if (S == 0) return XTS_OK;
     XTS_LAUNCH("k_boundary", gs, k_boundary_chord<<<S, 256, 0, gs>>>(w, a.src_sph, H, W, corners, info));
+    if (a.means_given) {
+        if ((rc = geo.join())) return rc;
+        if (a.out_f64 || !srcmap_adaptive_supported(E))
+            return set_error(XTS_ERR_ARG, "scale_model_map: FP32 maps with E <= 256 only");
+        return finish_mean_map(a, centers, omega, info, scale, nch, st);
+    }
     if (a.surrogate) {
         if ((rc = geo.join())) return rc;
         if (a.out_f64 || !srcmap_adaptive_supported(E))

@@ -7,11 +7,17 @@
 // an in-FOV source the window also enters the block's FP64 row histogram, whose
 // dot product with uPsf is the map integral of c7 (model_map.map_integral.cxx:4-48):
 //     sum_pix omega * value(pix, e) = sum_r Hist[r] * uPsf[r][e].
-// Every pixel's window is written once as a 36-byte record (8 FP32 weights and
-// the first row / row count).  Pixels whose points leave the window (those next
-// to the source) are "wide": they get a sparse record of their 24 (row, weight)
-// pairs from a shared pool instead, or, if the pool is full, are evaluated point
-// by point in pass B.
+// The rule points' squared chords are FP32 offsets from the pixel centre's FP64
+// squared chord (the biquadratic form of xts_point.cuh), compared with the
+// window's row edges, also as FP32 offsets from the centre: one FP64 table
+// search per pixel, none per point.  The histogram takes each window row of a
+// pixel inside the radius by one FP64 shared-memory atomic add.  Every pixel's
+// window is written once as a 16-byte record (3 FP32 weights and the first row /
+// row count), with the 8 weights of a window longer than 3 rows in a 32-byte
+// extension.  Pixels whose points leave the 8-row window (those next to the
+// source) are "wide": they get a sparse record of their 24 (row, weight) pairs
+// from a shared pool instead, or, if the pool is full, are evaluated point by
+// point in pass B.
 //
 // Pass B, k_srcmap_win (the write pass, d1 + d2 + c8 + c10): the source's scaled
 // table Y' = uPsf * exposure * correction (FP32, [401][EQ] float4, EQ odd so
@@ -33,146 +39,151 @@ constexpr size_t WA_OFF_BINS = 0;
 constexpr size_t WA_OFF_COEF = sizeof(SepBin) * NSB;
 constexpr size_t WA_OFF_HIST = WA_OFF_COEF + sizeof(float4) * 2 * ND;
 constexpr size_t WA_OFF_WTS = WA_OFF_HIST + (8 * ND + 15) / 16 * 16;
-constexpr size_t WA_OFF_BASE = WA_OFF_WTS + sizeof(float) * WT * RW;
-constexpr size_t WA_SMEM = WA_OFF_BASE + sizeof(int) * (WT + 4);
+constexpr size_t WA_SMEM = WA_OFF_WTS + sizeof(float) * WT * RW;
 
 constexpr int NSP = 24;  // entries of a sparse record: 12 points x 2 rows
 constexpr int META_OVERFLOW = -0x7fffffff - 1;  // wide pixel without a sparse record
+constexpr int REC_ROWS = 3;  // window rows held by the 16-byte main record
 
+// Per (source, pixel) the main record rec = {w0, w1, w2, meta}: meta >= 0 is the
+// window's first row (bits 0-15) and row count (bits 16-23), with the weights of
+// windows longer than REC_ROWS rows in ext (two float4, w0..w7); meta < 0 marks a
+// wide pixel (sparse record -1 - meta, or META_OVERFLOW).
 __global__ void __launch_bounds__(WT, 4) k_pixel_windows(const double* __restrict__ corners, const double* __restrict__ centers,
                                                       const double* __restrict__ omega, const SrcInfo* __restrict__ info,
                                                       const SepTab* __restrict__ septab, int H, int W, int nch,
-                                                      double* __restrict__ hist_out, float4* __restrict__ win,
-                                                      int* __restrict__ wmeta, float2* __restrict__ sparse,
+                                                      double* __restrict__ hist_out, float4* __restrict__ rec,
+                                                      float4* __restrict__ ext, float2* __restrict__ sparse,
                                                       int sparse_cap, int* __restrict__ sparse_count) {
     extern __shared__ __align__(16) unsigned char smem[];
     SepBin* sbin = (SepBin*)(smem + WA_OFF_BINS);
     float4* scoef = (float4*)(smem + WA_OFF_COEF);
     double* hist = (double*)(smem + WA_OFF_HIST);
     float* wts = (float*)(smem + WA_OFF_WTS);    // [RW][WT] windows (row-major by window slot)
-    int* wbase = (int*)(smem + WA_OFF_BASE);     // [WT] first row (-1: not in radius); [WT..WT+3] row min/max by parity
     const int s = blockIdx.y, t = threadIdx.x;
     const SrcInfo si = info[s];
     for (int k = t; k < NSB; k += WT) sbin[k] = septab->bins[k];
     for (int k = t; k < 2 * ND; k += WT) scoef[k] = ((const float4*)septab->coef)[k];
     for (int r = t; r < ND; r += WT) hist[r] = 0.;
-    if (t < 4) wbase[WT + t] = (t & 1) ? -1 : ND;
     double ch2 = 2.0 * sin(0.5 * si.radius_rad);
     ch2 *= ch2;
     const int npix = H * W, W1 = W + 1;
     const int ntiles = (npix + WT - 1) / WT;
     const size_t sp = (size_t)s * npix;
     __syncthreads();
-    int it = 0;
-    for (int tile = blockIdx.x; tile < ntiles; tile += nch, ++it) {
-        const int par = 2 * (it & 1);
-        // the other parity's min/max slots were last read before the previous
-        // iteration's closing barrier; reset them for the next iteration
-        if (t == 0) { wbase[WT + 2 - par] = ND; wbase[WT + 3 - par] = -1; }
+    for (int tile = blockIdx.x; tile < ntiles; tile += nch) {
         const int pix = tile * WT + t;
+        if (pix >= npix) continue;
+        const int h = pix / W, w = pix - h * W;
         bool inside = false;
-        int rb = -1;
-        if (pix < npix) {
-            const int h = pix / W, w = pix - h * W;
-            if (si.in_fov) {
-                const double* c = centers + 3 * (h * W1 + w);
-                const double x = si.dir[0] - c[0], y = si.dir[1] - c[1], z = si.dir[2] - c[2];
-                const double d2 = x * x + y * y + z * z;
-                if (d2 < ch2 * (1.0 - 1e-12)) inside = true;
-                else if (d2 > ch2 * (1.0 + 1e-12)) inside = false;
-                else inside = dir_diff(si.dir, c) <= si.radius_rad;
+        if (si.in_fov) {
+            const double* c = centers + 3 * (h * W1 + w);
+            const double x = si.dir[0] - c[0], y = si.dir[1] - c[1], z = si.dir[2] - c[2];
+            const double d2 = x * x + y * y + z * z;
+            if (d2 < ch2 * (1.0 - 1e-12)) inside = true;
+            else if (d2 > ch2 * (1.0 + 1e-12)) inside = false;
+            else inside = dir_diff(si.dir, c) <= si.radius_rad;
+        }
+        const PixQ g = pixel_q(pixel_geom(corners, W1, h, w, si));
+        const float om = (float)omega[pix];
+        float tc;
+        const int ic = point_row_bin(g.a0, sbin, scoef, &tc);
+        const int base = min(max(ic - 1 - RW / 2, 0), ND - RW);
+        // The window's row edges as FP32 offsets from the centre's FP64 squared
+        // chord, and the chord offsets of the rule points in FP32 from the
+        // biquadratic form: no FP64 per point, and no table search per point.
+        float d[RW];
+#pragma unroll
+        for (int j = 0; j < RW; ++j) {
+            const float4 cw = scoef[2 * (base + j) + 1];
+            d[j] = (float)(__hiloint2double(__float_as_int(cw.w), __float_as_int(cw.z)) - g.a0);
+        }
+        const float f1 = (float)g.a1, f2 = (float)g.a2, f3 = (float)g.a3, f4 = (float)g.a4;
+        const float f5 = (float)g.a5, f6 = (float)g.a6, f7 = (float)g.a7, f8 = (float)g.a8;
+        float* wd = wts + t;  // slot j at wd[j * WT]: lanes hit consecutive words
+#pragma unroll
+        for (int j = 0; j < RW; ++j) wd[j * WT] = 0.f;
+        bool wide = false;
+        int lo = RW, hi = -1;
+#pragma unroll
+        for (int p = 0; p < 12; ++p) {
+            const float u = c_rule_f[p][0], uu = c_rule_f[p][1], v = c_rule_f[p][2];
+            const float p0 = fmaf(f4, uu, f1 * u);
+            const float p1 = fmaf(f6, uu, fmaf(f3, u, f2));
+            const float p2 = fmaf(f8, uu, fmaf(f7, u, f5));
+            const float dq = fmaf(fmaf(p2, v, p1), v, p0);  // q(point) - q(centre)
+            int r = 0;
+            float dlo = d[0];
+#pragma unroll
+            for (int j = 1; j < RW; ++j) {
+                const bool ge = dq >= d[j];
+                r += ge;
+                dlo = ge ? d[j] : dlo;
             }
-            const PixQ g = pixel_q(pixel_geom(corners, W1, h, w, si));
-            const float om = (float)omega[pix];
-            float tc;
-            const int ic = point_row_bin(g.a0, sbin, scoef, &tc);
-            const int base = min(max(ic - 1 - RW / 2, 0), ND - RW);
-            float* wd = wts + t;  // slot j at wd[j * WT]: lanes hit consecutive words
+            const int k = base + r;  // the point's lower table row
+            const float wo = c_rule_w32[p] * om;
+            if (dq >= d[0] && r < RW - 1 && k >= 1) {
+                const float4 c0 = scoef[2 * k], c1 = scoef[2 * k + 1];
+                const float dl = (dq - dlo) * c0.x;  // q / q_k - 1
+                float tt;
+                if (dl >= -0.002f && dl <= 0.072f) {
+                    const float zz = fmaf(dl, 1.f / DPOLY_H, -DPOLY_C / DPOLY_H);
+                    const float P = fmaf(fmaf(fmaf(fmaf(c1.y, zz, c1.x), zz, c0.w), zz, c0.z), zz, c0.y);
+                    tt = (float)REDM1 * (dl * P);
+                } else {
+                    tt = t_exact(g.a0 + (double)dq, k + 1);
+                }
+                wd[r * WT] += (1.f - tt) * wo;
+                wd[(r + 1) * WT] += tt * wo;
+                lo = min(lo, r);
+                hi = max(hi, r + 1);
+            } else {
+                wide = true;
+            }
+        }
+        const size_t kk = sp + pix;
+        if (!wide) {
+            // map integral (c7): the window's rows of a pixel inside the radius
+            if (inside) {
 #pragma unroll
-            for (int j = 0; j < RW; ++j) wd[j * WT] = 0.f;
-            bool wide = false;
-            int lo = RW, hi = -1;
+                for (int j = 0; j < RW; ++j)
+                    if (j >= lo && j <= hi) atomicAdd(&hist[base + j], (double)wd[j * WT]);
+            }
+            const int nent = hi - lo + 1;
+            float f[RW];
 #pragma unroll
+            for (int j = 0; j < RW; ++j) f[j] = j < nent ? wd[min(j + lo, RW - 1) * WT] : 0.f;
+            const int meta = (base + lo) | (nent << 16);
+            rec[kk] = make_float4(f[0], f[1], f[2], __int_as_float(meta));
+            if (nent > REC_ROWS) {
+                ext[2 * kk] = make_float4(f[0], f[1], f[2], f[3]);
+                ext[2 * kk + 1] = make_float4(f[4], f[5], f[6], f[7]);
+            }
+        } else {
+            // a wide pixel (next to the source): its 12 points again with FP64 chords,
+            // for its sparse record and its map-integral rows alike
+            int meta = META_OVERFLOW;
+            const int slot = atomicAdd(sparse_count, 1);
+            float2* sr = slot < sparse_cap ? sparse + (size_t)slot * NSP : nullptr;
             for (int p = 0; p < 12; ++p) {
                 float tt;
                 const int idx = point_row_bin(point_q2(g, p), sbin, scoef, &tt);
-                const int r = idx - 1 - base;
                 const float wo = c_rule_w32[p] * om;
                 const float wa = (1.f - tt) * wo, wb = tt * wo;
-                if (r >= 0 && r < RW - 1) {
-                    wd[r * WT] += wa;
-                    wd[(r + 1) * WT] += wb;
-                    lo = min(lo, r);
-                    hi = max(hi, r + 1);
-                } else {
-                    wide = true;
-                    if (inside) {
-                        atomicAdd(&hist[idx - 1], (double)wa);
-                        atomicAdd(&hist[idx], (double)wb);
-                    }
+                if (sr) {
+                    sr[2 * p] = make_float2(wa, __int_as_float(idx - 1));
+                    sr[2 * p + 1] = make_float2(wb, __int_as_float(idx));
+                }
+                if (inside) {
+                    atomicAdd(&hist[idx - 1], (double)wa);
+                    atomicAdd(&hist[idx], (double)wb);
                 }
             }
-            // the FP32 window record of the write pass, shifted to its first row
-            float f[RW];
-#pragma unroll
-            for (int j = 0; j < RW; ++j) f[j] = 0.f;
-            int meta;
-            if (!wide) {
-#pragma unroll
-                for (int j = 0; j < RW; ++j)
-                    if (j <= hi - lo) f[j] = wd[min(j + lo, RW - 1) * WT];
-                meta = (base + lo) | ((hi - lo + 1) << 16);
-            } else {
-                const int slot = atomicAdd(sparse_count, 1);
-                if (slot < sparse_cap) {  // the 12 points again (rare: pixels next to the source)
-                    float2* rec = sparse + (size_t)slot * NSP;
-                    for (int p = 0; p < 12; ++p) {
-                        float tt;
-                        const int idx = point_row_bin(point_q2(g, p), sbin, scoef, &tt);
-                        const float wo = c_rule_w32[p] * om;
-                        rec[2 * p] = make_float2((1.f - tt) * wo, __int_as_float(idx - 1));
-                        rec[2 * p + 1] = make_float2(tt * wo, __int_as_float(idx));
-                    }
-                    meta = -1 - slot;
-                } else {
-                    meta = META_OVERFLOW;
-                }
-            }
-            win[2 * (sp + pix)] = make_float4(f[0], f[1], f[2], f[3]);
-            win[2 * (sp + pix) + 1] = make_float4(f[4], f[5], f[6], f[7]);
-            wmeta[sp + pix] = meta;
-            if (inside) {
-                rb = base;
-                atomicMin(&wbase[WT + par], base);
-                atomicMax(&wbase[WT + 1 + par], base + RW - 1);
-            }
+            if (sr) meta = -1 - slot;
+            rec[kk] = make_float4(0.f, 0.f, 0.f, __int_as_float(meta));
         }
-        wbase[t] = rb;
-        if (__syncthreads_or(inside)) {
-            const int rmin = wbase[WT + par], rmax = wbase[WT + 1 + par];
-            // 8 threads per row, each over 32 pixels (p = sub mod 8), combined in a
-            // fixed shuffle order; the four rows of a warp start at different pixels
-            // so that their window reads spread over the banks
-            const int sub = t & 7, a = (t >> 3) & 3;
-            for (int r0 = rmin; r0 <= rmax; r0 += WT / 8) {
-                const int r = r0 + (t >> 3);
-                double acc = 0.;
-                if (r <= rmax) {
-                    for (int i = 0; i < 32; ++i) {
-                        const int p = ((i + a) & 31) * 8 + sub;
-                        const int b0 = wbase[p];
-                        const int k = r - b0;
-                        if (b0 >= 0 && k >= 0 && k < RW) acc += (double)wts[k * WT + p];
-                    }
-                }
-                acc += __shfl_xor_sync(0xffffffffu, acc, 1);
-                acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-                acc += __shfl_xor_sync(0xffffffffu, acc, 4);
-                if (sub == 0 && r <= rmax) hist[r] += acc;
-            }
-        }
-        __syncthreads();
     }
+    __syncthreads();
     double* out = hist_out + ((size_t)s * nch + blockIdx.x) * ND;
     for (int r = t; r < ND; r += WT) out[r] = hist[r];
 }
@@ -197,18 +208,23 @@ static __host__ __device__ WinLayout win_layout(int E, int EQ) {
     return L;
 }
 
-// One pixel's record as read by pass B.
+// One pixel's record as read by pass B: the main record, and for a window of more
+// than REC_ROWS rows its extension.
 struct PixRec { int meta; float4 wa, wb; };
 
-__device__ __forceinline__ PixRec load_rec(const float4* win, const int* wmeta, size_t k, bool valid) {
+__device__ __forceinline__ PixRec load_rec(const float4* rec, const float4* ext, size_t k, bool valid) {
     PixRec r;
     r.meta = 0;
     r.wa = make_float4(0.f, 0.f, 0.f, 0.f);
     r.wb = r.wa;
     if (valid) {
-        r.meta = __ldg(wmeta + k);
-        r.wa = __ldg(win + 2 * k);
-        r.wb = __ldg(win + 2 * k + 1);
+        const float4 m = __ldg(rec + k);
+        r.meta = __float_as_int(m.w);
+        r.wa = make_float4(m.x, m.y, m.z, 0.f);
+        if (r.meta >= 0 && (r.meta >> 16) > REC_ROWS) {
+            r.wa = __ldg(ext + 2 * k);
+            r.wb = __ldg(ext + 2 * k + 1);
+        }
     }
     return r;
 }
@@ -218,7 +234,7 @@ __device__ __forceinline__ PixRec load_rec(const float4* win, const int* wmeta, 
 // block moves on to the next source's table.
 template <int NQ>
 __global__ void __launch_bounds__(BT, 2)
-k_srcmap_win(const float4* __restrict__ win, const int* __restrict__ wmeta, const float2* __restrict__ sparse,
+k_srcmap_win(const float4* __restrict__ win, const float4* __restrict__ ext, const float2* __restrict__ sparse,
              const float* __restrict__ lut, const double* __restrict__ corners, const double* __restrict__ omega,
              const SrcInfo* __restrict__ info, const SepTab* __restrict__ septab,
              int S, int s_base, int H, int W, int E, int EQ, int* status, float* __restrict__ out) {
@@ -242,7 +258,7 @@ k_srcmap_win(const float4* __restrict__ win, const int* __restrict__ wmeta, cons
     unsigned phase = 0;
     // (source, tile) of f, advanced by counting: no 64-bit division per tile
     int s = (int)(f0 / ntiles), tile = (int)(f0 - (long long)s * ntiles);
-    PixRec rec = load_rec(win, wmeta, (size_t)s * npix + tile * BT + t, f0 < f1 && tile * BT + t < npix);
+    PixRec rec = load_rec(win, ext, (size_t)s * npix + tile * BT + t, f0 < f1 && tile * BT + t < npix);
     for (long long f = f0; f < f1; ++f) {
         int sn = s, tn = tile + 1;  // the next tile
         if (tn == ntiles) { tn = 0; ++sn; }
@@ -260,12 +276,11 @@ k_srcmap_win(const float4* __restrict__ win, const int* __restrict__ wmeta, cons
         PixRec nxt;
         {
             const int pn = tn * BT;
-            nxt = load_rec(win, wmeta, (size_t)sn * npix + pn + t, f + 1 < f1 && pn + t < npix);
+            nxt = load_rec(win, ext, (size_t)sn * npix + pn + t, f + 1 < f1 && pn + t < npix);
             const int p2 = t2 * BT;
-            if (f + 2 < f1 && p2 + t < npix) {
+            if (f + 2 < f1 && p2 + t < npix && (t & 7) == 0) {  // one prefetch per 128-byte line
                 const size_t k2 = (size_t)s2 * npix + p2 + t;
-                asm volatile("prefetch.global.L2 [%0];" :: "l"(win + 2 * k2));
-                if ((t & 31) == 0) asm volatile("prefetch.global.L2 [%0];" :: "l"(wmeta + k2));
+                asm volatile("prefetch.global.L2 [%0];" :: "l"(win + k2));
             }
         }
         if (s != cur) {
@@ -398,7 +413,7 @@ k_srcmap_win(const float4* __restrict__ win, const int* __restrict__ wmeta, cons
 }
 
 template <int NQ>
-static int launch_write_pass(unsigned G, size_t smem, cudaStream_t st, const float4* win, const int* wmeta,
+static int launch_write_pass(unsigned G, size_t smem, cudaStream_t st, const float4* win, const float4* ext,
                              const float2* sparse, const float* lut, const double* corners, const double* omega,
                              const SrcInfo* info, const SepTab* tab, int S, int s_base, int H, int W, int E, int EQ,
                              int* status, float* out, int* per_sm, int nsm, bool query) {
@@ -407,12 +422,12 @@ static int launch_write_pass(unsigned G, size_t smem, cudaStream_t st, const flo
         XTS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_srcmap_win<NQ>, BT, smem));
         return XTS_OK;
     }
-    XTS_LAUNCH("k_srcmap", st, k_srcmap_win<NQ><<<G, BT, smem, st>>>(win, wmeta, sparse, lut, corners, omega, info, tab,
+    XTS_LAUNCH("k_srcmap", st, k_srcmap_win<NQ><<<G, BT, smem, st>>>(win, ext, sparse, lut, corners, omega, info, tab,
                                                                     S, s_base, H, W, E, EQ, status, out));
     return XTS_OK;
 }
 
-typedef int (*WritePassFn)(unsigned, size_t, cudaStream_t, const float4*, const int*, const float2*, const float*,
+typedef int (*WritePassFn)(unsigned, size_t, cudaStream_t, const float4*, const float4*, const float2*, const float*,
                            const double*, const double*, const SrcInfo*, const SepTab*, int, int, int, int, int, int,
                            int*, float*, int*, int, bool);
 static const WritePassFn k_write_pass[BQ] = {
@@ -426,7 +441,10 @@ bool srcmap_win_supported(int E) {
 }
 
 // Window records of one source chunk: 36 bytes per (source, pixel).
-static size_t win_bytes_per_source(int npix) { return (size_t)npix * 36; }
+// Window records of one source chunk: a 16-byte main record and a 32-byte
+// extension slot per (source, pixel); only windows of more than REC_ROWS rows
+// write and read their extension.
+static size_t win_bytes_per_source(int npix) { return (size_t)npix * 48; }
 
 // When the sources come in several chunks (host-mode copy-out, or records above
 // the buffer budget) and a geometry stream is given, the window pass of chunk k + 1
@@ -454,19 +472,19 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
     const int EQ = win_row_quads(E);
     const WinLayout L = win_layout(E, EQ);
     // sources per chunk: window records of at most ~1 GiB per buffer
-    const size_t budget = (size_t)1 << 30;
+    const size_t budget = (size_t)4 << 30;
     int Sc = (int)(budget / win_bytes_per_source(npix));
     if (chunk_sources > 0 && chunk_sources < Sc) Sc = chunk_sources;
     Sc = Sc < 1 ? 1 : (Sc > S ? S : Sc);
-    const size_t win_n = (size_t)Sc * npix * 2 + 4, meta_n = (size_t)Sc * npix + 4;
+    const size_t rec_n = (size_t)Sc * npix + 4, ext_n = (size_t)Sc * npix * 2 + 4;
     const size_t lut_n = (size_t)Sc * ND * EQ * 4 + 4;
     // sparse records for wide pixels: room for 1/8 of the chunk's pixels (at least 64k)
     long long cap = (long long)Sc * npix / 8;
     cap = cap < 65536 ? 65536 : cap;
     cap = cap > (long long)Sc * npix ? (long long)Sc * npix : cap;
     const size_t sp_n = (size_t)NSP * cap + 2;
-    float4* win0 = (float4*)workspace(W_WIN, sizeof(float4) * 2 * win_n);
-    int* wmeta0 = (int*)workspace(W_WMETA, sizeof(int) * 2 * meta_n);
+    float4* rec0 = (float4*)workspace(W_WIN, sizeof(float4) * 2 * rec_n);
+    float4* ext0 = (float4*)workspace(W_WMETA, sizeof(float4) * 2 * ext_n);
     float* lut0 = (float*)workspace(W_LUT, sizeof(float) * 2 * lut_n);
     float2* sparse0 = (float2*)workspace(W_SPARSE, sizeof(float2) * 2 * sp_n);
     int dev = 0, nsm = 148, per_sm = 0;
@@ -483,7 +501,7 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
     nch = nch < 1 ? 1 : (nch > maxch ? maxch : nch);
     const size_t hist_n = (size_t)Sc * nch * ND + 1;
     double* hist0 = (double*)workspace(W_PARTSUM, sizeof(double) * 2 * hist_n);
-    if (!win0 || !wmeta0 || !lut0 || !sparse0 || !hist0) return XTS_ERR_OOM;
+    if (!rec0 || !ext0 || !lut0 || !sparse0 || !hist0) return XTS_ERR_OOM;
     const WritePassFn wp = k_write_pass[(E + 3) / 4 - 1];
     rc = wp(0, L.total, st, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, 0, 0, E, EQ,
             nullptr, nullptr, &per_sm, nsm, true);
@@ -495,8 +513,8 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
     for (int s0 = 0; s0 < S; s0 += Sc, ++k) {
         const int n = S - s0 < Sc ? S - s0 : Sc, b = k & 1;
         const size_t oE = (size_t)s0 * E;
-        float4* win = win0 + b * win_n;
-        int* wmeta = wmeta0 + b * meta_n;
+        float4* rec = rec0 + b * rec_n;
+        float4* ext = ext0 + b * ext_n;
         float* lut = lut0 + b * lut_n;
         float2* sparse = sparse0 + b * sp_n;
         double* hist = hist0 + b * hist_n;
@@ -507,7 +525,7 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
         XTS_CUDA(cudaMemsetAsync(sparse_count, 0, sizeof(int), gs));
         XTS_LAUNCH("k_pixel_windows", gs, k_pixel_windows<<<dim3(nch, n), WT, WA_SMEM, gs>>>(
                                               corners, centers, omega, info + s0, tab, H, W, nch,
-                                              hist, win, wmeta, sparse, (int)cap,
+                                              hist, rec, ext, sparse, (int)cap,
                                               sparse_count));
         if (pipe) {
             XTS_CUDA(cudaEventRecord(evA[b], gs));
@@ -521,7 +539,7 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
         const long long T = (long long)n * ((npix + BT - 1) / BT);
         long long G = (long long)nsm * per_sm;
         if (G > T) G = T;
-        rc = wp((unsigned)G, L.total, st, win, wmeta, sparse, lut, corners, omega, info + s0, tab, n, s0, H, W, E, EQ,
+        rc = wp((unsigned)G, L.total, st, rec, ext, sparse, lut, corners, omega, info + s0, tab, n, s0, H, W, E, EQ,
                 status, out, nullptr, nsm, false);
         if (rc) return rc;
         if (on_chunk && (rc = on_chunk(on_chunk_ctx, s0, n, st))) return rc;

@@ -31,7 +31,7 @@
 
 namespace xts {
 
-constexpr int SUR_CHECK_EVERY = 61;         // every 61st pixel's values are also taken by the rule
+constexpr int SUR_CHECK_EVERY = 16;         // every 16th pixel's values are also taken by the rule
 constexpr long long SUR_CHUNK_VALUES = 1ll << 26;  // values per pass of the network (sources chunked)
 
 __device__ __forceinline__ int sur_row(double sdeg, double* t) {
@@ -182,7 +182,27 @@ int launch_surrogate_samples(const double* upsf, const double* logEs, int S, int
 }
 
 // ------------------------------------------------------------------ model map
-struct SurRange { float lo[5], hi[5], rho_min; };
+struct SurRange {
+    float lo[5], hi[5], rho_min;
+    float c0, cs0, c1, cs1;          // cell bins: a = (f0 - c0) * cs0, b = (slope - c1) * cs1
+    const unsigned char* cell_ok;    // [NR * NS] device, or NULL
+};
+constexpr int SUR_NCELL = XTS_MLP_CELL_NR * XTS_MLP_CELL_NS;
+
+// Whether the value's error cell (log10 rho, segment slope) is one the network was
+// calibrated to meet its bound in; cells: [NCELL] in shared memory (NULL: all).
+__device__ __forceinline__ bool sur_cell_ok(const SurRange& rg, const unsigned char* cells, float f0, float sl) {
+    if (!cells) return true;
+    const float a = (f0 - rg.c0) * rg.cs0, b = (sl - rg.c1) * rg.cs1;
+    if (!(a >= 0.f && a < (float)XTS_MLP_CELL_NR && b >= 0.f && b < (float)XTS_MLP_CELL_NS)) return false;
+    return cells[(int)a * XTS_MLP_CELL_NS + (int)b] != 0;
+}
+
+__device__ __forceinline__ const unsigned char* sur_cells_to_shared(const SurRange& rg, unsigned char* sh) {
+    if (!rg.cell_ok) return nullptr;
+    for (int k = threadIdx.x; k < SUR_NCELL; k += blockDim.x) sh[k] = rg.cell_ok[k];
+    return sh;
+}
 
 // Per block: SF_PIX pixels of one source of a chunk.  Phase 1, one thread per
 // pixel: the centre, the features that do not depend on energy and the 12 rule
@@ -208,13 +228,18 @@ __device__ __forceinline__ bool sur_geo_ok(const SurPix& q, const SurRange& rg) 
 }
 
 // Centre value and segment slope of one energy, and whether the network takes the value.
-__device__ __forceinline__ bool sur_value(const double* U, int E, int e, int ic, double tc, bool geo_ok,
-                                          float le, const SurRange& rg, double* uc, float* sl) {
+__device__ __forceinline__ bool sur_value(const double* U, int E, int e, int ic, double tc, bool geo_ok, float f0,
+                                          float le, const SurRange& rg, const unsigned char* cells, double* uc,
+                                          float* sl) {
     const double lo = U[(size_t)(ic - 1) * E + e], hi = U[(size_t)ic * E + e];
     *uc = (1.0 - tc) * lo + tc * hi;
     *sl = sur_slope(lo, hi);
-    return geo_ok && *uc > 0. && le >= rg.lo[3] && le <= rg.hi[3] && *sl >= rg.lo[4] && *sl <= rg.hi[4];
+    return geo_ok && *uc > 0. && le >= rg.lo[3] && le <= rg.hi[3] && *sl >= rg.lo[4] && *sl <= rg.hi[4] &&
+           sur_cell_ok(rg, cells, f0, *sl);
 }
+
+// Pixels of a chunk the check evaluates by the rule: every SUR_CHECK_EVERY-th.
+__device__ __forceinline__ bool sur_checked(int pix) { return pix % SUR_CHECK_EVERY == 0; }
 
 // Per block: SF_PIX pixels of one source of a chunk.  Phase 1, one thread per
 // pixel: the centre, the features that do not depend on energy and the 12 rule
@@ -237,10 +262,12 @@ __global__ void __launch_bounds__(SF_THREADS) k_sur_features(const double* __res
     __shared__ unsigned okbits[SF_PIX * 256 / 32];  // one bit per (pixel, energy) value, E <= 256
     __shared__ unsigned wsum[SF_THREADS / 32];
     __shared__ unsigned long long base_s;
+    __shared__ unsigned char cells_s[SUR_NCELL];
     const int s = s0 + blockIdx.y, t = threadIdx.x, lane = t & 31, wp = t >> 5;
     const int npix = H * W, p0 = blockIdx.x * SF_PIX;
     const int np = min(SF_PIX, npix - p0);
     const int nv = np * E;
+    const unsigned char* cells = sur_cells_to_shared(rg, cells_s);
     for (int k = t; k < (nv + 31) / 32; k += SF_THREADS) okbits[k] = 0u;
     if (t < np) {
         const int pix = p0 + t, h = pix / W, w = pix - h * W;
@@ -265,7 +292,7 @@ __global__ void __launch_bounds__(SF_THREADS) k_sur_features(const double* __res
         const SurPixS& o = sp[lp];
         double uc;
         float sl;
-        if (sur_value(U, E, e, o.ic, o.tc, o.geo_ok, (float)logEs[e], rg, &uc, &sl)) {
+        if (sur_value(U, E, e, o.ic, o.tc, o.geo_ok, o.f0, (float)logEs[e], rg, cells, &uc, &sl)) {
             atomicOr(&okbits[k >> 5], 1u << (k & 31));
             ++cnt;
         } else {
@@ -301,7 +328,7 @@ __global__ void __launch_bounds__(SF_THREADS) k_sur_features(const double* __res
         double uc;
         float sl;
         const float le = (float)logEs[e];
-        sur_value(U, E, e, o.ic, o.tc, o.geo_ok, le, rg, &uc, &sl);
+        sur_value(U, E, e, o.ic, o.tc, o.geo_ok, o.f0, le, rg, cells, &uc, &sl);
         float* x = X + j * 5;
         x[0] = o.f0; x[1] = o.f1; x[2] = o.f2; x[3] = le; x[4] = sl;
         aux[j] = make_float2((float)uc, o.eps);
@@ -310,22 +337,29 @@ __global__ void __launch_bounds__(SF_THREADS) k_sur_features(const double* __res
     }
 }
 
-// The network's values into the map: row i of the compacted input is value vidx[i].
+// The network's values into the map: row i of the compacted input is value vidx[i];
+// n_acc rows (counted on the device), at most n_max.
 __global__ void k_sur_assemble(const float2* __restrict__ aux, const unsigned* __restrict__ vidx,
-                               const float* __restrict__ y, long long n, float* __restrict__ mean) {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float2 a = aux[i];
-    mean[vidx[i]] = a.x * expf(y[i] * a.y);
+                               const float* __restrict__ y, const unsigned long long* __restrict__ n_acc,
+                               long long n_max, float* __restrict__ mean) {
+    const long long n = min(n_max, (long long)*n_acc);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float2 a = aux[i];
+        mean[vidx[i]] = a.x * expf(y[i] * a.y);
+    }
 }
 
-// The check: every SUR_CHECK_EVERY-th pixel of the chunk, all energies taken by
-// the network, against the rule; the largest relative difference per source.
+// The check: every SUR_CHECK_EVERY-th pixel of the chunk, all energies, by the
+// rule.  The rule's values replace the network's there, and the largest relative
+// difference over the values the network took is kept per source.
 __global__ void __launch_bounds__(128) k_sur_check(const double* __restrict__ corners, const SrcInfo* __restrict__ info,
                                                    const double* __restrict__ upsf, const double* __restrict__ logEs,
                                                    int s0, int H, int W, int E, SurRange rg,
-                                                   const float* __restrict__ mean, float* __restrict__ err,
-                                                   unsigned long long* __restrict__ counts) {
+                                                   float* __restrict__ mean, float* __restrict__ err,
+                                                   unsigned long long* __restrict__ chk) {
+    __shared__ unsigned char cells_s[SUR_NCELL];
+    const unsigned char* cells = sur_cells_to_shared(rg, cells_s);
+    __syncthreads();
     const int s = s0 + blockIdx.y, npix = H * W;
     const int pix = (blockIdx.x * blockDim.x + threadIdx.x) * SUR_CHECK_EVERY;
     float worst = 0.f;
@@ -336,14 +370,16 @@ __global__ void __launch_bounds__(128) k_sur_check(const double* __restrict__ co
         sur_pixel(pixel_geom(corners, W + 1, h, w, info[s]), sp);
         const bool geo_ok = sur_geo_ok(sp, rg);
         const double* U = upsf + (size_t)s * ND * E;
+        float* mrow = mean + ((size_t)s * npix + pix) * E;
         for (int e = 0; geo_ok && e < E; ++e) {
             double uc;
             float sl;
-            if (!sur_value(U, E, e, sp.ic, sp.tc, true, (float)logEs[e], rg, &uc, &sl)) continue;
+            if (!sur_value(U, E, e, sp.ic, sp.tc, true, sp.f0, (float)logEs[e], rg, cells, &uc, &sl)) continue;
             const double m = sur_rule(sp, U, E, e);
-            const double got = mean[((size_t)s * npix + pix) * E + e];
+            const double got = mrow[e];
             const float r = (float)(m != 0. ? fabs(got - m) / fabs(m) : fabs(got));
             worst = fmaxf(worst, r != r ? 3.4e38f : r);
+            mrow[e] = (float)m;
             ++nchk;
         }
     }
@@ -353,22 +389,83 @@ __global__ void __launch_bounds__(128) k_sur_check(const double* __restrict__ co
     }
     if ((threadIdx.x & 31) == 0) {
         if (worst > 0.f) atomicMax((int*)(err + s), __float_as_int(worst));  // non-negative floats order as ints
-        if (nchk) atomicAdd(counts, (unsigned long long)nchk);
+        if (nchk) atomicAdd(chk + s, (unsigned long long)nchk);
     }
 }
 
-// Every value of the listed sources by the rule.
+// Sources whose check exceeded tol, in source order: list [S], count list_n[0].
+__global__ void k_sur_fail_list(const float* __restrict__ err, int S, float tol, int* __restrict__ list,
+                                int* __restrict__ list_n) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int n = 0;
+    for (int s = 0; s < S; ++s)
+        if (!(err[s] <= tol)) list[n++] = s;
+    *list_n = n;
+}
+
+// Every value of the listed sources by the rule: a persistent grid over
+// (listed source, 128-pixel tile) items, the list's length read on the device.
 __global__ void __launch_bounds__(128) k_sur_fallback(const double* __restrict__ corners, const SrcInfo* __restrict__ info,
                                                       const double* __restrict__ upsf, const int* __restrict__ list,
-                                                      int H, int W, int E, float* __restrict__ mean) {
-    const int s = list[blockIdx.y], npix = H * W;
-    const int pix = blockIdx.x * blockDim.x + threadIdx.x;
-    if (pix >= npix) return;
-    const int h = pix / W, w = pix - h * W;
-    SurPix sp;
-    sur_pixel(pixel_geom(corners, W + 1, h, w, info[s]), sp);
-    const double* U = upsf + (size_t)s * ND * E;
-    for (int e = 0; e < E; ++e) mean[((size_t)s * npix + pix) * E + e] = (float)sur_rule(sp, U, E, e);
+                                                      const int* __restrict__ list_n, int H, int W, int E,
+                                                      float* __restrict__ mean) {
+    const int npix = H * W, ntile = (npix + 127) / 128;
+    const long long items = (long long)(*list_n) * ntile;
+    for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+        const int s = list[it / ntile];
+        const int pix = (int)(it % ntile) * 128 + threadIdx.x;
+        if (pix >= npix) continue;
+        const int h = pix / W, w = pix - h * W;
+        SurPix sp;
+        sur_pixel(pixel_geom(corners, W + 1, h, w, info[s]), sp);
+        const double* U = upsf + (size_t)s * ND * E;
+        for (int e = 0; e < E; ++e) mean[((size_t)s * npix + pix) * E + e] = (float)sur_rule(sp, U, E, e);
+    }
+}
+
+// The latest call's device counters, for xts_surrogate_last_stats.
+struct SurLast {
+    bool valid = false;
+    int S = 0;
+    long long per_src = 0;
+    float tol = 0.f;
+    const float* err = nullptr;
+    const unsigned long long* acc = nullptr;
+    const unsigned long long* chk = nullptr;
+    int* status = nullptr;
+};
+static SurLast g_sur_last;
+
+int surrogate_last_stats(xts_surrogate_stats* stats, cudaStream_t st) {
+    if (!stats) return set_error(XTS_ERR_ARG, "surrogate_last_stats: null argument");
+    memset(stats, 0, sizeof(*stats));
+    if (!g_sur_last.valid) return XTS_OK;
+    const SurLast& L = g_sur_last;
+    const int S = L.S;
+    std::vector<float> herr(S > 0 ? S : 1);
+    std::vector<unsigned long long> hacc(S > 0 ? S : 1), hchk(S > 0 ? S : 1);
+    XTS_CUDA(cudaMemcpyAsync(herr.data(), L.err, sizeof(float) * S, cudaMemcpyDeviceToHost, st));
+    XTS_CUDA(cudaMemcpyAsync(hacc.data(), L.acc, sizeof(unsigned long long) * S, cudaMemcpyDeviceToHost, st));
+    XTS_CUDA(cudaMemcpyAsync(hchk.data(), L.chk, sizeof(unsigned long long) * S, cudaMemcpyDeviceToHost, st));
+    int rc = mlp_check_status(L.status, st);  // synchronises the stream
+    if (rc) return rc;
+    float worst = 0.f;
+    long long accepted = 0, evaluated = 0, checked = 0;
+    int nfail = 0;
+    for (int s = 0; s < S; ++s) {
+        worst = herr[s] > worst ? herr[s] : worst;
+        evaluated += (long long)hacc[s];
+        checked += (long long)hchk[s];
+        if (!(herr[s] <= L.tol)) ++nfail;
+        else accepted += (long long)(hacc[s] - hchk[s]);
+    }
+    stats->values = (long long)S * L.per_src;
+    stats->accepted = accepted;  // the checked pixels' and the redone maps' values are the rule's
+    stats->checked = checked;
+    stats->maps_fallback = nfail;
+    stats->max_check_err = worst;
+    stats->evaluated = evaluated;
+    return XTS_OK;
 }
 
 int launch_srcmap_surrogate(const SrcmapDev& a, const double* corners, const double* centers, const double* omega,
@@ -380,6 +477,8 @@ int launch_srcmap_surrogate(const SrcmapDev& a, const double* corners, const dou
     for (int k = 0; k < XTS_MLP_IN; ++k)
         if (!(net->in_sd[k] > 0.f)) return set_error(XTS_ERR_ARG, "surrogate map: in_sd[%d] must be > 0", k);
     if (!(net->out_sd > 0.f)) return set_error(XTS_ERR_ARG, "surrogate map: out_sd must be > 0");
+    if (net->cell_ok && !(net->cell_hi[0] > net->cell_lo[0] && net->cell_hi[1] > net->cell_lo[1]))
+        return set_error(XTS_ERR_ARG, "surrogate map: error-cell ranges must be increasing");
     int rc = upload_rule_uv(st);
     if (rc) return rc;
     const long long per_src = npix * E;
@@ -391,22 +490,34 @@ int launch_srcmap_surrogate(const SrcmapDev& a, const double* corners, const dou
     float* yv = (float*)workspace(W_SUR_Y, sizeof(float) * (size_t)nmax + 16);
     unsigned* vidx = (unsigned*)workspace(W_SUR_IDX, sizeof(unsigned) * (size_t)nmax + 16);
     if (!vidx) return XTS_ERR_OOM;
-    // per source: largest check difference, values accepted; then the checked count,
-    // the status word, and the list of sources redone by the rule
-    const size_t o_cnt = align_up(sizeof(float) * S, 16), o_ctr = o_cnt + align_up(8 * (size_t)S, 16);
+    // per source: largest check difference, values the network evaluated, values
+    // checked; then the compacted row count, the status word, the failed-source
+    // count and list
+    const size_t o_cnt = align_up(sizeof(float) * S, 16), o_chk = o_cnt + align_up(8 * (size_t)S, 16);
+    const size_t o_ctr = o_chk + align_up(8 * (size_t)S, 16);
     const size_t o_list = o_ctr + 64;
     char* misc = (char*)workspace(W_SUR_ERR, o_list + sizeof(int) * (size_t)S + 16);
     if (!X || !aux || !yv || !misc) return XTS_ERR_OOM;
     float* err = (float*)misc;
     unsigned long long* acc_d = (unsigned long long*)(misc + o_cnt);
-    unsigned long long* counts = (unsigned long long*)(misc + o_ctr);  // [0] checked, [1] compacted rows
+    unsigned long long* chk_d = (unsigned long long*)(misc + o_chk);
+    unsigned long long* counts = (unsigned long long*)(misc + o_ctr);  // [1] compacted rows
     int* status = (int*)(counts + 4);
+    int* list_n = status + 1;
     int* list_d = (int*)(misc + o_list);
     XTS_CUDA(cudaMemsetAsync(misc, 0, o_list, st));
     SurRange rg;
     for (int k = 0; k < 5; ++k) { rg.lo[k] = net->lo[k]; rg.hi[k] = net->hi[k]; }
     rg.rho_min = net->rho_min;
+    rg.cell_ok = net->cell_ok;
+    rg.c0 = net->cell_lo[0];
+    rg.c1 = net->cell_lo[1];
+    rg.cs0 = net->cell_ok ? (float)XTS_MLP_CELL_NR / (net->cell_hi[0] - net->cell_lo[0]) : 0.f;
+    rg.cs1 = net->cell_ok ? (float)XTS_MLP_CELL_NS / (net->cell_hi[1] - net->cell_lo[1]) : 0.f;
     float* mean = (float*)a.out;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     for (int s0 = 0; s0 < S; s0 += sc) {
         const int ns = S - s0 < sc ? S - s0 : sc;
         const long long n = per_src * ns;
@@ -415,51 +526,29 @@ int launch_srcmap_surrogate(const SrcmapDev& a, const double* corners, const dou
         XTS_LAUNCH("k_sur_features", st, k_sur_features<<<gf, SF_THREADS, 0, st>>>(
                                              corners, info, a.upsf, a.logEs, s0, H, W, E, rg, X, aux, vidx,
                                              counts + 1, mean, acc_d));
-        unsigned long long n_acc = 0;  // rows of the compacted network input
-        XTS_CUDA(cudaMemcpyAsync(&n_acc, counts + 1, sizeof(n_acc), cudaMemcpyDeviceToHost, st));
-        XTS_CUDA(cudaStreamSynchronize(st));
-        if (n_acc > (unsigned long long)n) return set_error(XTS_ERR_CUDA, "surrogate map: compaction overflow");
-        if (n_acc) {
-            if ((rc = launch_mlp_forward(net, X, (long long)n_acc, yv, status, st))) return rc;
-            float* m0 = mean + (size_t)s0 * per_src;
-            XTS_LAUNCH("k_sur_assemble", st, k_sur_assemble<<<(unsigned)((n_acc + 255) / 256), 256, 0, st>>>(
-                                                 aux, vidx, yv, (long long)n_acc, m0));
-        }
+        // the network on the compacted rows; their count stays on the device
+        if ((rc = launch_mlp_forward_dev(net, X, counts + 1, n, yv, status, st))) return rc;
+        float* m0 = mean + (size_t)s0 * per_src;
+        XTS_LAUNCH("k_sur_assemble", st, k_sur_assemble<<<(unsigned)(8 * nsm), 256, 0, st>>>(
+                                             aux, vidx, yv, counts + 1, n, m0));
         const long long nck = (npix + SUR_CHECK_EVERY - 1) / SUR_CHECK_EVERY;
         const dim3 gc((unsigned)((nck + 127) / 128), (unsigned)ns);
         XTS_LAUNCH("k_sur_check", st, k_sur_check<<<gc, 128, 0, st>>>(corners, info, a.upsf, a.logEs, s0, H, W, E,
-                                                                      rg, mean, err, counts));
+                                                                      rg, mean, err, chk_d));
     }
-    if ((rc = mlp_check_status(status, st))) return rc;
-    std::vector<float> herr(S > 0 ? S : 1);
-    std::vector<unsigned long long> hacc(S > 0 ? S : 1);
-    unsigned long long hc = 0;
-    XTS_CUDA(cudaMemcpyAsync(herr.data(), err, sizeof(float) * S, cudaMemcpyDeviceToHost, st));
-    XTS_CUDA(cudaMemcpyAsync(hacc.data(), acc_d, sizeof(unsigned long long) * S, cudaMemcpyDeviceToHost, st));
-    XTS_CUDA(cudaMemcpyAsync(&hc, counts, sizeof(hc), cudaMemcpyDeviceToHost, st));
-    XTS_CUDA(cudaStreamSynchronize(st));
-    std::vector<int> list;
-    float worst = 0.f;
-    long long accepted = 0, evaluated = 0;
-    for (int s = 0; s < S; ++s) {
-        worst = herr[s] > worst ? herr[s] : worst;
-        evaluated += (long long)hacc[s];
-        if (!(herr[s] <= (float)a.check_tol)) list.push_back(s);
-        else accepted += (long long)hacc[s];
-    }
-    if (!list.empty()) {
-        XTS_CUDA(cudaMemcpyAsync(list_d, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, st));
-        const dim3 gb((unsigned)((npix + 127) / 128), (unsigned)list.size());
-        XTS_LAUNCH("k_sur_fallback", st, k_sur_fallback<<<gb, 128, 0, st>>>(corners, info, a.upsf, list_d, H, W, E, mean));
-    }
-    if (a.sur_stats) {
-        a.sur_stats->values = (long long)S * per_src;
-        a.sur_stats->accepted = accepted;  // the redone maps' values are the rule's
-        a.sur_stats->checked = (long long)hc;
-        a.sur_stats->maps_fallback = (int)list.size();
-        a.sur_stats->max_check_err = worst;
-        a.sur_stats->evaluated = evaluated;
-    }
+    // maps whose check failed are redone by the rule, listed and scheduled on the device
+    XTS_LAUNCH("k_sur_fail_list", st, k_sur_fail_list<<<1, 32, 0, st>>>(err, S, (float)a.check_tol, list_d, list_n));
+    XTS_LAUNCH("k_sur_fallback", st, k_sur_fallback<<<(unsigned)(4 * nsm), 128, 0, st>>>(
+                                          corners, info, a.upsf, list_d, list_n, H, W, E, mean));
+    g_sur_last.valid = true;
+    g_sur_last.S = S;
+    g_sur_last.per_src = per_src;
+    g_sur_last.tol = (float)a.check_tol;
+    g_sur_last.err = err;
+    g_sur_last.acc = acc_d;
+    g_sur_last.chk = chk_d;
+    g_sur_last.status = status;
+    if (a.sur_stats && (rc = surrogate_last_stats(a.sur_stats, st))) return rc;
     return finish_mean_map(a, centers, omega, info, scale, nch, st);
 }
 

@@ -7,12 +7,15 @@ bracket it, log10 of the pixel's solid angle, log10 of the energy and the log
 slope of the mean PSF's table segment at the centre -- to y = ln(m / u_c) rho^2, where m is the 12-point rule mean of the mean PSF over
 the pixel (the plain path's cubature, model_map/mm_cubature/cubature.implementation.cxx:21-55)
 and u_c the mean PSF at the centre.  Training samples come from the same FP64
-rule on synthetic pixels (``samples``); the network is trained on the GPU by the
-library's own kernels (forward on tcgen05 with BF16 operands, backward GEMMs on
-tcgen05, Adam); the model map (``api.point_src_model_map_wcs_surrogate``) takes
-the network's values where the centre is at least ``rho_min`` pixel sizes from
-the source and every feature lies in the training range, the rule's elsewhere,
-and checks every 61st pixel against the rule.
+rule on synthetic pixels (``samples``: separations log-uniform in 0.001-30 deg,
+pixel sizes 0.025-0.2 deg); the network is trained on the GPU by the library's
+own kernels (forward on tcgen05 with BF16 operands, backward GEMMs on tcgen05,
+Adam).  ``Surrogate.calibrate`` then measures the network's largest error on
+held-out samples per cell of (log10 rho, segment slope) and keeps the cells
+within half the error bound.  The model map (``model_map``) takes the network's
+values in those cells (and inside the training range), the rule's elsewhere,
+evaluates every 16th pixel by the rule as well (those pixels keep the rule's
+values) and redoes by the rule every map whose check exceeds the tolerance.
 
 All tensors live on the CUDA device; there is no CPU path.
 """
@@ -43,7 +46,7 @@ def _stream(dev) -> C.c_void_p:
     return C.c_void_p(h if h else 1)  # 0 would mean the library's own stream
 
 
-def samples(upsf, logEs, n: int, seed: int = 1, rho_min: float = 100.0):
+def samples(upsf, logEs, n: int, seed: int = 1, rho_min: float = 0.0):
     """Training samples from mean-PSF tables upsf [S, 401, E] (float64, CUDA) and
     log10 energies [E]: features X [n, 5] and targets Y [n] (float32, CUDA)."""
     torch = _torch()
@@ -77,7 +80,7 @@ class Surrogate:
     """Parameters (FP32 master copy, BF16 copies of the hidden layers), Adam
     state and standardisation of one surrogate network."""
 
-    def __init__(self, device=None, seed: int = 0, rho_min: float = 100.0):
+    def __init__(self, device=None, seed: int = 0, rho_min: float = 0.0):
         torch = _torch()
         self.device = torch.device(device) if device is not None else torch.device("cuda")
         rng = np.random.default_rng(seed)
@@ -105,6 +108,11 @@ class Surrogate:
         self.lo = np.full(I, -np.inf, np.float32)
         self.hi = np.full(I, np.inf, np.float32)
         self.rho_min = float(rho_min)
+        # error cells over (log10 rho, segment slope); None until calibrated: no restriction
+        self.cell_lo = np.zeros(2, np.float32)
+        self.cell_hi = np.ones(2, np.float32)
+        self.cell_ok = None  # uint8 CUDA tensor [NR * NS]
+        self.cell_err = None  # float64 numpy [NR, NS]: held-out max relative error per cell
 
     def refresh_bf16(self) -> None:
         """BF16 copies of W2 and W3 from the FP32 parameters (round to nearest even)."""
@@ -116,8 +124,47 @@ class Surrogate:
 
     def struct(self) -> L.XtsMlp:
         f5 = C.c_float * L.MLP_IN
+        f2 = C.c_float * 2
+        cells = _ptr(self.cell_ok) if self.cell_ok is not None else None
         return L.XtsMlp(_ptr(self.params), _ptr(self.wbf16), f5(*self.in_mu), f5(*self.in_sd),
-                        float(self.out_mu), float(self.out_sd), f5(*self.lo), f5(*self.hi), float(self.rho_min))
+                        float(self.out_mu), float(self.out_sd), f5(*self.lo), f5(*self.hi), float(self.rho_min),
+                        f2(*self.cell_lo), f2(*self.cell_hi), cells)
+
+    def calibrate(self, X, Y, tol: float = 1e-4, margin: float = 0.5, min_count: int = 200) -> dict:
+        """Error cells from held-out samples X [n, 5], Y [n] (not used in training):
+        per cell of (log10 rho, segment slope) the largest relative error of the
+        pixel mean, |exp((y_net - y) / rho^2) - 1|; the network takes values only in
+        cells with at least ``min_count`` samples whose largest error is within
+        ``margin * tol``.  Returns the share of held-out samples in accepted cells
+        and their largest error."""
+        torch = _torch()
+        NR, NS = L.MLP_CELL_NR, L.MLP_CELL_NS
+        yp = self.predict(X).double()
+        Xd = X.double()
+        rho2 = (10.0 ** Xd[:, 0]) ** 2
+        err = torch.expm1((yp - Y.double()) / rho2).abs()
+        err = torch.where(torch.isfinite(err), err, torch.full_like(err, float("inf")))
+        lo = np.array([float(self.lo[0]), float(self.lo[4])], np.float64)
+        hi = np.array([float(self.hi[0]), float(self.hi[4])], np.float64)
+        hi = np.where(hi > lo, hi, lo + 1.0)
+        self.cell_lo = lo.astype(np.float32)
+        self.cell_hi = (hi + 1e-6 * (hi - lo)).astype(np.float32)  # the training maximum falls inside
+        a = ((Xd[:, 0] - float(self.cell_lo[0])) * (NR / float(self.cell_hi[0] - self.cell_lo[0]))).floor().long()
+        b = ((Xd[:, 4] - float(self.cell_lo[1])) * (NS / float(self.cell_hi[1] - self.cell_lo[1]))).floor().long()
+        inside = (a >= 0) & (a < NR) & (b >= 0) & (b < NS)
+        cell = (a.clamp(0, NR - 1) * NS + b.clamp(0, NS - 1))[inside]
+        e_in = err[inside]
+        count = torch.zeros(NR * NS, dtype=torch.float64, device=X.device).index_add_(0, cell, torch.ones_like(e_in))
+        worst = torch.zeros(NR * NS, dtype=torch.float64, device=X.device).scatter_reduce_(
+            0, cell, e_in, reduce="amax", include_self=True)
+        ok = (count >= min_count) & (worst <= margin * tol)
+        self.cell_ok = ok.to(torch.uint8).contiguous()
+        self.cell_err = worst.view(NR, NS).cpu().numpy()
+        taken = ok[cell]
+        return {"held_out": int(X.shape[0]), "share_in_accepted_cells": float(taken.double().mean()),
+                "max_rel_err_in_accepted_cells": float(e_in[taken].max()) if bool(taken.any()) else 0.0,
+                "cells_accepted": int(ok.sum()), "cells": NR * NS, "tol": tol, "margin": margin,
+                "min_count": min_count}
 
     def fit_standardisation(self, X, Y) -> None:
         """Feature and target standardisation, and the accepted feature range, from
@@ -194,9 +241,12 @@ class Surrogate:
         return out
 
     def state(self) -> dict:
-        return {"params": self.params.cpu().numpy(), "in_mu": self.in_mu, "in_sd": self.in_sd,
-                "out": np.array([self.out_mu, self.out_sd], np.float64), "lo": self.lo, "hi": self.hi,
-                "rho_min": np.array(self.rho_min)}
+        st = {"params": self.params.cpu().numpy(), "in_mu": self.in_mu, "in_sd": self.in_sd,
+              "out": np.array([self.out_mu, self.out_sd], np.float64), "lo": self.lo, "hi": self.hi,
+              "rho_min": np.array(self.rho_min), "cell_lo": self.cell_lo, "cell_hi": self.cell_hi}
+        if self.cell_ok is not None:
+            st["cell_ok"] = self.cell_ok.cpu().numpy()
+        return st
 
     def save(self, path: str) -> None:
         np.savez(path, **self.state())
@@ -210,15 +260,33 @@ class Surrogate:
         net.in_mu, net.in_sd = z["in_mu"].astype(np.float32), z["in_sd"].astype(np.float32)
         net.out_mu, net.out_sd = float(z["out"][0]), float(z["out"][1])
         net.lo, net.hi = z["lo"].astype(np.float32), z["hi"].astype(np.float32)
+        if "cell_ok" in z:
+            net.cell_lo, net.cell_hi = z["cell_lo"].astype(np.float32), z["cell_hi"].astype(np.float32)
+            net.cell_ok = _torch().as_tensor(z["cell_ok"].astype(np.uint8), device=net.device)
         return net
 
 
+def _stats_dict(st) -> dict:
+    return {"values": st.values, "accepted": st.accepted, "checked": st.checked,
+            "maps_fallback": st.maps_fallback, "max_check_err": st.max_check_err, "evaluated": st.evaluated}
+
+
+def last_stats(device=None) -> dict:
+    """Counts of the latest surrogate model map (waits for it on torch's current stream)."""
+    torch = _torch()
+    st = L.XtsSurrogateStats()
+    L.check(L.lib().xts_surrogate_last_stats(C.byref(st), _stream(device or torch.device("cuda"))))
+    return _stats_dict(st)
+
+
 def model_map(wcs, src_sph, exposure, uPsf, partial_integrals, logEs, net: Surrogate,
-              check_tol: float = 1e-4, with_info: bool = True):
+              check_tol: float = 1e-4, with_info: bool = True, out=None, stats: bool = True):
     """point_src_model_map_wcs with the pixel means from the network where it
     applies (the FP64 12-point rule elsewhere, and for every map whose check
     fails).  CUDA tensors in; returns (float32 maps [S, H, W, E], SrcmapInfo or
-    None, stats dict)."""
+    None, stats dict or None).  With stats=False the call does not synchronise
+    (and, once warm, can be captured into a CUDA graph); ``last_stats`` reads the
+    counts afterwards."""
     torch = _torch()
     from .api import SrcmapInfo, _wcs_struct
 
@@ -226,19 +294,19 @@ def model_map(wcs, src_sph, exposure, uPsf, partial_integrals, logEs, net: Surro
     t = lambda x, dt=torch.float64: torch.as_tensor(x, dtype=dt, device=dev).contiguous()
     src, ex, up, pp, le = t(src_sph), t(exposure), t(uPsf), t(partial_integrals), t(logEs)
     S, E = int(src.shape[0]), int(ex.shape[1])
-    maps = torch.empty((S, int(wcs.naxis1), int(wcs.naxis2), E), dtype=torch.float32, device=dev)
+    maps = out if out is not None else torch.empty((S, int(wcs.naxis1), int(wcs.naxis2), E), dtype=torch.float32,
+                                                   device=dev)
     info = info_s = None
     if with_info:
         o = [torch.empty((S, E), dtype=torch.float64, device=dev), torch.empty((S, E), dtype=torch.float64, device=dev),
              torch.empty((S,), dtype=torch.float64, device=dev), torch.empty((S,), dtype=torch.int32, device=dev)]
         info_s = L.XtsSrcmapInfo(*[_ptr(x) for x in o])
         info = SrcmapInfo(*o)
-    st = L.XtsSurrogateStats()
+    st = L.XtsSurrogateStats() if stats else None
     s = net.struct()
     w = _wcs_struct(wcs)
     L.check(L.lib().xts_point_src_model_map_wcs_surrogate(
         C.byref(w), _ptr(src), S, _ptr(ex), _ptr(up), _ptr(pp), _ptr(le), E, C.byref(s), float(check_tol),
-        _ptr(maps), C.byref(info_s) if info_s is not None else None, C.byref(st), _stream(dev)))
-    stats = {"values": st.values, "accepted": st.accepted, "checked": st.checked,
-             "maps_fallback": st.maps_fallback, "max_check_err": st.max_check_err, "evaluated": st.evaluated}
-    return maps, info, stats
+        _ptr(maps), C.byref(info_s) if info_s is not None else None, C.byref(st) if st is not None else None,
+        _stream(dev)))
+    return maps, info, (_stats_dict(st) if st is not None else None)
