@@ -66,6 +66,7 @@ def parse():
                     help="time only the plain path (value is then the plain path's)")
     ap.add_argument("--no-c4", action="store_true", help="skip the chunked c4 measurement")
     ap.add_argument("--no-f64", action="store_true", help="skip the FP64-output plain path")
+    ap.add_argument("--no-cutouts", action="store_true", help="skip the c2 per-source cutout measurement")
     ap.add_argument("--no-oracle", action="store_true", help="skip the FP64 oracle error on sampled sources")
     ap.add_argument("--surrogate-samples", type=int, default=10_000_000)
     ap.add_argument("--surrogate-epochs", type=int, default=20)
@@ -525,6 +526,10 @@ def run_ours(args, rank, world, local_rank):
         ps_t = A.compute_psf_data(nf, nb, ex_t, d["logEs"], ltf)
         autotune = tune_write_pass(job.wcs, d["src"], ex_t.exposure, ps_t.uPsf, ps_t.partial_psf_integral)
 
+    cutouts = None
+    if args.config == "c2" and not args.no_cutouts and world == 1:
+        cutouts = measure_cutouts(args, A, job, d, nf, nb, ltf, stepper, torch, dev, rank)
+
     c4 = None
     if args.config == "c2" and not args.no_c4 and world == 1:
         del out_s
@@ -562,7 +567,8 @@ def run_ours(args, rank, world, local_rank):
         "dominant_kernel": dominant_of(head), "dominant_kernel_plain": dominant_of("plain"),
         "kernels": kernels_of(head), "kernels_plain": kernels_of("plain"), "gpu_launches": gpu_launches,
         "clocks": ck, "e2e": e2e, "cpu_baseline": cpu, "errors_vs_fp64_oracle": errors,
-        "surrogate": surrogate, "f64": f64, "c4": c4, "adaptive": adaptive, "autotune_write_pass": autotune,
+        "surrogate": surrogate, "f64": f64, "c2_cutouts": cutouts, "c4": c4, "adaptive": adaptive,
+        "autotune_write_pass": autotune,
     }
     print(json.dumps(line), flush=True)
 
@@ -649,6 +655,72 @@ def measure_f64(args, A, job, d, nf, nb, ltf, stepper, torch, dev, n_values, out
         idx = sample_sources(S, 4)
         res["errors_vs_fp64_oracle"] = oracle_errors(job, idx, {"f64": out})["f64"]
         res["errors_vs_fp64_oracle"]["sources"] = [int(i) for i in idx]
+    del out
+    torch.cuda.empty_cache()
+    return res
+
+
+def measure_cutouts(args, A, job, d, nf, nb, ltf, stepper, torch, dev, rank):
+    """c2 with its per-source cutout radii (2-15 deg): every source's map is its
+    window of the map (ragged output), the plain path's window and write passes
+    each one persistent launch over a work queue of (source, tile) items; exposure,
+    mean PSF and cutout maps captured in one CUDA graph per step; the FP64 oracle of
+    the same windows on sampled sources."""
+    cut, total = A.cutout_windows(job.wcs, job.src_sph, job.cutout_deg)
+    E = job.E
+    cut_d = torch.as_tensor(np.frombuffer(cut.tobytes(), dtype=np.uint8).copy(), device=dev)
+    out = torch.empty((total, E), dtype=torch.float32, device=dev)
+
+    def step():
+        with torch.cuda.stream(stepper.stream):
+            ex = A.compute_exposure(d["cube"], d["wcube"], d["logEs"], d["src"], d["af"], d["ab"], ltf)
+            ps = A.compute_psf_data(nf, nb, ex, d["logEs"], ltf)
+            A.point_src_model_map_cutouts(job.wcs, d["src"], cut_d, ex.exposure, ps.uPsf, ps.partial_psf_integral,
+                                          out=out, with_info=False)
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize(dev)
+    launch = "eager launches"
+    run = step
+    if stepper.use_graph:
+        try:
+            run = stepper.capture(step, args.warmup)
+            launch = "one CUDA graph per step"
+        except Exception as exc:
+            launch = "eager launches (graph capture failed: %s)" % str(exc).splitlines()[0][:120]
+    k = max(3, min(args.steps, 10))
+    ms = stepper.time(run, k)
+    nv = total * E
+    res = {"workload": "c2 with per-source cutouts (radii uniform 2-15 deg): source s's map is its window of the "
+                       "map, the reference's model map of that sub-map",
+           "value": nv / (ms / k * 1e-3), "unit": UNIT, "ms_per_step": ms / k, "steps": k, "launch": launch,
+           "values_per_step": nv, "dense_values": job.n_values, "pixels": total,
+           "hbm_gbs": 4.0 * nv / (ms / k * 1e-3) / 1e9}
+    if rank == 0 and not args.no_oracle:
+        from oracle import oracle as O
+
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import copy
+
+        from helpers import oracle_pipeline
+
+        idx = sample_sources(job.S, 8)
+        sub = copy.copy(job)
+        sub.src_sph = job.src_sph[idx]
+        r = oracle_pipeline(sub, with_map=False)
+        sc = cut[idx].copy()
+        sc["offset"] = np.concatenate([[0], np.cumsum(sc["nh"].astype(np.int64) * sc["nw"])[:-1]])
+        ref = O.point_src_model_map_cutouts(job.wcs, sub.src_sph, sc, r["exposure"], r["upsf"], r["partial"])
+        g = out.cpu().numpy()
+        worst = 0.0
+        for k_, s in enumerate(idx):
+            n = int(cut[s]["nh"]) * int(cut[s]["nw"])
+            if n:
+                a = g[int(cut[s]["offset"]):int(cut[s]["offset"]) + n].astype(np.float64)
+                b = ref["map"][int(sc[k_]["offset"]):int(sc[k_]["offset"]) + n]
+                worst = max(worst, float((np.abs(a - b) / np.maximum(np.abs(b), 1e-300)).max()))
+        res["errors_vs_fp64_oracle"] = {"max_rel_err": worst, "sources": [int(i) for i in idx]}
     del out
     torch.cuda.empty_cache()
     return res

@@ -206,6 +206,38 @@ int xts_point_src_model_map_wcs(const xts_wcs* wcs, const double* src_sph, int S
                                 const double* partial, int E, void* model_map,
                                 xts_srcmap_info* info, unsigned flags, void* stream);
 
+/* Per-source cutouts (no counterpart in the reference, which writes every source's
+ * map over the whole H x W grid, model_map/mm_cubature/cubature.implementation.cxx:33):
+ * source s's map covers the window of rows h0 .. h0 + nh - 1 and columns
+ * w0 .. w0 + nw - 1 of the map, stored [nh][nw][E] from value offset * E of a
+ * ragged output (offset = the pixels of all earlier windows). */
+typedef struct xts_cutout {
+    int h0, w0, nh, nw;
+    long long offset;
+} xts_cutout;
+
+/* Cutout windows for radii radius_deg [S]: the source's pixel (p1, p2) =
+ * sph2pix(src) (1-based), n = ceil(radius / |CDELTn|), rows round(p1) - 1 - n ..
+ * round(p1) - 1 + n clipped to the map (columns likewise; an empty window when the
+ * clipped range is empty).  Host pointers; total_pixels = the sum of nh * nw. */
+int xts_cutout_windows(const xts_wcs* wcs, const double* src_sph, const double* radius_deg, int S,
+                       xts_cutout* cut, long long* total_pixels);
+
+/* ModelMap::point_src_model_map_wcs (model_map/model_map.point_src_model_map_wcs.cxx:6-45)
+ * on per-source cutouts: source s's map is the reference's model map of the
+ * sub-map its window describes (the WCS with CRPIX shifted by the window's origin):
+ * its boundary radius and in-FOV flag (3.5 pixel buffer) are those of the window,
+ * its map integral runs over the window's pixels within that radius, and the
+ * correction follows from them (model_map.psf_boundary_radius.cxx:9-62,
+ * model_map.map_integral.cxx:4-48, model_map.map_correction_factor.cxx:3-53).
+ * model_map is float [sum of nh * nw, E] in source order (cut[s].offset); cut is
+ * [S] (device with XTS_DEVICE_PTRS).  The window pass runs as one persistent launch
+ * over a work queue of (source, 256-pixel tile) items, the write pass as one
+ * persistent launch over the same items. */
+int xts_point_src_model_map_cutouts(const xts_wcs* wcs, const double* src_sph, int S, const xts_cutout* cut,
+                                    const double* exposure, const double* upsf, const double* partial, int E,
+                                    float* model_map, xts_srcmap_info* info, unsigned flags, void* stream);
+
 /* The model map of xts_point_src_model_map_wcs with adaptive cubature of each
  * pixel in place of the fixed 12-point rule: the Genz-Malik degree-7/5 rule on
  * the pixel (17 points), regions halved along the dimension with the larger

@@ -12,6 +12,7 @@ Objects passed as IRF grids need cosths, logEs, params and min_cos_theta.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 
@@ -342,3 +343,55 @@ def point_src_model_map_wcs_adaptive(wcs, src_sph, expo, upsf, partial, rtol: fl
                                               C.c_double(rtol), C.c_int(max_depth), mp, ip, fp, rp,
                                               fov.ctypes.data_as(_ip), n.ctypes.data_as(_ip))
     return dict(map=m, inv_integ=inv, factor=fac, radius=rad, in_fov=fov.astype(bool), nregions=n)
+
+
+def cutout_windows(wcs, src_sph, radius_deg):
+    """Per-source cutout windows (the library's xts_cutout_windows, restated): the
+    source's pixel (p1, p2) = sph2pix (1-based), n = ceil(radius / |CDELT|), rows
+    round(p1) - 1 - n .. round(p1) - 1 + n and columns likewise, clipped to the map.
+    Returns a list of (h0, w0, nh, nw, offset)."""
+    out, off = [], 0
+    H, W = int(wcs.naxis1), int(wcs.naxis2)
+    for (ra, dec), r in zip(np.asarray(src_sph, dtype=np.float64), np.asarray(radius_deg, dtype=np.float64)):
+        ra = ra - 360.0 if ra > 180.0 else (ra + 360.0 if ra < -180.0 else ra)
+        p1, p2 = sph2pix(wcs, ra, dec)
+        c = (0, 0, 0, 0)
+        if np.isfinite(p1) and np.isfinite(p2) and abs(p1) < 1e9 and abs(p2) < 1e9:
+            n1 = int(math.ceil(r / abs(wcs.cdelt1)))
+            n2 = int(math.ceil(r / abs(wcs.cdelt2)))
+            i = int(math.floor(abs(p1) + 0.5)) * (1 if p1 >= 0 else -1) - 1  # lround
+            j = int(math.floor(abs(p2) + 0.5)) * (1 if p2 >= 0 else -1) - 1
+            h0, h1 = max(0, i - n1), min(H, i + n1 + 1)
+            w0, w1 = max(0, j - n2), min(W, j + n2 + 1)
+            if h1 > h0 and w1 > w0:
+                c = (h0, w0, h1 - h0, w1 - w0)
+        out.append(c + (off,))
+        off += c[2] * c[3]
+    return out
+
+
+def point_src_model_map_cutouts(wcs, src_sph, cut, expo, upsf, partial):
+    """point_src_model_map_wcs of every source on its own window's sub-map (the WCS
+    with CRPIX shifted by the window's origin): the ragged map [sum nh nw, E] and
+    the per-source inv_integ, factor [S, E], radius, in_fov [S]."""
+    import copy
+
+    src = np.asarray(src_sph, dtype=np.float64)
+    E = np.asarray(expo).shape[1]
+    cut = [tuple(int(v) for v in c) for c in cut]
+    total = sum(c[2] * c[3] for c in cut)
+    m = np.zeros((total, E))
+    S = len(cut)
+    inv, fac = np.zeros((S, E)), np.ones((S, E))
+    rad, fov = np.zeros(S), np.zeros(S, dtype=bool)
+    for s, (h0, w0, nh, nw, off) in enumerate(cut):
+        if nh == 0 or nw == 0:
+            continue
+        sub = copy.copy(wcs)
+        sub.naxis1, sub.naxis2 = nh, nw
+        sub.crpix1, sub.crpix2 = wcs.crpix1 - h0, wcs.crpix2 - w0
+        r = point_src_model_map_wcs(sub, src[s:s + 1], np.asarray(expo)[s:s + 1], np.asarray(upsf)[s:s + 1],
+                                    np.asarray(partial)[s:s + 1])
+        m[off:off + nh * nw] = r["map"][0].reshape(nh * nw, E)
+        inv[s], fac[s], rad[s], fov[s] = r["inv_integ"][0], r["factor"][0], r["radius"][0], r["in_fov"][0]
+    return {"map": m, "inv_integ": inv, "factor": fac, "radius": rad, "in_fov": fov}

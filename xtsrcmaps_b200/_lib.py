@@ -7,6 +7,8 @@ calls raise.
 from __future__ import annotations
 
 import ctypes as C
+
+import numpy as np
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -28,6 +30,9 @@ XTS_FITS_F32 = 1 << 5
 
 ND = 401
 NOALLOC_SCRATCH_DOUBLES = 1 << 20  # XTS_NOALLOC_SCRATCH_DOUBLES
+
+# xts_cutout: one source's window of the map and its first pixel in the ragged output
+CUTOUT_DTYPE = np.dtype([("h0", "<i4"), ("w0", "<i4"), ("nh", "<i4"), ("nw", "<i4"), ("offset", "<i8")])
 
 _vp = C.c_void_p
 
@@ -155,6 +160,9 @@ SIGNATURES = {
                                                         C.POINTER(XtsSrcmapInfo),
                                                         C.POINTER(XtsSurrogateStats), _vp]),
     "xts_surrogate_last_stats": (C.c_int, [C.POINTER(XtsSurrogateStats), _vp]),
+    "xts_cutout_windows": (C.c_int, [C.POINTER(XtsWcs), _vp, _vp, C.c_int, _vp, C.POINTER(C.c_longlong)]),
+    "xts_point_src_model_map_cutouts": (C.c_int, [C.POINTER(XtsWcs), _vp, C.c_int, _vp, _vp, _vp, _vp, C.c_int,
+                                                  _vp, C.POINTER(XtsSrcmapInfo), C.c_uint, _vp]),
     "xts_rebin_wcs": (C.c_int, [C.POINTER(XtsWcs), C.c_double, C.POINTER(XtsWcs)]),
     "xts_allsky_crop_range": (C.c_int, [C.POINTER(XtsWcs), C.POINTER(XtsWcs), C.POINTER(C.c_long)]),
     "xts_crop_allsky": (C.c_int, [_vp, C.c_int, C.c_long, C.c_long, C.POINTER(C.c_long), _vp, C.c_uint, _vp]),

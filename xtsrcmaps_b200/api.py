@@ -518,6 +518,71 @@ def convolve_map_psf(image, kernel):
     return o
 
 
+def cutout_windows(wcs: Wcs, src_sph, radius_deg):
+    """Per-source cutout windows for radii ``radius_deg`` [S] (degrees): a structured
+    array [S] of (h0, w0, nh, nw, offset) (xts_cutout) and the total pixel count of
+    the ragged map.  Host function."""
+    src = np.ascontiguousarray(np.asarray(src_sph, dtype=np.float64).reshape(-1, 2))
+    rad = np.ascontiguousarray(np.asarray(radius_deg, dtype=np.float64).reshape(-1))
+    S = src.shape[0]
+    if rad.shape[0] != S:
+        raise ValueError("one radius per source")
+    cut = np.zeros(S, dtype=L.CUTOUT_DTYPE)
+    total = C.c_longlong(0)
+    w = _wcs_struct(wcs)
+    L.check(L.lib().xts_cutout_windows(C.byref(w), C.c_void_p(src.ctypes.data), C.c_void_p(rad.ctypes.data), S,
+                                       C.c_void_p(cut.ctypes.data), C.byref(total)))
+    return cut, int(total.value)
+
+
+def point_src_model_map_cutouts(wcs: Wcs, src_sph, cut, exposure, uPsf, partial_integrals, out=None,
+                                with_info: bool = True):
+    """ModelMap::point_src_model_map_wcs (model_map/model_map.point_src_model_map_wcs.cxx:6-45)
+    on per-source cutouts ``cut`` (cutout_windows): source s's map is the reference's
+    model map of its window's sub-map, stored [nh, nw, E] from pixel cut[s].offset of
+    a ragged float32 map [total_pixels, E].  CUDA inputs run on the device (``cut``
+    then as the uint8 CUDA tensor of the structured array's bytes, or the numpy
+    array itself, which is copied).  Returns (map, SrcmapInfo or None)."""
+    cut_np = None if _is_cuda(cut) else np.ascontiguousarray(np.asarray(cut, dtype=L.CUTOUT_DTYPE))
+    like = _device_of(src_sph, exposure, uPsf)
+    c = _Call(like is not None, like)
+    sp, sa = c.inp(src_sph)
+    S = int(sa.shape[0]) if sa.ndim == 2 else 0
+    ep, ea = c.inp(exposure)
+    E = int(ea.shape[1])
+    up, _ = c.inp(uPsf)
+    pp, _ = c.inp(partial_integrals)
+    if cut_np is not None:
+        total = int((cut_np["nh"].astype(np.int64) * cut_np["nw"]).sum())
+    if c.device:
+        if cut_np is not None:
+            cut_d = c.torch.as_tensor(np.frombuffer(cut_np.tobytes(), dtype=np.uint8).copy(), device=c.dev)
+        else:
+            cut_d = cut
+        c.keep.append(cut_d)
+        cutp = C.c_void_p(cut_d.data_ptr())
+        if out is None:
+            if cut_np is None:
+                raise ValueError("pass out (the ragged map) with a device-resident cut")
+            out = c.torch.empty((total, E), dtype=c.torch.float32, device=c.dev)
+        mp = C.c_void_p(out.data_ptr())
+    else:
+        cutp = C.c_void_p(cut_np.ctypes.data)
+        if out is None:
+            out = np.empty((total, E), dtype=np.float32)
+        mp = C.c_void_p(out.ctypes.data)
+    info = info_s = None
+    if with_info:
+        o = [c.out((S, E)), c.out((S, E)), c.out((S,)), c.out((S,), "i32")]
+        info_s = L.XtsSrcmapInfo(*[x[0] for x in o])
+        info = SrcmapInfo(*[x[1] for x in o])
+    w = _wcs_struct(wcs)
+    L.check(L.lib().xts_point_src_model_map_cutouts(C.byref(w), sp, S, cutp, ep, up, pp, E, mp,
+                                                    C.byref(info_s) if info_s is not None else None, c.flags,
+                                                    c.stream))
+    return out, info
+
+
 def rebin_wcs(wcs: Wcs, target_pix_size: float) -> Wcs:
     """rebin_wcs_config (sky_geom/sky_geom.hxx:352-371): the WCS of the same region at
     pixel size ``target_pix_size`` degrees (CDELT2 rebinned, where the reference

@@ -5,9 +5,11 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
+#include "xts_geom.cuh"
 #include "xts_internal.cuh"
 
 namespace xts {
@@ -915,6 +917,84 @@ int xts_convolve_map_psf(const double* image, int E, int H, int W, const double*
     double* o = sg.out(out, (size_t)E * PH * PW);
     int rc = sg.rc ? sg.rc : convolve_map_psf(im, E, H, W, ke, K, o, sg.st);
     return sg.finish(rc);
+}
+
+static bool wcs_ok(const xts_wcs* w);
+
+int xts_cutout_windows(const xts_wcs* wcs, const double* src_sph, const double* radius_deg, int S,
+                       xts_cutout* cut, long long* total_pixels) {
+    if (!wcs_ok(wcs) || S < 0 || (S > 0 && (!src_sph || !radius_deg || !cut)))
+        return set_error(XTS_ERR_ARG, "cutout_windows: bad WCS or null argument");
+    const WcsDev w = make_wcs(*wcs);
+    const long H = wcs->naxis1, W = wcs->naxis2;
+    long long off = 0;
+    for (int s = 0; s < S; ++s) {
+        if (!(radius_deg[s] >= 0.) || !std::isfinite(radius_deg[s]))
+            return set_error(XTS_ERR_ARG, "cutout_windows: radius %d must be finite and >= 0", s);
+        double ra = src_sph[2 * s], p1 = 0., p2 = 0.;
+        ra = ra > 180. ? ra - 360. : (ra < -180. ? ra + 360. : ra);
+        sph2pix(w, ra, src_sph[2 * s + 1], &p1, &p2);
+        xts_cutout c{0, 0, 0, 0, off};
+        if (std::isfinite(p1) && std::isfinite(p2) && fabs(p1) < 1e9 && fabs(p2) < 1e9) {
+            const long n1 = (long)ceil(radius_deg[s] / fabs(wcs->cdelt1));
+            const long n2 = (long)ceil(radius_deg[s] / fabs(wcs->cdelt2));
+            const long i = lround(p1) - 1, j = lround(p2) - 1;
+            const long h0 = std::max(0L, i - n1), h1 = std::min(H, i + n1 + 1);
+            const long w0 = std::max(0L, j - n2), w1 = std::min(W, j + n2 + 1);
+            if (h1 > h0 && w1 > w0) {
+                c.h0 = (int)h0; c.nh = (int)(h1 - h0);
+                c.w0 = (int)w0; c.nw = (int)(w1 - w0);
+            }
+        }
+        cut[s] = c;
+        off += (long long)c.nh * c.nw;
+    }
+    if (total_pixels) *total_pixels = off;
+    return XTS_OK;
+}
+
+int xts_point_src_model_map_cutouts(const xts_wcs* wcs, const double* src_sph, int S, const xts_cutout* cut,
+                                    const double* exposure, const double* upsf, const double* partial, int E,
+                                    float* model_map, xts_srcmap_info* info, unsigned flags, void* stream) {
+    XTS_ENTER();
+    if (!wcs_ok(wcs))
+        return set_error(XTS_ERR_ARG, "point_src_model_map_cutouts: bad WCS (CAR/AIT, nonzero CDELT)");
+    if (S < 0 || E <= 0 || E > 52 || (S > 0 && (!src_sph || !cut || !exposure || !upsf || !partial || !model_map)))
+        return set_error(XTS_ERR_ARG, "point_src_model_map_cutouts: null argument or bad size (E <= 52)");
+    if ((long long)wcs->naxis1 * wcs->naxis2 > (1LL << 30) || S > 65535)
+        return set_error(XTS_ERR_ARG, "point_src_model_map_cutouts: map or source count too large");
+    if (flags & ~(unsigned)XTS_DEVICE_PTRS)
+        return set_error(XTS_ERR_ARG, "point_src_model_map_cutouts: only XTS_DEVICE_PTRS applies");
+    const bool dev = (flags & XTS_DEVICE_PTRS) != 0;
+    long long total = 0;
+    if (!dev) {  // host windows: check them and size the staged map
+        for (int s = 0; s < S; ++s) {
+            const xts_cutout& c = cut[s];
+            if (c.nh < 0 || c.nw < 0 || c.h0 < 0 || c.w0 < 0 || c.h0 + c.nh > wcs->naxis1 ||
+                c.w0 + c.nw > wcs->naxis2 || c.offset != total)
+                return set_error(XTS_ERR_ARG, "point_src_model_map_cutouts: window %d outside the map or out of order",
+                                 s);
+            total += (long long)c.nh * c.nw;
+        }
+    }
+    Stager sg{dev, stream ? (cudaStream_t)stream : g_ctx.stream};
+    SrcmapDev a;
+    a.wcs = *wcs;
+    a.src_sph = sg.in(src_sph, (size_t)2 * S); a.S = S;
+    a.cut = sg.in(cut, (size_t)S);
+    a.exposure = sg.in(exposure, (size_t)S * E);
+    a.upsf = sg.in(upsf, (size_t)S * ND * E);
+    a.partial = sg.in(partial, (size_t)S * ND * E); a.E = E;
+    a.out_f64 = false;
+    a.out = sg.out(model_map, (size_t)(dev ? 1 : total) * E);
+    a.inv_integ = info ? sg.out(info->inv_map_integral, (size_t)S * E) : nullptr;
+    a.correction = info ? sg.out(info->correction, (size_t)S * E) : nullptr;
+    a.radius = info ? sg.out(info->psf_radius, (size_t)S) : nullptr;
+    a.in_fov = info ? sg.out(info->in_fov, (size_t)S) : nullptr;
+    int rc = sg.rc ? sg.rc : (S > 0 ? launch_srcmap(a, sg.st) : XTS_OK);
+    rc = sg.finish(rc);
+    if (rc == XTS_OK && !dev && S > 0) rc = srcmap_status(sg.st);
+    return rc;
 }
 
 static bool wcs_ok(const xts_wcs* w) {

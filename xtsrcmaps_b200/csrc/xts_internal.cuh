@@ -64,7 +64,7 @@ enum Slot {
     // internal scratch
     W_CORNERS, W_CENTERS, W_OMEGA, W_LUT, W_PARTSUM, W_SRCINFO, W_SCALE, W_PSFTAB,
     W_KING, W_MISC, W_WIN, W_WMETA, W_SPARSE, W_MISC2, W_EXPMAP,
-    W_FITS_IN, W_FITS_OUT, W_FITS_SUM, W_FFT_A, W_FFT_B, W_FFT_C, W_FFT_WORK, W_SRCPIX,
+    W_FITS_IN, W_FITS_OUT, W_FITS_SUM, W_FFT_A, W_FFT_B, W_FFT_C, W_FFT_WORK, W_SRCPIX, W_CUT_ITEMS,
     W_MLP_Z, W_MLP_H, W_MLP_DZ, W_MLP_DH, W_MLP_Y, W_MLP_ST, W_MLP_PART, W_MLP_PART2, W_SUR_X, W_SUR_AUX, W_SUR_Y, W_SUR_IDX, W_SUR_ERR,
     N_SLOTS
 };
@@ -140,6 +140,8 @@ struct SrcmapDev {
     // a.out holds FP32 pixel means on entry: only the scalings of c7-c10 and d2 are
     // applied (the diffuse map's final steps)
     bool means_given = false;
+    // per-source cutout windows [S] (device), or NULL for the dense map
+    const xts_cutout* cut = nullptr;
     // pixel means from the surrogate network (with the 12-point rule as fallback)
     const xts_mlp* surrogate = nullptr;
     const double* logEs = nullptr;  // [E] log10 energies (the network's fourth feature)
@@ -231,6 +233,10 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
                       int (*on_chunk)(void*, int, int, cudaStream_t), void* on_chunk_ctx,
                       StreamJoin& geo,  // the first chunk's window pass runs on geo.from
                       cudaStream_t st);  // 0, or XTS_ERR_TIMEOUT if a bounded device wait gave up
+int launch_srcmap_win_cut(const double* corners, const double* centers, const double* omega, const SrcInfo* info,
+                          const xts_cutout* cut, int S, int H, int W, int E, const double* upsf,
+                          const double* partial, const double* exposure, double* scale, double* inv_integ,
+                          double* correction, double* radius, int* in_fov, int* status, float* out, cudaStream_t st);
 int launch_srcmap_fast(const double* corners, const double* omega, const SrcInfo* info,
                        const double* upsf, const double* scale, int S, int H, int W, int E,
                        float* out, cudaStream_t st);

@@ -158,17 +158,36 @@ __device__ __forceinline__ double block_reduce(double x, double* red, Op op) {
     return x;
 }
 
-__global__ void __launch_bounds__(256) k_boundary_chord(WcsDev w, const double* src_sph, int H, int W,
-                                                        const double* corners, SrcInfo* info) {
+// With cut given, source s's map is its cutout window: the border is the window's
+// (corner rows h0 .. h0 + nh, columns w0 .. w0 + nw) and the in-FOV buffer is
+// measured from the window's edges; an empty window is out of the FOV.
+__global__ void __launch_bounds__(256) k_boundary_chord(WcsDev w, const double* src_sph, int Hf, int Wf,
+                                                        const double* corners, SrcInfo* info,
+                                                        const xts_cutout* cut) {
     __shared__ double red[32];
-    const int s = blockIdx.x, W1 = W + 1, nb = 2 * (H + 1) + 2 * (W + 1);
+    const int s = blockIdx.x, W1 = Wf + 1;
+    int h0 = 0, w0 = 0, H = Hf, W = Wf;
+    if (cut) {
+        const xts_cutout c = cut[s];
+        h0 = c.h0; w0 = c.w0; H = c.nh; W = c.nw;
+    }
+    const int nb = 2 * (H + 1) + 2 * (W + 1);
     const double ra = src_sph[2 * s], dec = src_sph[2 * s + 1];
     double sd[3];
     sph2dir(ra, dec, sd);
+    if (H <= 0 || W <= 0) {  // empty cutout (block-uniform)
+        if (threadIdx.x == 0) {
+            SrcInfo si;
+            si.dir[0] = sd[0]; si.dir[1] = sd[1]; si.dir[2] = sd[2];
+            si.radius_deg = 0.; si.radius_rad = 0.; si.in_fov = 0; si.pad = 0;
+            info[s] = si;
+        }
+        return;
+    }
     auto chord2 = [&](int k) {
         int i, j;
         border_point(k, H, W, &i, &j);
-        const double* c = corners + 3 * ((size_t)i * W1 + j);
+        const double* c = corners + 3 * ((size_t)(h0 + i) * W1 + (w0 + j));
         const double x = sd[0] - c[0], y = sd[1] - c[1], z = sd[2] - c[2];
         return x * x + y * y + z * z;
     };
@@ -181,13 +200,15 @@ __global__ void __launch_bounds__(256) k_boundary_chord(WcsDev w, const double* 
         if (chord2(k) <= lim) {
             int i, j;
             border_point(k, H, W, &i, &j);
-            const double d = R2D * dir_diff(sd, corners + 3 * ((size_t)i * W1 + j));
+            const double d = R2D * dir_diff(sd, corners + 3 * ((size_t)(h0 + i) * W1 + (w0 + j)));
             mn = mn < d ? mn : d;
         }
     mn = block_reduce(mn, red, [](double a, double b) { return a < b ? a : b; });
     if (threadIdx.x == 0) {
         double r = ra > 180. ? ra - 360. : (ra < -180. ? ra + 360. : ra), p1, p2;
         sph2pix(w, r, dec, &p1, &p2);
+        p1 -= h0;  // pixel coordinates of the (window's) sub-map
+        p2 -= w0;
         const double buf = 3.5;
         SrcInfo si;
         si.dir[0] = sd[0]; si.dir[1] = sd[1]; si.dir[2] = sd[2];
@@ -539,7 +560,18 @@ int launch_srcmap(const SrcmapDev& a, cudaStream_t st) {
     const dim3 gg((unsigned)((W + GT) / GT), (unsigned)((H + GT) / GT));  // tiles over the (H+1) x (W+1) grid
     XTS_LAUNCH("k_map_geometry", gs, k_map_geometry<<<gg, GEO_THREADS, 0, gs>>>(w, H, W, corners, centers, omega));
     if (S == 0) return XTS_OK;
-    XTS_LAUNCH("k_boundary", gs, k_boundary_chord<<<S, 256, 0, gs>>>(w, a.src_sph, H, W, corners, info));
+    XTS_LAUNCH("k_boundary", gs, k_boundary_chord<<<S, 256, 0, gs>>>(w, a.src_sph, H, W, corners, info, a.cut));
+    if (a.cut) {
+        if ((rc = geo.join())) return rc;
+        if (a.out_f64 || !srcmap_win_supported(E))
+            return set_error(XTS_ERR_ARG, "cutout maps: FP32 maps with E <= %d only", 52);
+        int* status = (int*)workspace(W_MISC, 64);
+        if (!status) return XTS_ERR_OOM;
+        XTS_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
+        return launch_srcmap_win_cut(corners, centers, omega, info, a.cut, S, H, W, E, a.upsf, a.partial,
+                                     a.exposure, scale, a.inv_integ, a.correction, a.radius, a.in_fov, status,
+                                     (float*)a.out, st);
+    }
     if (a.means_given) {
         if ((rc = geo.join())) return rc;
         if (a.out_f64 || !srcmap_adaptive_supported(E))

@@ -49,6 +49,162 @@ constexpr int REC_ROWS = 3;  // window rows held by the 16-byte main record
 // window's first row (bits 0-15) and row count (bits 16-23), with the weights of
 // windows longer than REC_ROWS rows in ext (two float4, w0..w7); meta < 0 marks a
 // wide pixel (sparse record -1 - meta, or META_OVERFLOW).
+struct PassA {
+    const SepBin* sbin;    // shared: row bins
+    const float4* scoef;   // shared: per-row records
+    double* hist;          // shared: the block's map-integral rows
+    float* wts;            // shared: [RW][WT] windows
+    float4* rec;
+    float4* ext;
+    float2* sparse;
+    int sparse_cap;
+    int* sparse_count;
+};
+
+// Shared tables of pass A, loaded by every block.
+__device__ __forceinline__ PassA pass_a_tables(unsigned char* smem, const SepTab* septab, float4* rec, float4* ext,
+                                               float2* sparse, int sparse_cap, int* sparse_count) {
+    PassA A;
+    A.sbin = (const SepBin*)(smem + WA_OFF_BINS);
+    A.scoef = (const float4*)(smem + WA_OFF_COEF);
+    A.hist = (double*)(smem + WA_OFF_HIST);
+    A.wts = (float*)(smem + WA_OFF_WTS);
+    A.rec = rec; A.ext = ext; A.sparse = sparse; A.sparse_cap = sparse_cap; A.sparse_count = sparse_count;
+    SepBin* sb = (SepBin*)(smem + WA_OFF_BINS);
+    float4* sc = (float4*)(smem + WA_OFF_COEF);
+    for (int k = threadIdx.x; k < NSB; k += WT) sb[k] = septab->bins[k];
+    for (int k = threadIdx.x; k < 2 * ND; k += WT) sc[k] = ((const float4*)septab->coef)[k];
+    for (int r = threadIdx.x; r < ND; r += WT) A.hist[r] = 0.;
+    return A;
+}
+
+// One (source, pixel): map pixel (h, w) of the full grid (W1 = W + 1 corner columns,
+// omega index om_idx), record index kk.  Pixels whose centre lies within the
+// boundary radius (squared chord ch2) add their window rows to the block's
+// histogram; the rows they touch widen [*rlo, *rhi] when those are given.
+__device__ __forceinline__ void window_pixel(const double* __restrict__ corners, const double* __restrict__ centers,
+                                             const double* __restrict__ omega, const SrcInfo& si, double ch2, int W1,
+                                             int h, int w, size_t om_idx, size_t kk, const PassA& A, int* rlo,
+                                             int* rhi) {
+    const int t = threadIdx.x;
+    bool inside = false;
+    if (si.in_fov) {
+        const double* c = centers + 3 * ((size_t)h * W1 + w);
+        const double x = si.dir[0] - c[0], y = si.dir[1] - c[1], z = si.dir[2] - c[2];
+        const double d2 = x * x + y * y + z * z;
+        if (d2 < ch2 * (1.0 - 1e-12)) inside = true;
+        else if (d2 > ch2 * (1.0 + 1e-12)) inside = false;
+        else inside = dir_diff(si.dir, c) <= si.radius_rad;
+    }
+    const PixQ g = pixel_q(pixel_geom(corners, W1, h, w, si));
+    const float om = (float)omega[om_idx];
+    float tc;
+    const int ic = point_row_bin(g.a0, A.sbin, A.scoef, &tc);
+    const int base = min(max(ic - 1 - RW / 2, 0), ND - RW);
+    // The window's row edges as FP32 offsets from the centre's FP64 squared
+    // chord, and the chord offsets of the rule points in FP32 from the
+    // biquadratic form: no FP64 per point, and no table search per point.
+    float d[RW];
+#pragma unroll
+    for (int j = 0; j < RW; ++j) {
+        const float4 cw = A.scoef[2 * (base + j) + 1];
+        d[j] = (float)(__hiloint2double(__float_as_int(cw.w), __float_as_int(cw.z)) - g.a0);
+    }
+    const float f1 = (float)g.a1, f2 = (float)g.a2, f3 = (float)g.a3, f4 = (float)g.a4;
+    const float f5 = (float)g.a5, f6 = (float)g.a6, f7 = (float)g.a7, f8 = (float)g.a8;
+    float* wd = A.wts + t;  // slot j at wd[j * WT]: lanes hit consecutive words
+#pragma unroll
+    for (int j = 0; j < RW; ++j) wd[j * WT] = 0.f;
+    bool wide = false;
+    int lo = RW, hi = -1;
+#pragma unroll
+    for (int p = 0; p < 12; ++p) {
+        const float u = c_rule_f[p][0], uu = c_rule_f[p][1], v = c_rule_f[p][2];
+        const float p0 = fmaf(f4, uu, f1 * u);
+        const float p1 = fmaf(f6, uu, fmaf(f3, u, f2));
+        const float p2 = fmaf(f8, uu, fmaf(f7, u, f5));
+        const float dq = fmaf(fmaf(p2, v, p1), v, p0);  // q(point) - q(centre)
+        int r = 0;
+        float dlo = d[0];
+#pragma unroll
+        for (int j = 1; j < RW; ++j) {
+            const bool ge = dq >= d[j];
+            r += ge;
+            dlo = ge ? d[j] : dlo;
+        }
+        const int k = base + r;  // the point's lower table row
+        const float wo = c_rule_w32[p] * om;
+        if (dq >= d[0] && r < RW - 1 && k >= 1) {
+            const float4 c0 = A.scoef[2 * k], c1 = A.scoef[2 * k + 1];
+            const float dl = (dq - dlo) * c0.x;  // q / q_k - 1
+            float tt;
+            if (dl >= -0.002f && dl <= 0.072f) {
+                const float zz = fmaf(dl, 1.f / DPOLY_H, -DPOLY_C / DPOLY_H);
+                const float P = fmaf(fmaf(fmaf(fmaf(c1.y, zz, c1.x), zz, c0.w), zz, c0.z), zz, c0.y);
+                tt = (float)REDM1 * (dl * P);
+            } else {
+                tt = t_exact(g.a0 + (double)dq, k + 1);
+            }
+            wd[r * WT] += (1.f - tt) * wo;
+            wd[(r + 1) * WT] += tt * wo;
+            lo = min(lo, r);
+            hi = max(hi, r + 1);
+        } else {
+            wide = true;
+        }
+    }
+    if (!wide) {
+        // map integral (c7): the window's rows of a pixel inside the radius
+        if (inside) {
+#pragma unroll
+            for (int j = 0; j < RW; ++j)
+                if (j >= lo && j <= hi) atomicAdd(&A.hist[base + j], (double)wd[j * WT]);
+            if (rlo) {
+                atomicMin(rlo, base + lo);
+                atomicMax(rhi, base + hi);
+            }
+        }
+        const int nent = hi - lo + 1;
+        float f[RW];
+#pragma unroll
+        for (int j = 0; j < RW; ++j) f[j] = j < nent ? wd[min(j + lo, RW - 1) * WT] : 0.f;
+        const int meta = (base + lo) | (nent << 16);
+        A.rec[kk] = make_float4(f[0], f[1], f[2], __int_as_float(meta));
+        if (nent > REC_ROWS) {
+            A.ext[2 * kk] = make_float4(f[0], f[1], f[2], f[3]);
+            A.ext[2 * kk + 1] = make_float4(f[4], f[5], f[6], f[7]);
+        }
+    } else {
+        // a wide pixel (next to the source): its 12 points again with FP64 chords,
+        // for its sparse record and its map-integral rows alike
+        int meta = META_OVERFLOW;
+        const int slot = atomicAdd(A.sparse_count, 1);
+        float2* sr = slot < A.sparse_cap ? A.sparse + (size_t)slot * NSP : nullptr;
+        for (int p = 0; p < 12; ++p) {
+            float tt;
+            const int idx = point_row_bin(point_q2(g, p), A.sbin, A.scoef, &tt);
+            const float wo = c_rule_w32[p] * om;
+            const float wa = (1.f - tt) * wo, wb = tt * wo;
+            if (sr) {
+                sr[2 * p] = make_float2(wa, __int_as_float(idx - 1));
+                sr[2 * p + 1] = make_float2(wb, __int_as_float(idx));
+            }
+            if (inside) {
+                atomicAdd(&A.hist[idx - 1], (double)wa);
+                atomicAdd(&A.hist[idx], (double)wb);
+                if (rlo) {
+                    atomicMin(rlo, idx - 1);
+                    atomicMax(rhi, idx);
+                }
+            }
+        }
+        if (sr) meta = -1 - slot;
+        A.rec[kk] = make_float4(0.f, 0.f, 0.f, __int_as_float(meta));
+    }
+}
+
+// The dense map: grid (nch, S), block (c, s) takes tiles c, c + nch, ... of source
+// s's H x W pixels and writes its histogram to hist_out[s][c].
 __global__ void __launch_bounds__(WT, 4) k_pixel_windows(const double* __restrict__ corners, const double* __restrict__ centers,
                                                       const double* __restrict__ omega, const SrcInfo* __restrict__ info,
                                                       const SepTab* __restrict__ septab, int H, int W, int nch,
@@ -56,15 +212,9 @@ __global__ void __launch_bounds__(WT, 4) k_pixel_windows(const double* __restric
                                                       float4* __restrict__ ext, float2* __restrict__ sparse,
                                                       int sparse_cap, int* __restrict__ sparse_count) {
     extern __shared__ __align__(16) unsigned char smem[];
-    SepBin* sbin = (SepBin*)(smem + WA_OFF_BINS);
-    float4* scoef = (float4*)(smem + WA_OFF_COEF);
-    double* hist = (double*)(smem + WA_OFF_HIST);
-    float* wts = (float*)(smem + WA_OFF_WTS);    // [RW][WT] windows (row-major by window slot)
+    const PassA A = pass_a_tables(smem, septab, rec, ext, sparse, sparse_cap, sparse_count);
     const int s = blockIdx.y, t = threadIdx.x;
     const SrcInfo si = info[s];
-    for (int k = t; k < NSB; k += WT) sbin[k] = septab->bins[k];
-    for (int k = t; k < 2 * ND; k += WT) scoef[k] = ((const float4*)septab->coef)[k];
-    for (int r = t; r < ND; r += WT) hist[r] = 0.;
     double ch2 = 2.0 * sin(0.5 * si.radius_rad);
     ch2 *= ch2;
     const int npix = H * W, W1 = W + 1;
@@ -75,117 +225,67 @@ __global__ void __launch_bounds__(WT, 4) k_pixel_windows(const double* __restric
         const int pix = tile * WT + t;
         if (pix >= npix) continue;
         const int h = pix / W, w = pix - h * W;
-        bool inside = false;
-        if (si.in_fov) {
-            const double* c = centers + 3 * (h * W1 + w);
-            const double x = si.dir[0] - c[0], y = si.dir[1] - c[1], z = si.dir[2] - c[2];
-            const double d2 = x * x + y * y + z * z;
-            if (d2 < ch2 * (1.0 - 1e-12)) inside = true;
-            else if (d2 > ch2 * (1.0 + 1e-12)) inside = false;
-            else inside = dir_diff(si.dir, c) <= si.radius_rad;
-        }
-        const PixQ g = pixel_q(pixel_geom(corners, W1, h, w, si));
-        const float om = (float)omega[pix];
-        float tc;
-        const int ic = point_row_bin(g.a0, sbin, scoef, &tc);
-        const int base = min(max(ic - 1 - RW / 2, 0), ND - RW);
-        // The window's row edges as FP32 offsets from the centre's FP64 squared
-        // chord, and the chord offsets of the rule points in FP32 from the
-        // biquadratic form: no FP64 per point, and no table search per point.
-        float d[RW];
-#pragma unroll
-        for (int j = 0; j < RW; ++j) {
-            const float4 cw = scoef[2 * (base + j) + 1];
-            d[j] = (float)(__hiloint2double(__float_as_int(cw.w), __float_as_int(cw.z)) - g.a0);
-        }
-        const float f1 = (float)g.a1, f2 = (float)g.a2, f3 = (float)g.a3, f4 = (float)g.a4;
-        const float f5 = (float)g.a5, f6 = (float)g.a6, f7 = (float)g.a7, f8 = (float)g.a8;
-        float* wd = wts + t;  // slot j at wd[j * WT]: lanes hit consecutive words
-#pragma unroll
-        for (int j = 0; j < RW; ++j) wd[j * WT] = 0.f;
-        bool wide = false;
-        int lo = RW, hi = -1;
-#pragma unroll
-        for (int p = 0; p < 12; ++p) {
-            const float u = c_rule_f[p][0], uu = c_rule_f[p][1], v = c_rule_f[p][2];
-            const float p0 = fmaf(f4, uu, f1 * u);
-            const float p1 = fmaf(f6, uu, fmaf(f3, u, f2));
-            const float p2 = fmaf(f8, uu, fmaf(f7, u, f5));
-            const float dq = fmaf(fmaf(p2, v, p1), v, p0);  // q(point) - q(centre)
-            int r = 0;
-            float dlo = d[0];
-#pragma unroll
-            for (int j = 1; j < RW; ++j) {
-                const bool ge = dq >= d[j];
-                r += ge;
-                dlo = ge ? d[j] : dlo;
-            }
-            const int k = base + r;  // the point's lower table row
-            const float wo = c_rule_w32[p] * om;
-            if (dq >= d[0] && r < RW - 1 && k >= 1) {
-                const float4 c0 = scoef[2 * k], c1 = scoef[2 * k + 1];
-                const float dl = (dq - dlo) * c0.x;  // q / q_k - 1
-                float tt;
-                if (dl >= -0.002f && dl <= 0.072f) {
-                    const float zz = fmaf(dl, 1.f / DPOLY_H, -DPOLY_C / DPOLY_H);
-                    const float P = fmaf(fmaf(fmaf(fmaf(c1.y, zz, c1.x), zz, c0.w), zz, c0.z), zz, c0.y);
-                    tt = (float)REDM1 * (dl * P);
-                } else {
-                    tt = t_exact(g.a0 + (double)dq, k + 1);
-                }
-                wd[r * WT] += (1.f - tt) * wo;
-                wd[(r + 1) * WT] += tt * wo;
-                lo = min(lo, r);
-                hi = max(hi, r + 1);
-            } else {
-                wide = true;
-            }
-        }
-        const size_t kk = sp + pix;
-        if (!wide) {
-            // map integral (c7): the window's rows of a pixel inside the radius
-            if (inside) {
-#pragma unroll
-                for (int j = 0; j < RW; ++j)
-                    if (j >= lo && j <= hi) atomicAdd(&hist[base + j], (double)wd[j * WT]);
-            }
-            const int nent = hi - lo + 1;
-            float f[RW];
-#pragma unroll
-            for (int j = 0; j < RW; ++j) f[j] = j < nent ? wd[min(j + lo, RW - 1) * WT] : 0.f;
-            const int meta = (base + lo) | (nent << 16);
-            rec[kk] = make_float4(f[0], f[1], f[2], __int_as_float(meta));
-            if (nent > REC_ROWS) {
-                ext[2 * kk] = make_float4(f[0], f[1], f[2], f[3]);
-                ext[2 * kk + 1] = make_float4(f[4], f[5], f[6], f[7]);
-            }
-        } else {
-            // a wide pixel (next to the source): its 12 points again with FP64 chords,
-            // for its sparse record and its map-integral rows alike
-            int meta = META_OVERFLOW;
-            const int slot = atomicAdd(sparse_count, 1);
-            float2* sr = slot < sparse_cap ? sparse + (size_t)slot * NSP : nullptr;
-            for (int p = 0; p < 12; ++p) {
-                float tt;
-                const int idx = point_row_bin(point_q2(g, p), sbin, scoef, &tt);
-                const float wo = c_rule_w32[p] * om;
-                const float wa = (1.f - tt) * wo, wb = tt * wo;
-                if (sr) {
-                    sr[2 * p] = make_float2(wa, __int_as_float(idx - 1));
-                    sr[2 * p + 1] = make_float2(wb, __int_as_float(idx));
-                }
-                if (inside) {
-                    atomicAdd(&hist[idx - 1], (double)wa);
-                    atomicAdd(&hist[idx], (double)wb);
-                }
-            }
-            if (sr) meta = -1 - slot;
-            rec[kk] = make_float4(0.f, 0.f, 0.f, __int_as_float(meta));
-        }
+        window_pixel(corners, centers, omega, si, ch2, W1, h, w, (size_t)pix, sp + pix, A, nullptr, nullptr);
     }
     __syncthreads();
     double* out = hist_out + ((size_t)s * nch + blockIdx.x) * ND;
-    for (int r = t; r < ND; r += WT) out[r] = hist[r];
+    for (int r = t; r < ND; r += WT) out[r] = A.hist[r];
+}
+
+// Cutouts: one persistent launch over a work queue of (source, tile) items, tile
+// = WT consecutive pixels of the source's window (row-major, nw wide).  A block
+// takes the next item from the queue (one atomic), builds its pixels' records
+// and the item's map-integral rows in shared memory, and adds the rows it touched
+// to hist_out[s] with FP64 atomics.  item_src[i] is the source of item i, tile_off[s]
+// its first item and tile_off[S] the number of items.
+__global__ void __launch_bounds__(WT, 4) k_pixel_windows_cut(const double* __restrict__ corners,
+                                                          const double* __restrict__ centers,
+                                                          const double* __restrict__ omega,
+                                                          const SrcInfo* __restrict__ info,
+                                                          const xts_cutout* __restrict__ cut,
+                                                          const int* __restrict__ item_src,
+                                                          const long long* __restrict__ tile_off,
+                                                          unsigned long long* __restrict__ queue,
+                                                          const SepTab* __restrict__ septab, int S, int W,
+                                                          double* __restrict__ hist_out, float4* __restrict__ rec,
+                                                          float4* __restrict__ ext, float2* __restrict__ sparse,
+                                                          int sparse_cap, int* __restrict__ sparse_count) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ long long item_s;
+    __shared__ int rmin_s, rmax_s;
+    const PassA A = pass_a_tables(smem, septab, rec, ext, sparse, sparse_cap, sparse_count);
+    const int t = threadIdx.x, W1 = W + 1;
+    const long long n_items = tile_off[S];
+    for (;;) {
+        if (t == 0) {
+            item_s = (long long)atomicAdd(queue, 1ull);
+            rmin_s = ND;
+            rmax_s = -1;
+        }
+        __syncthreads();  // also orders the previous item's flush before this item's adds
+        const long long item = item_s;
+        if (item >= n_items) break;
+        const int s = item_src[item];
+        const xts_cutout cw = cut[s];
+        const SrcInfo si = info[s];
+        double ch2 = 2.0 * sin(0.5 * si.radius_rad);
+        ch2 *= ch2;
+        const long long npix = (long long)cw.nh * cw.nw;
+        const long long pix = (item - tile_off[s]) * WT + t;
+        if (pix < npix) {
+            const int i = (int)(pix / cw.nw), j = (int)(pix - (long long)i * cw.nw);
+            const int h = cw.h0 + i, w = cw.w0 + j;
+            window_pixel(corners, centers, omega, si, ch2, W1, h, w, (size_t)h * W + w, (size_t)(cw.offset + pix), A,
+                         &rmin_s, &rmax_s);
+        }
+        __syncthreads();
+        for (int r = rmin_s + t; r <= rmax_s; r += WT) {
+            const double v = A.hist[r];
+            if (v != 0.) atomicAdd(hist_out + (size_t)s * ND + r, v);
+            A.hist[r] = 0.;
+        }
+        __syncthreads();  // the flush has read rmin_s / rmax_s before thread 0 resets them
+    }
 }
 
 // ============================================================================ pass B
@@ -232,11 +332,30 @@ __device__ __forceinline__ PixRec load_rec(const float4* rec, const float4* ext,
 // Warps run independently: each owns 32 pixels of the tile, a slice of the
 // stage and its own TMA bulk store, so no block barrier is needed except when the
 // block moves on to the next source's table.
-template <int NQ>
+// Pixels of a source in the write pass: the dense map (every source H * W pixels,
+// records from s * npix, output from (s_base + s) * npix) or a cutout window
+// (cut[s].nh * cut[s].nw pixels, records and output from cut[s].offset).
+template <bool CUT>
+struct SrcSpan {
+    const xts_cutout* cut;
+    int S, s_base, npix;
+    __device__ __forceinline__ int pixels(int s) const {
+        if (!CUT) return npix;
+        return s < S ? cut[s].nh * cut[s].nw : 0;
+    }
+    __device__ __forceinline__ long long rec_base(int s) const { return CUT ? cut[s].offset : (long long)s * npix; }
+    __device__ __forceinline__ long long out_base(int s) const {
+        return CUT ? cut[s].offset : (long long)(s_base + s) * npix;
+    }
+    __device__ __forceinline__ int tiles(int s) const { return (pixels(s) + BT - 1) / BT; }
+};
+
+template <int NQ, bool CUT>
 __global__ void __launch_bounds__(BT, 2)
 k_srcmap_win(const float4* __restrict__ win, const float4* __restrict__ ext, const float2* __restrict__ sparse,
              const float* __restrict__ lut, const double* __restrict__ corners, const double* __restrict__ omega,
-             const SrcInfo* __restrict__ info, const SepTab* __restrict__ septab,
+             const SrcInfo* __restrict__ info, const SepTab* __restrict__ septab, const xts_cutout* __restrict__ cut,
+             const long long* __restrict__ tile_off,
              int S, int s_base, int H, int W, int E, int EQ, int* status, float* __restrict__ out) {
     extern __shared__ __align__(16) unsigned char smem[];
     const WinLayout L = win_layout(E, EQ);
@@ -244,9 +363,9 @@ k_srcmap_win(const float4* __restrict__ win, const float4* __restrict__ ext, con
     const unsigned bar = smem_u32(smem + L.bar);
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     float* stage = (float*)(smem + L.stage) + warp * (32 * E + 8);
-    const int npix = H * W, W1 = W + 1;
-    const int ntiles = (npix + BT - 1) / BT;
-    const long long T = (long long)S * ntiles;
+    const int W1 = W + 1;
+    const SrcSpan<CUT> sp_{cut, S, s_base, H * W};
+    const long long T = CUT ? tile_off[S] : (long long)S * sp_.tiles(0);
     const long long f0 = T * blockIdx.x / gridDim.x, f1 = T * (blockIdx.x + 1) / gridDim.x;
     const unsigned tab_bytes = (unsigned)(ND * EQ * 16);
 
@@ -257,16 +376,31 @@ k_srcmap_win(const float4* __restrict__ win, const float4* __restrict__ ext, con
     int cur = -1;
     unsigned phase = 0;
     // (source, tile) of f, advanced by counting: no 64-bit division per tile
-    int s = (int)(f0 / ntiles), tile = (int)(f0 - (long long)s * ntiles);
-    PixRec rec = load_rec(win, ext, (size_t)s * npix + tile * BT + t, f0 < f1 && tile * BT + t < npix);
+    int s, tile;
+    if (CUT) {  // the source whose items hold f0: the last s with tile_off[s] <= f0
+        int a = 0, b = S;
+        while (b - a > 1) {
+            const int mid = (a + b) >> 1;
+            if (tile_off[mid] <= f0) a = mid; else b = mid;
+        }
+        s = a;
+        while (s < S && tile_off[s + 1] <= f0) ++s;  // skip sources without tiles
+        tile = (int)(f0 - tile_off[s]);
+    } else {
+        s = (int)(f0 / sp_.tiles(0));
+        tile = (int)(f0 - (long long)s * sp_.tiles(0));
+    }
+    int np_s = sp_.pixels(s), nt_s = sp_.tiles(s);
+    const bool any = f0 < f1 && s < S;
+    PixRec rec = load_rec(win, ext, any ? (size_t)(sp_.rec_base(s) + tile * BT + t) : 0, any && tile * BT + t < np_s);
     for (long long f = f0; f < f1; ++f) {
         int sn = s, tn = tile + 1;  // the next tile
-        if (tn == ntiles) { tn = 0; ++sn; }
+        while (tn >= sp_.tiles(sn) && sn < S) { tn = 0; ++sn; }
         int s2 = sn, t2 = tn + 1;   // and the one after
-        if (t2 == ntiles) { t2 = 0; ++s2; }
+        while (t2 >= sp_.tiles(s2) && s2 < S) { t2 = 0; ++s2; }
         const int px0 = tile * BT + warp * 32;  // this warp's first pixel
-        const int npw = min(32, npix - px0);                                // may be <= 0 in the last tile
-        const long long g0 = ((long long)(s_base + s) * npix + px0) * E;    // first flat output of the whole map
+        const int npw = min(32, np_s - px0);                                // may be <= 0 in the last tile
+        const long long g0 = (sp_.out_base(s) + px0) * E;                   // first flat output of the whole map
         const int m = (int)(g0 & 3);                                        // staging residue
         const int nflat = npw > 0 ? npw * E : 0;
         const int pix = px0 + lane;
@@ -276,10 +410,12 @@ k_srcmap_win(const float4* __restrict__ win, const float4* __restrict__ ext, con
         PixRec nxt;
         {
             const int pn = tn * BT;
-            nxt = load_rec(win, ext, (size_t)sn * npix + pn + t, f + 1 < f1 && pn + t < npix);
+            const bool more = f + 1 < f1 && sn < S;
+            nxt = load_rec(win, ext, more ? (size_t)(sp_.rec_base(sn) + pn + t) : 0,
+                           more && pn + t < sp_.pixels(sn));
             const int p2 = t2 * BT;
-            if (f + 2 < f1 && p2 + t < npix && (t & 7) == 0) {  // one prefetch per 128-byte line
-                const size_t k2 = (size_t)s2 * npix + p2 + t;
+            if (f + 2 < f1 && s2 < S && p2 + t < sp_.pixels(s2) && (t & 7) == 0) {  // one prefetch per 128-byte line
+                const size_t k2 = (size_t)(sp_.rec_base(s2) + p2 + t);
                 asm volatile("prefetch.global.L2 [%0];" :: "l"(win + k2));
             }
         }
@@ -371,9 +507,17 @@ k_srcmap_win(const float4* __restrict__ win, const float4* __restrict__ ext, con
         }
         if (slow) {  // sparse pool full: point by point from the shared table, compensated sum
             const SrcInfo si = info[s];
-            const int h = pix / W, wc = pix - h * W;
+            int h, wc;
+            if (CUT) {
+                const xts_cutout cw = cut[s];
+                h = cw.h0 + pix / cw.nw;
+                wc = cw.w0 + pix % cw.nw;
+            } else {
+                h = pix / W;
+                wc = pix - h * W;
+            }
             const PixGeom g = pixel_geom(corners, W1, h, wc, si);
-            const float om = (float)omega[pix];
+            const float om = (float)omega[(size_t)h * W + wc];
             const float* Y = (const float*)tab;
             const int ES = 4 * EQ;
             for (int e = 0; e < E; ++e) {
@@ -406,30 +550,48 @@ k_srcmap_win(const float4* __restrict__ win, const float4* __restrict__ ext, con
             }
         }
         rec = nxt;
+        if (sn != s) {
+            np_s = sp_.pixels(sn);
+            nt_s = sp_.tiles(sn);
+        }
         s = sn;
         tile = tn;
     }
+    (void)nt_s;
     if (lane == 0) bulk_wait_all();
 }
 
+struct WriteArgs {
+    const float4* win; const float4* ext; const float2* sparse; const float* lut;
+    const double* corners; const double* omega; const SrcInfo* info; const SepTab* tab;
+    const xts_cutout* cut; const long long* tile_off;  // cutouts (cut != NULL): tile_off [S + 1]
+    int S, s_base, H, W, E, EQ;
+    int* status; float* out;
+};
+
 template <int NQ>
-static int launch_write_pass(unsigned G, size_t smem, cudaStream_t st, const float4* win, const float4* ext,
-                             const float2* sparse, const float* lut, const double* corners, const double* omega,
-                             const SrcInfo* info, const SepTab* tab, int S, int s_base, int H, int W, int E, int EQ,
-                             int* status, float* out, int* per_sm, int nsm, bool query) {
+static int launch_write_pass(unsigned G, size_t smem, cudaStream_t st, const WriteArgs& a, int* per_sm, bool query) {
     if (query) {
-        XTS_CUDA(cudaFuncSetAttribute(k_srcmap_win<NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        XTS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_srcmap_win<NQ>, BT, smem));
+        int pd = 0, pc = 0;
+        XTS_CUDA(cudaFuncSetAttribute(k_srcmap_win<NQ, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        XTS_CUDA(cudaFuncSetAttribute(k_srcmap_win<NQ, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        XTS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pd, k_srcmap_win<NQ, false>, BT, smem));
+        XTS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pc, k_srcmap_win<NQ, true>, BT, smem));
+        *per_sm = pd < pc ? pd : pc;
         return XTS_OK;
     }
-    XTS_LAUNCH("k_srcmap", st, k_srcmap_win<NQ><<<G, BT, smem, st>>>(win, ext, sparse, lut, corners, omega, info, tab,
-                                                                    S, s_base, H, W, E, EQ, status, out));
+    if (a.cut)
+        XTS_LAUNCH("k_srcmap", st, k_srcmap_win<NQ, true><<<G, BT, smem, st>>>(
+                                       a.win, a.ext, a.sparse, a.lut, a.corners, a.omega, a.info, a.tab, a.cut,
+                                       a.tile_off, a.S, a.s_base, a.H, a.W, a.E, a.EQ, a.status, a.out));
+    else
+        XTS_LAUNCH("k_srcmap", st, k_srcmap_win<NQ, false><<<G, BT, smem, st>>>(
+                                       a.win, a.ext, a.sparse, a.lut, a.corners, a.omega, a.info, a.tab, nullptr,
+                                       nullptr, a.S, a.s_base, a.H, a.W, a.E, a.EQ, a.status, a.out));
     return XTS_OK;
 }
 
-typedef int (*WritePassFn)(unsigned, size_t, cudaStream_t, const float4*, const float4*, const float2*, const float*,
-                           const double*, const double*, const SrcInfo*, const SepTab*, int, int, int, int, int, int,
-                           int*, float*, int*, int, bool);
+typedef int (*WritePassFn)(unsigned, size_t, cudaStream_t, const WriteArgs&, int*, bool);
 static const WritePassFn k_write_pass[BQ] = {
     launch_write_pass<1>, launch_write_pass<2>, launch_write_pass<3>, launch_write_pass<4>, launch_write_pass<5>,
     launch_write_pass<6>, launch_write_pass<7>, launch_write_pass<8>, launch_write_pass<9>, launch_write_pass<10>,
@@ -440,7 +602,6 @@ bool srcmap_win_supported(int E) {
     return E >= 1 && E <= 4 * BQ && win_layout(E, win_row_quads(E)).total <= 227 * 1024;
 }
 
-// Window records of one source chunk: 36 bytes per (source, pixel).
 // Window records of one source chunk: a 16-byte main record and a 32-byte
 // extension slot per (source, pixel); only windows of more than REC_ROWS rows
 // write and read their extension.
@@ -503,8 +664,7 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
     double* hist0 = (double*)workspace(W_PARTSUM, sizeof(double) * 2 * hist_n);
     if (!rec0 || !ext0 || !lut0 || !sparse0 || !hist0) return XTS_ERR_OOM;
     const WritePassFn wp = k_write_pass[(E + 3) / 4 - 1];
-    rc = wp(0, L.total, st, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, 0, 0, E, EQ,
-            nullptr, nullptr, &per_sm, nsm, true);
+    rc = wp(0, L.total, st, WriteArgs{}, &per_sm, true);
     if (rc) return rc;
     if (per_sm < 1) return set_error(XTS_ERR_ARG, "source-map write pass does not fit on an SM (E=%d)", E);
     cudaEvent_t evA[2], evB[2];  // window pass of a buffer done; write pass of a buffer done
@@ -539,13 +699,107 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
         const long long T = (long long)n * ((npix + BT - 1) / BT);
         long long G = (long long)nsm * per_sm;
         if (G > T) G = T;
-        rc = wp((unsigned)G, L.total, st, rec, ext, sparse, lut, corners, omega, info + s0, tab, n, s0, H, W, E, EQ,
-                status, out, nullptr, nsm, false);
+        WriteArgs wa{rec, ext, sparse, lut, corners, omega, info + s0, tab, nullptr, nullptr, n, s0, H, W, E, EQ,
+                     status, out};
+        rc = wp((unsigned)G, L.total, st, wa, nullptr, false);
         if (rc) return rc;
         if (on_chunk && (rc = on_chunk(on_chunk_ctx, s0, n, st))) return rc;
         if (pipe) XTS_CUDA(cudaEventRecord(evB[b], st));
     }
     return geo.join();
+}
+
+// ============================================================================ cutouts
+// Items of the cutout work queue: tile_off[s] = the first (source, tile) item of
+// source s (tiles of WT pixels of its window), tile_off[S] = the item count.  One
+// block; the sources in runs of 1024 with a block scan.
+__global__ void __launch_bounds__(1024) k_cut_tiles(const xts_cutout* __restrict__ cut, int S,
+                                                    long long* __restrict__ tile_off) {
+    __shared__ long long part[32];
+    __shared__ long long carry_s;
+    const int t = threadIdx.x, lane = t & 31, wp = t >> 5;
+    if (t == 0) carry_s = 0;
+    __syncthreads();
+    for (int s0 = 0; s0 < S; s0 += 1024) {
+        const int s = s0 + t;
+        const long long n = s < S ? ((long long)cut[s].nh * cut[s].nw + WT - 1) / WT : 0;
+        long long inc = n;
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long v = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += v;
+        }
+        if (lane == 31) part[wp] = inc;
+        __syncthreads();
+        long long before = carry_s;
+        for (int k = 0; k < wp; ++k) before += part[k];
+        if (s < S) tile_off[s] = before + inc - n;
+        __syncthreads();
+        if (t == 1023) carry_s = before + inc;
+        __syncthreads();
+    }
+    if (t == 0) tile_off[S] = carry_s;
+}
+
+// item_src[i] = the source of item i (one block per source).
+__global__ void k_cut_item_src(const long long* __restrict__ tile_off, int* __restrict__ item_src) {
+    const int s = blockIdx.x;
+    for (long long i = tile_off[s] + threadIdx.x; i < tile_off[s + 1]; i += blockDim.x) item_src[i] = s;
+}
+
+int launch_srcmap_win_cut(const double* corners, const double* centers, const double* omega, const SrcInfo* info,
+                          const xts_cutout* cut, int S, int H, int W, int E, const double* upsf,
+                          const double* partial, const double* exposure, double* scale, double* inv_integ,
+                          double* correction, double* radius, int* in_fov, int* status, float* out, cudaStream_t st) {
+    int rc = upload_rule_uv(st);
+    if (rc) return rc;
+    const SepTab* tab = nullptr;
+    if ((rc = build_septab(st, &tab))) return rc;
+    const long long npix = (long long)H * W;
+    const int EQ = win_row_quads(E);
+    const WinLayout L = win_layout(E, EQ);
+    // buffers sized for the largest windows (every window the whole map): nothing here
+    // depends on the windows' sizes on the host, so the call needs no synchronisation
+    const long long max_items = (long long)S * ((npix + WT - 1) / WT);
+    const size_t rec_n = (size_t)S * npix + 4;
+    float4* rec = (float4*)workspace(W_WIN, sizeof(float4) * rec_n);
+    float4* ext = (float4*)workspace(W_WMETA, sizeof(float4) * 2 * rec_n);
+    float* lut = (float*)workspace(W_LUT, sizeof(float) * ((size_t)S * ND * EQ * 4 + 4));
+    long long cap = (long long)S * npix / 8;
+    cap = cap < 65536 ? 65536 : cap;
+    float2* sparse = (float2*)workspace(W_SPARSE, sizeof(float2) * ((size_t)NSP * cap + 2));
+    double* hist = (double*)workspace(W_PARTSUM, sizeof(double) * ((size_t)S * ND + 1));
+    char* items = (char*)workspace(W_CUT_ITEMS, align_up(sizeof(long long) * (S + 1), 256) +
+                                                    align_up(sizeof(int) * (size_t)max_items, 256) + 256);
+    if (!rec || !ext || !lut || !sparse || !hist || !items) return XTS_ERR_OOM;
+    long long* tile_off = (long long*)items;
+    int* item_src = (int*)(items + align_up(sizeof(long long) * (S + 1), 256));
+    unsigned long long* queue = (unsigned long long*)(items + align_up(sizeof(long long) * (S + 1), 256) +
+                                                      align_up(sizeof(int) * (size_t)max_items, 256));
+    int* sparse_count = status + 1;
+    XTS_CUDA(cudaMemsetAsync(hist, 0, sizeof(double) * (size_t)S * ND, st));
+    XTS_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st));
+    XTS_CUDA(cudaMemsetAsync(sparse_count, 0, sizeof(int), st));
+    XTS_LAUNCH("k_cut_tiles", st, k_cut_tiles<<<1, 1024, 0, st>>>(cut, S, tile_off));
+    XTS_LAUNCH("k_cut_item_src", st, k_cut_item_src<<<S, 256, 0, st>>>(tile_off, item_src));
+    int dev = 0, nsm = 148, resident = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    XTS_CUDA(cudaFuncSetAttribute(k_pixel_windows_cut, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WA_SMEM));
+    XTS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_pixel_windows_cut, WT, WA_SMEM));
+    resident = resident < 1 ? 1 : resident;
+    // pass A: one persistent wave pulling (source, tile) items from the queue
+    XTS_LAUNCH("k_pixel_windows", st, k_pixel_windows_cut<<<(unsigned)(resident * nsm), WT, WA_SMEM, st>>>(
+                                          corners, centers, omega, info, cut, item_src, tile_off, queue, tab, S, W,
+                                          hist, rec, ext, sparse, (int)cap, sparse_count));
+    rc = launch_correction(hist, 1, info, S, upsf, partial, exposure, E, scale, inv_integ, correction, radius, in_fov,
+                           st, lut, EQ * 4);
+    if (rc) return rc;
+    const WritePassFn wp = k_write_pass[(E + 3) / 4 - 1];
+    if ((rc = wp(0, L.total, st, WriteArgs{}, &per_sm, true))) return rc;
+    if (per_sm < 1) return set_error(XTS_ERR_ARG, "source-map write pass does not fit on an SM (E=%d)", E);
+    WriteArgs wa{rec, ext, sparse, lut, corners, omega, info, tab, cut, tile_off, S, 0, H, W, E, EQ, status, out};
+    // pass B: one persistent wave over the same items, split evenly between the blocks
+    return wp((unsigned)(nsm * per_sm), L.total, st, wa, nullptr, false);
 }
 
 }  // namespace xts
