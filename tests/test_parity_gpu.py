@@ -366,9 +366,11 @@ def test_srcmap_vs_compiled_reference(api, c1_small):
 
 def test_adaptive_map_vs_oracle(api, c1_small):
     """Adaptive Genz-Malik cubature on the GPU against the oracle's FP64 version
-    of the same algorithm (rtol 1e-4, depth 6).  Region decisions near the
-    threshold can differ between FP32 and FP64, which moves a pixel by about
-    rtol at most; nearly all pixels agree to FP32 rounding."""
+    of the same algorithm (rtol 1e-4, depth 6).  The GPU decides a region in FP64,
+    with the oracle's arithmetic, whenever its FP32 estimate lies near the
+    threshold or the split dimension is nearly tied, and accumulates the pixel
+    means in FP64: every region is decided as in the oracle, so every value
+    agrees to FP32 rounding (1e-5) and the map integrals to 1e-7."""
     from oracle import oracle as O
 
     job, ref, gpu = c1_small
@@ -378,9 +380,8 @@ def test_adaptive_map_vs_oracle(api, c1_small):
                                            1e-4, 6)
     assert m.dtype == np.float32
     rel = np.abs(m - o["map"]) / np.abs(o["map"])
-    assert rel.max() < 3e-4
-    assert (rel > 1e-5).mean() < 1e-3
-    assert max_rel(info.inv_map_integral, o["inv_integ"]) < 1e-6
+    assert rel.max() < 1e-5, (rel.max(), (rel > 1e-5).sum())
+    assert max_rel(info.inv_map_integral, o["inv_integ"]) < 1e-7
     np.testing.assert_array_equal(info.in_fov.astype(bool), o["in_fov"])
 
 

@@ -64,7 +64,7 @@ enum Slot {
     // internal scratch
     W_CORNERS, W_CENTERS, W_OMEGA, W_LUT, W_PARTSUM, W_SRCINFO, W_SCALE, W_PSFTAB,
     W_KING, W_MISC, W_WIN, W_WMETA, W_SPARSE, W_MISC2, W_EXPMAP,
-    W_FITS_IN, W_FITS_OUT, W_FITS_SUM, W_FFT_A, W_FFT_B, W_FFT_C, W_FFT_WORK, W_SRCPIX, W_CUT_ITEMS,
+    W_FITS_IN, W_FITS_OUT, W_FITS_SUM, W_FFT_A, W_FFT_B, W_FFT_C, W_FFT_WORK, W_SRCPIX, W_CUT_ITEMS, W_ADAPT_MEAN,
     W_MLP_Z, W_MLP_H, W_MLP_DZ, W_MLP_DH, W_MLP_Y, W_MLP_ST, W_MLP_PART, W_MLP_PART2, W_SUR_X, W_SUR_AUX, W_SUR_Y, W_SUR_IDX, W_SUR_ERR,
     N_SLOTS
 };
@@ -198,7 +198,11 @@ int launch_exposure_map_tc(const float* cube, const float* wcube, long long npix
 bool srcmap_adaptive_supported(int E);
 int launch_adaptive_map(const double* corners, const double* centers, const double* omega, const SrcInfo* info,
                         const double* upsf, int S, int H, int W, int E, double rtol, int max_depth, int nch,
-                        double* sums, float* out, cudaStream_t st);
+                        double* sums, double* mean64, int* status, cudaStream_t st);
+int launch_mean_integral64(const double* centers, const double* omega, const SrcInfo* info, const double* mean, int S,
+                           int H, int W, int E, int nch, double* sums, cudaStream_t st);
+int launch_scale_map64(const double* mean, float* out, const double* omega, const double* scale, int S, int npix,
+                       int E, cudaStream_t st);
 int launch_scale_map(float* out, const double* omega, const double* scale, int S, int npix, int E,
                      cudaStream_t st);
 // c7 sums [S][nch][E] of pixel means [S][H*W][E] times solid angle over the pixels

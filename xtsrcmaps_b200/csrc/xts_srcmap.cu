@@ -495,11 +495,19 @@ static int launch_srcmap_adaptive(const SrcmapDev& a, const double* corners, con
     const int H = (int)a.wcs.naxis1, W = (int)a.wcs.naxis2, S = a.S, E = a.E;
     const int npix = H * W;
     double* sums = (double*)workspace(W_PARTSUM, sizeof(double) * (size_t)S * nch * E + 8);
-    if (!sums) return XTS_ERR_OOM;
+    double* mean64 = (double*)workspace(W_ADAPT_MEAN, sizeof(double) * (size_t)S * npix * E + 8);
+    int* status = (int*)workspace(W_MISC, 64);
+    if (!sums || !mean64 || !status) return XTS_ERR_OOM;
+    XTS_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
     int rc = launch_adaptive_map(corners, centers, omega, info, a.upsf, S, H, W, E, a.rtol, a.max_depth, nch,
-                                 sums, (float*)a.out, st);
+                                 sums, mean64, status, st);
     if (rc) return rc;
-    return finish_mean_map(a, centers, omega, info, scale, nch, st);
+    // c7 from the FP64 means, c9, then the scalings into the FP32 map
+    if ((rc = launch_mean_integral64(centers, omega, info, mean64, S, H, W, E, nch, sums, st))) return rc;
+    XTS_LAUNCH("k_correction", st, k_correction_sums<<<S, 128, 0, st>>>(sums, nch, info, a.upsf, a.partial,
+                                                                        a.exposure, E, scale, a.inv_integ,
+                                                                        a.correction, a.radius, a.in_fov));
+    return launch_scale_map64(mean64, (float*)a.out, omega, scale, S, npix, E, st);
 }
 
 // A map of pixel means [S][H*W][E] (a.out, FP32) -> the model map: the map
