@@ -350,6 +350,16 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_surrogate:
         net, train = train_surrogate(args, A, dev)
 
+    # launch shapes by measurement on this job (window-pass waves, write-pass and
+    # network blocks per SM), set for everything timed below
+    from xtsrcmaps_b200.autotune import tune_launch_shapes
+
+    with torch.cuda.stream(stream):
+        ex_t = A.compute_exposure(d["cube"], d["wcube"], d["logEs"], d["src"], d["af"], d["ab"], ltf)
+        ps_t = A.compute_psf_data(nf, nb, ex_t, d["logEs"], ltf)
+        shapes = tune_launch_shapes(job.wcs, d["src"], ex_t.exposure, ps_t.uPsf, ps_t.partial_psf_integral, net=net)
+    del ex_t, ps_t
+
     # one plain step = the public call that replaces main.cxx:28-30 (point_source_maps:
     # exposure, mean PSF and model maps; the map geometry runs on a second stream
     # beside exposure and PSF)
@@ -568,7 +578,7 @@ def run_ours(args, rank, world, local_rank):
         "kernels": kernels_of(head), "kernels_plain": kernels_of("plain"), "gpu_launches": gpu_launches,
         "clocks": ck, "e2e": e2e, "cpu_baseline": cpu, "errors_vs_fp64_oracle": errors,
         "surrogate": surrogate, "f64": f64, "c2_cutouts": cutouts, "c4": c4, "adaptive": adaptive,
-        "autotune_write_pass": autotune,
+        "autotune_launch_shapes": shapes, "autotune_write_pass": autotune,
     }
     print(json.dumps(line), flush=True)
 

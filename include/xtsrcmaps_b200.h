@@ -108,6 +108,20 @@ void        xts_release(void);          /* free every cached device buffer */
 const char* xts_last_error(void);
 int         xts_version(void);
 
+/* Launch shapes the autotuner chooses by measurement (no counterpart in the
+ * reference, whose equivalents are compile-time: model_map.psf_boundary_radius.cxx:25,
+ * misc/simdwidth.hpp).  0 in a field keeps its default.  Applies to the calls made
+ * after it on every device of the process. */
+typedef struct xts_tuning {
+    int window_waves;         /* window pass of the dense map: blocks = waves x the blocks resident at once
+                                 (1..8; default 1) */
+    int write_blocks_per_sm;  /* write pass: persistent blocks per SM (1..2; default: as many as fit) */
+    int queue_blocks_per_sm;  /* cutout window pass (work queue): blocks per SM (1..4; default: as many as fit) */
+    int mlp_blocks_per_sm;    /* surrogate network forward: blocks per SM (1..2; default 2) */
+} xts_tuning;
+int xts_set_tuning(const xts_tuning* t);  /* NULL restores the defaults */
+int xts_get_tuning(xts_tuning* t);
+
 /* Kernel timing for profiling and the roofline report (no counterpart in the
  * reference, which has no tracing).  While enabled, every kernel the library
  * launches is bracketed by CUDA events on its stream.  xts_profile_read waits

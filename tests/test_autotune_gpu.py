@@ -49,3 +49,41 @@ def test_autotune_choices(api):
     assert a["ms"] == min(ok)
     print(f"\nwrite pass: {w}\nadaptive: rtol {a['rtol']:g}, depth {a['max_depth']}, {a['ms']:.3f} ms, "
           f"err {a['err']:.2e}")
+
+
+def test_launch_shape_tuning(api):
+    """The launch-shape tuner times each candidate, sets the fastest, and the maps
+    stay the same whatever the shape (the shapes change the work split, not the
+    arithmetic of a value)."""
+    import torch
+
+    from xtsrcmaps_b200 import autotune as T
+    from xtsrcmaps_b200.synth import make_job
+
+    job = make_job("c1", seed=19, n_sources=6)
+    ltf = api.livetime_efficiency_factors(job.logEs, job.effic_front)
+    nf = api.normalize_rpsf(job.rpsf_front, job.scale_front)
+    nb = api.normalize_rpsf(job.rpsf_back, job.scale_back)
+    ex = api.compute_exposure(job.exp_cube, job.wexp_cube, job.logEs, job.src_sph, job.aeff_front,
+                              job.aeff_back, ltf)
+    ps = api.compute_psf_data(nf, nb, ex, job.logEs, ltf)
+    d = torch.device("cuda")
+    t = lambda x: torch.as_tensor(np.ascontiguousarray(x), device=d)
+    src, expo, upsf, part = t(job.src_sph), t(ex.exposure), t(ps.uPsf), t(ps.partial_psf_integral)
+    api.reset_tuning()
+    ref, _ = api.point_src_model_map_wcs(job.wcs, src, expo, upsf, part, with_info=False)
+    res = T.tune_launch_shapes(job.wcs, src, expo, upsf, part)
+    assert len(res["ms"]) == 6 and all(v > 0 for v in res["ms"].values())
+    assert api.get_tuning()["window_waves"] == res["choice"]["window_waves"]
+    for wv, wb in ((2, 1), (4, 2)):
+        api.set_tuning(window_waves=wv, write_blocks_per_sm=wb)
+        m, _ = api.point_src_model_map_wcs(job.wcs, src, expo, upsf, part, with_info=False)
+        torch.cuda.synchronize()
+        rel = ((m.double() - ref.double()).abs() / ref.double().abs().clamp_min(1e-300)).max().item()
+        assert rel < 1e-6, (wv, wb, rel)
+    from xtsrcmaps_b200 import _lib as L
+
+    with pytest.raises(L.XtsError):
+        api.set_tuning(window_waves=9)
+    api.reset_tuning()
+    assert api.get_tuning() == {k: 0 for k in api.TUNING_FIELDS}

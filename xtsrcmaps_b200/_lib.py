@@ -104,6 +104,11 @@ class XtsMlp(C.Structure):
     ]
 
 
+class XtsTuning(C.Structure):
+    _fields_ = [("window_waves", C.c_int), ("write_blocks_per_sm", C.c_int), ("queue_blocks_per_sm", C.c_int),
+                ("mlp_blocks_per_sm", C.c_int)]
+
+
 class XtsSurrogateStats(C.Structure):
     _fields_ = [
         ("values", C.c_longlong), ("accepted", C.c_longlong), ("checked", C.c_longlong),
@@ -163,6 +168,8 @@ SIGNATURES = {
     "xts_cutout_windows": (C.c_int, [C.POINTER(XtsWcs), _vp, _vp, C.c_int, _vp, C.POINTER(C.c_longlong)]),
     "xts_point_src_model_map_cutouts": (C.c_int, [C.POINTER(XtsWcs), _vp, C.c_int, _vp, _vp, _vp, _vp, C.c_int,
                                                   _vp, C.POINTER(XtsSrcmapInfo), C.c_uint, _vp]),
+    "xts_set_tuning": (C.c_int, [C.POINTER(XtsTuning)]),
+    "xts_get_tuning": (C.c_int, [C.POINTER(XtsTuning)]),
     "xts_rebin_wcs": (C.c_int, [C.POINTER(XtsWcs), C.c_double, C.POINTER(XtsWcs)]),
     "xts_allsky_crop_range": (C.c_int, [C.POINTER(XtsWcs), C.POINTER(XtsWcs), C.POINTER(C.c_long)]),
     "xts_crop_allsky": (C.c_int, [_vp, C.c_int, C.c_long, C.c_long, C.POINTER(C.c_long), _vp, C.c_uint, _vp]),

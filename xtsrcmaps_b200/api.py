@@ -673,6 +673,32 @@ def compute_srcmaps(wcs: Wcs, src_sph, exp: XtExp, psf: XtPsf, out_dtype: str = 
     return m
 
 
+TUNING_FIELDS = ("window_waves", "write_blocks_per_sm", "queue_blocks_per_sm", "mlp_blocks_per_sm")
+
+
+def set_tuning(**fields) -> None:
+    """Launch shapes for the following calls (xts_set_tuning); unnamed fields keep
+    their current value, 0 means the default.  set_tuning() with no fields keeps
+    everything; reset_tuning() restores the defaults."""
+    t = L.XtsTuning()
+    L.check(L.lib().xts_get_tuning(C.byref(t)))
+    for k, v in fields.items():
+        if k not in TUNING_FIELDS:
+            raise ValueError(f"unknown tuning field {k!r}")
+        setattr(t, k, int(v))
+    L.check(L.lib().xts_set_tuning(C.byref(t)))
+
+
+def reset_tuning() -> None:
+    L.check(L.lib().xts_set_tuning(None))
+
+
+def get_tuning() -> dict:
+    t = L.XtsTuning()
+    L.check(L.lib().xts_get_tuning(C.byref(t)))
+    return {k: int(getattr(t, k)) for k in TUNING_FIELDS}
+
+
 def init(device: int = 0) -> None:
     L.check(L.lib().xts_init(int(device)))
 

@@ -1,11 +1,16 @@
 """Autotuner of the model-map step (no counterpart in the reference).
 
-Two choices are made by measurement on the job at hand rather than fixed:
+Three choices are made by measurement on the job at hand rather than fixed:
 
 * ``tune_write_pass``: the FP32 write pass of the 12-point rule -- the two-pass
   window path, the single-pass CUDA-core kernel or the tcgen05 window-times-table
   product (all three parity-tested against the FP64 oracle) -- timed with CUDA
   events on the job's own geometry; the fastest wins.
+* ``tune_launch_shapes``: the launch shapes of the plain path (xts_set_tuning):
+  the window pass's grid in waves of resident blocks, the write pass's
+  persistent blocks per SM and, with a network given, the surrogate forward
+  pass's blocks per SM -- each candidate timed on the job's own maps, the
+  fastest set for the calls that follow;
 * ``tune_adaptive``: the subdivision threshold (rtol) and depth limit of the
   adaptive Genz-Malik cubature.  rtol bounds the rule's own |R7 - R5| / |R7|
   estimate, not the error of the result, so the tuner measures the error against
@@ -105,3 +110,50 @@ def tune_adaptive(wcs, src_sph, exposure, uPsf, partial_integrals, target: float
     _CACHE[key] = {"rtol": r, "max_depth": d, "ms": t, "err": e,
                    "table": {f"{r_:g}/{d_}": {"ms": v[0], "err": v[1]} for (r_, d_), v in table.items()}}
     return _CACHE[key]
+
+
+def tune_launch_shapes(wcs, src_sph, exposure, uPsf, partial_integrals, net=None,
+                       window_waves: Sequence[int] = (1, 2, 4), write_blocks_per_sm: Sequence[int] = (1, 2),
+                       mlp_blocks_per_sm: Sequence[int] = (1, 2), reps: int = 3, apply: bool = True) -> dict:
+    """Time the plain model map for every (window waves, write-pass blocks per SM)
+    pair and, with ``net``, the network's forward pass on a million rows for each
+    blocks-per-SM count; set the fastest (apply) and return
+    {"choice": {...}, "ms": {...}}."""
+    from . import api as A
+
+    key = _key("shapes", wcs, src_sph, uPsf, (tuple(window_waves), tuple(write_blocks_per_sm),
+                                               tuple(mlp_blocks_per_sm), net is not None))
+    if key in _CACHE:
+        res = _CACHE[key]
+        if apply:
+            A.set_tuning(**res["choice"])
+        return res
+    import torch
+
+    out = torch.empty((int(src_sph.shape[0]), int(wcs.naxis1), int(wcs.naxis2), int(uPsf.shape[-1])),
+                      dtype=torch.float32, device=uPsf.device)
+    before = A.get_tuning()
+    ms = {}
+    for wv in window_waves:
+        for wb in write_blocks_per_sm:
+            A.set_tuning(window_waves=wv, write_blocks_per_sm=wb)
+            ms[f"waves{wv}/write{wb}"] = (_timed(lambda: A.point_src_model_map_wcs(
+                wcs, src_sph, exposure, uPsf, partial_integrals, out=out, with_info=False), reps), wv, wb)
+    best = min(ms.values())
+    choice = {"window_waves": best[1], "write_blocks_per_sm": best[2]}
+    table = {k: v[0] for k, v in ms.items()}
+    if net is not None:
+        X = torch.randn((1 << 20, 5), device=uPsf.device) * torch.as_tensor(net.in_sd, device=uPsf.device) + \
+            torch.as_tensor(net.in_mu, device=uPsf.device)
+        mm = {}
+        for mb in mlp_blocks_per_sm:
+            A.set_tuning(mlp_blocks_per_sm=mb)
+            mm[mb] = _timed(lambda: net.predict(X), reps)
+            table[f"mlp{mb}"] = mm[mb]
+        choice["mlp_blocks_per_sm"] = min(mm, key=mm.get)
+    A.set_tuning(**before)
+    res = {"choice": choice, "ms": table}
+    _CACHE[key] = res
+    if apply:
+        A.set_tuning(**choice)
+    return res

@@ -41,6 +41,9 @@ int cuda_error(cudaError_t e, const char* what);
         if (e__ != cudaSuccess) return ::xts::cuda_error(e__, name); \
     } while (0)
 
+// Launch shapes chosen by the autotuner (xts_set_tuning); fields are 0 for the default.
+extern xts_tuning g_tuning;
+
 // Optional per-kernel timing (xts_profile_enable): CUDA events recorded on the
 // launching stream around each kernel.  A no-op while profiling is off.
 void prof_mark(const char* name, cudaStream_t st, bool begin);

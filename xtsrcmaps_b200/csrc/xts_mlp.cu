@@ -607,7 +607,8 @@ static int forward(const xts_mlp* net, const float* X, long long n, const unsign
     if (save && !(sv.z2 && sv.z3 && sv.h1 && sv.h2 && sv.yn)) return set_error(XTS_ERR_ARG, "mlp forward: saves");
     if (!save && !y) return set_error(XTS_ERR_ARG, "mlp forward: output");
     const long long ntiles = (n + MT - 1) / MT;
-    const long long g = ntiles < 2 * sm_count() ? ntiles : 2 * sm_count();  // two blocks per SM
+    const int bps = g_tuning.mlp_blocks_per_sm > 0 ? g_tuning.mlp_blocks_per_sm : 2;  // blocks per SM (two fit)
+    const long long g = ntiles < bps * sm_count() ? ntiles : bps * sm_count();
     if (save)
         XTS_LAUNCH("k_mlp_forward", st, k_mlp_forward<true><<<(unsigned)g, FT, FWD_SMEM, st>>>(
                                             net->params, (const __nv_bfloat16*)net->wbf16, mlp_norm(net), X, n, n_dev,

@@ -657,7 +657,7 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
     XTS_CUDA(cudaFuncSetAttribute(k_pixel_windows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WA_SMEM));
     XTS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_pixel_windows, WT, WA_SMEM));
     resident = resident < 1 ? 1 : resident;
-    int nch = resident * nsm / Sc;
+    int nch = (g_tuning.window_waves > 0 ? g_tuning.window_waves : 1) * resident * nsm / Sc;
     const int maxch = (npix + WT - 1) / WT;
     nch = nch < 1 ? 1 : (nch > maxch ? maxch : nch);
     const size_t hist_n = (size_t)Sc * nch * ND + 1;
@@ -697,7 +697,8 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
                                in_fov ? in_fov + s0 : nullptr, st, lut, EQ * 4);
         if (rc) return rc;
         const long long T = (long long)n * ((npix + BT - 1) / BT);
-        long long G = (long long)nsm * per_sm;
+        long long G = (long long)nsm * (g_tuning.write_blocks_per_sm > 0 && g_tuning.write_blocks_per_sm < per_sm
+                                            ? g_tuning.write_blocks_per_sm : per_sm);
         if (G > T) G = T;
         WriteArgs wa{rec, ext, sparse, lut, corners, omega, info + s0, tab, nullptr, nullptr, n, s0, H, W, E, EQ,
                      status, out};
@@ -787,6 +788,7 @@ int launch_srcmap_win_cut(const double* corners, const double* centers, const do
     XTS_CUDA(cudaFuncSetAttribute(k_pixel_windows_cut, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WA_SMEM));
     XTS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_pixel_windows_cut, WT, WA_SMEM));
     resident = resident < 1 ? 1 : resident;
+    if (g_tuning.queue_blocks_per_sm > 0 && g_tuning.queue_blocks_per_sm < resident) resident = g_tuning.queue_blocks_per_sm;
     // pass A: one persistent wave pulling (source, tile) items from the queue
     XTS_LAUNCH("k_pixel_windows", st, k_pixel_windows_cut<<<(unsigned)(resident * nsm), WT, WA_SMEM, st>>>(
                                           corners, centers, omega, info, cut, item_src, tile_off, queue, tab, S, W,
@@ -798,6 +800,7 @@ int launch_srcmap_win_cut(const double* corners, const double* centers, const do
     if ((rc = wp(0, L.total, st, WriteArgs{}, &per_sm, true))) return rc;
     if (per_sm < 1) return set_error(XTS_ERR_ARG, "source-map write pass does not fit on an SM (E=%d)", E);
     WriteArgs wa{rec, ext, sparse, lut, corners, omega, info, tab, cut, tile_off, S, 0, H, W, E, EQ, status, out};
+    if (g_tuning.write_blocks_per_sm > 0 && g_tuning.write_blocks_per_sm < per_sm) per_sm = g_tuning.write_blocks_per_sm;
     // pass B: one persistent wave over the same items, split evenly between the blocks
     return wp((unsigned)(nsm * per_sm), L.total, st, wa, nullptr, false);
 }
