@@ -390,8 +390,6 @@ def run_ours(args, rank, world, local_rank):
         try:
             for name, fn in steps:
                 runs[name] = stepper.capture(fn, args.warmup)
-            for name, fn in steps:  # last: enabling the profiler clears its records
-                prof_runs[name] = stepper.capture(fn, args.warmup, profiled=True)
             launch = "one CUDA graph per step (each path captured once)"
         except Exception as exc:  # capture refused: both paths eager
             runs, prof_runs = {}, {}
@@ -427,8 +425,12 @@ def run_ours(args, rank, world, local_rank):
                 a_ = p.get(k_, (0, 0.0))
                 p[k_] = (a_[0] + n_, a_[1] + t_)
 
-        if name in prof_runs:
+        if stepper.use_graph and launch.startswith("one CUDA graph"):
+            # an instrumented graph of this path, captured and read before the next one:
+            # enabling or disabling the library's timers clears their records
+            prof_runs[name] = stepper.capture(fn, args.warmup, profiled=True)
             msp = stepper.time(prof_runs[name], args.steps, None, lambda: add(A.profile_read()))
+            A.profile_enable(False)
         else:
             A.profile_enable(True)
             msp = stepper.time(fn, args.steps, None, lambda: add(A.profile_read()))
@@ -849,7 +851,10 @@ def measure_c4(args, A, net, torch, dev, stream, flush, rank, chunk: int = 250):
         errs["sources"] = [int(i) for i in idx]
         res["errors_vs_fp64_oracle"] = errs
     if rank == 0 and not args.no_cpu_baseline:
-        res["cpu_baseline"] = cpu_baseline(job, max_sources=64)
+        # a c4 source is 3.2e7 values (~6 s of one reference thread), and the reference hands
+        # out 16 sources per thread, so any sample that keeps more than one thread busy takes
+        # over 90 s: two sources on one thread, one pass, declared as such
+        res["cpu_baseline"] = cpu_baseline(job, max_sources=2, warm=False)
     del buf
     torch.cuda.empty_cache()
     return res
@@ -900,10 +905,12 @@ def _source_sample(job, max_sources: int):
     return sub
 
 
-def cpu_baseline(job, max_sources: int = 256):
+def cpu_baseline(job, max_sources: int = 256, warm: bool = True):
     """The CPU reference (compiled reference code, else the FP64 oracle port) on
-    the host cores over a sample of the bench job's sources (one warm pass, then
-    timed passes for about 10 s); values/s of the sample."""
+    the host cores over a sample of the bench job's sources (a warm pass unless
+    warm is False, then timed passes for about 10 s); values/s of the sample.
+    cores = the threads that had work: the reference's source loops hand out
+    chunks of 16 sources (schedule(static, 16))."""
     sub = _source_sample(job, max_sources)
     run, threads, desc = _reference_runner(sub)
     kind = "reference"
@@ -913,7 +920,10 @@ def cpu_baseline(job, max_sources: int = 256):
 
         run, threads, kind = (lambda: oracle_pipeline(sub)), 1, "port"
         desc = "the FP64 oracle (a scalar C restatement of the reference path) on one core"
-    run()
+    else:
+        threads = min(threads, (sub.S + 15) // 16)
+    if warm:
+        run()
     t0 = time.perf_counter()
     reps = 0
     while reps < 1 or (time.perf_counter() - t0 < 10.0 and reps < 20):

@@ -19,7 +19,8 @@
 //
 // Decisions near the threshold are taken in FP64: when the FP32 estimate of
 // max_e |R5 - R7| / |R7| lies within 5 % of rtol, or the two fourth differences
-// that choose the split dimension are within 0.1 % of each other, the region is
+// that choose the split dimension are within 0.1 % of each other (or within their
+// FP32 error, 4e-6 of the summed values), the region is
 // evaluated again point by point in FP64 from the FP64 mean PSF, with the
 // reference design's arithmetic (math/genz_malik.hxx:127-195) and no fused
 // multiply-adds, and that evaluation decides (and gives the value).
@@ -274,7 +275,7 @@ __device__ __noinline__ bool gm_region(const PixGeom& g, float c0, float c1, flo
             }
         }
     };
-    float rel = 0.f, dd0 = 0.f, dd1 = 0.f;
+    float rel = 0.f, dd0 = 0.f, dd1 = 0.f, sx7 = 0.f;
     if (!last) {
         for (int qd = 0; qd < EQ4; ++qd) {
             float4 v7, vd, a0, a1;
@@ -289,6 +290,7 @@ __device__ __noinline__ bool gm_region(const PixGeom& g, float c0, float c1, flo
                     rel = fmaxf(rel, r);
                     dd0 += fabsf(f4c(a0, c));
                     dd1 += fabsf(f4c(a1, c));
+                    sx7 += fabsf(x7);
                     // added now, so an accepted region needs no second pass; a split
                     // region is taken back out below
                     if (atomic) atomicAdd(mean + e, (double)(area * x7));
@@ -300,7 +302,9 @@ __device__ __noinline__ bool gm_region(const PixGeom& g, float c0, float c1, flo
         const bool near_tol = fabsf(rel - rtol) <= fmaxf(0.05f * rtol, 4e-6f);
         const bool accept = rel <= rtol;
         if (accept && !near_tol) return true;
-        const bool near_dim = !accept && fabsf(dd0 - dd1) <= 1e-3f * (dd0 + dd1);
+        // the fourth differences cancel most of the values they are formed from, so
+        // their FP32 error is measured against the values (sx7), not against themselves
+        const bool near_dim = !accept && fabsf(dd0 - dd1) <= 1e-3f * (dd0 + dd1) + 4e-6f * sx7;
         for (int qd = 0; qd < EQ4; ++qd) {  // take the FP32 values back out
             float4 v7, vd, a0, a1;
             rule(qd, v7, vd, a0, a1);
