@@ -74,9 +74,9 @@ def test_launch_shape_tuning(api):
     ref, _ = api.point_src_model_map_wcs(job.wcs, src, expo, upsf, part, with_info=False)
     res = T.tune_launch_shapes(job.wcs, src, expo, upsf, part)
     assert len(res["ms"]) == 6 and all(v > 0 for v in res["ms"].values())
-    assert api.get_tuning()["window_waves"] == res["choice"]["window_waves"]
+    assert api.get_tuning()["window_blocks_per_sm"] == res["choice"]["window_blocks_per_sm"]
     for wv, wb in ((2, 1), (4, 2)):
-        api.set_tuning(window_waves=wv, write_blocks_per_sm=wb)
+        api.set_tuning(window_blocks_per_sm=wv, write_blocks_per_sm=wb)
         m, _ = api.point_src_model_map_wcs(job.wcs, src, expo, upsf, part, with_info=False)
         torch.cuda.synchronize()
         rel = ((m.double() - ref.double()).abs() / ref.double().abs().clamp_min(1e-300)).max().item()
@@ -84,6 +84,6 @@ def test_launch_shape_tuning(api):
     from xtsrcmaps_b200 import _lib as L
 
     with pytest.raises(L.XtsError):
-        api.set_tuning(window_waves=9)
+        api.set_tuning(window_blocks_per_sm=9)
     api.reset_tuning()
     assert api.get_tuning() == {k: 0 for k in api.TUNING_FIELDS}

@@ -41,7 +41,7 @@ def main(argv=None) -> int:
     ap.add_argument("--train-surrogate", metavar="NET.npz", help="train a surrogate network on samples of this "
                     "job's mean PSFs, save it here and use it")
     ap.add_argument("--surrogate-samples", type=int, default=10_000_000)
-    ap.add_argument("--surrogate-epochs", type=int, default=20)
+    ap.add_argument("--surrogate-epochs", type=int, default=60)
     ap.add_argument("--check-tol", type=float, default=1e-4,
                     help="surrogate maps whose check against the rule exceeds this are redone by the rule")
     ap.add_argument("--device", type=int, default=0)
@@ -114,6 +114,13 @@ def main(argv=None) -> int:
                 net = Surrogate(device=dev, seed=args.seed)
                 losses = net.train(X, Y, epochs=args.surrogate_epochs)
                 del X, Y
+                # error cells from held-out samples of the same tables (another seed)
+                Xc, Yc = samples(t(ps.uPsf), job.logEs, max(1_000_000, args.surrogate_samples // 3),
+                                 seed=args.seed + 1)
+                cal = net.calibrate(Xc, Yc, tol=args.check_tol, margin=0.7)
+                del Xc, Yc
+                print(f"surrogate calibrated: {cal['cells_accepted']} of {cal['cells']} cells served, "
+                      f"{cal['share_in_accepted_cells']:.3f} of held-out samples in them")
                 net.save(args.train_surrogate)
                 print(f"surrogate trained: {args.surrogate_samples} samples, {args.surrogate_epochs} epochs, "
                       f"loss {losses[0]:.3e} -> {losses[-1]:.3e}, saved to {args.train_surrogate}")

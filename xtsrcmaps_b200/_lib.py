@@ -105,7 +105,7 @@ class XtsMlp(C.Structure):
 
 
 class XtsTuning(C.Structure):
-    _fields_ = [("window_waves", C.c_int), ("write_blocks_per_sm", C.c_int), ("queue_blocks_per_sm", C.c_int),
+    _fields_ = [("window_blocks_per_sm", C.c_int), ("write_blocks_per_sm", C.c_int), ("queue_blocks_per_sm", C.c_int),
                 ("mlp_blocks_per_sm", C.c_int)]
 
 

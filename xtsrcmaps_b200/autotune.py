@@ -7,7 +7,7 @@ Three choices are made by measurement on the job at hand rather than fixed:
   product (all three parity-tested against the FP64 oracle) -- timed with CUDA
   events on the job's own geometry; the fastest wins.
 * ``tune_launch_shapes``: the launch shapes of the plain path (xts_set_tuning):
-  the window pass's grid in waves of resident blocks, the write pass's
+  the window pass's blocks per SM (one persistent wave), the write pass's
   persistent blocks per SM and, with a network given, the surrogate forward
   pass's blocks per SM -- each candidate timed on the job's own maps, the
   fastest set for the calls that follow;
@@ -113,15 +113,15 @@ def tune_adaptive(wcs, src_sph, exposure, uPsf, partial_integrals, target: float
 
 
 def tune_launch_shapes(wcs, src_sph, exposure, uPsf, partial_integrals, net=None,
-                       window_waves: Sequence[int] = (1, 2, 4), write_blocks_per_sm: Sequence[int] = (1, 2),
+                       window_blocks_per_sm: Sequence[int] = (1, 2, 3), write_blocks_per_sm: Sequence[int] = (1, 2),
                        mlp_blocks_per_sm: Sequence[int] = (1, 2), reps: int = 3, apply: bool = True) -> dict:
-    """Time the plain model map for every (window waves, write-pass blocks per SM)
+    """Time the plain model map for every (window-pass blocks per SM, write-pass blocks per SM)
     pair and, with ``net``, the network's forward pass on a million rows for each
     blocks-per-SM count; set the fastest (apply) and return
     {"choice": {...}, "ms": {...}}."""
     from . import api as A
 
-    key = _key("shapes", wcs, src_sph, uPsf, (tuple(window_waves), tuple(write_blocks_per_sm),
+    key = _key("shapes", wcs, src_sph, uPsf, (tuple(window_blocks_per_sm), tuple(write_blocks_per_sm),
                                                tuple(mlp_blocks_per_sm), net is not None))
     if key in _CACHE:
         res = _CACHE[key]
@@ -134,13 +134,13 @@ def tune_launch_shapes(wcs, src_sph, exposure, uPsf, partial_integrals, net=None
                       dtype=torch.float32, device=uPsf.device)
     before = A.get_tuning()
     ms = {}
-    for wv in window_waves:
+    for wv in window_blocks_per_sm:
         for wb in write_blocks_per_sm:
-            A.set_tuning(window_waves=wv, write_blocks_per_sm=wb)
-            ms[f"waves{wv}/write{wb}"] = (_timed(lambda: A.point_src_model_map_wcs(
+            A.set_tuning(window_blocks_per_sm=wv, write_blocks_per_sm=wb)
+            ms[f"window{wv}/write{wb}"] = (_timed(lambda: A.point_src_model_map_wcs(
                 wcs, src_sph, exposure, uPsf, partial_integrals, out=out, with_info=False), reps), wv, wb)
     best = min(ms.values())
-    choice = {"window_waves": best[1], "write_blocks_per_sm": best[2]}
+    choice = {"window_blocks_per_sm": best[1], "write_blocks_per_sm": best[2]}
     table = {k: v[0] for k, v in ms.items()}
     if net is not None:
         X = torch.randn((1 << 20, 5), device=uPsf.device) * torch.as_tensor(net.in_sd, device=uPsf.device) + \

@@ -928,7 +928,7 @@ int xts_set_tuning(const xts_tuning* t) {
         g_tuning = xts_tuning{0, 0, 0, 0};
         return XTS_OK;
     }
-    if (t->window_waves < 0 || t->window_waves > 8 || t->write_blocks_per_sm < 0 || t->write_blocks_per_sm > 2 ||
+    if (t->window_blocks_per_sm < 0 || t->window_blocks_per_sm > 4 || t->write_blocks_per_sm < 0 || t->write_blocks_per_sm > 2 ||
         t->queue_blocks_per_sm < 0 || t->queue_blocks_per_sm > 4 || t->mlp_blocks_per_sm < 0 ||
         t->mlp_blocks_per_sm > 2)
         return set_error(XTS_ERR_ARG, "set_tuning: a field is outside its range");

@@ -283,8 +283,16 @@ int launch_exposure_map_tc(const float* cube, const float* wcube, long long npix
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    // as many blocks per SM as shared memory allows, within the 512 tensor-memory
+    // columns of an SM (each block allocates its accumulator's columns): the blocks'
+    // load -> split -> MMA -> epilogue chains overlap one another
+    int per_sm = 1;
+    XTS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_exposure_map_tc, XM, smem));
+    const int ncols = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));
+    per_sm = per_sm < 1 ? 1 : per_sm;
+    per_sm = per_sm > 512 / ncols ? 512 / ncols : per_sm;
     const long long ntiles = (npix + XM - 1) / XM;
-    const int G = (int)(ntiles < 2LL * nsm ? ntiles : 2LL * nsm);
+    const int G = (int)(ntiles < (long long)per_sm * nsm ? ntiles : (long long)per_sm * nsm);
     XTS_LAUNCH("k_exposure_map_tc", st, k_exposure_map_tc<<<G, XM, smem, st>>>(mx, mw, mbh, mbl, (int)npix, E, out,
                                                                                 status));
     return XTS_OK;

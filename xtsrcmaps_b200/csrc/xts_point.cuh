@@ -45,8 +45,11 @@ struct SepTab {
                            // z = (d - DPOLY_C)/DPOLY_H
     SepBin bins[NSB];
 };
-constexpr float DPOLY_C = 0.035f;  // centre and half-width of the fitted d range
-constexpr float DPOLY_H = 0.037f;
+// centre and half-width of the fitted d range, [-0.002, 0.146]: two table rows (the
+// ratio q[k + 2] / q[k] - 1 is at most 0.1445), so one row's polynomial also gives
+// t for the points of the next row (t error below 1e-8 over the range)
+constexpr float DPOLY_C = 0.072f;
+constexpr float DPOLY_H = 0.074f;
 
 constexpr int RW = 8;   // dense row window per pixel
 constexpr int WST = 9;  // padded stride of a window in shared memory (bank-conflict free)
@@ -119,6 +122,11 @@ static __constant__ double c_rule_uv[12][4];
 static __constant__ float c_rule_w32[12];
 static __constant__ double c_rule_q[12][3];  // u, u*u, v (biquadratic chord form)
 static __constant__ float c_rule_f[12][4];   // u, u*u, v in FP32 (chord offsets from the centre), pad
+// The rule's points come in mirror pairs (p + 6 = -p, same weight): for pair p < 6,
+// u, v, uv, u^2, v^2, u^2 v, u v^2, u^2 v^2 in FP32, so the chord offset of the pair is
+// E +- O with E the even and O the odd part of the biquadratic form.
+static __constant__ float c_pair[6][8];
+static __constant__ float c_rule_wsum;       // sum of the 12 FP32 weights
 
 static int upload_rule_uv(cudaStream_t st) {
     static int dev_done = -1;
@@ -152,6 +160,15 @@ static int upload_rule_uv(cudaStream_t st) {
         bq[p][0] = R[3 * p]; bq[p][1] = R[3 * p] * R[3 * p]; bq[p][2] = R[3 * p + 1];
         bf[p][0] = (float)bq[p][0]; bf[p][1] = (float)bq[p][1]; bf[p][2] = (float)bq[p][2]; bf[p][3] = 0.f;
     }
+    float pr[6][8], wsum = 0.f;
+    for (int p = 0; p < 6; ++p) {
+        const double u = R[3 * p], v = R[3 * p + 1];
+        const double k[8] = {u, v, u * v, u * u, v * v, u * u * v, u * v * v, u * u * v * v};
+        for (int j = 0; j < 8; ++j) pr[p][j] = (float)k[j];
+    }
+    for (int p = 0; p < 12; ++p) wsum += w32[p];
+    XTS_CUDA(cudaMemcpyToSymbolAsync(c_pair, pr, sizeof(pr), 0, cudaMemcpyHostToDevice, st));
+    XTS_CUDA(cudaMemcpyToSymbolAsync(c_rule_wsum, &wsum, sizeof(wsum), 0, cudaMemcpyHostToDevice, st));
     XTS_CUDA(cudaMemcpyToSymbolAsync(c_rule_f, bf, sizeof(bf), 0, cudaMemcpyHostToDevice, st));
     XTS_CUDA(cudaMemcpyToSymbolAsync(c_rule_uv, b, sizeof(b), 0, cudaMemcpyHostToDevice, st));
     XTS_CUDA(cudaMemcpyToSymbolAsync(c_rule_w32, w32, sizeof(w32), 0, cudaMemcpyHostToDevice, st));

@@ -34,16 +34,19 @@ namespace xts {
 
 // ============================================================================ pass A
 constexpr int WT = 256;  // pixels per tile == threads per block
+constexpr int NSG = 4;   // sources per group: one pixel's source-independent geometry serves NSG sources
 
 constexpr size_t WA_OFF_BINS = 0;
 constexpr size_t WA_OFF_COEF = sizeof(SepBin) * NSB;
 constexpr size_t WA_OFF_HIST = WA_OFF_COEF + sizeof(float4) * 2 * ND;
-constexpr size_t WA_OFF_WTS = WA_OFF_HIST + (8 * ND + 15) / 16 * 16;
-constexpr size_t WA_SMEM = WA_OFF_WTS + sizeof(float) * WT * RW;
+constexpr size_t WA_OFF_WTS = WA_OFF_HIST + (8 * NSG * ND + 15) / 16 * 16;
+constexpr size_t WA_OFF_SRC = WA_OFF_WTS + sizeof(float) * WT * RW;
+constexpr size_t WA_SMEM = WA_OFF_SRC + sizeof(SrcInfo) * NSG;
 
 constexpr int NSP = 24;  // entries of a sparse record: 12 points x 2 rows
 constexpr int META_OVERFLOW = -0x7fffffff - 1;  // wide pixel without a sparse record
 constexpr int REC_ROWS = 3;  // window rows held by the 16-byte main record
+constexpr float EMSTEP = (float)(REDM1 / (REDM1 + 1.0));  // e^-step: t in row k + 1 = (t in row k - 1) e^-step
 
 // Per (source, pixel) the main record rec = {w0, w1, w2, meta}: meta >= 0 is the
 // window's first row (bits 0-15) and row count (bits 16-23), with the weights of
@@ -52,7 +55,7 @@ constexpr int REC_ROWS = 3;  // window rows held by the 16-byte main record
 struct PassA {
     const SepBin* sbin;    // shared: row bins
     const float4* scoef;   // shared: per-row records
-    double* hist;          // shared: the block's map-integral rows
+    double* hist;          // shared: the block's map-integral rows ([NSG][ND] in the dense pass)
     float* wts;            // shared: [RW][WT] windows
     float4* rec;
     float4* ext;
@@ -61,7 +64,7 @@ struct PassA {
     int* sparse_count;
 };
 
-// Shared tables of pass A, loaded by every block.
+// Shared tables of pass A, loaded by every block (the histogram is zeroed by the caller).
 __device__ __forceinline__ PassA pass_a_tables(unsigned char* smem, const SepTab* septab, float4* rec, float4* ext,
                                                float2* sparse, int sparse_cap, int* sparse_count) {
     PassA A;
@@ -74,44 +77,164 @@ __device__ __forceinline__ PassA pass_a_tables(unsigned char* smem, const SepTab
     float4* sc = (float4*)(smem + WA_OFF_COEF);
     for (int k = threadIdx.x; k < NSB; k += WT) sb[k] = septab->bins[k];
     for (int k = threadIdx.x; k < 2 * ND; k += WT) sc[k] = ((const float4*)septab->coef)[k];
-    for (int r = threadIdx.x; r < ND; r += WT) A.hist[r] = 0.;
     return A;
 }
 
-// One (source, pixel): map pixel (h, w) of the full grid (W1 = W + 1 corner columns,
-// omega index om_idx), record index kk.  Pixels whose centre lies within the
-// boundary radius (squared chord ch2) add their window rows to the block's
-// histogram; the rows they touch widen [*rlo, *rhi] when those are given.
-__device__ __forceinline__ void window_pixel(const double* __restrict__ corners, const double* __restrict__ centers,
-                                             const double* __restrict__ omega, const SrcInfo& si, double ch2, int W1,
-                                             int h, int w, size_t om_idx, size_t kk, const PassA& A, int* rlo,
-                                             int* rhi) {
+// Source-independent geometry of one pixel: its rule points are the bilinear
+// blend P(u, v) = M + B u + C v + D uv of the corners, so relative to a source s
+// with A = M - s the squared chord is q(u, v) = |A + B u + C v + D uv|^2, whose
+// coefficients split into source-dependent ones (|A|^2, 2 A.B, 2 A.C, 2 A.D) and
+// the rest (|B|^2, |C|^2, 2 B.C, 2 B.D, 2 C.D, |D|^2).  The latter enter each
+// mirror pair's chord offset through eb (even part) and ob (odd part), formed once
+// per pixel for a group of sources.
+struct PixBase {
+    double m[3];      // M, the corners' average (FP64)
+    double c[3];      // pixel centre (boundary-radius test)
+    float b2[3], c2[3], d2[3];  // 2B, 2C, 2D
+    float bc2;        // 2 B.C
+    float eb[6], ob[6];
+    float om;         // solid angle
+};
+
+__device__ __forceinline__ PixBase pixel_base(const double* __restrict__ corners, const double* __restrict__ centers,
+                                              const double* __restrict__ omega, int W1, int h, int w, size_t om_idx) {
+    const double* a = corners + 3 * (h * W1 + w);            // LL
+    const double* b = corners + 3 * (h * W1 + w + 1);        // LR
+    const double* c = corners + 3 * ((h + 1) * W1 + w + 1);  // UR
+    const double* d = corners + 3 * ((h + 1) * W1 + w);      // UL
+    PixBase P;
+    double B[3], C[3], D[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        P.m[i] = 0.25 * ((a[i] + b[i]) + (c[i] + d[i]));
+        B[i] = 0.25 * ((b[i] + c[i]) - (a[i] + d[i]));
+        C[i] = 0.25 * ((c[i] + d[i]) - (a[i] + b[i]));
+        D[i] = 0.25 * ((a[i] + c[i]) - (b[i] + d[i]));
+        P.b2[i] = (float)(2.0 * B[i]);
+        P.c2[i] = (float)(2.0 * C[i]);
+        P.d2[i] = (float)(2.0 * D[i]);
+    }
+    const double* pc = centers + 3 * ((size_t)h * W1 + w);
+    P.c[0] = pc[0]; P.c[1] = pc[1]; P.c[2] = pc[2];
+    const float q4 = (float)fma(B[0], B[0], fma(B[1], B[1], B[2] * B[2]));
+    const float q5 = (float)fma(C[0], C[0], fma(C[1], C[1], C[2] * C[2]));
+    const float q6 = (float)(2.0 * fma(B[0], D[0], fma(B[1], D[1], B[2] * D[2])));
+    const float q7 = (float)(2.0 * fma(C[0], D[0], fma(C[1], D[1], C[2] * D[2])));
+    const float q8 = (float)fma(D[0], D[0], fma(D[1], D[1], D[2] * D[2]));
+    P.bc2 = (float)(2.0 * fma(B[0], C[0], fma(B[1], C[1], B[2] * C[2])));
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        P.eb[k] = fmaf(q8, c_pair[k][7], fmaf(q5, c_pair[k][4], q4 * c_pair[k][3]));
+        P.ob[k] = fmaf(q7, c_pair[k][6], q6 * c_pair[k][5]);
+    }
+    P.om = (float)omega[om_idx];
+    return P;
+}
+
+// Lower table row of the squared chord q: one bin load and one FP64 compare.
+__device__ __forceinline__ int row_lower(double q, const SepBin* bins) {
+    int b = (__double2hiint(q) >> (20 - SB_BITS)) - (SB_EXP0 << SB_BITS);
+    b = min(max(b, 0), NSB - 1);
+    const SepBin sb = bins[b];
+    return sb.k0 + (q >= sb.thr);
+}
+
+// One (source, pixel): the pixel's window for source si, record index kk.  Pixels
+// whose centre lies within the boundary radius (squared chord ch2) add their window
+// rows to hist (the source's map-integral rows); the rows they touch widen
+// [*rlo, *rhi] when those are given.  (h, w) and W1 locate the pixel's corners for
+// the rare wide pixel, which is redone in FP64 point by point.
+__device__ __forceinline__ void window_source(const PixBase& P, const SrcInfo& si, double ch2,
+                                              const double* __restrict__ corners, int W1, int h, int w,
+                                              size_t kk, const PassA& A, double* hist, int* rlo, int* rhi) {
     const int t = threadIdx.x;
+    const double Ax = P.m[0] - si.dir[0], Ay = P.m[1] - si.dir[1], Az = P.m[2] - si.dir[2];
+    const double a0 = fma(Ax, Ax, fma(Ay, Ay, Az * Az));  // q at the centre of the blend
     bool inside = false;
     if (si.in_fov) {
-        const double* c = centers + 3 * ((size_t)h * W1 + w);
-        const double x = si.dir[0] - c[0], y = si.dir[1] - c[1], z = si.dir[2] - c[2];
+        const double x = si.dir[0] - P.c[0], y = si.dir[1] - P.c[1], z = si.dir[2] - P.c[2];
         const double d2 = x * x + y * y + z * z;
         if (d2 < ch2 * (1.0 - 1e-12)) inside = true;
         else if (d2 > ch2 * (1.0 + 1e-12)) inside = false;
-        else inside = dir_diff(si.dir, c) <= si.radius_rad;
+        else inside = dir_diff(si.dir, P.c) <= si.radius_rad;
     }
-    const PixQ g = pixel_q(pixel_geom(corners, W1, h, w, si));
-    const float om = (float)omega[om_idx];
-    float tc;
-    const int ic = point_row_bin(g.a0, A.sbin, A.scoef, &tc);
-    const int base = min(max(ic - 1 - RW / 2, 0), ND - RW);
-    // The window's row edges as FP32 offsets from the centre's FP64 squared
-    // chord, and the chord offsets of the rule points in FP32 from the
-    // biquadratic form: no FP64 per point, and no table search per point.
+    // q(point) - a0 in FP32: 2 A.B u + 2 A.C v + (2 A.D + 2 B.C) uv + the pixel's part
+    const float ax = (float)Ax, ay = (float)Ay, az = (float)Az;
+    const float f1 = fmaf(ax, P.b2[0], fmaf(ay, P.b2[1], az * P.b2[2]));
+    const float f2 = fmaf(ax, P.c2[0], fmaf(ay, P.c2[1], az * P.c2[2]));
+    const float f3 = fmaf(ax, P.d2[0], fmaf(ay, P.d2[1], fmaf(az, P.d2[2], P.bc2)));
+    float dqs[12];
+    float mn = INFINITY, mx = -INFINITY;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const float E = fmaf(f3, c_pair[k][2], P.eb[k]);
+        const float O = fmaf(f2, c_pair[k][1], fmaf(f1, c_pair[k][0], P.ob[k]));
+        dqs[k] = E + O;
+        dqs[k + 6] = E - O;
+        mn = fminf(mn, fminf(dqs[k], dqs[k + 6]));
+        mx = fmaxf(mx, fmaxf(dqs[k], dqs[k + 6]));
+    }
+    const float om = P.om;
+    auto edge = [&](int k) {  // q[k] - a0 in FP32
+        const float4 cw = A.scoef[2 * k + 1];
+        return (float)(__hiloint2double(__float_as_int(cw.w), __float_as_int(cw.z)) - a0);
+    };
+    // Most pixels' points lie in the centre's table row, or in it and one
+    // neighbour.  Then one row's polynomial (fitted over two rows) gives every
+    // point's t relative to the lower row kl, u = t - 1; a point past the upper
+    // edge eb has t' = u e^-step in row kl + 1.  With T = sum w u over all points
+    // and S2 = sum w u over those past eb, the three row weights are
+    //     s0 = om (S2 - T),  s2 = om e^-step S2,  s1 = om sum(w) - s0 - s2.
+    const int kc = row_lower(a0, A.sbin);  // the centre's lower table row
+    if (kc >= 2 && kc <= ND - 4) {
+        const float em1 = edge(kc - 1), e0 = edge(kc), e1 = edge(kc + 1), e2 = edge(kc + 2);
+        // rows kc (and kc + 1), or kc - 1 and kc; eb = +inf for one row.  The case is
+        // made opaque to the compiler: specialising the point loop per case would run
+        // up to three copies of it per warp, each with a part of the lanes.
+        const bool up = mn >= e0 && mx < e2, dn = mn >= em1 && mx < e1;
+        int kl = up ? kc : (dn ? kc - 1 : -1);
+        float eb = (mn >= e0 && mx < e1) ? INFINITY : (up ? e1 : e0);
+        float eL = up ? e0 : em1;
+        asm volatile("" : "+r"(kl), "+f"(eb), "+f"(eL));
+        if (kl >= 0) {  // (warp-divergent: a warp's pixels usually agree)
+            const float4 c0 = A.scoef[2 * kl], c1 = A.scoef[2 * kl + 1];
+            // zz = (dl - C)/H and REDM1 dl, dl = q / q_kl - 1 = (dq - eL) / q_kl, as FMAs in dq
+            const float kz = c0.x * (1.f / DPOLY_H), z0 = fmaf(-eL, kz, -DPOLY_C / DPOLY_H);
+            const float kr = c0.x * (float)REDM1, r0 = -eL * kr;
+            float T = 0.f, S2 = 0.f;
+#pragma unroll
+            for (int p = 0; p < 12; ++p) {
+                const float dq = dqs[p];
+                const float zz = fmaf(dq, kz, z0);
+                const float P4 = fmaf(fmaf(fmaf(fmaf(c1.y, zz, c1.x), zz, c0.w), zz, c0.z), zz, c0.y);
+                const float u = fmaf(fmaf(dq, kr, r0), P4, -1.f);
+                const float wp = c_rule_w32[p];
+                T = fmaf(wp, u, T);
+                S2 = fmaf(dq >= eb ? wp : 0.f, u, S2);
+            }
+            const float s0 = om * (S2 - T), s2 = om * (EMSTEP * S2);
+            const float s1 = fmaf(om, c_rule_wsum, -s0) - s2;
+            const bool two = eb != INFINITY;
+            const int nent = two ? 3 : 2;
+            if (inside) {
+                atomicAdd(&hist[kl], (double)s0);
+                atomicAdd(&hist[kl + 1], (double)s1);
+                if (two) atomicAdd(&hist[kl + 2], (double)s2);
+                if (rlo) {
+                    atomicMin(rlo, kl);
+                    atomicMax(rhi, kl + nent - 1);
+                }
+            }
+            A.rec[kk] = make_float4(s0, s1, s2, __int_as_float(kl | (nent << 16)));
+            return;
+        }
+    }
+    // General path: the window of RW rows around the centre's row, the row edges
+    // as FP32 offsets from a0.
+    const int base = min(max(kc - RW / 2, 0), ND - RW);
     float d[RW];
 #pragma unroll
-    for (int j = 0; j < RW; ++j) {
-        const float4 cw = A.scoef[2 * (base + j) + 1];
-        d[j] = (float)(__hiloint2double(__float_as_int(cw.w), __float_as_int(cw.z)) - g.a0);
-    }
-    const float f1 = (float)g.a1, f2 = (float)g.a2, f3 = (float)g.a3, f4 = (float)g.a4;
-    const float f5 = (float)g.a5, f6 = (float)g.a6, f7 = (float)g.a7, f8 = (float)g.a8;
+    for (int j = 0; j < RW; ++j) d[j] = edge(base + j);
     float* wd = A.wts + t;  // slot j at wd[j * WT]: lanes hit consecutive words
 #pragma unroll
     for (int j = 0; j < RW; ++j) wd[j * WT] = 0.f;
@@ -119,11 +242,7 @@ __device__ __forceinline__ void window_pixel(const double* __restrict__ corners,
     int lo = RW, hi = -1;
 #pragma unroll
     for (int p = 0; p < 12; ++p) {
-        const float u = c_rule_f[p][0], uu = c_rule_f[p][1], v = c_rule_f[p][2];
-        const float p0 = fmaf(f4, uu, f1 * u);
-        const float p1 = fmaf(f6, uu, fmaf(f3, u, f2));
-        const float p2 = fmaf(f8, uu, fmaf(f7, u, f5));
-        const float dq = fmaf(fmaf(p2, v, p1), v, p0);  // q(point) - q(centre)
+        const float dq = dqs[p];
         int r = 0;
         float dlo = d[0];
 #pragma unroll
@@ -140,10 +259,10 @@ __device__ __forceinline__ void window_pixel(const double* __restrict__ corners,
             float tt;
             if (dl >= -0.002f && dl <= 0.072f) {
                 const float zz = fmaf(dl, 1.f / DPOLY_H, -DPOLY_C / DPOLY_H);
-                const float P = fmaf(fmaf(fmaf(fmaf(c1.y, zz, c1.x), zz, c0.w), zz, c0.z), zz, c0.y);
-                tt = (float)REDM1 * (dl * P);
+                const float P4 = fmaf(fmaf(fmaf(fmaf(c1.y, zz, c1.x), zz, c0.w), zz, c0.z), zz, c0.y);
+                tt = (float)REDM1 * (dl * P4);
             } else {
-                tt = t_exact(g.a0 + (double)dq, k + 1);
+                tt = t_exact(a0 + (double)dq, k + 1);
             }
             wd[r * WT] += (1.f - tt) * wo;
             wd[(r + 1) * WT] += tt * wo;
@@ -158,7 +277,7 @@ __device__ __forceinline__ void window_pixel(const double* __restrict__ corners,
         if (inside) {
 #pragma unroll
             for (int j = 0; j < RW; ++j)
-                if (j >= lo && j <= hi) atomicAdd(&A.hist[base + j], (double)wd[j * WT]);
+                if (j >= lo && j <= hi) atomicAdd(&hist[base + j], (double)wd[j * WT]);
             if (rlo) {
                 atomicMin(rlo, base + lo);
                 atomicMax(rhi, base + hi);
@@ -175,8 +294,9 @@ __device__ __forceinline__ void window_pixel(const double* __restrict__ corners,
             A.ext[2 * kk + 1] = make_float4(f[4], f[5], f[6], f[7]);
         }
     } else {
-        // a wide pixel (next to the source): its 12 points again with FP64 chords,
-        // for its sparse record and its map-integral rows alike
+        // a wide pixel (next to the source): its 12 points again with FP64 chords
+        // from the corners, for its sparse record and its map-integral rows alike
+        const PixQ g = pixel_q(pixel_geom(corners, W1, h, w, si));
         int meta = META_OVERFLOW;
         const int slot = atomicAdd(A.sparse_count, 1);
         float2* sr = slot < A.sparse_cap ? A.sparse + (size_t)slot * NSP : nullptr;
@@ -190,8 +310,8 @@ __device__ __forceinline__ void window_pixel(const double* __restrict__ corners,
                 sr[2 * p + 1] = make_float2(wb, __int_as_float(idx));
             }
             if (inside) {
-                atomicAdd(&A.hist[idx - 1], (double)wa);
-                atomicAdd(&A.hist[idx], (double)wb);
+                atomicAdd(&hist[idx - 1], (double)wa);
+                atomicAdd(&hist[idx], (double)wb);
                 if (rlo) {
                     atomicMin(rlo, idx - 1);
                     atomicMax(rhi, idx);
@@ -203,33 +323,58 @@ __device__ __forceinline__ void window_pixel(const double* __restrict__ corners,
     }
 }
 
-// The dense map: grid (nch, S), block (c, s) takes tiles c, c + nch, ... of source
-// s's H x W pixels and writes its histogram to hist_out[s][c].
-__global__ void __launch_bounds__(WT, 4) k_pixel_windows(const double* __restrict__ corners, const double* __restrict__ centers,
+__device__ __forceinline__ double boundary_chord2(const SrcInfo& si) {
+    const double c = 2.0 * sin(0.5 * si.radius_rad);
+    return c * c;
+}
+
+// The dense map, one persistent wave over a work queue: item (g, p) is part p of
+// the P parts of group g (NSG sources; tiles [p nt / P, (p + 1) nt / P) of WT pixels).
+// A block takes the next item (one atomic), forms each pixel's source-independent
+// geometry once and the windows of the group's sources from it, and adds the item's
+// non-zero rows to hist_out[s] (cleared before the launch) with FP64 atomics.
+__global__ void __launch_bounds__(WT, 2) k_pixel_windows(const double* __restrict__ corners, const double* __restrict__ centers,
                                                       const double* __restrict__ omega, const SrcInfo* __restrict__ info,
-                                                      const SepTab* __restrict__ septab, int H, int W, int nch,
+                                                      const SepTab* __restrict__ septab, int S, int H, int W,
+                                                      int P, unsigned* __restrict__ queue,
                                                       double* __restrict__ hist_out, float4* __restrict__ rec,
                                                       float4* __restrict__ ext, float2* __restrict__ sparse,
                                                       int sparse_cap, int* __restrict__ sparse_count) {
     extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int item_s;
     const PassA A = pass_a_tables(smem, septab, rec, ext, sparse, sparse_cap, sparse_count);
-    const int s = blockIdx.y, t = threadIdx.x;
-    const SrcInfo si = info[s];
-    double ch2 = 2.0 * sin(0.5 * si.radius_rad);
-    ch2 *= ch2;
+    SrcInfo* ssrc = (SrcInfo*)(smem + WA_OFF_SRC);
+    const int t = threadIdx.x;
     const int npix = H * W, W1 = W + 1;
-    const int ntiles = (npix + WT - 1) / WT;
-    const size_t sp = (size_t)s * npix;
-    __syncthreads();
-    for (int tile = blockIdx.x; tile < ntiles; tile += nch) {
-        const int pix = tile * WT + t;
-        if (pix >= npix) continue;
-        const int h = pix / W, w = pix - h * W;
-        window_pixel(corners, centers, omega, si, ch2, W1, h, w, (size_t)pix, sp + pix, A, nullptr, nullptr);
+    const int nt = (npix + WT - 1) / WT;
+    const int ng = (S + NSG - 1) / NSG, n_items = ng * P;
+    for (;;) {
+        if (t == 0) item_s = (int)atomicAdd(queue, 1u);
+        __syncthreads();  // also: the previous item's rows are written out
+        const int item = item_s;
+        if (item >= n_items) break;
+        const int g = item / P, p = item - g * P, s0 = g * NSG, ns = min(NSG, S - s0);
+        if (t < ns) ssrc[t] = info[s0 + t];
+        for (int r = t; r < NSG * ND; r += WT) A.hist[r] = 0.;
+        __syncthreads();
+        const int ta = (int)((long long)p * nt / P), tb = (int)((long long)(p + 1) * nt / P);
+        for (int tile = ta; tile < tb; ++tile) {
+            const int pix = tile * WT + t;
+            if (pix >= npix) continue;
+            const int h = pix / W, w = pix - h * W;
+            const PixBase Q = pixel_base(corners, centers, omega, W1, h, w, (size_t)pix);
+            for (int j = 0; j < ns; ++j) {
+                const SrcInfo& si = ssrc[j];
+                window_source(Q, si, boundary_chord2(si), corners, W1, h, w, (size_t)(s0 + j) * npix + pix, A,
+                              A.hist + j * ND, nullptr, nullptr);
+            }
+        }
+        __syncthreads();
+        for (int r = t; r < ns * ND; r += WT) {
+            const double v = A.hist[r];
+            if (v != 0.) atomicAdd(hist_out + (size_t)s0 * ND + r, v);
+        }
     }
-    __syncthreads();
-    double* out = hist_out + ((size_t)s * nch + blockIdx.x) * ND;
-    for (int r = t; r < ND; r += WT) out[r] = A.hist[r];
 }
 
 // Cutouts: one persistent launch over a work queue of (source, tile) items, tile
@@ -238,7 +383,7 @@ __global__ void __launch_bounds__(WT, 4) k_pixel_windows(const double* __restric
 // and the item's map-integral rows in shared memory, and adds the rows it touched
 // to hist_out[s] with FP64 atomics.  item_src[i] is the source of item i, tile_off[s]
 // its first item and tile_off[S] the number of items.
-__global__ void __launch_bounds__(WT, 4) k_pixel_windows_cut(const double* __restrict__ corners,
+__global__ void __launch_bounds__(WT, 3) k_pixel_windows_cut(const double* __restrict__ corners,
                                                           const double* __restrict__ centers,
                                                           const double* __restrict__ omega,
                                                           const SrcInfo* __restrict__ info,
@@ -255,6 +400,7 @@ __global__ void __launch_bounds__(WT, 4) k_pixel_windows_cut(const double* __res
     __shared__ int rmin_s, rmax_s;
     const PassA A = pass_a_tables(smem, septab, rec, ext, sparse, sparse_cap, sparse_count);
     const int t = threadIdx.x, W1 = W + 1;
+    for (int r = t; r < ND; r += WT) A.hist[r] = 0.;
     const long long n_items = tile_off[S];
     for (;;) {
         if (t == 0) {
@@ -268,15 +414,14 @@ __global__ void __launch_bounds__(WT, 4) k_pixel_windows_cut(const double* __res
         const int s = item_src[item];
         const xts_cutout cw = cut[s];
         const SrcInfo si = info[s];
-        double ch2 = 2.0 * sin(0.5 * si.radius_rad);
-        ch2 *= ch2;
+        const double ch2 = boundary_chord2(si);
         const long long npix = (long long)cw.nh * cw.nw;
         const long long pix = (item - tile_off[s]) * WT + t;
         if (pix < npix) {
             const int i = (int)(pix / cw.nw), j = (int)(pix - (long long)i * cw.nw);
             const int h = cw.h0 + i, w = cw.w0 + j;
-            window_pixel(corners, centers, omega, si, ch2, W1, h, w, (size_t)h * W + w, (size_t)(cw.offset + pix), A,
-                         &rmin_s, &rmax_s);
+            const PixBase P = pixel_base(corners, centers, omega, W1, h, w, (size_t)h * W + w);
+            window_source(P, si, ch2, corners, W1, h, w, (size_t)(cw.offset + pix), A, A.hist, &rmin_s, &rmax_s);
         }
         __syncthreads();
         for (int r = rmin_s + t; r <= rmax_s; r += WT) {
@@ -602,6 +747,15 @@ bool srcmap_win_supported(int E) {
     return E >= 1 && E <= 4 * BQ && win_layout(E, win_row_quads(E)).total <= 227 * 1024;
 }
 
+// Parts per source group of the dense window pass (n sources of ntile tiles, G
+// blocks): about 8 queue items per block, at most one part per tile.
+static int window_parts(int n, int ntile, int G) {
+    const long long ng = (n + NSG - 1) / NSG;
+    long long P = (8LL * G + ng - 1) / ng;
+    if (P > ntile) P = ntile;
+    return P < 1 ? 1 : (int)P;
+}
+
 // Window records of one source chunk: a 16-byte main record and a 32-byte
 // extension slot per (source, pixel); only windows of more than REC_ROWS rows
 // write and read their extension.
@@ -651,16 +805,16 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
     int dev = 0, nsm = 148, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    // pass A: as many blocks as fit on the GPU at once (one full wave: a partial
-    // second wave would run at low occupancy)
+    // pass A: one persistent wave (at most window_blocks_per_sm blocks per SM) over
+    // a work queue of about 8 items per block
     int resident = 0;
     XTS_CUDA(cudaFuncSetAttribute(k_pixel_windows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WA_SMEM));
     XTS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_pixel_windows, WT, WA_SMEM));
     resident = resident < 1 ? 1 : resident;
-    int nch = (g_tuning.window_waves > 0 ? g_tuning.window_waves : 1) * resident * nsm / Sc;
-    const int maxch = (npix + WT - 1) / WT;
-    nch = nch < 1 ? 1 : (nch > maxch ? maxch : nch);
-    const size_t hist_n = (size_t)Sc * nch * ND + 1;
+    if (g_tuning.window_blocks_per_sm > 0 && g_tuning.window_blocks_per_sm < resident)
+        resident = g_tuning.window_blocks_per_sm;
+    const int nparts = window_parts(Sc, (npix + WT - 1) / WT, resident * nsm);
+    const size_t hist_n = (size_t)Sc * ND + 1;
     double* hist0 = (double*)workspace(W_PARTSUM, sizeof(double) * 2 * hist_n);
     if (!rec0 || !ext0 || !lut0 || !sparse0 || !hist0) return XTS_ERR_OOM;
     const WritePassFn wp = k_write_pass[(E + 3) / 4 - 1];
@@ -682,16 +836,22 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
         // the window pass is geometry only: it runs on the geometry stream, once
         // the write pass that last read its buffers is done
         if (pipe && k >= 2) XTS_CUDA(cudaStreamWaitEvent(gs, evB[b], 0));
+        // the chunk's queue counter sits next to its sparse-record count
+        unsigned* queue = (unsigned*)(status + 3 + b);
+        const int n_items = (n + NSG - 1) / NSG * nparts;
+        const int Gw = n_items < resident * nsm ? n_items : resident * nsm;
         XTS_CUDA(cudaMemsetAsync(sparse_count, 0, sizeof(int), gs));
-        XTS_LAUNCH("k_pixel_windows", gs, k_pixel_windows<<<dim3(nch, n), WT, WA_SMEM, gs>>>(
-                                              corners, centers, omega, info + s0, tab, H, W, nch,
+        XTS_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned), gs));
+        XTS_CUDA(cudaMemsetAsync(hist, 0, sizeof(double) * (size_t)n * ND, gs));
+        XTS_LAUNCH("k_pixel_windows", gs, k_pixel_windows<<<Gw, WT, WA_SMEM, gs>>>(
+                                              corners, centers, omega, info + s0, tab, n, H, W, nparts, queue,
                                               hist, rec, ext, sparse, (int)cap,
                                               sparse_count));
         if (pipe) {
             XTS_CUDA(cudaEventRecord(evA[b], gs));
             XTS_CUDA(cudaStreamWaitEvent(st, evA[b], 0));
         }
-        rc = launch_correction(hist, nch, info + s0, n, upsf + oE * ND, partial + oE * ND,
+        rc = launch_correction(hist, 1, info + s0, n, upsf + oE * ND, partial + oE * ND,
                                exposure + oE, E, scale + oE, inv_integ ? inv_integ + oE : nullptr,
                                correction ? correction + oE : nullptr, radius ? radius + s0 : nullptr,
                                in_fov ? in_fov + s0 : nullptr, st, lut, EQ * 4);
