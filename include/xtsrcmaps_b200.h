@@ -117,7 +117,12 @@ typedef struct xts_tuning {
                                  (1..4; default: as many as fit) */
     int write_blocks_per_sm;  /* write pass: persistent blocks per SM (1..2; default: as many as fit) */
     int queue_blocks_per_sm;  /* cutout window pass (work queue): blocks per SM (1..4; default: as many as fit) */
-    int mlp_blocks_per_sm;    /* surrogate network forward: blocks per SM (1..2; default 2) */
+    int mlp_blocks_per_sm;    /* surrogate network inference: 0 (default) four tiles in flight per SM in
+                                 one block of four warpgroups; 1..2 the two-warpgroup kernel at that
+                                 many blocks per SM */
+    int chunk_sources;        /* dense map: sources per chunk of the window and write passes; the
+                                 window pass of chunk k + 1 runs beside the write pass of chunk k
+                                 (0: one chunk while the window records fit 4 GiB) */
 } xts_tuning;
 int xts_set_tuning(const xts_tuning* t);  /* NULL restores the defaults */
 int xts_get_tuning(xts_tuning* t);

@@ -64,6 +64,7 @@ int main(void) {
            offsetof(xts_mlp, out_mu), offsetof(xts_mlp, lo), offsetof(xts_mlp, rho_min),
            offsetof(xts_mlp, cell_lo), offsetof(xts_mlp, cell_hi), offsetof(xts_mlp, cell_ok),
            sizeof(xts_surrogate_stats), offsetof(xts_surrogate_stats, evaluated));
+    printf("%zu %zu\n", sizeof(xts_tuning), offsetof(xts_tuning, chunk_sources));
     printf("%d %d %d %d %d %d\n", XTS_MLP_W2, XTS_MLP_W3, XTS_MLP_B4, XTS_MLP_NPARAM, XTS_MLP_CELL_NR,
            XTS_MLP_CELL_NS);
     return 0;
@@ -79,7 +80,8 @@ int main(void) {
     assert sizes == [C.sizeof(L.XtsMlp), L.XtsMlp.in_mu.offset, L.XtsMlp.out_mu.offset, L.XtsMlp.lo.offset,
                      L.XtsMlp.rho_min.offset, L.XtsMlp.cell_lo.offset, L.XtsMlp.cell_hi.offset,
                      L.XtsMlp.cell_ok.offset, C.sizeof(L.XtsSurrogateStats), L.XtsSurrogateStats.evaluated.offset]
-    consts = [int(v) for v in out[1].split()]
+    assert [int(v) for v in out[1].split()] == [C.sizeof(L.XtsTuning), L.XtsTuning.chunk_sources.offset]
+    consts = [int(v) for v in out[2].split()]
     assert consts[:4] == [L.MLP_W2, L.MLP_W3, L.MLP_B4, L.MLP_NPARAM] == [MO.W2, MO.W3, MO.B4, MO.NPARAM]
     assert consts[4:] == [L.MLP_CELL_NR, L.MLP_CELL_NS]
 

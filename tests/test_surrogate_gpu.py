@@ -103,14 +103,40 @@ def test_forward_and_gradient_match_oracle(api):
     p = net.params.cpu().numpy()
     y = net.predict(torch.as_tensor(X, device=d)).cpu().numpy()
     y_ref = MO.predict(p, X, net.in_mu, net.in_sd, net.out_mu, net.out_sd)
-    assert _rel_l2(y, y_ref) < 2e-2
+    # the GPU's tanh.approx against the oracle's exact tanh (rel-L2 measured 7e-5)
+    assert _rel_l2(y, y_ref) < 5e-4
     g, loss = net.gradient(torch.as_tensor(X, device=d), torch.as_tensor(Y, device=d))
     loss_ref, g_ref = MO.loss_and_grads(p, X, Y, net.in_mu, net.in_sd, net.out_mu, net.out_sd)
-    assert abs(loss - loss_ref) <= 1e-2 * loss_ref
+    assert abs(loss - loss_ref) <= 1e-3 * loss_ref
     g = g.cpu().numpy()
     for name, lo, hi in (("W1", MO.W1, MO.B1), ("b1", MO.B1, MO.W2), ("W2", MO.W2, MO.B2), ("b2", MO.B2, MO.W3),
                          ("W3", MO.W3, MO.B3), ("b3", MO.B3, MO.W4), ("W4", MO.W4, MO.B4), ("b4", MO.B4, MO.NPARAM)):
-        assert _rel_l2(g[lo:hi], g_ref[lo:hi]) < 5e-2, name
+        assert _rel_l2(g[lo:hi], g_ref[lo:hi]) < 2e-3, name  # measured at most 1.8e-4
+
+
+def test_inference_kernels_agree(api):
+    """The four-tile inference kernel (the default) and the two-warpgroup kernel at
+    one or two blocks per SM compute the same arithmetic: identical outputs, also
+    for a row count that leaves the last tile and slots partly empty."""
+    import torch
+
+    from xtsrcmaps_b200.surrogate import Surrogate
+
+    d = torch.device("cuda")
+    net = Surrogate(device=d, seed=3)
+    rng = np.random.default_rng(5)
+    X = torch.as_tensor(rng.normal(0.0, 1.5, (128 * 700 + 77, 5)).astype(np.float32), device=d)
+    before = api.get_tuning()
+    try:
+        ys = []
+        for mb in (0, 1, 2):
+            api.set_tuning(mlp_blocks_per_sm=mb)
+            ys.append(net.predict(X).cpu().numpy())
+    finally:
+        api.set_tuning(**before)
+    assert np.isfinite(ys[0]).all()
+    np.testing.assert_array_equal(ys[0], ys[1])
+    np.testing.assert_array_equal(ys[0], ys[2])
 
 
 def test_samples_match_oracle(api):

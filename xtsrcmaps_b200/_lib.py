@@ -106,7 +106,7 @@ class XtsMlp(C.Structure):
 
 class XtsTuning(C.Structure):
     _fields_ = [("window_blocks_per_sm", C.c_int), ("write_blocks_per_sm", C.c_int), ("queue_blocks_per_sm", C.c_int),
-                ("mlp_blocks_per_sm", C.c_int)]
+                ("mlp_blocks_per_sm", C.c_int), ("chunk_sources", C.c_int)]
 
 
 class XtsSurrogateStats(C.Structure):

@@ -673,7 +673,7 @@ def compute_srcmaps(wcs: Wcs, src_sph, exp: XtExp, psf: XtPsf, out_dtype: str = 
     return m
 
 
-TUNING_FIELDS = ("window_blocks_per_sm", "write_blocks_per_sm", "queue_blocks_per_sm", "mlp_blocks_per_sm")
+TUNING_FIELDS = ("window_blocks_per_sm", "write_blocks_per_sm", "queue_blocks_per_sm", "mlp_blocks_per_sm", "chunk_sources")
 
 
 def set_tuning(**fields) -> None:

@@ -114,7 +114,7 @@ def tune_adaptive(wcs, src_sph, exposure, uPsf, partial_integrals, target: float
 
 def tune_launch_shapes(wcs, src_sph, exposure, uPsf, partial_integrals, net=None,
                        window_blocks_per_sm: Sequence[int] = (1, 2, 3), write_blocks_per_sm: Sequence[int] = (1, 2),
-                       mlp_blocks_per_sm: Sequence[int] = (1, 2), reps: int = 3, apply: bool = True) -> dict:
+                       mlp_blocks_per_sm: Sequence[int] = (0, 1, 2), reps: int = 3, apply: bool = True) -> dict:
     """Time the plain model map for every (window-pass blocks per SM, write-pass blocks per SM)
     pair and, with ``net``, the network's forward pass on a million rows for each
     blocks-per-SM count; set the fastest (apply) and return

@@ -16,7 +16,7 @@ namespace xts {
 
 static thread_local char g_err[512] = "";
 static std::mutex g_mu;  // serialises calls that share the workspace
-xts_tuning g_tuning = {0, 0, 0, 0};
+xts_tuning g_tuning = {0, 0, 0, 0, 0};
 
 int set_error(int code, const char* fmt, ...) {
     va_list ap;
@@ -925,12 +925,12 @@ static bool wcs_ok(const xts_wcs* w);
 int xts_set_tuning(const xts_tuning* t) {
     std::lock_guard<std::mutex> lock(g_mu);
     if (!t) {
-        g_tuning = xts_tuning{0, 0, 0, 0};
+        g_tuning = xts_tuning{0, 0, 0, 0, 0};
         return XTS_OK;
     }
     if (t->window_blocks_per_sm < 0 || t->window_blocks_per_sm > 4 || t->write_blocks_per_sm < 0 || t->write_blocks_per_sm > 2 ||
         t->queue_blocks_per_sm < 0 || t->queue_blocks_per_sm > 4 || t->mlp_blocks_per_sm < 0 ||
-        t->mlp_blocks_per_sm > 2)
+        t->mlp_blocks_per_sm > 2 || t->chunk_sources < 0)
         return set_error(XTS_ERR_ARG, "set_tuning: a field is outside its range");
     g_tuning = *t;
     return XTS_OK;

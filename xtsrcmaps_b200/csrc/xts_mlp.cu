@@ -73,6 +73,13 @@ __device__ __forceinline__ float2 gelu2(float2 z) {
     const float2 hz = __fmul2_rn(make_float2(0.5f, 0.5f), z);
     return __ffma2_rn(hz, make_float2(tanh_fast(u.x), tanh_fast(u.y)), hz);
 }
+// 2 gelu(z) for two values: the same rounding as gelu2 scaled by 2 (exact), one
+// multiply fewer; the inference kernel halves the next layer's weights to match
+__device__ __forceinline__ float2 gelu2x(float2 z) {
+    const float2 t = __ffma2_rn(make_float2(GK1, GK1), __fmul2_rn(z, z), make_float2(1.f, 1.f));
+    const float2 u = __fmul2_rn(__fmul2_rn(make_float2(GK0, GK0), z), t);
+    return __ffma2_rn(z, make_float2(tanh_fast(u.x), tanh_fast(u.y)), z);
+}
 __device__ __forceinline__ float gelu_grad(float z) {
     const float z2 = z * z, th = tanh_fast(GK0 * fmaf(GK1 * z2, z, z));
     return 0.5f * (1.f + th) + 0.5f * z * (1.f - th * th) * GK0 * fmaf(3.f * GK1, z2, 1.f);
@@ -337,6 +344,194 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
     __syncthreads();
     tc_fence_after();
     if (warp == 0) tmem_free(tmem, 128);
+}
+
+// ====================================================================== inference
+// k_mlp_infer: the same forward arithmetic as k_mlp_forward<false>, with four tiles in
+// flight per SM.  One block per SM of four warpgroups; warpgroup g owns tile slot g
+// (its BF16 activation operand and accumulator columns [128 g, 128 g + 128) of tensor
+// memory) and runs its own tiles, thread = row, all 128 columns per thread; the two
+// weight operands are shared.  A warpgroup synchronises only with itself (named
+// barrier 1 + g, its own mbarrier), so while one waits for its MMAs the other three
+// run their GELUs: the tensor pipe, the FMA pipe and the tanh unit overlap across
+// the four tiles.  The hidden activations are kept as 2 gelu(z) (gelu2x, one multiply
+// fewer per value) and the weights that read them (W2, W3, w4) are halved on loading;
+// both scalings are exact, so the outputs are those of k_mlp_forward bit for bit.
+constexpr int IG = 4;                    // warpgroups (tile slots) per block
+constexpr int IT = IG * MT;              // threads per block
+struct InfLayout {
+    static constexpr size_t w2 = 0, w3 = 2 * ATOM, act = 4 * ATOM;  // act: IG slots of 2 atoms
+    static constexpr size_t f32 = act + (size_t)IG * 2 * ATOM;      // W1^T [5][128], b1, pad, b2, b3, w4, b4
+    static constexpr size_t bars = f32 + 4 * (MH * 8 + 3 * MH + 4);
+    static constexpr size_t total = bars + 64;
+};
+constexpr size_t INF_SMEM = InfLayout::total + 1024;
+
+__device__ __forceinline__ void group_sync(int g) {
+    asm volatile("bar.sync %0, %1;" :: "r"(1 + g), "r"(MT) : "memory");
+}
+__device__ __forceinline__ bool group_and(int g, bool v) {
+    int r;
+    asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.s32 p, %1, 0;\n\tbar.red.and.pred q, %2, %3, p;\n\t"
+                 "selp.s32 %0, 1, 0, q;\n\t}\n" : "=r"(r) : "r"((int)v), "r"(1 + g), "r"(MT) : "memory");
+    return r != 0;
+}
+
+__global__ void __launch_bounds__(IT, 1)
+k_mlp_infer(const float* __restrict__ params, const __nv_bfloat16* __restrict__ wbf, MlpNorm nm,
+            const float* __restrict__ X, long long n, const unsigned long long* __restrict__ n_dev,
+            float* __restrict__ y, int* __restrict__ status) {
+    if (n_dev) n = min(n, (long long)*n_dev);  // rows counted on the device (at most n)
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
+    const int t = threadIdx.x, warp = t >> 5, g = t >> 7, r = t & (MT - 1);
+    float* w1 = (float*)(smem + InfLayout::f32);  // [6][128]: W1^T rows, then b1
+    float* b2 = w1 + MH * 8;
+    float* b3 = b2 + MH;
+    float* w4 = b3 + MH;
+    float* b4 = w4 + MH;
+    unsigned long long* bars = (unsigned long long*)(smem + InfLayout::bars);
+    unsigned* tmem_slot = (unsigned*)(smem + InfLayout::bars + 8 * IG);
+    const unsigned bar = smem_u32(&bars[g]);
+    const unsigned s_w2 = smem_u32(smem + InfLayout::w2), s_w3 = smem_u32(smem + InfLayout::w3);
+    unsigned char* act = smem + InfLayout::act + (size_t)g * 2 * ATOM;
+    const unsigned s_act = smem_u32(act);
+
+    for (int idx = t; idx < 2 * MH * (MH / 8); idx += IT) {
+        const int l = idx / (MH * (MH / 8)), rem = idx - l * (MH * (MH / 8));
+        const int row = rem >> 4, ch = rem & 15;
+        uint4 v = *reinterpret_cast<const uint4*>(wbf + (size_t)l * MH * MH + row * MH + ch * 8);
+        __nv_bfloat162* h2 = reinterpret_cast<__nv_bfloat162*>(&v);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) h2[q] = __hmul2(h2[q], __float2bfloat162_rn(0.5f));  // exact: a power of 2
+        *reinterpret_cast<uint4*>(smem + (l ? InfLayout::w3 : InfLayout::w2) + sw_off(row, ch * 8)) = v;
+    }
+    for (int k = t; k < MH * 8; k += IT) {
+        const int q = k >> 7, j = k & (MH - 1);
+        w1[k] = q < MI ? __bfloat162float(__float2bfloat16_rn(params[XTS_MLP_W1 + j * MI + q]))
+                       : (q == MI ? params[XTS_MLP_B1 + j] : 0.f);
+    }
+    for (int k = t; k < MH; k += IT) {
+        b2[k] = params[XTS_MLP_B2 + k];
+        b3[k] = params[XTS_MLP_B3 + k];
+        w4[k] = 0.5f * __bfloat162float(__float2bfloat16_rn(params[XTS_MLP_W4 + k]));
+    }
+    if (t < IG) mbar_init(smem_u32(&bars[t]), 1);
+    if (t == 0) b4[0] = params[XTS_MLP_B4];
+    if (warp == 0) tmem_alloc(smem_u32(tmem_slot), 128 * IG);
+    fence_async_shared();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tmem = *tmem_slot + (unsigned)(MH * g);  // this slot's accumulator columns
+    const unsigned trow = tmem + ((unsigned)((warp & 3) * 32) << 16);
+    unsigned ph = 0;
+    bool ok = true;
+    const long long ntiles = (n + MT - 1) / MT;
+    const long long stride = (long long)gridDim.x * IG;
+    // the features of this slot's next row, loaded one tile ahead
+    float xn[MI];
+    auto load_x = [&](long long tl) {
+        const long long rw = tl * MT + r;
+#pragma unroll
+        for (int k = 0; k < MI; ++k) xn[k] = tl < ntiles && rw < n ? X[rw * MI + k] : 0.f;
+    };
+    load_x((long long)blockIdx.x * IG + g);
+    for (long long tile = (long long)blockIdx.x * IG + g; tile < ntiles && ok; tile += stride) {
+        const long long row = tile * MT + r;
+        const bool live = row < n;
+        // layer 1 on CUDA cores, the row's 128 BF16 activations into the A operand
+        {
+            float x[MI];
+#pragma unroll
+            for (int k = 0; k < MI; ++k) x[k] = live ? (xn[k] - nm.mu[k]) / nm.sd[k] : 0.f;
+            load_x(tile + stride);
+#pragma unroll 2
+            for (int g8 = 0; g8 < MH / 8; ++g8) {
+                const int j0 = 8 * g8;
+                float h[8];
+#pragma unroll
+                for (int j = 0; j < 8; j += 4) {
+                    const float4* wp = reinterpret_cast<const float4*>(w1 + j0 + j);
+                    const float4 bq = wp[MI * MH / 4];  // b1
+                    float2 za = make_float2(bq.x, bq.y), zb = make_float2(bq.z, bq.w);
+#pragma unroll
+                    for (int k = 0; k < MI; ++k) {
+                        const float4 wq = wp[k * MH / 4];
+                        za = __ffma2_rn(make_float2(wq.x, wq.y), make_float2(x[k], x[k]), za);
+                        zb = __ffma2_rn(make_float2(wq.z, wq.w), make_float2(x[k], x[k]), zb);
+                    }
+                    const float2 ga = gelu2x(za), gb = gelu2x(zb);
+                    h[j] = ga.x; h[j + 1] = ga.y; h[j + 2] = gb.x; h[j + 3] = gb.y;
+                }
+                *reinterpret_cast<uint4*>(act + sw_off(r, j0)) =
+                    make_uint4(pack_bf16(h[0], h[1]), pack_bf16(h[2], h[3]), pack_bf16(h[4], h[5]),
+                               pack_bf16(h[6], h[7]));
+            }
+        }
+        float ylo = 0.f, yhi = 0.f;  // the output layer over columns 0..63 and 64..127
+        for (int layer = 2; layer <= 3 && ok; ++layer) {
+            fence_async_shared();
+            tc_fence_before();
+            group_sync(g);
+            if (r == 0) {
+                tc_fence_after();
+                mma_chain(tmem, s_act, layer == 2 ? s_w2 : s_w3, MH / 16, false);
+                mma_commit(bar);
+            }
+            const bool got = mbar_wait(bar, ph);
+            if (!group_and(g, got)) { ok = false; break; }  // ph stays: the exit path waits on it
+            ph ^= 1;
+            tc_fence_after();
+            const float* bias = layer == 2 ? b2 : b3;
+#pragma unroll 1
+            for (int c0 = 0; c0 < MH; c0 += 16) {
+                float v[16], bv[16];
+                tmem_ld16(trow + (unsigned)c0, v);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float4 b = reinterpret_cast<const float4*>(bias + c0)[q];
+                    bv[4 * q] = b.x; bv[4 * q + 1] = b.y; bv[4 * q + 2] = b.z; bv[4 * q + 3] = b.w;
+                }
+#pragma unroll
+                for (int j = 0; j < 16; j += 2) {
+                    const float2 z = __fadd2_rn(make_float2(v[j], v[j + 1]), make_float2(bv[j], bv[j + 1]));
+                    const float2 g2 = gelu2x(z);
+                    v[j] = g2.x;
+                    v[j + 1] = g2.y;
+                }
+                if (layer == 2) {
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {
+                        const float* u = v + 8 * q;
+                        *reinterpret_cast<uint4*>(act + sw_off(r, c0 + 8 * q)) =
+                            make_uint4(pack_bf16(u[0], u[1]), pack_bf16(u[2], u[3]), pack_bf16(u[4], u[5]),
+                                       pack_bf16(u[6], u[7]));
+                    }
+                } else {
+                    float ya = c0 < 64 ? ylo : yhi;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const float4 wv = reinterpret_cast<const float4*>(w4 + c0)[q];
+                        ya = fmaf(v[4 * q], wv.x, fmaf(v[4 * q + 1], wv.y, fmaf(v[4 * q + 2], wv.z,
+                                                                                fmaf(v[4 * q + 3], wv.w, ya))));
+                    }
+                    if (c0 < 64) ylo = ya; else yhi = ya;
+                }
+            }
+            tc_fence_before();  // the next MMA overwrites the accumulator read above
+        }
+        if (!ok) break;
+        if (live) y[row] = fmaf((ylo + yhi) + b4[0], nm.out_sd, nm.out_mu);
+    }
+    if (!ok && r == 0) {
+        atomicExch(status, 1);
+        mbar_wait(bar, ph);  // bounded: let this slot's issued MMA land
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) tmem_free(*tmem_slot, 128 * IG);
 }
 
 // ====================================================================== GEMM
@@ -609,14 +804,22 @@ static int forward(const xts_mlp* net, const float* X, long long n, const unsign
     const long long ntiles = (n + MT - 1) / MT;
     const int bps = g_tuning.mlp_blocks_per_sm > 0 ? g_tuning.mlp_blocks_per_sm : 2;  // blocks per SM (two fit)
     const long long g = ntiles < bps * sm_count() ? ntiles : bps * sm_count();
-    if (save)
+    if (save) {
         XTS_LAUNCH("k_mlp_forward", st, k_mlp_forward<true><<<(unsigned)g, FT, FWD_SMEM, st>>>(
                                             net->params, (const __nv_bfloat16*)net->wbf16, mlp_norm(net), X, n, n_dev,
                                             y, sv, status));
-    else
+    } else if (g_tuning.mlp_blocks_per_sm == 0) {
+        // inference: four tiles in flight per SM, one block per SM
+        XTS_CUDA(cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INF_SMEM));
+        const long long gi = (ntiles + IG - 1) / IG < sm_count() ? (ntiles + IG - 1) / IG : sm_count();
+        XTS_LAUNCH("k_mlp_forward", st, k_mlp_infer<<<(unsigned)gi, IT, INF_SMEM, st>>>(
+                                            net->params, (const __nv_bfloat16*)net->wbf16, mlp_norm(net), X, n, n_dev,
+                                            y, status));
+    } else {
         XTS_LAUNCH("k_mlp_forward", st, k_mlp_forward<false><<<(unsigned)g, FT, FWD_SMEM, st>>>(
                                             net->params, (const __nv_bfloat16*)net->wbf16, mlp_norm(net), X, n, n_dev,
                                             y, sv, status));
+    }
     return XTS_OK;
 }
 

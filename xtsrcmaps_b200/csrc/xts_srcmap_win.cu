@@ -790,6 +790,7 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
     const size_t budget = (size_t)4 << 30;
     int Sc = (int)(budget / win_bytes_per_source(npix));
     if (chunk_sources > 0 && chunk_sources < Sc) Sc = chunk_sources;
+    if (g_tuning.chunk_sources > 0 && g_tuning.chunk_sources < Sc) Sc = g_tuning.chunk_sources;
     Sc = Sc < 1 ? 1 : (Sc > S ? S : Sc);
     const size_t rec_n = (size_t)Sc * npix + 4, ext_n = (size_t)Sc * npix * 2 + 4;
     const size_t lut_n = (size_t)Sc * ND * EQ * 4 + 4;
