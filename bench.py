@@ -483,14 +483,13 @@ def run_ours(args, rank, world, local_rank):
     try:
         tr = json.load(open(os.path.join(ROOT, "profiles", "k_srcmap_traffic.json")))
         if args.kernel == "windows" and tr.get("dram_bytes_per_launch"):
-            # captured on a small case (c1: 74 M values per launch); the write pass's DRAM
-            # traffic grows with the values it writes, so it is scaled to this launch's values
-            from xtsrcmaps_b200.synth import make_job as _mk
-
-            ref_values = _mk(tr["workload"], seed=1).n_values
+            # captured on a smaller case (c2's map with 50 sources: 296 M values per
+            # launch); the write pass's DRAM traffic grows with the values it writes, so it
+            # is scaled to this launch's values
+            ref_values = tr["values"]
             traffic = tr["dram_bytes_per_launch"] * (n_values / per_step) / ref_values
-            traffic_note = (f"ncu DRAM bytes of one {tr['workload']} launch ({tr['dram_bytes_per_launch']} B), "
-                            f"scaled by values written" if tr["workload"] != args.config else "ncu, this workload")
+            traffic_note = (f"ncu DRAM bytes of one launch on {tr['workload']} ({tr['dram_bytes_per_launch']} B "
+                            f"for {ref_values} values), scaled by values written")
     except (OSError, ValueError, KeyError):
         pass
     roof_write = {"bound": "hbm", "kernel": "k_srcmap", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
@@ -507,13 +506,28 @@ def run_ours(args, rank, world, local_rank):
     if net is not None:
         # the surrogate step's dominant kernel: the network's forward pass on tcgen05
         p_s, msp_s = prof["surrogate"]
-        fn_, fms = p_s.get("k_mlp_forward", (0, 0.0))
+        # the network's inference launches: the four-tile kernel (default) or the
+        # two-warpgroup kernel (mlp_blocks_per_sm 1 or 2)
+        kname = "k_mlp_infer" if "k_mlp_infer" in p_s else "k_mlp_forward"
+        fn_, fms = p_s.get(kname, (0, 0.0))
         rows = (sur_stats or {}).get("evaluated", 0)
         flop = 2 * (5 * 128 + 2 * 128 * 128 + 128) * rows
         tflops = flop / (fms / args.steps * 1e-3) / 1e12 if fms else None
-        roofline = {"bound": "tensor", "kernel": "k_mlp_forward", "achieved": tflops, "peak": tensor_peak,
+        # DRAM traffic per launch from the committed ncu capture of the kernel, scaled by
+        # the rows of an average launch here (the traffic is the rows' features and outputs)
+        m_traffic, m_note = None, None
+        try:
+            tm = json.load(open(os.path.join(ROOT, "profiles", "k_mlp_infer_traffic.json")))
+            if kname == tm["kernel"] and fn_:
+                m_traffic = tm["dram_bytes_per_launch"] * (rows / (fn_ / args.steps)) / tm["rows"]
+                m_note = (f"ncu DRAM bytes of one launch over {tm['rows']} rows ({tm['dram_bytes_per_launch']} B), "
+                          "scaled by this step's rows per launch")
+        except (OSError, KeyError, ValueError):
+            pass
+        roofline = {"bound": "tensor", "kernel": kname, "achieved": tflops, "peak": tensor_peak,
                     "unit": "TFLOP/s", "frac": tflops / tensor_peak if tflops else None, "peak_source": peak_src,
-                    "traffic": None, "alg_flops_per_step": flop, "launches_per_step": fn_ / args.steps,
+                    "traffic": m_traffic, "traffic_source": m_note,
+                    "alg_flops_per_step": flop, "launches_per_step": fn_ / args.steps,
                     "avg_launch_ms": fms / fn_ if fn_ else None,
                     "note": "67,072 FLOP per network row (5-128-128-128-1, hidden layers on tcgen05 BF16 with "
                             "FP32 accumulation); rows = values the network evaluated per step"}

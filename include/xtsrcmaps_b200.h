@@ -446,7 +446,7 @@ int xts_surrogate_samples(const double* upsf, const double* logEs, int S, int E,
 typedef struct xts_surrogate_stats {
     long long values;        /* S * H * W * E */
     long long accepted;      /* values served by the network (maps that passed the check, checked pixels excluded) */
-    long long checked;       /* values the network took in the checked pixels, replaced there by the 12-point rule */
+    long long checked;       /* values the network took in the checked pixels, where the 12-point rule's stay */
     int maps_fallback;       /* sources whose check failed: all their values by the rule */
     float max_check_err;     /* largest relative difference seen by the check */
     long long evaluated;     /* rows the network evaluated (before the check) */
@@ -455,10 +455,11 @@ typedef struct xts_surrogate_stats {
 /* The model map of xts_point_src_model_map_wcs with the pixel means taken from
  * the network wherever the centre lies at least rho_min pixel sizes from the
  * source, every feature is inside [lo, hi] and the value's error cell is marked
- * cell_ok; the other values take the FP64 12-point rule.  Every 16th pixel is
- * also evaluated by the rule, which replaces the network's values there; a
- * source whose largest relative difference on those pixels exceeds check_tol is
- * redone entirely by the rule.  Map integral, correction and scalings as
+ * cell_ok; the other values take the 12-point rule (the plain map's FP32 window
+ * and write passes over the unscaled mean PSF for E <= 52, the FP64 rule per value
+ * above).  At every 16th pixel the rule's values stay and the network's are
+ * compared with them; a source whose largest relative difference there exceeds
+ * check_tol is redone entirely by the FP64 rule.  Map integral, correction and scalings as
  * xts_point_src_model_map_wcs.  Device pointers; model_map float [S, H, W, E].
  * With stats NULL the call neither synchronises nor allocates once its buffers
  * have grown (it can be captured into a CUDA graph); xts_surrogate_last_stats

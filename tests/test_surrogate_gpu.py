@@ -7,12 +7,12 @@ value alone.
 
 Tolerances:
   * GEMM: relative 1e-5 of the output scale (FP32 accumulation of BF16 products);
-  * forward output: relative L2 2e-2; gradient blocks: relative L2 5e-2 -- the
-    kernels use tanh.approx (relative error ~5e-4) where the oracle uses tanh,
-    which flips some BF16 roundings of activations;
+  * forward output: relative L2 5e-4; gradient blocks: relative L2 2e-3 -- the
+    kernels use tanh.approx where the oracle uses tanh, which flips some BF16
+    roundings of activations (measured 7e-5 and at most 1.8e-4);
   * samples: features 1e-5, targets 1e-4 relative (FP64 math, FP32 storage);
   * the model map with every map redone by the rule: 1e-5 relative against the
-    plain FP32 map (both the FP64 12-point rule, stored in FP32).
+    plain FP32 map (the FP64 12-point rule against the FP32 window path).
 """
 import numpy as np
 import pytest
@@ -171,6 +171,29 @@ def test_map_fallback_equals_rule(api):
     plain, pinfo = api.point_src_model_map_wcs(job.wcs, src, expo, upsf, partial)
     assert st["values"] == m.numel() and st["maps_fallback"] >= 1 and st["accepted"] == 0
     assert st["checked"] > 0
+    assert max_rel(m.cpu().numpy(), plain.cpu().numpy()) < 1e-5
+    assert max_rel(info.inv_map_integral.cpu().numpy(), pinfo.inv_map_integral.cpu().numpy()) < 1e-7
+
+
+def test_surrogate_map_many_energies(api):
+    """More energies than the window path's write pass holds (60 > 52): the rule's
+    means come from the FP64 rule per value instead; with a check no network meets,
+    the map is the plain map's."""
+    import torch
+
+    from xtsrcmaps_b200.surrogate import Surrogate, model_map, samples
+
+    job, upsf, partial, expo = _psf_tables(api, "c1", seed=8, n=3)
+    sel = torch.arange(60, device=upsf.device) % upsf.shape[-1]
+    u60, p60, e60 = (upsf[..., sel].contiguous(), partial[..., sel].contiguous(), expo[..., sel].contiguous())
+    logEs = np.asarray(job.logEs)[sel.cpu().numpy()]
+    net = Surrogate(device=upsf.device, seed=0)
+    X, Y = samples(upsf, job.logEs, 128 * 64, seed=3)
+    net.fit_standardisation(X, Y)
+    src = torch.as_tensor(job.src_sph, device=upsf.device)
+    m, info, st = model_map(job.wcs, src, e60, u60, p60, logEs, net, check_tol=1e-12)
+    plain, pinfo = api.point_src_model_map_wcs(job.wcs, src, e60, u60, p60)
+    assert st["values"] == m.numel() and st["accepted"] == 0
     assert max_rel(m.cpu().numpy(), plain.cpu().numpy()) < 1e-5
     assert max_rel(info.inv_map_integral.cpu().numpy(), pinfo.inv_map_integral.cpu().numpy()) < 1e-7
 

@@ -239,7 +239,9 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
                       int* in_fov, int* status, float* out, int chunk_sources,
                       int (*on_chunk)(void*, int, int, cudaStream_t), void* on_chunk_ctx,
                       StreamJoin& geo,  // the first chunk's window pass runs on geo.from
-                      cudaStream_t st);  // 0, or XTS_ERR_TIMEOUT if a bounded device wait gave up
+                      cudaStream_t st,  // 0, or XTS_ERR_TIMEOUT if a bounded device wait gave up
+                      bool means_only = false);  // the rule's pixel means (the table uPsf unscaled): no
+                                                 // map integral, correction or scale outputs
 int launch_srcmap_win_cut(const double* corners, const double* centers, const double* omega, const SrcInfo* info,
                           const xts_cutout* cut, int S, int H, int W, int E, const double* upsf,
                           const double* partial, const double* exposure, double* scale, double* inv_integ,

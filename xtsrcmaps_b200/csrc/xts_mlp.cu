@@ -812,7 +812,7 @@ static int forward(const xts_mlp* net, const float* X, long long n, const unsign
         // inference: four tiles in flight per SM, one block per SM
         XTS_CUDA(cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INF_SMEM));
         const long long gi = (ntiles + IG - 1) / IG < sm_count() ? (ntiles + IG - 1) / IG : sm_count();
-        XTS_LAUNCH("k_mlp_forward", st, k_mlp_infer<<<(unsigned)gi, IT, INF_SMEM, st>>>(
+        XTS_LAUNCH("k_mlp_infer", st, k_mlp_infer<<<(unsigned)gi, IT, INF_SMEM, st>>>(
                                             net->params, (const __nv_bfloat16*)net->wbf16, mlp_norm(net), X, n, n_dev,
                                             y, status));
     } else {

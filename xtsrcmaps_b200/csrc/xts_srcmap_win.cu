@@ -127,7 +127,7 @@ __device__ __forceinline__ PixBase pixel_base(const double* __restrict__ corners
         P.eb[k] = fmaf(q8, c_pair[k][7], fmaf(q5, c_pair[k][4], q4 * c_pair[k][3]));
         P.ob[k] = fmaf(q7, c_pair[k][6], q6 * c_pair[k][5]);
     }
-    P.om = (float)omega[om_idx];
+    P.om = omega ? (float)omega[om_idx] : 1.f;  // omega NULL: the pixel means (unit solid angle)
     return P;
 }
 
@@ -333,7 +333,7 @@ __device__ __forceinline__ double boundary_chord2(const SrcInfo& si) {
 // A block takes the next item (one atomic), forms each pixel's source-independent
 // geometry once and the windows of the group's sources from it, and adds the item's
 // non-zero rows to hist_out[s] (cleared before the launch) with FP64 atomics.
-__global__ void __launch_bounds__(WT, 2) k_pixel_windows(const double* __restrict__ corners, const double* __restrict__ centers,
+__global__ void __launch_bounds__(WT, 3) k_pixel_windows(const double* __restrict__ corners, const double* __restrict__ centers,
                                                       const double* __restrict__ omega, const SrcInfo* __restrict__ info,
                                                       const SepTab* __restrict__ septab, int S, int H, int W,
                                                       int P, unsigned* __restrict__ queue,
@@ -662,7 +662,7 @@ k_srcmap_win(const float4* __restrict__ win, const float4* __restrict__ ext, con
                 wc = pix - h * W;
             }
             const PixGeom g = pixel_geom(corners, W1, h, wc, si);
-            const float om = (float)omega[(size_t)h * W + wc];
+            const float om = omega ? (float)omega[(size_t)h * W + wc] : 1.f;
             const float* Y = (const float*)tab;
             const int ES = 4 * EQ;
             for (int e = 0; e < E; ++e) {
@@ -775,7 +775,7 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
                       double* scale, double* inv_integ, double* correction, double* radius,
                       int* in_fov, int* status, float* out, int chunk_sources,
                       int (*on_chunk)(void*, int, int, cudaStream_t), void* on_chunk_ctx,
-                      StreamJoin& geo, cudaStream_t st) {
+                      StreamJoin& geo, cudaStream_t st, bool means_only) {
     int rc = upload_rule_uv(st);
     if (rc) return rc;
     const SepTab* tab = nullptr;
@@ -845,24 +845,30 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
         XTS_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned), gs));
         XTS_CUDA(cudaMemsetAsync(hist, 0, sizeof(double) * (size_t)n * ND, gs));
         XTS_LAUNCH("k_pixel_windows", gs, k_pixel_windows<<<Gw, WT, WA_SMEM, gs>>>(
-                                              corners, centers, omega, info + s0, tab, n, H, W, nparts, queue,
+                                              corners, centers, means_only ? nullptr : omega, info + s0, tab, n, H, W,
+                                              nparts, queue,
                                               hist, rec, ext, sparse, (int)cap,
                                               sparse_count));
         if (pipe) {
             XTS_CUDA(cudaEventRecord(evA[b], gs));
             XTS_CUDA(cudaStreamWaitEvent(st, evA[b], 0));
         }
-        rc = launch_correction(hist, 1, info + s0, n, upsf + oE * ND, partial + oE * ND,
-                               exposure + oE, E, scale + oE, inv_integ ? inv_integ + oE : nullptr,
-                               correction ? correction + oE : nullptr, radius ? radius + s0 : nullptr,
-                               in_fov ? in_fov + s0 : nullptr, st, lut, EQ * 4);
-        if (rc) return rc;
+        if (means_only) {
+            XTS_LAUNCH("k_lut_scaled", st, k_lut_scaled<<<lut_scaled_grid(n), 256, 0, st>>>(
+                                               upsf + oE * ND, nullptr, n, E, EQ * 4, lut, nullptr, nullptr));
+        } else {
+            rc = launch_correction(hist, 1, info + s0, n, upsf + oE * ND, partial + oE * ND,
+                                   exposure + oE, E, scale + oE, inv_integ ? inv_integ + oE : nullptr,
+                                   correction ? correction + oE : nullptr, radius ? radius + s0 : nullptr,
+                                   in_fov ? in_fov + s0 : nullptr, st, lut, EQ * 4);
+            if (rc) return rc;
+        }
         const long long T = (long long)n * ((npix + BT - 1) / BT);
         long long G = (long long)nsm * (g_tuning.write_blocks_per_sm > 0 && g_tuning.write_blocks_per_sm < per_sm
                                             ? g_tuning.write_blocks_per_sm : per_sm);
         if (G > T) G = T;
-        WriteArgs wa{rec, ext, sparse, lut, corners, omega, info + s0, tab, nullptr, nullptr, n, s0, H, W, E, EQ,
-                     status, out};
+        WriteArgs wa{rec, ext, sparse, lut, corners, means_only ? nullptr : omega, info + s0, tab, nullptr, nullptr,
+                     n, s0, H, W, E, EQ, status, out};
         rc = wp((unsigned)G, L.total, st, wa, nullptr, false);
         if (rc) return rc;
         if (on_chunk && (rc = on_chunk(on_chunk_ctx, s0, n, st))) return rc;

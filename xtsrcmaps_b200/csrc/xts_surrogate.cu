@@ -18,13 +18,15 @@
 // The network's target is y = ln(m / u_c) rho^2; a value is m = u_c exp(y / rho^2).
 // All of this is FP64 up to the network's FP32 input.
 //
-// The map, per chunk of sources: k_sur_features writes the rule's mean for every
-// value the network may not take (rho < rho_min or a feature outside the training
-// range) and the features of the others, compacted; the network runs on the
-// compacted rows only; k_sur_assemble scatters its values into the map; k_sur_check
-// re-evaluates every 61st pixel by the rule.  Sources whose check fails are redone
-// by k_sur_fallback, and the map integral, correction and scalings follow as for
-// the adaptive map.
+// The map: first the rule's pixel means for every value, by the plain path's
+// window and write passes over the unscaled FP32 table (xts_srcmap_win.cu).  Then,
+// per chunk of sources, k_sur_features writes the features of the values the
+// network may take (inside the training range and a served error cell), compacted;
+// the network runs on the compacted rows only; k_sur_assemble puts its values into
+// the map, except at every SUR_CHECK_EVERY-th pixel, where the rule's value stays and
+// the relative difference to the network's is recorded per source.  Sources whose
+// check fails are redone by the FP64 rule (k_sur_fallback), and the map integral,
+// correction and scalings follow as for the adaptive map.
 #include <vector>
 
 #include "xts_point.cuh"
@@ -204,13 +206,6 @@ __device__ __forceinline__ const unsigned char* sur_cells_to_shared(const SurRan
     return sh;
 }
 
-// Per block: SF_PIX pixels of one source of a chunk.  Phase 1, one thread per
-// pixel: the centre, the features that do not depend on energy and the 12 rule
-// points, into shared memory.  Phase 2, one thread per (pixel, energy) value in the
-// maps' order, so that the feature rows [v][5], aux [v] and fallback values are
-// written coalesced: the centre value and segment slope, the five features, and
-// either aux = (u_c, 1 / rho^2) or, for a value the network does not take,
-// aux = (0, -1) and the rule's mean.
 constexpr int SF_PIX = 128;
 constexpr int SF_THREADS = 256;
 
@@ -218,8 +213,6 @@ struct SurPixS {
     float f0, f1, f2, eps;
     double tc;
     int ic, geo_ok;
-    short idx[12];
-    double tt[12];
 };
 
 __device__ __forceinline__ bool sur_geo_ok(const SurPix& q, const SurRange& rg) {
@@ -242,13 +235,12 @@ __device__ __forceinline__ bool sur_value(const double* U, int E, int e, int ic,
 __device__ __forceinline__ bool sur_checked(int pix) { return pix % SUR_CHECK_EVERY == 0; }
 
 // Per block: SF_PIX pixels of one source of a chunk.  Phase 1, one thread per
-// pixel: the centre, the features that do not depend on energy and the 12 rule
-// points, into shared memory.  Pass 1, one thread per (pixel, energy) value in
-// the maps' order: whether the network takes the value (a bit in shared memory),
-// and for a value it does not, the rule's mean written to the map.  The block then
-// reserves room for its accepted values in the compacted network input with one
-// atomic, and pass 2 writes each accepted value's five features, aux = (u_c,
-// 1 / rho^2) and its chunk-relative value index there.
+// pixel: the centre and the features that do not depend on energy, into shared
+// memory.  Pass 1, one thread per (pixel, energy) value in the maps' order: whether
+// the network takes the value (a bit in shared memory).  The block then reserves
+// room for its accepted values in the compacted network input with one atomic, and
+// pass 2 writes each accepted value's five features, aux = (u_c, 1 / rho^2) and its
+// chunk-relative value index there.
 __global__ void __launch_bounds__(SF_THREADS) k_sur_features(const double* __restrict__ corners,
                                                              const SrcInfo* __restrict__ info,
                                                              const double* __restrict__ upsf,
@@ -256,7 +248,6 @@ __global__ void __launch_bounds__(SF_THREADS) k_sur_features(const double* __res
                                                              int E, SurRange rg, float* __restrict__ X,
                                                              float2* __restrict__ aux, unsigned* __restrict__ vidx,
                                                              unsigned long long* __restrict__ n_acc,
-                                                             float* __restrict__ mean,
                                                              unsigned long long* __restrict__ accepted) {
     __shared__ SurPixS sp[SF_PIX];
     __shared__ unsigned okbits[SF_PIX * 256 / 32];  // one bit per (pixel, energy) value, E <= 256
@@ -268,39 +259,34 @@ __global__ void __launch_bounds__(SF_THREADS) k_sur_features(const double* __res
     const int np = min(SF_PIX, npix - p0);
     const int nv = np * E;
     const unsigned char* cells = sur_cells_to_shared(rg, cells_s);
-    for (int k = t; k < (nv + 31) / 32; k += SF_THREADS) okbits[k] = 0u;
     if (t < np) {
         const int pix = p0 + t, h = pix / W, w = pix - h * W;
         SurPix q;
-        sur_pixel(pixel_geom(corners, W + 1, h, w, info[s]), q);
+        sur_centre_geom(pixel_geom(corners, W + 1, h, w, info[s]), q);
         SurPixS& o = sp[t];
         o.f0 = q.f0; o.f1 = q.f1; o.f2 = q.f2;
         o.eps = (float)(1.0 / (q.rho * q.rho));
         o.tc = q.tc;
         o.ic = q.ic;
         o.geo_ok = sur_geo_ok(q, rg);
-#pragma unroll
-        for (int p = 0; p < 12; ++p) { o.idx[p] = (short)q.idx[p]; o.tt[p] = q.tt[p]; }
     }
     __syncthreads();
     const double* U = upsf + (size_t)s * ND * E;
     const size_t vb = ((size_t)blockIdx.y * npix + p0) * E;  // first value of the block (chunk-relative)
-    const size_t mb = ((size_t)s * npix + p0) * E;           // the same value in the map
     unsigned cnt = 0;
-    for (int k = t; k < nv; k += SF_THREADS) {
-        const int lp = k / E, e = k - lp * E;
-        const SurPixS& o = sp[lp];
-        double uc;
-        float sl;
-        if (sur_value(U, E, e, o.ic, o.tc, o.geo_ok, o.f0, (float)logEs[e], rg, cells, &uc, &sl)) {
-            atomicOr(&okbits[k >> 5], 1u << (k & 31));
-            ++cnt;
-        } else {
-            double m = 0.;
-#pragma unroll
-            for (int p = 0; p < 12; ++p) m += c_rule_uv[p][3] * sur_lerp(U, E, e, o.idx[p], o.tt[p]);
-            mean[mb + k] = (float)m;
+    for (int k0 = t - lane; k0 < nv; k0 += SF_THREADS) {  // a warp takes 32 consecutive values
+        const int k = k0 + lane;
+        bool ok = false;
+        if (k < nv) {
+            const int lp = k / E, e = k - lp * E;
+            const SurPixS& o = sp[lp];
+            double uc;
+            float sl;
+            ok = sur_value(U, E, e, o.ic, o.tc, o.geo_ok, o.f0, (float)logEs[e], rg, cells, &uc, &sl);
         }
+        const unsigned bits = __ballot_sync(0xffffffffu, ok);
+        if (lane == 0) okbits[k0 >> 5] = bits;
+        cnt += ok;
     }
     // exclusive scan of the per-thread counts; one reservation per block
     unsigned inc = cnt;
@@ -337,60 +323,58 @@ __global__ void __launch_bounds__(SF_THREADS) k_sur_features(const double* __res
     }
 }
 
-// The network's values into the map: row i of the compacted input is value vidx[i];
-// n_acc rows (counted on the device), at most n_max.
+// The network's values into the map: row i of the compacted input is chunk value
+// vidx[i]; n_acc rows (counted on the device), at most n_max.  At every
+// SUR_CHECK_EVERY-th pixel the map keeps the rule's value and the relative
+// difference of the network's is recorded: the largest per source in err and the
+// count in chk (s0: the chunk's first source; per_src = H W E values per source).
 __global__ void k_sur_assemble(const float2* __restrict__ aux, const unsigned* __restrict__ vidx,
                                const float* __restrict__ y, const unsigned long long* __restrict__ n_acc,
-                               long long n_max, float* __restrict__ mean) {
+                               long long n_max, int s0, long long per_src, int E, float* __restrict__ mean,
+                               float* __restrict__ err, unsigned long long* __restrict__ chk) {
     const long long n = min(n_max, (long long)*n_acc);
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const float2 a = aux[i];
-        mean[vidx[i]] = a.x * expf(y[i] * a.y);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const unsigned ps = (unsigned)per_src;
+    for (long long i0 = (long long)blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
+        const long long i = i0 + threadIdx.x;
+        const bool live = i < n;
+        int sl = -1;  // the chunk-relative source of a checked value
+        float r = 0.f;
+        if (live) {
+            const unsigned v = vidx[i];
+            const float2 a = aux[i];
+            const float m = a.x * expf(y[i] * a.y);
+            const unsigned j = v / ps;  // chunk values fit 32 bits
+            const unsigned pix = (v - j * ps) / (unsigned)E;
+            if (pix % SUR_CHECK_EVERY == 0) {
+                const float rule = mean[v];
+                const float d = rule != 0.f ? fabsf(m - rule) / fabsf(rule) : fabsf(m);
+                r = d != d ? 3.4e38f : d;
+                sl = (int)j;
+            } else {
+                mean[v] = m;
+            }
+        }
+        // per warp: lanes of the same source merged before one atomic each
+        if (!__any_sync(0xffffffffu, sl >= 0)) continue;
+        const unsigned grp = __match_any_sync(0xffffffffu, sl);
+        float worst = r;
+        for (int o = 0; o < 32; ++o) {
+            const float ro = __shfl_sync(0xffffffffu, r, o);
+            if ((grp >> o) & 1u) worst = fmaxf(worst, ro);
+        }
+        if (sl >= 0 && (threadIdx.x & 31) == __ffs(grp) - 1) {
+            if (worst > 0.f) atomicMax((int*)(err + s0 + sl), __float_as_int(worst));  // non-negative floats order as ints
+            atomicAdd(chk + s0 + sl, (unsigned long long)__popc(grp));  // the group's lanes are its checked values
+        }
     }
 }
 
-// The check: every SUR_CHECK_EVERY-th pixel of the chunk, all energies, by the
-// rule.  The rule's values replace the network's there, and the largest relative
-// difference over the values the network took is kept per source.
-__global__ void __launch_bounds__(128) k_sur_check(const double* __restrict__ corners, const SrcInfo* __restrict__ info,
-                                                   const double* __restrict__ upsf, const double* __restrict__ logEs,
-                                                   int s0, int H, int W, int E, SurRange rg,
-                                                   float* __restrict__ mean, float* __restrict__ err,
-                                                   unsigned long long* __restrict__ chk) {
-    __shared__ unsigned char cells_s[SUR_NCELL];
-    const unsigned char* cells = sur_cells_to_shared(rg, cells_s);
-    __syncthreads();
-    const int s = s0 + blockIdx.y, npix = H * W;
-    const int pix = (blockIdx.x * blockDim.x + threadIdx.x) * SUR_CHECK_EVERY;
-    float worst = 0.f;
-    unsigned nchk = 0;
-    if (pix < npix) {
-        const int h = pix / W, w = pix - h * W;
-        SurPix sp;
-        sur_pixel(pixel_geom(corners, W + 1, h, w, info[s]), sp);
-        const bool geo_ok = sur_geo_ok(sp, rg);
-        const double* U = upsf + (size_t)s * ND * E;
-        float* mrow = mean + ((size_t)s * npix + pix) * E;
-        for (int e = 0; geo_ok && e < E; ++e) {
-            double uc;
-            float sl;
-            if (!sur_value(U, E, e, sp.ic, sp.tc, true, sp.f0, (float)logEs[e], rg, cells, &uc, &sl)) continue;
-            const double m = sur_rule(sp, U, E, e);
-            const double got = mrow[e];
-            const float r = (float)(m != 0. ? fabs(got - m) / fabs(m) : fabs(got));
-            worst = fmaxf(worst, r != r ? 3.4e38f : r);
-            mrow[e] = (float)m;
-            ++nchk;
-        }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        worst = fmaxf(worst, __shfl_xor_sync(0xffffffffu, worst, o));
-        nchk += __shfl_xor_sync(0xffffffffu, nchk, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        if (worst > 0.f) atomicMax((int*)(err + s), __float_as_int(worst));  // non-negative floats order as ints
-        if (nchk) atomicAdd(chk + s, (unsigned long long)nchk);
-    }
+// Every source listed (the rule for every value when the window path does not
+// take the map's energy count).
+__global__ void k_sur_all_list(int S, int* __restrict__ list, int* __restrict__ list_n) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) list[s] = s;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *list_n = S;
 }
 
 // Sources whose check exceeded tol, in source order: list [S], count list_n[0].
@@ -518,6 +502,21 @@ int launch_srcmap_surrogate(const SrcmapDev& a, const double* corners, const dou
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    // the rule's pixel means for every value (the window and write passes of the plain
+    // path over the unscaled table); the network's values replace them below
+    if (srcmap_win_supported(E)) {
+        int* wstatus = (int*)workspace(W_MISC, 64);
+        if (!wstatus) return XTS_ERR_OOM;
+        XTS_CUDA(cudaMemsetAsync(wstatus, 0, sizeof(int), st));
+        StreamJoin same(st, st, nullptr);
+        rc = launch_srcmap_win(corners, centers, omega, info, S, H, W, E, a.upsf, a.partial, a.exposure, nullptr,
+                               nullptr, nullptr, nullptr, nullptr, wstatus, mean, 0, nullptr, nullptr, same, st, true);
+        if (rc) return rc;
+    } else {  // more energies than the write pass holds: the FP64 rule per value
+        XTS_LAUNCH("k_sur_all_list", st, k_sur_all_list<<<(unsigned)((S + 255) / 256), 256, 0, st>>>(S, list_d, list_n));
+        XTS_LAUNCH("k_sur_fallback", st, k_sur_fallback<<<(unsigned)(4 * nsm), 128, 0, st>>>(
+                                              corners, info, a.upsf, list_d, list_n, H, W, E, mean));
+    }
     for (int s0 = 0; s0 < S; s0 += sc) {
         const int ns = S - s0 < sc ? S - s0 : sc;
         const long long n = per_src * ns;
@@ -525,16 +524,12 @@ int launch_srcmap_surrogate(const SrcmapDev& a, const double* corners, const dou
         XTS_CUDA(cudaMemsetAsync(counts + 1, 0, sizeof(unsigned long long), st));
         XTS_LAUNCH("k_sur_features", st, k_sur_features<<<gf, SF_THREADS, 0, st>>>(
                                              corners, info, a.upsf, a.logEs, s0, H, W, E, rg, X, aux, vidx,
-                                             counts + 1, mean, acc_d));
+                                             counts + 1, acc_d));
         // the network on the compacted rows; their count stays on the device
         if ((rc = launch_mlp_forward_dev(net, X, counts + 1, n, yv, status, st))) return rc;
         float* m0 = mean + (size_t)s0 * per_src;
         XTS_LAUNCH("k_sur_assemble", st, k_sur_assemble<<<(unsigned)(8 * nsm), 256, 0, st>>>(
-                                             aux, vidx, yv, counts + 1, n, m0));
-        const long long nck = (npix + SUR_CHECK_EVERY - 1) / SUR_CHECK_EVERY;
-        const dim3 gc((unsigned)((nck + 127) / 128), (unsigned)ns);
-        XTS_LAUNCH("k_sur_check", st, k_sur_check<<<gc, 128, 0, st>>>(corners, info, a.upsf, a.logEs, s0, H, W, E,
-                                                                      rg, mean, err, chk_d));
+                                             aux, vidx, yv, counts + 1, n, s0, per_src, E, m0, err, chk_d));
     }
     // maps whose check failed are redone by the rule, listed and scheduled on the device
     XTS_LAUNCH("k_sur_fail_list", st, k_sur_fail_list<<<1, 32, 0, st>>>(err, S, (float)a.check_tol, list_d, list_n));

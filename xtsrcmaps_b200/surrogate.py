@@ -282,8 +282,9 @@ def last_stats(device=None) -> dict:
 def model_map(wcs, src_sph, exposure, uPsf, partial_integrals, logEs, net: Surrogate,
               check_tol: float = 1e-4, with_info: bool = True, out=None, stats: bool = True):
     """point_src_model_map_wcs with the pixel means from the network where it
-    applies (the FP64 12-point rule elsewhere, and for every map whose check
-    fails).  CUDA tensors in; returns (float32 maps [S, H, W, E], SrcmapInfo or
+    applies (the 12-point rule elsewhere: the plain path's window and write passes
+    for up to 52 energies, the FP64 rule per value above; the FP64 rule for every
+    map whose check fails).  CUDA tensors in; returns (float32 maps [S, H, W, E], SrcmapInfo or
     None, stats dict or None).  With stats=False the call does not synchronise
     (and, once warm, can be captured into a CUDA graph); ``last_stats`` reads the
     counts afterwards."""
