@@ -586,11 +586,75 @@ int launch_adaptive_map(const double* corners, const double* centers, const doub
     return XTS_OK;
 }
 
+// The map integral of FP32 pixel means: block (c, s) takes pixels
+// [c npix / nc, (c + 1) npix / nc) of source s; warp w of the block pixels w, w + 8, ...
+// of that range, lane l energies l, l + 32, ... (a pixel's E means are contiguous, so
+// the loads coalesce); the boundary test is per pixel, the same in every lane.  Per
+// block the warps' partial sums are added in a fixed order into sums[s][c][e].
+constexpr int MI_WARPS = 8;
+constexpr int MI_EQ = 8;  // energies per lane: E <= 256
+__global__ void __launch_bounds__(32 * MI_WARPS) k_mean_integral(const double* __restrict__ centers,
+                                                                 const double* __restrict__ omega,
+                                                                 const SrcInfo* __restrict__ info,
+                                                                 const float* __restrict__ mean, int H, int W, int E,
+                                                                 int nc, double* __restrict__ sums_out) {
+    __shared__ double part[MI_WARPS][AT];
+    const int s = blockIdx.y, t = threadIdx.x, lane = t & 31, wp = t >> 5;
+    const SrcInfo si = info[s];
+    const int npix = H * W, W1 = W + 1;
+    double ch2 = 2.0 * sin(0.5 * si.radius_rad);
+    ch2 *= ch2;
+    const int p_lo = (int)((long long)npix * blockIdx.x / nc), p_hi = (int)((long long)npix * (blockIdx.x + 1) / nc);
+    const int nq = (E + 31) >> 5;
+    double acc[MI_EQ];
+#pragma unroll
+    for (int q = 0; q < MI_EQ; ++q) acc[q] = 0.;
+    if (si.in_fov) {
+        const float* m = mean + (size_t)s * npix * E;
+        for (int pix = p_lo + wp; pix < p_hi; pix += MI_WARPS) {
+            const int h = pix / W, w = pix - h * W;
+            const double* c = centers + 3 * (h * W1 + w);
+            const double x = si.dir[0] - c[0], y = si.dir[1] - c[1], z = si.dir[2] - c[2];
+            const double d2 = x * x + y * y + z * z;
+            bool inside;
+            if (d2 < ch2 * (1.0 - 1e-12)) inside = true;
+            else if (d2 > ch2 * (1.0 + 1e-12)) inside = false;
+            else inside = dir_diff(si.dir, c) <= si.radius_rad;
+            if (!inside) continue;
+            const double om = omega[pix];
+            const float* mp = m + (size_t)pix * E;
+#pragma unroll
+            for (int q = 0; q < MI_EQ; ++q) {
+                const int e = lane + 32 * q;
+                if (q < nq && e < E) acc[q] += (double)mp[e] * om;
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < MI_EQ; ++q) {
+        const int e = lane + 32 * q;
+        if (q < nq && e < E) part[wp][e] = acc[q];
+    }
+    __syncthreads();
+    for (int e = t; e < E; e += 32 * MI_WARPS) {
+        double v = 0.;
+        for (int k = 0; k < MI_WARPS; ++k) v += part[k][e];
+        sums_out[((size_t)s * nc + blockIdx.x) * E + e] = v;
+    }
+}
+
+// Chunks of the FP32 mean-map integral per source: enough blocks for every SM.
+int mean_integral_chunks(int S, int npix) {
+    int nc = (2400 + (S > 0 ? S : 1) - 1) / (S > 0 ? S : 1);
+    const int mx = (npix + 255) / 256;
+    return nc < 1 ? 1 : (nc > mx ? mx : nc);
+}
+
 int launch_mean_integral(const double* centers, const double* omega, const SrcInfo* info, const float* mean, int S,
                          int H, int W, int E, int nch, double* sums, cudaStream_t st) {
     if (E < 1 || E > AT) return set_error(XTS_ERR_ARG, "map integral of pixel means: E (%d) above %d", E, AT);
-    XTS_LAUNCH("k_adaptive_integral", st, k_adaptive_integral<float><<<dim3(nch, S), AT, 0, st>>>(
-                                              centers, omega, info, mean, H, W, E, nch, sums));
+    XTS_LAUNCH("k_mean_integral", st, k_mean_integral<<<dim3(nch, S), 32 * MI_WARPS, 0, st>>>(
+                                          centers, omega, info, mean, H, W, E, nch, sums));
     return XTS_OK;
 }
 

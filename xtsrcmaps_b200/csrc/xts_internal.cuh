@@ -68,7 +68,7 @@ enum Slot {
     W_CORNERS, W_CENTERS, W_OMEGA, W_LUT, W_PARTSUM, W_SRCINFO, W_SCALE, W_PSFTAB,
     W_KING, W_MISC, W_WIN, W_WMETA, W_SPARSE, W_MISC2, W_EXPMAP,
     W_FITS_IN, W_FITS_OUT, W_FITS_SUM, W_FFT_A, W_FFT_B, W_FFT_C, W_FFT_WORK, W_SRCPIX, W_CUT_ITEMS, W_ADAPT_MEAN,
-    W_MLP_Z, W_MLP_H, W_MLP_DZ, W_MLP_DH, W_MLP_Y, W_MLP_ST, W_MLP_PART, W_MLP_PART2, W_SUR_X, W_SUR_AUX, W_SUR_Y, W_SUR_IDX, W_SUR_ERR,
+    W_MLP_Z, W_MLP_H, W_MLP_DZ, W_MLP_DH, W_MLP_Y, W_MLP_ST, W_MLP_PART, W_MLP_PART2, W_SUR_X, W_SUR_AUX, W_SUR_Y, W_SUR_IDX, W_SUR_ERR, W_SUR_SEG,
     N_SLOTS
 };
 void* workspace(int slot, size_t bytes);  // nullptr + error set on OOM
@@ -210,6 +210,7 @@ int launch_scale_map(float* out, const double* omega, const double* scale, int S
                      cudaStream_t st);
 // c7 sums [S][nch][E] of pixel means [S][H*W][E] times solid angle over the pixels
 // inside each source's boundary radius (E <= 256)
+int mean_integral_chunks(int S, int npix);  // blocks per source of launch_mean_integral
 int launch_mean_integral(const double* centers, const double* omega, const SrcInfo* info, const float* mean, int S,
                          int H, int W, int E, int nch, double* sums, cudaStream_t st);
 // map of pixel means -> model map: c7 sums, c9 correction, c8/c10 scalings with the solid angle
@@ -221,7 +222,8 @@ int launch_gemm_bf16(const void* A, int a_trans, const void* B, int b_trans, int
 int launch_mlp_forward(const xts_mlp* net, const float* X, long long n, float* y, int* status, cudaStream_t st);
 // the same with the row count read on the device (at most n_max rows; no host sync)
 int launch_mlp_forward_dev(const xts_mlp* net, const float* X, const unsigned long long* n_dev, long long n_max,
-                           float* y, int* status, cudaStream_t st);
+                           float* y, int* status, cudaStream_t st,
+                           long long ldx = 0);  // X row-major [n][5] (0) or feature-major [5][ldx]
 int launch_mlp_grads(const xts_mlp* net, const float* X, const float* Y, long long n, float* grads, float* loss,
                      int* status, cudaStream_t st);
 int launch_mlp_train_step(const xts_mlp* net, const float* X, const float* Y, long long n, float* grads,

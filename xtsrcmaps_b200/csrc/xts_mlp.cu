@@ -173,7 +173,7 @@ template <bool SAVE>
 __global__ void __launch_bounds__(FT, 2)
 k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict__ wbf, MlpNorm nm,
               const float* __restrict__ X, long long n, const unsigned long long* __restrict__ n_dev,
-              float* __restrict__ y, FwdSaves sv, int* __restrict__ status) {
+              long long ldx, float* __restrict__ y, FwdSaves sv, int* __restrict__ status) {
     if (n_dev) n = min(n, (long long)*n_dev);  // rows counted on the device (at most n)
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
@@ -227,7 +227,8 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
         const bool lv = rw < n;
         float x[MI];
 #pragma unroll
-        for (int k = 0; k < MI; ++k) x[k] = lv ? (X[rw * MI + k] - nm.mu[k]) / nm.sd[k] : 0.f;
+        for (int k = 0; k < MI; ++k)
+            x[k] = lv ? (X[ldx ? k * ldx + rw : rw * MI + k] - nm.mu[k]) / nm.sd[k] : 0.f;
 #pragma unroll
         for (int g = 0; g < 8; ++g) {
             const int j0 = cb + 8 * g;
@@ -380,7 +381,7 @@ __device__ __forceinline__ bool group_and(int g, bool v) {
 __global__ void __launch_bounds__(IT, 1)
 k_mlp_infer(const float* __restrict__ params, const __nv_bfloat16* __restrict__ wbf, MlpNorm nm,
             const float* __restrict__ X, long long n, const unsigned long long* __restrict__ n_dev,
-            float* __restrict__ y, int* __restrict__ status) {
+            long long ldx, float* __restrict__ y, int* __restrict__ status) {
     if (n_dev) n = min(n, (long long)*n_dev);  // rows counted on the device (at most n)
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
@@ -434,7 +435,7 @@ k_mlp_infer(const float* __restrict__ params, const __nv_bfloat16* __restrict__ 
     auto load_x = [&](long long tl) {
         const long long rw = tl * MT + r;
 #pragma unroll
-        for (int k = 0; k < MI; ++k) xn[k] = tl < ntiles && rw < n ? X[rw * MI + k] : 0.f;
+        for (int k = 0; k < MI; ++k) xn[k] = tl < ntiles && rw < n ? X[ldx ? k * ldx + rw : rw * MI + k] : 0.f;
     };
     load_x((long long)blockIdx.x * IG + g);
     for (long long tile = (long long)blockIdx.x * IG + g; tile < ntiles && ok; tile += stride) {
@@ -793,8 +794,9 @@ int launch_gemm_bf16(const void* A, int a_trans, const void* B, int b_trans, int
     return XTS_OK;
 }
 
+// X: row-major [n][5] (ldx 0) or feature-major [5][ldx] (ldx >= n)
 static int forward(const xts_mlp* net, const float* X, long long n, const unsigned long long* n_dev, float* y,
-                   FwdSaves sv, int* status, cudaStream_t st) {
+                   FwdSaves sv, int* status, cudaStream_t st, long long ldx = 0) {
     // per call: the attribute belongs to the current device's context
     XTS_CUDA(cudaFuncSetAttribute(k_mlp_forward<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM));
     XTS_CUDA(cudaFuncSetAttribute(k_mlp_forward<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM));
@@ -807,18 +809,18 @@ static int forward(const xts_mlp* net, const float* X, long long n, const unsign
     if (save) {
         XTS_LAUNCH("k_mlp_forward", st, k_mlp_forward<true><<<(unsigned)g, FT, FWD_SMEM, st>>>(
                                             net->params, (const __nv_bfloat16*)net->wbf16, mlp_norm(net), X, n, n_dev,
-                                            y, sv, status));
+                                            ldx, y, sv, status));
     } else if (g_tuning.mlp_blocks_per_sm == 0) {
         // inference: four tiles in flight per SM, one block per SM
         XTS_CUDA(cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INF_SMEM));
         const long long gi = (ntiles + IG - 1) / IG < sm_count() ? (ntiles + IG - 1) / IG : sm_count();
         XTS_LAUNCH("k_mlp_infer", st, k_mlp_infer<<<(unsigned)gi, IT, INF_SMEM, st>>>(
                                             net->params, (const __nv_bfloat16*)net->wbf16, mlp_norm(net), X, n, n_dev,
-                                            y, status));
+                                            ldx, y, status));
     } else {
         XTS_LAUNCH("k_mlp_forward", st, k_mlp_forward<false><<<(unsigned)g, FT, FWD_SMEM, st>>>(
                                             net->params, (const __nv_bfloat16*)net->wbf16, mlp_norm(net), X, n, n_dev,
-                                            y, sv, status));
+                                            ldx, y, sv, status));
     }
     return XTS_OK;
 }
@@ -829,9 +831,10 @@ int launch_mlp_forward(const xts_mlp* net, const float* X, long long n, float* y
 }
 
 int launch_mlp_forward_dev(const xts_mlp* net, const float* X, const unsigned long long* n_dev, long long n_max,
-                           float* y, int* status, cudaStream_t st) {
+                           float* y, int* status, cudaStream_t st, long long ldx) {
     if (n_max <= 0) return XTS_OK;
-    return forward(net, X, n_max, n_dev, y, FwdSaves{}, status, st);
+    if (ldx && ldx < n_max) return set_error(XTS_ERR_ARG, "mlp forward: feature stride below the row count");
+    return forward(net, X, n_max, n_dev, y, FwdSaves{}, status, st, ldx);
 }
 
 // forward with saves, then the gradient accumulated into grads (zero on entry)

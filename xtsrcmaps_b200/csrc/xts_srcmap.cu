@@ -516,6 +516,7 @@ static int launch_srcmap_adaptive(const SrcmapDev& a, const double* corners, con
 int finish_mean_map(const SrcmapDev& a, const double* centers, const double* omega, const SrcInfo* info,
                     double* scale, int nch, cudaStream_t st) {
     const int H = (int)a.wcs.naxis1, W = (int)a.wcs.naxis2, S = a.S, E = a.E;
+    nch = mean_integral_chunks(S, H * W);
     double* sums = (double*)workspace(W_PARTSUM, sizeof(double) * (size_t)S * nch * E + 8);
     if (!sums) return XTS_ERR_OOM;
     int rc = launch_mean_integral(centers, omega, info, (const float*)a.out, S, H, W, E, nch, sums, st);

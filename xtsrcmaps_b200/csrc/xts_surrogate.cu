@@ -27,6 +27,7 @@
 // the relative difference to the network's is recorded per source.  Sources whose
 // check fails are redone by the FP64 rule (k_sur_fallback), and the map integral,
 // correction and scalings follow as for the adaptive map.
+#include <cfloat>
 #include <vector>
 
 #include "xts_point.cuh"
@@ -212,8 +213,40 @@ constexpr int SF_THREADS = 256;
 struct SurPixS {
     float f0, f1, f2, eps;
     double tc;
-    int ic, geo_ok;
+    int ic;
+    int crow;  // error-cell row of log10 rho (0 without cells); -1: the network takes none of the pixel's values
+    int tc01;  // the centre's offset tc lies in [0, 1]
 };
+
+// Per (segment row ic, energy) of the sources of a chunk: whether the network may take
+// a value whose centre falls in that table segment -- the energy and the segment's log
+// slope inside the training range and the slope inside the error-cell grid -- as
+// code = slope cell column | sign class << 8 (sign class 1: both rows positive, so
+// u_c > 0 for tc in [0, 1]; 2: neither positive, u_c <= 0; 0: u_c decided per value),
+// or -1; and the slope itself.  seg, slope: [ns][ND][E] (row 0 unused).
+__global__ void k_sur_segments(const double* __restrict__ upsf, const double* __restrict__ logEs, int ns, int E,
+                               SurRange rg, short* __restrict__ seg, float* __restrict__ slope) {
+    const long long n = (long long)ns * ND * E;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int e = (int)(i % E);
+        const long long jr = i / E;
+        const int r = (int)(jr % ND);
+        if (r == 0) { seg[i] = -1; slope[i] = 0.f; continue; }
+        const double lo = upsf[i - E], hi = upsf[i];
+        const float sl = sur_slope(lo, hi);
+        const float le = (float)logEs[e];
+        bool ok = le >= rg.lo[3] && le <= rg.hi[3] && sl >= rg.lo[4] && sl <= rg.hi[4];
+        int b = 0;
+        if (rg.cell_ok) {
+            const float bf = (sl - rg.c1) * rg.cs1;
+            ok = ok && bf >= 0.f && bf < (float)XTS_MLP_CELL_NS;
+            b = ok ? (int)bf : 0;
+        }
+        const int cls = (lo > 4.0 * DBL_MIN && hi > 4.0 * DBL_MIN) ? 1 : ((lo <= 0. && hi <= 0.) ? 2 : 0);
+        seg[i] = ok ? (short)(b | (cls << 8)) : (short)-1;
+        slope[i] = sl;
+    }
+}
 
 __device__ __forceinline__ bool sur_geo_ok(const SurPix& q, const SurRange& rg) {
     return q.rho >= rg.rho_min && q.f0 >= rg.lo[0] && q.f0 <= rg.hi[0] && q.f1 >= rg.lo[1] && q.f1 <= rg.hi[1] &&
@@ -248,9 +281,12 @@ __global__ void __launch_bounds__(SF_THREADS) k_sur_features(const double* __res
                                                              int E, SurRange rg, float* __restrict__ X,
                                                              float2* __restrict__ aux, unsigned* __restrict__ vidx,
                                                              unsigned long long* __restrict__ n_acc,
-                                                             unsigned long long* __restrict__ accepted) {
+                                                             unsigned long long* __restrict__ accepted,
+                                                             const short* __restrict__ seg,
+                                                             const float* __restrict__ slope, long long ldx) {
     __shared__ SurPixS sp[SF_PIX];
     __shared__ unsigned okbits[SF_PIX * 256 / 32];  // one bit per (pixel, energy) value, E <= 256
+    __shared__ unsigned wpre[SF_PIX * 256 / 32];    // accepted values before each word
     __shared__ unsigned wsum[SF_THREADS / 32];
     __shared__ unsigned long long base_s;
     __shared__ unsigned char cells_s[SUR_NCELL];
@@ -268,28 +304,57 @@ __global__ void __launch_bounds__(SF_THREADS) k_sur_features(const double* __res
         o.eps = (float)(1.0 / (q.rho * q.rho));
         o.tc = q.tc;
         o.ic = q.ic;
-        o.geo_ok = sur_geo_ok(q, rg);
+        o.tc01 = q.tc >= 0. && q.tc <= 1.;
+        int crow = sur_geo_ok(q, rg) ? 0 : -1;
+        if (crow == 0 && cells) {
+            const float a = (q.f0 - rg.c0) * rg.cs0;
+            crow = (a >= 0.f && a < (float)XTS_MLP_CELL_NR) ? (int)a : -1;
+        }
+        o.crow = crow;
     }
     __syncthreads();
     const double* U = upsf + (size_t)s * ND * E;
+    const short* sg = seg + (size_t)blockIdx.y * ND * E;
     const size_t vb = ((size_t)blockIdx.y * npix + p0) * E;  // first value of the block (chunk-relative)
     unsigned cnt = 0;
+    // the value of thread t in round i is k = t + 256 i: its pixel and energy by steps
+    const int dq = SF_THREADS / E, dr = SF_THREADS - dq * E;
+    int lp = t / E, e = t - lp * E;
     for (int k0 = t - lane; k0 < nv; k0 += SF_THREADS) {  // a warp takes 32 consecutive values
         const int k = k0 + lane;
         bool ok = false;
         if (k < nv) {
-            const int lp = k / E, e = k - lp * E;
             const SurPixS& o = sp[lp];
-            double uc;
-            float sl;
-            ok = sur_value(U, E, e, o.ic, o.tc, o.geo_ok, o.f0, (float)logEs[e], rg, cells, &uc, &sl);
+            if (o.crow >= 0) {
+                const int code = sg[(size_t)o.ic * E + e];
+                if (code >= 0) {
+                    const int cls = code >> 8;
+                    bool pos;
+                    if (o.tc01 && cls == 1) pos = true;
+                    else if (o.tc01 && cls == 2) pos = false;
+                    else {
+                        const double lo = U[(size_t)(o.ic - 1) * E + e], hi = U[(size_t)o.ic * E + e];
+                        pos = (1.0 - o.tc) * lo + o.tc * hi > 0.;
+                    }
+                    ok = pos && (!cells || cells[o.crow * XTS_MLP_CELL_NS + (code & 255)] != 0);
+                }
+            }
         }
         const unsigned bits = __ballot_sync(0xffffffffu, ok);
         if (lane == 0) okbits[k0 >> 5] = bits;
         cnt += ok;
+        lp += dq;
+        e += dr;
+        if (e >= E) { e -= E; ++lp; }
     }
-    // exclusive scan of the per-thread counts; one reservation per block
-    unsigned inc = cnt;
+    // the block's accepted values in value order: exclusive prefix counts of the
+    // acceptance words, one reservation per block
+    __syncthreads();
+    const int nw = (nv + 31) >> 5, cpt = (nw + SF_THREADS - 1) / SF_THREADS;
+    const int w0 = t * cpt, w1 = min(nw, w0 + cpt);
+    unsigned mine = 0;
+    for (int w = w0; w < w1; ++w) mine += __popc(okbits[w]);
+    unsigned inc = mine;
     for (int o = 1; o < 32; o <<= 1) {
         const unsigned v = __shfl_up_sync(0xffffffffu, inc, o);
         if (lane >= o) inc += v;
@@ -301,25 +366,40 @@ __global__ void __launch_bounds__(SF_THREADS) k_sur_features(const double* __res
         before += w < wp ? wsum[w] : 0u;
         total += wsum[w];
     }
+    unsigned run = before + inc - mine;
+    for (int w = w0; w < w1; ++w) {
+        wpre[w] = run;
+        run += __popc(okbits[w]);
+    }
     if (t == 0) {
         base_s = total ? atomicAdd(n_acc, (unsigned long long)total) : 0ull;
         if (total) atomicAdd(accepted + s, (unsigned long long)total);
     }
     __syncthreads();
-    unsigned long long j = base_s + before + (inc - cnt);
-    for (int k = t; k < nv; k += SF_THREADS) {
-        if (!((okbits[k >> 5] >> (k & 31)) & 1u)) continue;
-        const int lp = k / E, e = k - lp * E;
-        const SurPixS& o = sp[lp];
-        double uc;
-        float sl;
-        const float le = (float)logEs[e];
-        sur_value(U, E, e, o.ic, o.tc, o.geo_ok, o.f0, le, rg, cells, &uc, &sl);
-        float* x = X + j * 5;
-        x[0] = o.f0; x[1] = o.f1; x[2] = o.f2; x[3] = le; x[4] = sl;
-        aux[j] = make_float2((float)uc, o.eps);
-        vidx[j] = (unsigned)(vb + k);
-        ++j;
+    (void)cnt;
+    // pass 2: a warp's accepted lanes write consecutive rows (feature-major X [5][ldx])
+    const unsigned long long base = base_s;
+    const float* slp = slope + (size_t)blockIdx.y * ND * E;
+    lp = t / E;
+    e = t - lp * E;
+    for (int k0 = t - lane; k0 < nv; k0 += SF_THREADS) {
+        const unsigned word = okbits[k0 >> 5];
+        if ((word >> lane) & 1u) {
+            const unsigned long long j = base + wpre[k0 >> 5] + __popc(word & ((1u << lane) - 1u));
+            const SurPixS& o = sp[lp];
+            const double lo = U[(size_t)(o.ic - 1) * E + e], hi = U[(size_t)o.ic * E + e];
+            const double uc = (1.0 - o.tc) * lo + o.tc * hi;
+            X[j] = o.f0;
+            X[ldx + j] = o.f1;
+            X[2 * ldx + j] = o.f2;
+            X[3 * ldx + j] = (float)logEs[e];
+            X[4 * ldx + j] = slp[(size_t)o.ic * E + e];
+            aux[j] = make_float2((float)uc, o.eps);
+            vidx[j] = (unsigned)(vb + k0 + lane);
+        }
+        lp += dq;
+        e += dr;
+        if (e >= E) { e -= E; ++lp; }
     }
 }
 
@@ -473,6 +553,12 @@ int launch_srcmap_surrogate(const SrcmapDev& a, const double* corners, const dou
     float2* aux = (float2*)workspace(W_SUR_AUX, sizeof(float2) * (size_t)nmax + 16);
     float* yv = (float*)workspace(W_SUR_Y, sizeof(float) * (size_t)nmax + 16);
     unsigned* vidx = (unsigned*)workspace(W_SUR_IDX, sizeof(unsigned) * (size_t)nmax + 16);
+    // per chunk: the segment codes [sc][ND][E] (short) and slopes (float)
+    const size_t nseg = (size_t)sc * ND * E;
+    char* segbuf = (char*)workspace(W_SUR_SEG, align_up(sizeof(short) * nseg, 256) + sizeof(float) * nseg + 16);
+    if (!segbuf) return XTS_ERR_OOM;
+    short* seg = (short*)segbuf;
+    float* slope = (float*)(segbuf + align_up(sizeof(short) * nseg, 256));
     if (!vidx) return XTS_ERR_OOM;
     // per source: largest check difference, values the network evaluated, values
     // checked; then the compacted row count, the status word, the failed-source
@@ -522,11 +608,13 @@ int launch_srcmap_surrogate(const SrcmapDev& a, const double* corners, const dou
         const long long n = per_src * ns;
         const dim3 gf((unsigned)((npix + SF_PIX - 1) / SF_PIX), (unsigned)ns);
         XTS_CUDA(cudaMemsetAsync(counts + 1, 0, sizeof(unsigned long long), st));
+        XTS_LAUNCH("k_sur_segments", st, k_sur_segments<<<(unsigned)(4 * nsm), 256, 0, st>>>(
+                                             a.upsf + (size_t)s0 * ND * E, a.logEs, ns, E, rg, seg, slope));
         XTS_LAUNCH("k_sur_features", st, k_sur_features<<<gf, SF_THREADS, 0, st>>>(
                                              corners, info, a.upsf, a.logEs, s0, H, W, E, rg, X, aux, vidx,
-                                             counts + 1, acc_d));
+                                             counts + 1, acc_d, seg, slope, nmax));
         // the network on the compacted rows; their count stays on the device
-        if ((rc = launch_mlp_forward_dev(net, X, counts + 1, n, yv, status, st))) return rc;
+        if ((rc = launch_mlp_forward_dev(net, X, counts + 1, n, yv, status, st, nmax))) return rc;
         float* m0 = mean + (size_t)s0 * per_src;
         XTS_LAUNCH("k_sur_assemble", st, k_sur_assemble<<<(unsigned)(8 * nsm), 256, 0, st>>>(
                                              aux, vidx, yv, counts + 1, n, s0, per_src, E, m0, err, chk_d));
