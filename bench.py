@@ -672,10 +672,12 @@ def measure_e2e(args, A, job, nf_h, nb_h, ltf_h, net, torch, dev, dist, world, n
 
     te_s = wall(step_sur)
     return {"value": n_values * world * ke / te_s, "unit": UNIT,
-            "h2d_bytes_per_step": int(hcube.numel() * 4 * 2 + 8 * (E + 2 * S) + grids + 16 * E),
+            "h2d_bytes_per_step": int(2 * 4 * S * C_ + 8 * E + 16 * S + grids + 16 * E),
             "d2h_bytes_per_step": int(4 * n_values), "steps": ke,
-            "note": "point_source_maps_surrogate (exposure, mean PSF, surrogate model map) from pinned host "
-                    "buffers (whole livetime cubes) to a pinned host map, copies inside the timed region",
+            "note": "point_source_maps_surrogate (the three calls of main.cxx:28-30 fused, surrogate model map) "
+                    "from pinned host buffers to a pinned host map, copies inside the timed region; the library "
+                    "uploads only the livetime rows at the sources' pixels and copies the map out by groups of "
+                    "sources while later groups compute",
             "plain": plain}
 
 

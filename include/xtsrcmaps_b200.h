@@ -472,6 +472,21 @@ int xts_point_src_model_map_wcs_surrogate(const xts_wcs* wcs, const double* src_
                                           double check_tol, float* model_map, xts_srcmap_info* info,
                                           xts_surrogate_stats* stats, void* stream);
 
+/* xts_point_source_maps with the model map of the surrogate
+ * (xts_point_src_model_map_wcs_surrogate) in place of the plain cubature: the
+ * three calls of main.cxx:28-30 in one, FP32 maps.  Host or device pointers as
+ * xts_point_source_maps (flags XTS_DEVICE_PTRS); with host pointers the map is
+ * copied to the host in about eight groups of sources, each group finished
+ * (checks, map integral, correction, scaling) and copied while the next is
+ * computed.  stats: as xts_point_src_model_map_wcs_surrogate. */
+int xts_point_source_maps_surrogate(const xts_expcube* exp_cube, const xts_expcube* wexp_cube,
+                                    const double* logEs, int E, const double* src_sph, int S,
+                                    const xts_grid* aeff_front, const xts_grid* aeff_back,
+                                    const xts_grid* psf_front, const xts_grid* psf_back,
+                                    const double* front_ltf, const xts_wcs* wcs, const xts_mlp* net,
+                                    double check_tol, float* model_map, xts_srcmap_info* info,
+                                    xts_surrogate_stats* stats, unsigned flags, void* stream);
+
 /* Counts of the latest xts_point_src_model_map_wcs_surrogate call on the
  * library's device (waits for that call's work on `stream`); XTS_ERR_TIMEOUT if
  * one of its bounded tensor-core waits gave up. */

@@ -175,6 +175,52 @@ def test_map_fallback_equals_rule(api):
     assert max_rel(info.inv_map_integral.cpu().numpy(), pinfo.inv_map_integral.cpu().numpy()) < 1e-7
 
 
+def test_fused_surrogate_call_host_and_device(api):
+    """xts_point_source_maps_surrogate: the three calls in one with the surrogate's
+    map.  From host buffers (the map copied out in groups of sources, each group
+    finished on its own) and from device buffers (one group) it gives the map of the
+    separate calls, with the same counts."""
+    import torch
+
+    from xtsrcmaps_b200.surrogate import Surrogate, model_map, samples
+    from xtsrcmaps_b200.synth import make_job
+
+    job = make_job("c1", seed=5, n_sources=20)
+    ltf = api.livetime_efficiency_factors(job.logEs, job.effic_front)
+    nf = api.normalize_rpsf(job.rpsf_front, job.scale_front)
+    nb = api.normalize_rpsf(job.rpsf_back, job.scale_back)
+    ex = api.compute_exposure(job.exp_cube, job.wexp_cube, job.logEs, job.src_sph, job.aeff_front,
+                              job.aeff_back, ltf)
+    ps = api.compute_psf_data(nf, nb, ex, job.logEs, ltf)
+    d = torch.device("cuda")
+    t = lambda x: torch.as_tensor(np.ascontiguousarray(x), device=d)
+    upsf = t(ps.uPsf)
+    net = Surrogate(device=d, seed=2)
+    X, Y = samples(upsf, job.logEs, 200_000, seed=4)
+    net.train(X, Y, epochs=3)
+    ref, _, st_ref = model_map(job.wcs, t(job.src_sph), t(ex.exposure), upsf, t(ps.partial_psf_integral),
+                               job.logEs, net, check_tol=1e-3)
+    ref = ref.cpu().numpy()
+    hm, _, st_h = api.point_source_maps_surrogate(job.wcs, job.src_sph, job.exp_cube, job.wexp_cube, job.logEs,
+                                                  job.aeff_front, job.aeff_back, nf, nb, ltf, net, check_tol=1e-3)
+    assert st_h == st_ref
+    assert max_rel(hm, ref) < 1e-6
+    from xtsrcmaps_b200.api import ExpCube
+    from xtsrcmaps_b200.irf import IrfGrid
+
+    tt = lambda x, dt=torch.float64: torch.as_tensor(np.asarray(x), device=d).to(dt).contiguous()
+    grid = lambda g: IrfGrid(tt(g.cosths), tt(g.logEs), tt(g.params), g.min_cos_theta)
+    cube = ExpCube(tt(job.exp_cube.cosbins, torch.float32), job.exp_cube.nside, 40, job.exp_cube.cosmin,
+                   job.exp_cube.thetabin)
+    wcube = ExpCube(tt(job.wexp_cube.cosbins, torch.float32), job.wexp_cube.nside, 40, job.wexp_cube.cosmin,
+                    job.wexp_cube.thetabin)
+    dm, _, st_d = api.point_source_maps_surrogate(job.wcs, tt(job.src_sph), cube, wcube, tt(job.logEs),
+                                                  grid(job.aeff_front), grid(job.aeff_back), grid(nf), grid(nb),
+                                                  tt(ltf), net, check_tol=1e-3)
+    assert st_d == st_ref
+    assert max_rel(dm.cpu().numpy(), ref) < 1e-6
+
+
 def test_surrogate_map_many_energies(api):
     """More energies than the window path's write pass holds (60 > 52): the rule's
     means come from the FP64 rule per value instead; with a check no network meets,

@@ -165,6 +165,11 @@ SIGNATURES = {
                                                         C.POINTER(XtsSrcmapInfo),
                                                         C.POINTER(XtsSurrogateStats), _vp]),
     "xts_surrogate_last_stats": (C.c_int, [C.POINTER(XtsSurrogateStats), _vp]),
+    "xts_point_source_maps_surrogate": (C.c_int, [C.POINTER(XtsExpcube), C.POINTER(XtsExpcube), _vp, C.c_int, _vp,
+                                                  C.c_int, C.POINTER(XtsGrid), C.POINTER(XtsGrid),
+                                                  C.POINTER(XtsGrid), C.POINTER(XtsGrid), _vp, C.POINTER(XtsWcs),
+                                                  C.POINTER(XtsMlp), C.c_double, _vp, C.POINTER(XtsSrcmapInfo),
+                                                  C.POINTER(XtsSurrogateStats), C.c_uint, _vp]),
     "xts_cutout_windows": (C.c_int, [C.POINTER(XtsWcs), _vp, _vp, C.c_int, _vp, C.POINTER(C.c_longlong)]),
     "xts_point_src_model_map_cutouts": (C.c_int, [C.POINTER(XtsWcs), _vp, C.c_int, _vp, _vp, _vp, _vp, C.c_int,
                                                   _vp, C.POINTER(XtsSrcmapInfo), C.c_uint, _vp]),

@@ -406,43 +406,51 @@ def point_source_maps_surrogate(wcs: Wcs, src_sph, exp_cube: ExpCube, wexp_cube:
                                 front_ltf, net, check_tol: float = 1e-4, out=None, with_info: bool = False,
                                 stats: bool = True):
     """The three calls of main.cxx:28-30 with the model map of the learned
-    surrogate (point_src_model_map_wcs_surrogate) in place of the plain cubature.
-    Inputs may be host arrays (numpy, or CPU torch tensors, pinned for
-    asynchronous copies) or CUDA tensors; host inputs are copied to the network's
-    device and the map is copied back into ``out`` (a CPU tensor or numpy array;
-    allocated when None).  Returns (model_map, SrcmapInfo or None, stats or
-    None)."""
-    import torch
+    surrogate (point_src_model_map_wcs_surrogate) in place of the plain cubature,
+    in one library call (xts_point_source_maps_surrogate).  Inputs may be host
+    arrays (numpy, or CPU torch tensors, pinned for asynchronous copies) or CUDA
+    tensors on the network's device; with host arrays the maps are copied to the
+    host in groups of sources while the later groups are computed (pass a
+    page-locked ``out`` for full copy speed).  Returns (model_map, SrcmapInfo or
+    None, stats or None)."""
+    from .surrogate import _stats_dict
 
-    dev = net.device
-    host = not _is_cuda(src_sph)
-
-    def t(a, dt=torch.float64):
-        a = a if isinstance(a, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(a))
-        return a.to(device=dev, dtype=dt, non_blocking=True)
-
-    def grid(g):
-        return IrfGrid(t(g.cosths), t(g.logEs), t(g.params), g.min_cos_theta)
-
-    cube = ExpCube(t(exp_cube.cosbins, torch.float32), exp_cube.nside, exp_cube.nbrbins, exp_cube.cosmin,
-                   exp_cube.thetabin)
-    wcube = ExpCube(t(wexp_cube.cosbins, torch.float32), wexp_cube.nside, wexp_cube.nbrbins, wexp_cube.cosmin,
-                    wexp_cube.thetabin)
-    le, src, ltf = t(logEs), t(src_sph), t(front_ltf)
-    ex = compute_exposure(cube, wcube, le, src, grid(aeff_front), grid(aeff_back), ltf)
-    ps = compute_psf_data(grid(psf_front), grid(psf_back), ex, le, ltf)
-    from .surrogate import model_map
-
-    m, info, st = model_map(wcs, src, ex.exposure, ps.uPsf, ps.partial_psf_integral, le, net, check_tol,
-                            with_info, out=None if host else out, stats=stats)
-    if host:
-        if out is None:
-            out = torch.empty(tuple(m.shape), dtype=torch.float32, pin_memory=True)
-        dst = out if isinstance(out, torch.Tensor) else torch.from_numpy(out)
-        dst.copy_(m, non_blocking=True)
-        torch.cuda.current_stream(dev).synchronize()
+    like = _device_of(exp_cube.cosbins, src_sph, logEs)
+    c = _Call(like is not None, like)
+    cb, _ = c.inp(exp_cube.cosbins, "f32")
+    wb, _ = c.inp(wexp_cube.cosbins, "f32")
+    cube_s = L.XtsExpcube(cb, int(exp_cube.nside), int(exp_cube.nbrbins), float(exp_cube.cosmin),
+                          int(bool(exp_cube.thetabin)))
+    wcube_s = L.XtsExpcube(wb, int(wexp_cube.nside), int(wexp_cube.nbrbins), float(wexp_cube.cosmin),
+                           int(bool(wexp_cube.thetabin)))
+    lp, le = c.inp(logEs)
+    E = len(le)
+    sp, sa = c.inp(src_sph)
+    S = int(sa.shape[0]) if sa.ndim == 2 else 0
+    af = c.grid(aeff_front, 1)
+    ab = c.grid(aeff_back, 1)
+    gf = c.grid(psf_front, 6)
+    gb = c.grid(psf_back, 6)
+    ltfp, _ = c.inp(front_ltf)
+    shape = (S, int(wcs.naxis1), int(wcs.naxis2), E)
+    if out is None:
+        mp, m = c.out(shape, "f32")
+    else:
         m = out
-    return m, info, st
+        mp = C.c_void_p(m.data_ptr() if hasattr(m, "data_ptr") else m.ctypes.data)
+    info = info_s = None
+    if with_info:
+        o = [c.out((S, E)), c.out((S, E)), c.out((S,)), c.out((S,), "i32")]
+        info_s = L.XtsSrcmapInfo(*[x[0] for x in o])
+        info = SrcmapInfo(*[x[1] for x in o])
+    st = L.XtsSurrogateStats() if stats else None
+    ns = net.struct()
+    w = _wcs_struct(wcs)
+    L.check(L.lib().xts_point_source_maps_surrogate(
+        C.byref(cube_s), C.byref(wcube_s), lp, E, sp, S, C.byref(af), C.byref(ab), C.byref(gf), C.byref(gb), ltfp,
+        C.byref(w), C.byref(ns), float(check_tol), mp, C.byref(info_s) if info_s is not None else None,
+        C.byref(st) if st is not None else None, c.flags, c.stream))
+    return m, info, (_stats_dict(st) if st is not None else None)
 
 
 def write_src_model(filename: str, model_map, names=None, bitpix: int = -64) -> None:

@@ -801,12 +801,13 @@ int xts_surrogate_last_stats(xts_surrogate_stats* stats, void* stream) {
     return surrogate_last_stats(stats, stream ? (cudaStream_t)stream : g_ctx.stream);
 }
 
-int xts_point_source_maps(const xts_expcube* cube, const xts_expcube* wcube, const double* logEs,
-                          int E, const double* src_sph, int S, const xts_grid* aeff_front,
-                          const xts_grid* aeff_back, const xts_grid* psf_front,
-                          const xts_grid* psf_back, const double* front_ltf, const xts_wcs* wcs,
-                          void* model_map, xts_srcmap_info* info, unsigned flags, void* stream) {
-    XTS_ENTER();
+// The fused exposure -> mean PSF -> model map call; with net, the surrogate's map.
+static int fused_maps(const xts_expcube* cube, const xts_expcube* wcube, const double* logEs,
+                      int E, const double* src_sph, int S, const xts_grid* aeff_front,
+                      const xts_grid* aeff_back, const xts_grid* psf_front,
+                      const xts_grid* psf_back, const double* front_ltf, const xts_wcs* wcs,
+                      void* model_map, xts_srcmap_info* info, unsigned flags, void* stream,
+                      const xts_mlp* net, double check_tol, xts_surrogate_stats* stats) {
     if (!cube || !wcube || !cube->cosbins || !wcube->cosbins || !logEs || E <= 0 || S < 0 ||
         (S > 0 && (!src_sph || !model_map)) || !front_ltf)
         return set_error(XTS_ERR_ARG, "point_source_maps: null argument or bad size");
@@ -879,6 +880,13 @@ int xts_point_source_maps(const xts_expcube* cube, const xts_expcube* wcube, con
     ma.radius = info ? sg.out(info->psf_radius, (size_t)S) : nullptr;
     ma.in_fov = info ? sg.out(info->in_fov, (size_t)S) : nullptr;
     ma.kernel = srcmap_kernel(flags);
+    if (net) {
+        ma.surrogate = net;
+        ma.logEs = ea.logEs;
+        ma.check_tol = check_tol;
+        ma.sur_stats = stats;
+        if (stats) memset(stats, 0, sizeof(*stats));
+    }
     if (fork) { ma.geo_stream = g_ctx.geo_stream; ma.join_ev = g_ctx.join_ev; }
     int rc = sg.rc;
     if (rc == XTS_OK) rc = launch_exposure(ea, sg.st);
@@ -888,6 +896,35 @@ int xts_point_source_maps(const xts_expcube* cube, const xts_expcube* wcube, con
         return sg.finish(rc);
     }
     return run_srcmap(sg, ma, model_map, npix, f64);
+}
+
+int xts_point_source_maps(const xts_expcube* cube, const xts_expcube* wcube, const double* logEs,
+                          int E, const double* src_sph, int S, const xts_grid* aeff_front,
+                          const xts_grid* aeff_back, const xts_grid* psf_front,
+                          const xts_grid* psf_back, const double* front_ltf, const xts_wcs* wcs,
+                          void* model_map, xts_srcmap_info* info, unsigned flags, void* stream) {
+    XTS_ENTER();
+    return fused_maps(cube, wcube, logEs, E, src_sph, S, aeff_front, aeff_back, psf_front, psf_back, front_ltf, wcs,
+                      model_map, info, flags, stream, nullptr, 0., nullptr);
+}
+
+int xts_point_source_maps_surrogate(const xts_expcube* cube, const xts_expcube* wcube, const double* logEs,
+                                    int E, const double* src_sph, int S, const xts_grid* aeff_front,
+                                    const xts_grid* aeff_back, const xts_grid* psf_front,
+                                    const xts_grid* psf_back, const double* front_ltf, const xts_wcs* wcs,
+                                    const xts_mlp* net, double check_tol, float* model_map,
+                                    xts_srcmap_info* info, xts_surrogate_stats* stats, unsigned flags,
+                                    void* stream) {
+    XTS_ENTER();
+    int rc = mlp_ok(net, "point_source_maps_surrogate");
+    if (rc) return rc;
+    if (!(check_tol > 0.)) return set_error(XTS_ERR_ARG, "point_source_maps_surrogate: check_tol must be > 0");
+    if (flags & (XTS_OUT_F64 | XTS_CUDA_CORES | XTS_TCGEN05))
+        return set_error(XTS_ERR_ARG, "point_source_maps_surrogate: FP32 maps of the window path only");
+    if (!srcmap_adaptive_supported(E))
+        return set_error(XTS_ERR_ARG, "point_source_maps_surrogate: E must be in 1..256");
+    return fused_maps(cube, wcube, logEs, E, src_sph, S, aeff_front, aeff_back, psf_front, psf_back, front_ltf, wcs,
+                      model_map, info, flags, stream, net, check_tol, stats);
 }
 
 int xts_make_psf_kernel(const xts_wcs* kernel_wcs, int Nk, const double* upsf, int E, double* kernel,

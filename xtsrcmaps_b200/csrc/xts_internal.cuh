@@ -214,6 +214,9 @@ int mean_integral_chunks(int S, int npix);  // blocks per source of launch_mean_
 int launch_mean_integral(const double* centers, const double* omega, const SrcInfo* info, const float* mean, int S,
                          int H, int W, int E, int nch, double* sums, cudaStream_t st);
 // map of pixel means -> model map: c7 sums, c9 correction, c8/c10 scalings with the solid angle
+// finish_mean_map for sources [s0, s0 + ns) only
+int finish_mean_map_range(const SrcmapDev& a, int s0, int ns, const double* centers, const double* omega,
+                          const SrcInfo* info, double* scale, cudaStream_t st);
 int finish_mean_map(const SrcmapDev& a, const double* centers, const double* omega, const SrcInfo* info,
                     double* scale, int nch, cudaStream_t st);
 // the surrogate network (xts_mlp.cu) and the surrogate model map (xts_surrogate.cu)

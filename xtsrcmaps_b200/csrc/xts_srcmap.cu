@@ -513,18 +513,28 @@ static int launch_srcmap_adaptive(const SrcmapDev& a, const double* corners, con
 // A map of pixel means [S][H*W][E] (a.out, FP32) -> the model map: the map
 // integral sums over the pixels inside the boundary radius, the correction, and
 // value = mean * solid angle * exposure * correction.
+int finish_mean_map_range(const SrcmapDev& a, int s0, int ns, const double* centers, const double* omega,
+                          const SrcInfo* info, double* scale, cudaStream_t st) {
+    const int H = (int)a.wcs.naxis1, W = (int)a.wcs.naxis2, E = a.E;
+    if (ns <= 0) return XTS_OK;
+    const size_t npix = (size_t)H * W, oE = (size_t)s0 * E, oT = (size_t)s0 * ND * E;
+    const int nc = mean_integral_chunks(ns, (int)npix);
+    double* sums = (double*)workspace(W_PARTSUM, sizeof(double) * (size_t)ns * nc * E + 8);
+    if (!sums) return XTS_ERR_OOM;
+    float* out = (float*)a.out + (size_t)s0 * npix * E;
+    int rc = launch_mean_integral(centers, omega, info + s0, out, ns, H, W, E, nc, sums, st);
+    if (rc) return rc;
+    XTS_LAUNCH("k_correction", st, k_correction_sums<<<ns, 128, 0, st>>>(
+                                       sums, nc, info + s0, a.upsf + oT, a.partial + oT, a.exposure + oE, E, scale + oE,
+                                       a.inv_integ ? a.inv_integ + oE : nullptr, a.correction ? a.correction + oE : nullptr,
+                                       a.radius ? a.radius + s0 : nullptr, a.in_fov ? a.in_fov + s0 : nullptr));
+    return launch_scale_map(out, omega, scale + oE, ns, (int)npix, E, st);
+}
+
 int finish_mean_map(const SrcmapDev& a, const double* centers, const double* omega, const SrcInfo* info,
                     double* scale, int nch, cudaStream_t st) {
-    const int H = (int)a.wcs.naxis1, W = (int)a.wcs.naxis2, S = a.S, E = a.E;
-    nch = mean_integral_chunks(S, H * W);
-    double* sums = (double*)workspace(W_PARTSUM, sizeof(double) * (size_t)S * nch * E + 8);
-    if (!sums) return XTS_ERR_OOM;
-    int rc = launch_mean_integral(centers, omega, info, (const float*)a.out, S, H, W, E, nch, sums, st);
-    if (rc) return rc;
-    XTS_LAUNCH("k_correction", st, k_correction_sums<<<S, 128, 0, st>>>(sums, nch, info, a.upsf, a.partial,
-                                                                        a.exposure, E, scale, a.inv_integ,
-                                                                        a.correction, a.radius, a.in_fov));
-    return launch_scale_map((float*)a.out, omega, scale, S, H * W, E, st);
+    (void)nch;
+    return finish_mean_map_range(a, 0, a.S, centers, omega, info, scale, st);
 }
 
 int srcmap_status(cudaStream_t st) {

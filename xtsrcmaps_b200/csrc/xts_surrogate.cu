@@ -603,26 +603,42 @@ int launch_srcmap_surrogate(const SrcmapDev& a, const double* corners, const dou
         XTS_LAUNCH("k_sur_fallback", st, k_sur_fallback<<<(unsigned)(4 * nsm), 128, 0, st>>>(
                                               corners, info, a.upsf, list_d, list_n, H, W, E, mean));
     }
-    for (int s0 = 0; s0 < S; s0 += sc) {
-        const int ns = S - s0 < sc ? S - s0 : sc;
-        const long long n = per_src * ns;
-        const dim3 gf((unsigned)((npix + SF_PIX - 1) / SF_PIX), (unsigned)ns);
-        XTS_CUDA(cudaMemsetAsync(counts + 1, 0, sizeof(unsigned long long), st));
-        XTS_LAUNCH("k_sur_segments", st, k_sur_segments<<<(unsigned)(4 * nsm), 256, 0, st>>>(
-                                             a.upsf + (size_t)s0 * ND * E, a.logEs, ns, E, rg, seg, slope));
-        XTS_LAUNCH("k_sur_features", st, k_sur_features<<<gf, SF_THREADS, 0, st>>>(
-                                             corners, info, a.upsf, a.logEs, s0, H, W, E, rg, X, aux, vidx,
-                                             counts + 1, acc_d, seg, slope, nmax));
-        // the network on the compacted rows; their count stays on the device
-        if ((rc = launch_mlp_forward_dev(net, X, counts + 1, n, yv, status, st, nmax))) return rc;
-        float* m0 = mean + (size_t)s0 * per_src;
-        XTS_LAUNCH("k_sur_assemble", st, k_sur_assemble<<<(unsigned)(8 * nsm), 256, 0, st>>>(
-                                             aux, vidx, yv, counts + 1, n, s0, per_src, E, m0, err, chk_d));
+    // With host copy-out hooks (a host-mode call), the sources go in groups of about
+    // a.chunk_sources: each group is finished (failed maps redone, map integral,
+    // correction, scaling) and handed to the hook, so its copy to the host overlaps
+    // the next group's work.  Without hooks, one group.
+    const int gsz = a.on_chunk && a.chunk_sources > 0 ? a.chunk_sources : S;
+    for (int g0 = 0; g0 < S; g0 += gsz) {
+        const int g1 = S - g0 < gsz ? S : g0 + gsz;
+        for (int s0 = g0; s0 < g1; s0 += sc) {
+            const int ns = g1 - s0 < sc ? g1 - s0 : sc;
+            const long long n = per_src * ns;
+            const dim3 gf((unsigned)((npix + SF_PIX - 1) / SF_PIX), (unsigned)ns);
+            XTS_CUDA(cudaMemsetAsync(counts + 1, 0, sizeof(unsigned long long), st));
+            XTS_LAUNCH("k_sur_segments", st, k_sur_segments<<<(unsigned)(4 * nsm), 256, 0, st>>>(
+                                                 a.upsf + (size_t)s0 * ND * E, a.logEs, ns, E, rg, seg, slope));
+            XTS_LAUNCH("k_sur_features", st, k_sur_features<<<gf, SF_THREADS, 0, st>>>(
+                                                 corners, info, a.upsf, a.logEs, s0, H, W, E, rg, X, aux, vidx,
+                                                 counts + 1, acc_d, seg, slope, nmax));
+            // the network on the compacted rows; their count stays on the device
+            if ((rc = launch_mlp_forward_dev(net, X, counts + 1, n, yv, status, st, nmax))) return rc;
+            float* m0 = mean + (size_t)s0 * per_src;
+            XTS_LAUNCH("k_sur_assemble", st, k_sur_assemble<<<(unsigned)(8 * nsm), 256, 0, st>>>(
+                                                 aux, vidx, yv, counts + 1, n, s0, per_src, E, m0, err, chk_d));
+        }
+        // the group's maps whose check failed are redone by the rule, listed and
+        // scheduled on the device
+        const int gn = g1 - g0;
+        XTS_LAUNCH("k_sur_fail_list", st, k_sur_fail_list<<<1, 32, 0, st>>>(err + g0, gn, (float)a.check_tol, list_d,
+                                                                            list_n));
+        XTS_LAUNCH("k_sur_fallback", st, k_sur_fallback<<<(unsigned)(4 * nsm), 128, 0, st>>>(
+                                              corners, info + g0, a.upsf + (size_t)g0 * ND * E, list_d, list_n, H, W,
+                                              E, mean + (size_t)g0 * per_src));
+        if (gsz < S) {
+            if ((rc = finish_mean_map_range(a, g0, gn, centers, omega, info, scale, st))) return rc;
+            if ((rc = a.on_chunk(a.on_chunk_ctx, g0, gn, st))) return rc;
+        }
     }
-    // maps whose check failed are redone by the rule, listed and scheduled on the device
-    XTS_LAUNCH("k_sur_fail_list", st, k_sur_fail_list<<<1, 32, 0, st>>>(err, S, (float)a.check_tol, list_d, list_n));
-    XTS_LAUNCH("k_sur_fallback", st, k_sur_fallback<<<(unsigned)(4 * nsm), 128, 0, st>>>(
-                                          corners, info, a.upsf, list_d, list_n, H, W, E, mean));
     g_sur_last.valid = true;
     g_sur_last.S = S;
     g_sur_last.per_src = per_src;
@@ -632,6 +648,7 @@ int launch_srcmap_surrogate(const SrcmapDev& a, const double* corners, const dou
     g_sur_last.chk = chk_d;
     g_sur_last.status = status;
     if (a.sur_stats && (rc = surrogate_last_stats(a.sur_stats, st))) return rc;
+    if (gsz < S) return XTS_OK;
     return finish_mean_map(a, centers, omega, info, scale, nch, st);
 }
 
