@@ -192,15 +192,6 @@ struct SurRange {
 };
 constexpr int SUR_NCELL = XTS_MLP_CELL_NR * XTS_MLP_CELL_NS;
 
-// Whether the value's error cell (log10 rho, segment slope) is one the network was
-// calibrated to meet its bound in; cells: [NCELL] in shared memory (NULL: all).
-__device__ __forceinline__ bool sur_cell_ok(const SurRange& rg, const unsigned char* cells, float f0, float sl) {
-    if (!cells) return true;
-    const float a = (f0 - rg.c0) * rg.cs0, b = (sl - rg.c1) * rg.cs1;
-    if (!(a >= 0.f && a < (float)XTS_MLP_CELL_NR && b >= 0.f && b < (float)XTS_MLP_CELL_NS)) return false;
-    return cells[(int)a * XTS_MLP_CELL_NS + (int)b] != 0;
-}
-
 __device__ __forceinline__ const unsigned char* sur_cells_to_shared(const SurRange& rg, unsigned char* sh) {
     if (!rg.cell_ok) return nullptr;
     for (int k = threadIdx.x; k < SUR_NCELL; k += blockDim.x) sh[k] = rg.cell_ok[k];
@@ -253,19 +244,11 @@ __device__ __forceinline__ bool sur_geo_ok(const SurPix& q, const SurRange& rg) 
            q.f2 >= rg.lo[2] && q.f2 <= rg.hi[2];
 }
 
-// Centre value and segment slope of one energy, and whether the network takes the value.
-__device__ __forceinline__ bool sur_value(const double* U, int E, int e, int ic, double tc, bool geo_ok, float f0,
-                                          float le, const SurRange& rg, const unsigned char* cells, double* uc,
-                                          float* sl) {
-    const double lo = U[(size_t)(ic - 1) * E + e], hi = U[(size_t)ic * E + e];
-    *uc = (1.0 - tc) * lo + tc * hi;
-    *sl = sur_slope(lo, hi);
-    return geo_ok && *uc > 0. && le >= rg.lo[3] && le <= rg.hi[3] && *sl >= rg.lo[4] && *sl <= rg.hi[4] &&
-           sur_cell_ok(rg, cells, f0, *sl);
-}
-
-// Pixels of a chunk the check evaluates by the rule: every SUR_CHECK_EVERY-th.
-__device__ __forceinline__ bool sur_checked(int pix) { return pix % SUR_CHECK_EVERY == 0; }
+// The network takes a value iff its pixel's geometric features lie in the training
+// range (rho >= rho_min among them), the centre value u_c = (1 - tc) U[ic - 1] + tc U[ic]
+// is positive, log10 E and the log slope of the centre's table segment lie in range, and
+// the error cell (log10 rho, slope) is one the network was calibrated to serve: the pixel
+// part is phase 1's crow, the (segment, energy) part k_sur_segments' code.
 
 // Per block: SF_PIX pixels of one source of a chunk.  Phase 1, one thread per
 // pixel: the centre and the features that do not depend on energy, into shared
