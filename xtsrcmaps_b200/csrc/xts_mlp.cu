@@ -480,7 +480,10 @@ k_mlp_infer(const float* __restrict__ params, const __nv_bfloat16* __restrict__ 
                 mma_chain(tmem, s_act, layer == 2 ? s_w2 : s_w3, MH / 16, false);
                 mma_commit(bar);
             }
-            const bool got = mbar_wait(bar, ph);
+            // one warp of the group polls the MMA's mbarrier; the other three sleep in the
+            // group's barrier instead of spinning (their issue slots go to the other groups)
+            bool got = true;
+            if ((warp & 3) == 0) got = mbar_wait(bar, ph);
             if (!group_and(g, got)) { ok = false; break; }  // ph stays: the exit path waits on it
             ph ^= 1;
             tc_fence_after();
