@@ -609,6 +609,8 @@ def run_ours(args, rank, world, local_rank):
                    "output_dtype": "float32", "launch": launch, "headline_path": head},
         "plain_value": val["plain"], "plain_ms_per_step": ms["plain"] / args.steps,
         "surrogate_vs_plain": (val[head] / val["plain"]) if net is not None else None,
+        "source_pixel_rates": {"unit": "(source, pixel) pairs/s (all E energies of a pixel)",
+                               "value": val[head] / E, "plain": val["plain"] / E},
         "roofline": roofline, "roofline_write_pass": roof_write, "roofline_plain_path": roofline_plain_path,
         "dominant_kernel": dominant_of(head), "dominant_kernel_plain": dominant_of("plain"),
         "kernels": kernels_of(head), "kernels_plain": kernels_of("plain"), "gpu_launches": gpu_launches,
@@ -926,7 +928,7 @@ def _reference_runner(job):
     desc = (f"the reference's compiled exposure, mean-PSF and model-map code (oracle/_ref), OpenMP with "
             f"{threads} threads; its source loops use schedule(static, 16), so {busy} thread(s) share "
             f"the {job.S} sources")
-    return (lambda: reference_pipeline(job, setup)), threads, desc
+    return (lambda times=None: reference_pipeline(job, setup, times=times)), threads, desc
 
 
 def _source_sample(job, max_sources: int):
@@ -960,15 +962,22 @@ def cpu_baseline(job, max_sources: int = 256, warm: bool = True):
         threads = min(threads, (sub.S + 15) // 16)
     if warm:
         run()
+    times = {}
     t0 = time.perf_counter()
     reps = 0
     while reps < 1 or (time.perf_counter() - t0 < 10.0 and reps < 20):
-        run()
+        if kind == "reference":
+            run(times)
+        else:
+            run()
         reps += 1
     dt = (time.perf_counter() - t0) / reps
-    return {"value": sub.n_values / dt, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"{sub.S} of the job's {job.S} sources ({job.wcs.naxis1}x{job.wcs.naxis2}, {job.E} energies; "
-                      f"{sub.n_values:.3g} values) {reps} time(s): {desc}; rate scales with values"}
+    res = {"value": sub.n_values / dt, "unit": UNIT, "cores": threads, "kind": kind,
+           "sample": f"{sub.S} of the job's {job.S} sources ({job.wcs.naxis1}x{job.wcs.naxis2}, {job.E} energies; "
+                     f"{sub.n_values:.3g} values) {reps} time(s): {desc}; rate scales with values"}
+    if times:
+        res["seconds_per_pass"] = {k: v / reps for k, v in times.items()}
+    return res
 
 
 def run_reference(args, rank, world):

@@ -34,24 +34,34 @@ def irf_setup(job):
     return ltf, normalized(job.rpsf_front, job.scale_front), normalized(job.rpsf_back, job.scale_back)
 
 
-def reference_pipeline(job, setup=None, with_map: bool = True):
+def reference_pipeline(job, setup=None, with_map: bool = True, times=None):
     """The same steps through the reference's own code compiled under oracle/_ref
     (oracle/oracle_ref.py): exposure, mean PSF and the model map.  The effective
     area tables come from the oracle's restatement of Irf::aeff_value, whose
-    reference translation unit needs <mdspan>."""
+    reference translation unit needs <mdspan>.  times (a dict) accumulates the
+    seconds of compute_exposure, compute_psf_data and point_src_model_map_wcs."""
+    import time
+
     from oracle import oracle_ref as R
 
     ltf, nf, nb = setup if setup is not None else irf_setup(job)
     cube, wcube = job.exp_cube, job.wexp_cube
+    t0 = time.perf_counter()
     cos = O.costhetas(cube.nbrbins, cube.cosmin, cube.thetabin)
     af = O.aeff_value(cos, job.logEs, job.aeff_front)
     ab = O.aeff_value(cos, job.logEs, job.aeff_back)
     cos, ecb, wecb, expo = R.exposure(cube.cosbins, wcube.cosbins, cube.nside, cube.cosmin, cube.thetabin,
                                       job.src_sph, af, ab, ltf)
+    t1 = time.perf_counter()
     upsf, partial = R.psf(nf, nb, cos, job.logEs, af, ab, ecb, wecb, ltf, expo)
+    t2 = time.perf_counter()
     out = dict(costh=cos, ecb=ecb, wecb=wecb, af=af, ab=ab, ltf=ltf, exposure=expo, upsf=upsf, partial=partial)
     if with_map:
         out["map"] = R.point_src_model_map_wcs(job.wcs, job.src_sph, expo, upsf, partial)
+    t3 = time.perf_counter()
+    if times is not None:
+        for k, v in (("compute_exposure", t1 - t0), ("compute_psf_data", t2 - t1), ("point_src_model_map_wcs", t3 - t2)):
+            times[k] = times.get(k, 0.0) + v
     return out
 
 
