@@ -113,7 +113,8 @@ int         xts_version(void);
  * misc/simdwidth.hpp).  0 in a field keeps its default.  Applies to the calls made
  * after it on every device of the process. */
 typedef struct xts_tuning {
-    int window_blocks_per_sm; /* window pass of the dense map (one persistent wave): blocks per SM
+    int window_blocks_per_sm; /* window pass of the dense map: its work items (one block each) are
+                                 sized for about 16 per block at this many resident blocks per SM
                                  (1..4; default: as many as fit) */
     int write_blocks_per_sm;  /* write pass: persistent blocks per SM (1..2; default: as many as fit) */
     int queue_blocks_per_sm;  /* cutout window pass (work queue): blocks per SM (1..4; default: as many as fit) */

@@ -38,7 +38,9 @@ struct Ctx {
     cudaStream_t stream = nullptr;
     cudaStream_t copy_stream = nullptr;    // device-to-host copies of finished map chunks
     cudaStream_t geo_stream = nullptr;     // map geometry of the fused call, beside exposure and PSF
+    cudaStream_t prio_stream = nullptr;    // exposure and PSF of the fused call, at the highest priority
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    cudaEvent_t pfork_ev = nullptr, pjoin_ev = nullptr;
     cudaEvent_t pipe_a[2] = {}, pipe_b[2] = {};  // chunk pipeline of the window path
     cudaEvent_t chunk_ev[N_CHUNK_EV] = {};
     void* buf[N_SLOTS] = {};
@@ -67,8 +69,15 @@ int ensure_device() {
     XTS_CUDA(cudaStreamCreateWithFlags(&g_ctx.stream, cudaStreamNonBlocking));
     if (!g_ctx.copy_stream) XTS_CUDA(cudaStreamCreateWithFlags(&g_ctx.copy_stream, cudaStreamNonBlocking));
     if (!g_ctx.geo_stream) XTS_CUDA(cudaStreamCreateWithFlags(&g_ctx.geo_stream, cudaStreamNonBlocking));
+    if (!g_ctx.prio_stream) {
+        int least = 0, greatest = 0;
+        XTS_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        XTS_CUDA(cudaStreamCreateWithPriority(&g_ctx.prio_stream, cudaStreamNonBlocking, greatest));
+    }
     if (!g_ctx.fork_ev) XTS_CUDA(cudaEventCreateWithFlags(&g_ctx.fork_ev, cudaEventDisableTiming));
     if (!g_ctx.join_ev) XTS_CUDA(cudaEventCreateWithFlags(&g_ctx.join_ev, cudaEventDisableTiming));
+    if (!g_ctx.pfork_ev) XTS_CUDA(cudaEventCreateWithFlags(&g_ctx.pfork_ev, cudaEventDisableTiming));
+    if (!g_ctx.pjoin_ev) XTS_CUDA(cudaEventCreateWithFlags(&g_ctx.pjoin_ev, cudaEventDisableTiming));
     for (int i = 0; i < 2; ++i) {
         if (!g_ctx.pipe_a[i]) XTS_CUDA(cudaEventCreateWithFlags(&g_ctx.pipe_a[i], cudaEventDisableTiming));
         if (!g_ctx.pipe_b[i]) XTS_CUDA(cudaEventCreateWithFlags(&g_ctx.pipe_b[i], cudaEventDisableTiming));
@@ -378,8 +387,11 @@ int xts_init(int device) {
     if (g_ctx.stream) { cudaStreamDestroy(g_ctx.stream); g_ctx.stream = nullptr; }
     if (g_ctx.copy_stream) { cudaStreamDestroy(g_ctx.copy_stream); g_ctx.copy_stream = nullptr; }
     if (g_ctx.geo_stream) { cudaStreamDestroy(g_ctx.geo_stream); g_ctx.geo_stream = nullptr; }
+    if (g_ctx.prio_stream) { cudaStreamDestroy(g_ctx.prio_stream); g_ctx.prio_stream = nullptr; }
     if (g_ctx.fork_ev) { cudaEventDestroy(g_ctx.fork_ev); g_ctx.fork_ev = nullptr; }
     if (g_ctx.join_ev) { cudaEventDestroy(g_ctx.join_ev); g_ctx.join_ev = nullptr; }
+    if (g_ctx.pfork_ev) { cudaEventDestroy(g_ctx.pfork_ev); g_ctx.pfork_ev = nullptr; }
+    if (g_ctx.pjoin_ev) { cudaEventDestroy(g_ctx.pjoin_ev); g_ctx.pjoin_ev = nullptr; }
     for (int i = 0; i < 2; ++i) {
         if (g_ctx.pipe_a[i]) { cudaEventDestroy(g_ctx.pipe_a[i]); g_ctx.pipe_a[i] = nullptr; }
         if (g_ctx.pipe_b[i]) { cudaEventDestroy(g_ctx.pipe_b[i]); g_ctx.pipe_b[i] = nullptr; }
@@ -889,8 +901,18 @@ static int fused_maps(const xts_expcube* cube, const xts_expcube* wcube, const d
     }
     if (fork) { ma.geo_stream = g_ctx.geo_stream; ma.join_ev = g_ctx.join_ev; }
     int rc = sg.rc;
-    if (rc == XTS_OK) rc = launch_exposure(ea, sg.st);
-    if (rc == XTS_OK) rc = launch_psf(pa, sg.st);
+    // exposure and mean PSF on the library's highest-priority stream: the window pass
+    // (one short block per work item, on the geometry stream) fills the GPU, and these
+    // kernels' blocks are then scheduled ahead of its pending ones as slots free up
+    if (rc == XTS_OK) {
+        cudaStream_t ps = g_ctx.prio_stream;
+        XTS_CUDA(cudaEventRecord(g_ctx.pfork_ev, sg.st));
+        XTS_CUDA(cudaStreamWaitEvent(ps, g_ctx.pfork_ev, 0));
+        rc = launch_exposure(ea, ps);
+        if (rc == XTS_OK) rc = launch_psf(pa, ps);
+        XTS_CUDA(cudaEventRecord(g_ctx.pjoin_ev, ps));
+        XTS_CUDA(cudaStreamWaitEvent(sg.st, g_ctx.pjoin_ev, 0));
+    }
     if (rc != XTS_OK) {
         if (fork) StreamJoin{g_ctx.geo_stream, sg.st, g_ctx.join_ev}.join();
         return sg.finish(rc);

@@ -328,52 +328,47 @@ __device__ __forceinline__ double boundary_chord2(const SrcInfo& si) {
     return c * c;
 }
 
-// The dense map, one persistent wave over a work queue: item (g, p) is part p of
-// the P parts of group g (NSG sources; tiles [p nt / P, (p + 1) nt / P) of WT pixels).
-// A block takes the next item (one atomic), forms each pixel's source-independent
-// geometry once and the windows of the group's sources from it, and adds the item's
-// non-zero rows to hist_out[s] (cleared before the launch) with FP64 atomics.
+// The dense map: block b takes item b = (g, p), part p of the P parts of group g (NSG
+// sources; tiles [p nt / P, (p + 1) nt / P) of WT pixels), forms each pixel's
+// source-independent geometry once and the windows of the group's sources from it,
+// and adds the item's non-zero rows to hist_out[s] (cleared before the launch) with
+// FP64 atomics.  Items are small (about 16 per resident block), so blocks retire
+// steadily: the hardware balances them, and kernels of a higher-priority stream
+// (exposure and PSF beside this pass) get their slots as they free up.
 __global__ void __launch_bounds__(WT, 3) k_pixel_windows(const double* __restrict__ corners, const double* __restrict__ centers,
                                                       const double* __restrict__ omega, const SrcInfo* __restrict__ info,
                                                       const SepTab* __restrict__ septab, int S, int H, int W,
-                                                      int P, unsigned* __restrict__ queue,
+                                                      int P,
                                                       double* __restrict__ hist_out, float4* __restrict__ rec,
                                                       float4* __restrict__ ext, float2* __restrict__ sparse,
                                                       int sparse_cap, int* __restrict__ sparse_count) {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ int item_s;
     const PassA A = pass_a_tables(smem, septab, rec, ext, sparse, sparse_cap, sparse_count);
     SrcInfo* ssrc = (SrcInfo*)(smem + WA_OFF_SRC);
     const int t = threadIdx.x;
     const int npix = H * W, W1 = W + 1;
     const int nt = (npix + WT - 1) / WT;
-    const int ng = (S + NSG - 1) / NSG, n_items = ng * P;
-    for (;;) {
-        if (t == 0) item_s = (int)atomicAdd(queue, 1u);
-        __syncthreads();  // also: the previous item's rows are written out
-        const int item = item_s;
-        if (item >= n_items) break;
-        const int g = item / P, p = item - g * P, s0 = g * NSG, ns = min(NSG, S - s0);
-        if (t < ns) ssrc[t] = info[s0 + t];
-        for (int r = t; r < NSG * ND; r += WT) A.hist[r] = 0.;
-        __syncthreads();
-        const int ta = (int)((long long)p * nt / P), tb = (int)((long long)(p + 1) * nt / P);
-        for (int tile = ta; tile < tb; ++tile) {
-            const int pix = tile * WT + t;
-            if (pix >= npix) continue;
-            const int h = pix / W, w = pix - h * W;
-            const PixBase Q = pixel_base(corners, centers, omega, W1, h, w, (size_t)pix);
-            for (int j = 0; j < ns; ++j) {
-                const SrcInfo& si = ssrc[j];
-                window_source(Q, si, boundary_chord2(si), corners, W1, h, w, (size_t)(s0 + j) * npix + pix, A,
-                              A.hist + j * ND, nullptr, nullptr);
-            }
+    const int item = blockIdx.x;
+    const int g = item / P, p = item - g * P, s0 = g * NSG, ns = min(NSG, S - s0);
+    if (t < ns) ssrc[t] = info[s0 + t];
+    for (int r = t; r < NSG * ND; r += WT) A.hist[r] = 0.;
+    __syncthreads();
+    const int ta = (int)((long long)p * nt / P), tb = (int)((long long)(p + 1) * nt / P);
+    for (int tile = ta; tile < tb; ++tile) {
+        const int pix = tile * WT + t;
+        if (pix >= npix) continue;
+        const int h = pix / W, w = pix - h * W;
+        const PixBase Q = pixel_base(corners, centers, omega, W1, h, w, (size_t)pix);
+        for (int j = 0; j < ns; ++j) {
+            const SrcInfo& si = ssrc[j];
+            window_source(Q, si, boundary_chord2(si), corners, W1, h, w, (size_t)(s0 + j) * npix + pix, A,
+                          A.hist + j * ND, nullptr, nullptr);
         }
-        __syncthreads();
-        for (int r = t; r < ns * ND; r += WT) {
-            const double v = A.hist[r];
-            if (v != 0.) atomicAdd(hist_out + (size_t)s0 * ND + r, v);
-        }
+    }
+    __syncthreads();
+    for (int r = t; r < ns * ND; r += WT) {
+        const double v = A.hist[r];
+        if (v != 0.) atomicAdd(hist_out + (size_t)s0 * ND + r, v);
     }
 }
 
@@ -807,8 +802,8 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
     int dev = 0, nsm = 148, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    // pass A: one persistent wave (at most window_blocks_per_sm blocks per SM) over
-    // a work queue of about 8 items per block
+    // pass A: one block per work item, items sized for about 16 per block of the
+    // resident set (at most window_blocks_per_sm blocks per SM)
     int resident = 0;
     XTS_CUDA(cudaFuncSetAttribute(k_pixel_windows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WA_SMEM));
     XTS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_pixel_windows, WT, WA_SMEM));
@@ -838,16 +833,12 @@ int launch_srcmap_win(const double* corners, const double* centers, const double
         // the window pass is geometry only: it runs on the geometry stream, once
         // the write pass that last read its buffers is done
         if (pipe && k >= 2) XTS_CUDA(cudaStreamWaitEvent(gs, evB[b], 0));
-        // the chunk's queue counter sits next to its sparse-record count
-        unsigned* queue = (unsigned*)(status + 3 + b);
-        const int n_items = (n + NSG - 1) / NSG * nparts;
-        const int Gw = n_items < resident * nsm ? n_items : resident * nsm;
+        const int n_items = (n + NSG - 1) / NSG * nparts;  // one block per item
         XTS_CUDA(cudaMemsetAsync(sparse_count, 0, sizeof(int), gs));
-        XTS_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned), gs));
         XTS_CUDA(cudaMemsetAsync(hist, 0, sizeof(double) * (size_t)n * ND, gs));
-        XTS_LAUNCH("k_pixel_windows", gs, k_pixel_windows<<<Gw, WT, WA_SMEM, gs>>>(
+        XTS_LAUNCH("k_pixel_windows", gs, k_pixel_windows<<<n_items, WT, WA_SMEM, gs>>>(
                                               corners, centers, means_only ? nullptr : omega, info + s0, tab, n, H, W,
-                                              nparts, queue,
+                                              nparts,
                                               hist, rec, ext, sparse, (int)cap,
                                               sparse_count));
         if (pipe) {
