@@ -3,7 +3,7 @@
 // Linear Units", 2016: gelu(z) = z/2 (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3)))),
 // its forward pass, its gradient and an Adam update (Kingma & Ba, 2015).
 //
-// The two 128 x 128 layers run on tcgen05 tensor cores: BF16 operands in shared
+// The three hidden layers run on tcgen05 tensor cores: BF16 operands in shared
 // memory (K-major, 128-byte swizzle: a [128 rows][64] BF16 atom is 16 KB, rows
 // of 128 bytes whose 16-byte chunks are permuted by row & 7, 8-row groups 1024
 // bytes apart), one thread issuing tcgen05.mma.kind::f16 (M = N = 128, K = 16)
@@ -12,10 +12,11 @@
 //
 //   * k_mlp_forward: one tile of 128 rows per step of a persistent loop, two
 //     blocks of two warpgroups per SM (each row's 128 columns split between two
-//     threads).  Layer 1 (K = 5) and the GELUs on CUDA cores; each hidden layer's
-//     BF16 activations are written by their row's threads straight into the
-//     swizzled A operand of the next MMA; the output layer is a per-row dot
-//     product.  For training it
+//     threads).  Layer 1 (K = 5) is one K = 16 MMA over the features split into
+//     three BF16 terms; the GELUs run on CUDA cores; each hidden layer's BF16
+//     activations are written by their row's threads straight into the swizzled
+//     A operand of the next MMA; the output layer is a per-row dot product.  For
+//     training it
 //     also writes the pre-activations z1..z3 and the activations h1, h2,
 //     transposed ([128][n], coalesced across the threads of a warp).
 //   * k_gemm_bf16: C = A B^T for the backward pass (dW = dZ^T H, dH = dZ W), with
@@ -61,28 +62,32 @@ __device__ __forceinline__ float tanh_fast(float x) {
     asm("tanh.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
 }
-constexpr float GK0 = 0.7978845608028654f;  // sqrt(2 / pi)
-constexpr float GK1 = 0.044715f;
+constexpr float GK0 = 0.7978845608028654f;   // sqrt(2 / pi)
+constexpr float GK1 = 0.035677408136300125f; // sqrt(2 / pi) * 0.044715
+// the tanh argument sqrt(2/pi) (z + 0.044715 z^3) as z (GK0 + GK1 z^2): two multiplies and
+// one FMA
+__device__ __forceinline__ float gelu_arg(float z) { return z * fmaf(z * z, GK1, GK0); }
 __device__ __forceinline__ float gelu(float z) {
-    return 0.5f * z * (1.f + tanh_fast(GK0 * fmaf(GK1 * z * z, z, z)));
+    return 0.5f * z * (1.f + tanh_fast(gelu_arg(z)));
+}
+__device__ __forceinline__ float2 gelu_arg2(float2 z) {
+    return __fmul2_rn(z, __ffma2_rn(__fmul2_rn(z, z), make_float2(GK1, GK1), make_float2(GK0, GK0)));
 }
 // two GELUs with packed FP32 arithmetic (same formula as gelu, rounding order differs)
 __device__ __forceinline__ float2 gelu2(float2 z) {
-    const float2 t = __ffma2_rn(make_float2(GK1, GK1), __fmul2_rn(z, z), make_float2(1.f, 1.f));
-    const float2 u = __fmul2_rn(__fmul2_rn(make_float2(GK0, GK0), z), t);
+    const float2 u = gelu_arg2(z);
     const float2 hz = __fmul2_rn(make_float2(0.5f, 0.5f), z);
     return __ffma2_rn(hz, make_float2(tanh_fast(u.x), tanh_fast(u.y)), hz);
 }
 // 2 gelu(z) for two values: the same rounding as gelu2 scaled by 2 (exact), one
 // multiply fewer; the inference kernel halves the next layer's weights to match
 __device__ __forceinline__ float2 gelu2x(float2 z) {
-    const float2 t = __ffma2_rn(make_float2(GK1, GK1), __fmul2_rn(z, z), make_float2(1.f, 1.f));
-    const float2 u = __fmul2_rn(__fmul2_rn(make_float2(GK0, GK0), z), t);
+    const float2 u = gelu_arg2(z);
     return __ffma2_rn(z, make_float2(tanh_fast(u.x), tanh_fast(u.y)), z);
 }
 __device__ __forceinline__ float gelu_grad(float z) {
-    const float z2 = z * z, th = tanh_fast(GK0 * fmaf(GK1 * z2, z, z));
-    return 0.5f * (1.f + th) + 0.5f * z * (1.f - th * th) * GK0 * fmaf(3.f * GK1, z2, 1.f);
+    const float z2 = z * z, th = tanh_fast(z * fmaf(z2, GK1, GK0));
+    return 0.5f * (1.f + th) + 0.5f * z * (1.f - th * th) * fmaf(3.f * GK1, z2, GK0);
 }
 
 // byte offset of element (r, k) of a [128][K] BF16 operand made of [128][64] atoms
@@ -112,6 +117,60 @@ __device__ __forceinline__ void mma_chain(unsigned tmem, unsigned a, unsigned b,
     }
 }
 
+// K-major without swizzle (layer 1's W1 operand, K = 16): core matrices of 8 rows x 16
+// bytes, the two along K (leading byte offset) 128 bytes apart, 8-row groups (stride
+// byte offset) 256 bytes apart; version 1, layout type 0
+static __device__ __forceinline__ unsigned long long m_desc_ns(unsigned addr) {
+    return (unsigned long long)((addr >> 4) & 0x3FFF) | ((unsigned long long)(128 >> 4) << 16) |
+           ((unsigned long long)(256 >> 4) << 32) | (1ull << 46);
+}
+// byte offset of element (r, k) of that [128][16] BF16 operand
+__device__ __forceinline__ unsigned ns_off(int r, int k) {
+    return (unsigned)((r >> 3) * 256 + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+constexpr int W1OP = MH * 16 * 2;  // bytes of the W1 operand
+
+// Layer 1 on the tensor cores.  A row of A holds the standardised features split into
+// three BF16 terms, x = hi + mid + lo (each difference exact in FP32, so the sum
+// equals x to 2^-27 relative), at K = 0..4, 5..9, 10..14; B holds W1 (already BF16)
+// three times over, so one K = 16 MMA forms W1 x with every product exact.
+__device__ __forceinline__ void fill_w1_operand(unsigned char* dst, const float* params, int t, int nt) {
+    for (int e = t; e < MH * 16; e += nt) {
+        const int j = e >> 4, k = e & 15;
+        const __nv_bfloat16 w = k < 3 * MI ? __float2bfloat16_rn(params[XTS_MLP_W1 + j * MI + k % MI])
+                                           : __float2bfloat16_rn(0.f);
+        *reinterpret_cast<__nv_bfloat16*>(dst + ns_off(j, k)) = w;
+    }
+}
+__device__ __forceinline__ void store_x_split(unsigned char* act, int r, const float* x) {
+    unsigned short e[16];
+#pragma unroll
+    for (int k = 0; k < MI; ++k) {
+        const __nv_bfloat16 hi = __float2bfloat16_rn(x[k]);
+        const float r1 = x[k] - __bfloat162float(hi);
+        const __nv_bfloat16 mid = __float2bfloat16_rn(r1);
+        const __nv_bfloat16 lo = __float2bfloat16_rn(r1 - __bfloat162float(mid));
+        e[k] = __bfloat16_as_ushort(hi);
+        e[MI + k] = __bfloat16_as_ushort(mid);
+        e[2 * MI + k] = __bfloat16_as_ushort(lo);
+    }
+    e[15] = 0;
+    uint4 q[2];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        reinterpret_cast<unsigned*>(q)[i] = (unsigned)e[2 * i] | ((unsigned)e[2 * i + 1] << 16);
+    }
+    *reinterpret_cast<uint4*>(act + sw_off(r, 0)) = q[0];
+    *reinterpret_cast<uint4*>(act + sw_off(r, 8)) = q[1];
+}
+// the layer-1 MMA: A = K columns 0..15 of the swizzled activation operand, B = W1
+__device__ __forceinline__ void mma_layer1(unsigned tmem, unsigned a, unsigned w1op) {
+    const unsigned long long da = m_desc(a), db = m_desc_ns(w1op);
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n"
+                 :: "r"(tmem), "l"(da), "l"(db), "r"(M_IDESC), "r"(0u), "r"(0u));
+}
+
 __device__ __forceinline__ void mma_commit(unsigned bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" :: "r"(bar) : "memory");
 }
@@ -126,6 +185,21 @@ __device__ __forceinline__ void tmem_ld16(unsigned taddr, float* v) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
     for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+// the same load without its wait, for a load kept in flight while other columns are
+// worked on; tmem_ld_done waits for every load issued so far and ties r to that wait
+__device__ __forceinline__ void tmem_ld16_issue(unsigned taddr, unsigned* r) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                 : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_ld_done(unsigned* r) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    // no use of r may be moved above the wait
+    asm volatile("" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                      "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]));
 }
 
 __device__ __forceinline__ unsigned pack_bf16(float a, float b) {
@@ -149,11 +223,10 @@ __device__ __forceinline__ void tmem_free(unsigned tmem, unsigned ncols) {
 constexpr int FT = 2 * MT;  // forward threads: two warpgroups, each row's 128 columns split in halves
 
 struct FwdLayout {
-    static constexpr size_t w2 = 0, w3 = 2 * ATOM, act = 4 * ATOM;
-    // W1 transposed [5][128] and b1 [128] (six rows of 128), then 2 rows of padding, b2, b3,
-    // w4 [128], b4 (+3), partial y [128]
-    static constexpr size_t f32 = 6 * ATOM;
-    static constexpr size_t bars = f32 + 4 * (MH * 8 + 3 * MH + 4 + MT);
+    static constexpr size_t w2 = 0, w3 = 2 * ATOM, act = 4 * ATOM, w1 = 6 * ATOM;
+    // b1, b2, b3, w4 [128 each], b4 (+3), partial y [128]
+    static constexpr size_t f32 = w1 + W1OP;
+    static constexpr size_t bars = f32 + 4 * (4 * MH + 4 + MT);
     static constexpr size_t total = bars + 64;
 };
 constexpr size_t FWD_SMEM = FwdLayout::total + 1024;
@@ -166,7 +239,8 @@ struct FwdSaves {  // training only; all NULL for inference
 
 // Thread t works on row r = t & 127 of the tile and hidden columns [64 hf, 64 hf + 64),
 // hf = t >> 7: warp w reads tensor-memory lanes 32 (w & 3).. and, in the A operand,
-// writes the [128][64] atom hf of its rows.
+// writes the [128][64] atom hf of its rows.  All three layers run on the tensor cores
+// (layer 1 as one K = 16 MMA over the split features); the GELUs on CUDA cores.
 // SAVE: training (pre-activations, activations and the standardised output saved;
 // y unused); else inference (y only).
 template <bool SAVE>
@@ -178,8 +252,8 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
     const int t = threadIdx.x, warp = t >> 5, r = t & (MT - 1), hf = t >> 7, cb = 64 * hf;
-    float* w1 = (float*)(smem + FwdLayout::f32);  // [6][128]: W1^T rows, then b1
-    float* b2 = w1 + MH * 8;
+    float* b1 = (float*)(smem + FwdLayout::f32);
+    float* b2 = b1 + MH;
     float* b3 = b2 + MH;
     float* w4 = b3 + MH;
     float* b4 = w4 + MH;
@@ -188,6 +262,7 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
     unsigned* tmem_slot = (unsigned*)(smem + FwdLayout::bars + 32);
     const unsigned bar = smem_u32(&bars[0]);
     const unsigned s_w2 = smem_u32(smem + FwdLayout::w2), s_w3 = smem_u32(smem + FwdLayout::w3);
+    const unsigned s_w1 = smem_u32(smem + FwdLayout::w1);
     const unsigned s_act = smem_u32(smem + FwdLayout::act);
 
     // weights: W2, W3 [out][in] BF16 -> swizzled B operands (row = out, K = in)
@@ -197,12 +272,9 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
         const uint4 v = *reinterpret_cast<const uint4*>(wbf + (size_t)l * MH * MH + row * MH + ch * 8);
         *reinterpret_cast<uint4*>(smem + (l ? FwdLayout::w3 : FwdLayout::w2) + sw_off(row, ch * 8)) = v;
     }
-    for (int k = t; k < MH * 8; k += FT) {
-        const int q = k >> 7, j = k & (MH - 1);
-        w1[k] = q < MI ? __bfloat162float(__float2bfloat16_rn(params[XTS_MLP_W1 + j * MI + q]))
-                       : (q == MI ? params[XTS_MLP_B1 + j] : 0.f);
-    }
+    fill_w1_operand(smem + FwdLayout::w1, params, t, FT);
     for (int k = t; k < MH; k += FT) {
+        b1[k] = params[XTS_MLP_B1 + k];
         b2[k] = params[XTS_MLP_B2 + k];
         b3[k] = params[XTS_MLP_B3 + k];
         w4[k] = __bfloat162float(__float2bfloat16_rn(params[XTS_MLP_W4 + k]));
@@ -221,69 +293,36 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
     unsigned ph = 0;
     bool ok = true;
     const long long ntiles = (n + MT - 1) / MT;
-    // layer 1 of tile tl on CUDA cores: this thread's 64 BF16 activations of its row
-    auto layer1 = [&](long long tl, uint4* hq) {
-        const long long rw = tl * MT + r;
-        const bool lv = rw < n;
-        float x[MI];
-#pragma unroll
-        for (int k = 0; k < MI; ++k)
-            x[k] = lv ? (X[ldx ? k * ldx + rw : rw * MI + k] - nm.mu[k]) / nm.sd[k] : 0.f;
-#pragma unroll
-        for (int g = 0; g < 8; ++g) {
-            const int j0 = cb + 8 * g;
-            float h[8];
-#pragma unroll
-            for (int j = 0; j < 8; j += 2) {
-                const float2* wp = reinterpret_cast<const float2*>(w1 + j0 + j);  // units j0 + j, j0 + j + 1
-                float2 z = wp[MI * MH / 2];  // b1
-#pragma unroll
-                for (int k = 0; k < MI; ++k) z = __ffma2_rn(wp[k * MH / 2], make_float2(x[k], x[k]), z);
-                const float2 g2 = gelu2(z);
-                h[j] = g2.x;
-                h[j + 1] = g2.y;
-                if (SAVE && lv) {
-                    sv.z1[(size_t)(j0 + j) * n + rw] = z.x;
-                    sv.z1[(size_t)(j0 + j + 1) * n + rw] = z.y;
-                }
-            }
-            hq[g] = make_uint4(pack_bf16(h[0], h[1]), pack_bf16(h[2], h[3]), pack_bf16(h[4], h[5]),
-                               pack_bf16(h[6], h[7]));
-            if (SAVE && lv) {
-                const __nv_bfloat16* hb = reinterpret_cast<const __nv_bfloat16*>(&hq[g]);
-#pragma unroll
-                for (int j = 0; j < 8; ++j) sv.h1[(size_t)(j0 + j) * n + rw] = hb[j];
-            }
-        }
-    };
-    uint4 hq[8];
-    if (!SAVE && (long long)blockIdx.x < ntiles) layer1(blockIdx.x, hq);
     for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
         const long long row = tile * MT + r;
         const bool live = row < n;
-        // the A operand of layer 2: this tile's layer 1 (for inference computed while the
-        // previous tile's last MMA ran; the MMA that read the buffer has completed)
-        if (SAVE) layer1(tile, hq);
+        // layer 1's A operand (the accumulator's last reader, the previous tile's
+        // epilogue, has finished: the barrier below orders it before the MMA)
+        if (!hf) {
+            float x[MI];
 #pragma unroll
-        for (int g = 0; g < 8; ++g) *reinterpret_cast<uint4*>(smem + FwdLayout::act + sw_off(r, cb + 8 * g)) = hq[g];
+            for (int k = 0; k < MI; ++k)
+                x[k] = live ? (X[ldx ? k * ldx + row : row * MI + k] - nm.mu[k]) / nm.sd[k] : 0.f;
+            store_x_split(smem + FwdLayout::act, r, x);
+        }
         float yacc = 0.f;
-        for (int layer = 2; layer <= 3 && ok; ++layer) {
+        for (int layer = 1; layer <= 3 && ok; ++layer) {
             fence_async_shared();
             tc_fence_before();
             __syncthreads();
             if (t == 0) {
                 tc_fence_after();
-                mma_chain(tmem, s_act, layer == 2 ? s_w2 : s_w3, MH / 16, false);
+                if (layer == 1) mma_layer1(tmem, s_act, s_w1);
+                else mma_chain(tmem, s_act, layer == 2 ? s_w2 : s_w3, MH / 16, false);
                 mma_commit(bar);
             }
-            // inference: layer 1 of the next tile in registers while the last MMA of this one runs
-            if (!SAVE && layer == 3 && tile + gridDim.x < ntiles) layer1(tile + gridDim.x, hq);
             const bool got = mbar_wait(bar, ph);
             if (!__syncthreads_and(got)) { ok = false; break; }  // ph stays: the exit path waits on it
             ph ^= 1;
             tc_fence_after();
-            const float* bias = layer == 2 ? b2 : b3;
-            float* zs = SAVE ? (layer == 2 ? sv.z2 : sv.z3) : nullptr;
+            const float* bias = layer == 1 ? b1 : layer == 2 ? b2 : b3;
+            float* zs = SAVE ? (layer == 1 ? sv.z1 : layer == 2 ? sv.z2 : sv.z3) : nullptr;
+            __nv_bfloat16* hs = SAVE ? (layer == 1 ? sv.h1 : sv.h2) : nullptr;
             for (int c0 = 0; c0 < 64; c0 += 16) {
                 float v[16], bv[16];
                 tmem_ld16(trow + (unsigned)c0, v);
@@ -304,7 +343,7 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
                     v[j] = g2.x;
                     v[j + 1] = g2.y;
                 }
-                if (layer == 2) {
+                if (layer < 3) {
 #pragma unroll
                     for (int q = 0; q < 2; ++q) {
                         const float* u = v + 8 * q;
@@ -313,7 +352,7 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
                         if (SAVE && live) {
                             const __nv_bfloat16* hb = reinterpret_cast<const __nv_bfloat16*>(&pk);
 #pragma unroll
-                            for (int j = 0; j < 8; ++j) sv.h2[(size_t)(cc + 8 * q + j) * n + row] = hb[j];
+                            for (int j = 0; j < 8; ++j) hs[(size_t)(cc + 8 * q + j) * n + row] = hb[j];
                         }
                         *reinterpret_cast<uint4*>(smem + FwdLayout::act + sw_off(r, cc + 8 * q)) = pk;
                     }
@@ -351,7 +390,7 @@ k_mlp_forward(const float* __restrict__ params, const __nv_bfloat16* __restrict_
 // k_mlp_infer: the same forward arithmetic as k_mlp_forward<false>, with four tiles in
 // flight per SM.  One block per SM of four warpgroups; warpgroup g owns tile slot g
 // (its BF16 activation operand and accumulator columns [128 g, 128 g + 128) of tensor
-// memory) and runs its own tiles, thread = row, all 128 columns per thread; the two
+// memory) and runs its own tiles, thread = row, all 128 columns per thread; the three
 // weight operands are shared.  A warpgroup synchronises only with itself (named
 // barrier 1 + g, its own mbarrier), so while one waits for its MMAs the other three
 // run their GELUs: the tensor pipe, the FMA pipe and the tanh unit overlap across
@@ -362,8 +401,9 @@ constexpr int IG = 4;                    // warpgroups (tile slots) per block
 constexpr int IT = IG * MT;              // threads per block
 struct InfLayout {
     static constexpr size_t w2 = 0, w3 = 2 * ATOM, act = 4 * ATOM;  // act: IG slots of 2 atoms
-    static constexpr size_t f32 = act + (size_t)IG * 2 * ATOM;      // W1^T [5][128], b1, pad, b2, b3, w4, b4
-    static constexpr size_t bars = f32 + 4 * (MH * 8 + 3 * MH + 4);
+    static constexpr size_t w1 = act + (size_t)IG * 2 * ATOM;       // layer 1's B operand
+    static constexpr size_t f32 = w1 + W1OP;                        // b1, b2, b3, w4, b4
+    static constexpr size_t bars = f32 + 4 * (4 * MH + 4);
     static constexpr size_t total = bars + 64;
 };
 constexpr size_t INF_SMEM = InfLayout::total + 1024;
@@ -386,8 +426,8 @@ k_mlp_infer(const float* __restrict__ params, const __nv_bfloat16* __restrict__ 
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
     const int t = threadIdx.x, warp = t >> 5, g = t >> 7, r = t & (MT - 1);
-    float* w1 = (float*)(smem + InfLayout::f32);  // [6][128]: W1^T rows, then b1
-    float* b2 = w1 + MH * 8;
+    float* b1 = (float*)(smem + InfLayout::f32);
+    float* b2 = b1 + MH;
     float* b3 = b2 + MH;
     float* w4 = b3 + MH;
     float* b4 = w4 + MH;
@@ -395,6 +435,7 @@ k_mlp_infer(const float* __restrict__ params, const __nv_bfloat16* __restrict__ 
     unsigned* tmem_slot = (unsigned*)(smem + InfLayout::bars + 8 * IG);
     const unsigned bar = smem_u32(&bars[g]);
     const unsigned s_w2 = smem_u32(smem + InfLayout::w2), s_w3 = smem_u32(smem + InfLayout::w3);
+    const unsigned s_w1 = smem_u32(smem + InfLayout::w1);
     unsigned char* act = smem + InfLayout::act + (size_t)g * 2 * ATOM;
     const unsigned s_act = smem_u32(act);
 
@@ -407,12 +448,9 @@ k_mlp_infer(const float* __restrict__ params, const __nv_bfloat16* __restrict__ 
         for (int q = 0; q < 4; ++q) h2[q] = __hmul2(h2[q], __float2bfloat162_rn(0.5f));  // exact: a power of 2
         *reinterpret_cast<uint4*>(smem + (l ? InfLayout::w3 : InfLayout::w2) + sw_off(row, ch * 8)) = v;
     }
-    for (int k = t; k < MH * 8; k += IT) {
-        const int q = k >> 7, j = k & (MH - 1);
-        w1[k] = q < MI ? __bfloat162float(__float2bfloat16_rn(params[XTS_MLP_W1 + j * MI + q]))
-                       : (q == MI ? params[XTS_MLP_B1 + j] : 0.f);
-    }
+    fill_w1_operand(smem + InfLayout::w1, params, t, IT);
     for (int k = t; k < MH; k += IT) {
+        b1[k] = params[XTS_MLP_B1 + k];
         b2[k] = params[XTS_MLP_B2 + k];
         b3[k] = params[XTS_MLP_B3 + k];
         w4[k] = 0.5f * __bfloat162float(__float2bfloat16_rn(params[XTS_MLP_W4 + k]));
@@ -441,43 +479,24 @@ k_mlp_infer(const float* __restrict__ params, const __nv_bfloat16* __restrict__ 
     for (long long tile = (long long)blockIdx.x * IG + g; tile < ntiles && ok; tile += stride) {
         const long long row = tile * MT + r;
         const bool live = row < n;
-        // layer 1 on CUDA cores, the row's 128 BF16 activations into the A operand
+        // layer 1's A operand: the row's split features (the slot's last MMA, which read
+        // the operand, has completed)
         {
             float x[MI];
 #pragma unroll
             for (int k = 0; k < MI; ++k) x[k] = live ? (xn[k] - nm.mu[k]) / nm.sd[k] : 0.f;
             load_x(tile + stride);
-#pragma unroll 2
-            for (int g8 = 0; g8 < MH / 8; ++g8) {
-                const int j0 = 8 * g8;
-                float h[8];
-#pragma unroll
-                for (int j = 0; j < 8; j += 4) {
-                    const float4* wp = reinterpret_cast<const float4*>(w1 + j0 + j);
-                    const float4 bq = wp[MI * MH / 4];  // b1
-                    float2 za = make_float2(bq.x, bq.y), zb = make_float2(bq.z, bq.w);
-#pragma unroll
-                    for (int k = 0; k < MI; ++k) {
-                        const float4 wq = wp[k * MH / 4];
-                        za = __ffma2_rn(make_float2(wq.x, wq.y), make_float2(x[k], x[k]), za);
-                        zb = __ffma2_rn(make_float2(wq.z, wq.w), make_float2(x[k], x[k]), zb);
-                    }
-                    const float2 ga = gelu2x(za), gb = gelu2x(zb);
-                    h[j] = ga.x; h[j + 1] = ga.y; h[j + 2] = gb.x; h[j + 3] = gb.y;
-                }
-                *reinterpret_cast<uint4*>(act + sw_off(r, j0)) =
-                    make_uint4(pack_bf16(h[0], h[1]), pack_bf16(h[2], h[3]), pack_bf16(h[4], h[5]),
-                               pack_bf16(h[6], h[7]));
-            }
+            store_x_split(act, r, x);
         }
         float ylo = 0.f, yhi = 0.f;  // the output layer over columns 0..63 and 64..127
-        for (int layer = 2; layer <= 3 && ok; ++layer) {
+        for (int layer = 1; layer <= 3 && ok; ++layer) {
             fence_async_shared();
             tc_fence_before();
             group_sync(g);
             if (r == 0) {
                 tc_fence_after();
-                mma_chain(tmem, s_act, layer == 2 ? s_w2 : s_w3, MH / 16, false);
+                if (layer == 1) mma_layer1(tmem, s_act, s_w1);
+                else mma_chain(tmem, s_act, layer == 2 ? s_w2 : s_w3, MH / 16, false);
                 mma_commit(bar);
             }
             // one warp of the group polls the MMA's mbarrier; the other three sleep in the
@@ -487,11 +506,18 @@ k_mlp_infer(const float* __restrict__ params, const __nv_bfloat16* __restrict__ 
             if (!group_and(g, got)) { ok = false; break; }  // ph stays: the exit path waits on it
             ph ^= 1;
             tc_fence_after();
-            const float* bias = layer == 2 ? b2 : b3;
-#pragma unroll 1
+            const float* bias = layer == 1 ? b1 : layer == 2 ? b2 : b3;
+            // the accumulator read 16 columns at a time, the next 16 in flight while
+            // these are worked on
+            unsigned ra[16], rb[16];
+            tmem_ld16_issue(trow, ra);
+            tmem_ld_done(ra);
+#pragma unroll
             for (int c0 = 0; c0 < MH; c0 += 16) {
+                if (c0 + 16 < MH) tmem_ld16_issue(trow + (unsigned)(c0 + 16), rb);
                 float v[16], bv[16];
-                tmem_ld16(trow + (unsigned)c0, v);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(ra[j]);
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     const float4 b = reinterpret_cast<const float4*>(bias + c0)[q];
@@ -504,7 +530,7 @@ k_mlp_infer(const float* __restrict__ params, const __nv_bfloat16* __restrict__ 
                     v[j] = g2.x;
                     v[j + 1] = g2.y;
                 }
-                if (layer == 2) {
+                if (layer < 3) {
 #pragma unroll
                     for (int q = 0; q < 2; ++q) {
                         const float* u = v + 8 * q;
@@ -521,6 +547,11 @@ k_mlp_infer(const float* __restrict__ params, const __nv_bfloat16* __restrict__ 
                                                                                 fmaf(v[4 * q + 3], wv.w, ya))));
                     }
                     if (c0 < 64) ylo = ya; else yhi = ya;
+                }
+                if (c0 + 16 < MH) {
+                    tmem_ld_done(rb);
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) ra[j] = rb[j];
                 }
             }
             tc_fence_before();  // the next MMA overwrites the accumulator read above
