@@ -493,7 +493,6 @@ int xts_compute_exposure(const xts_expcube* cube, const xts_expcube* wcube, cons
     if (!grid_ok(aeff_front, 1) || !grid_ok(aeff_back, 1))
         return set_error(XTS_ERR_ARG, "compute_exposure: effective-area grids need n_par == 1");
     int C = cube->nbrbins;
-    long long npix = 12LL * cube->nside * cube->nside;
     Stager sg{(flags & XTS_DEVICE_PTRS) != 0, stream ? (cudaStream_t)stream : g_ctx.stream};
     ExposureDev a;
     a.src_sph = sg.in(src_sph, (size_t)2 * S); a.S = S;
@@ -840,7 +839,6 @@ static int fused_maps(const xts_expcube* cube, const xts_expcube* wcube, const d
     if ((flags & XTS_DEVICE_PTRS) && !f64 && ((uintptr_t)model_map & 15))
         return set_error(XTS_ERR_ARG, "point_source_maps: device model_map must be 16-byte aligned");
     const int C = cube->nbrbins;
-    const long long nhp = 12LL * cube->nside * cube->nside;
     Stager sg{(flags & XTS_DEVICE_PTRS) != 0, stream ? (cudaStream_t)stream : g_ctx.stream};
     // The map geometry (pixel grids, solid angles, source boundaries, the window
     // pass) needs only the source list and the WCS: it runs on the geometry

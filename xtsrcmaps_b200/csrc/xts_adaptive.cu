@@ -44,7 +44,6 @@ namespace xts {
 
 constexpr int AT = 256;     // threads per block
 constexpr int AW = 8;       // rows of a region window
-constexpr int AMAXD = 16;   // deepest subdivision accepted by the entry point
 
 // Points of the rule in half-widths along (dimension 0 = map axis h, dimension 1
 // = map axis w) and the coefficients of the four windows per point.

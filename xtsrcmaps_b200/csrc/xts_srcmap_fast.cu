@@ -237,7 +237,6 @@ __global__ void __launch_bounds__(FT) k_map_integral_fast(const double* __restri
             double* wd = wts + t * RW;
 #pragma unroll
             for (int j = 0; j < RW; ++j) wd[j] = 0.;
-            bool wide = false;
 #pragma unroll
             for (int p = 0; p < 12; ++p) {
                 float tt;
@@ -249,7 +248,6 @@ __global__ void __launch_bounds__(FT) k_map_integral_fast(const double* __restri
                     wd[r] += wa;
                     wd[r + 1] += wb;
                 } else {
-                    wide = true;
                     atomicAdd(&hist[idx - 1], wa);
                     atomicAdd(&hist[idx], wb);
                 }
@@ -308,7 +306,6 @@ int launch_srcmap_fast(const double* corners, const double* omega, const SrcInfo
     int Epad = (E + 3) & ~3;
     float* lut = (float*)workspace(W_LUT, sizeof(float) * (size_t)S * ND * Epad + 16);
     if (!lut) return XTS_ERR_OOM;
-    size_t n = (size_t)S * ND * Epad;
     XTS_LAUNCH("k_lut_scaled", st, k_lut_scaled<<<lut_scaled_grid(S), 256, 0, st>>>(upsf, scale, S, E, Epad, lut, nullptr, nullptr));
     size_t smem = srcmap_fast_smem(E);
     if (smem > 227 * 1024) return set_error(XTS_ERR_ARG, "E=%d too large for the fast source-map kernel", E);

@@ -102,7 +102,7 @@ k_srcmap_tc(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ C
 
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int s = blockIdx.y;
-    const int N = L.N, na = L.na;
+    const int N = L.N;
     const unsigned ncols = N <= 32 ? 32u : (N <= 64 ? 64u : (N <= 128 ? 128u : 256u));
     const unsigned idesc = tf32_idesc(N);
 
