@@ -519,17 +519,42 @@ __global__ void k_scale_map64(const double* __restrict__ mean, float* __restrict
 }
 
 // c8 + c10 and the solid angle: value = mean * omega * exposure * correction.
+// out[s][pix][e] *= omega[pix] (FP64 product rounded to FP32) * scale[s][e]; four
+// consecutive values per thread (one 16-byte load and store, one division), the
+// source's first values up to a 16-byte boundary and its last ones one by one.
+__device__ __forceinline__ float scale_value(float v, const double* omega, const float* sc, unsigned pix,
+                                             unsigned e) {
+    return (float)((double)v * omega[pix]) * sc[e];
+}
 __global__ void k_scale_map(float* __restrict__ out, const double* __restrict__ omega,
                             const double* __restrict__ scale, int npix, int E) {
     __shared__ float sc[256];
     const int s = blockIdx.y;
     for (int e = threadIdx.x; e < E; e += blockDim.x) sc[e] = (float)scale[(size_t)s * E + e];
     __syncthreads();
-    const unsigned n = (unsigned)npix * (unsigned)E;
+    const unsigned n = (unsigned)npix * (unsigned)E, uE = (unsigned)E;
     float* o = out + (size_t)s * n;
-    for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const unsigned pix = k / (unsigned)E;
-        o[k] = (float)((double)o[k] * omega[pix]) * sc[k - pix * (unsigned)E];
+    const unsigned mis = (unsigned)(((uintptr_t)o >> 2) & 3u);  // o is 4-byte aligned
+    const unsigned head = min((4u - mis) & 3u, n);
+    const unsigned nq = (n - head) >> 2, tail0 = head + 4 * nq;
+    const unsigned tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    if (tid < head) o[tid] = scale_value(o[tid], omega, sc, tid / uE, tid % uE);
+    if (tid < n - tail0) {
+        const unsigned k = tail0 + tid;
+        o[k] = scale_value(o[k], omega, sc, k / uE, k % uE);
+    }
+    float4* o4 = reinterpret_cast<float4*>(o + head);
+    for (unsigned q = tid; q < nq; q += nth) {
+        const unsigned k = head + 4 * q;
+        unsigned pix = k / uE, e = k - pix * uE;
+        float4 v = o4[q];
+        float* f = reinterpret_cast<float*>(&v);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            f[i] = scale_value(f[i], omega, sc, pix, e);
+            if (++e == uE) { e = 0; ++pix; }
+        }
+        o4[q] = v;
     }
 }
 
@@ -586,10 +611,11 @@ int launch_adaptive_map(const double* corners, const double* centers, const doub
 }
 
 // The map integral of FP32 pixel means: block (c, s) takes pixels
-// [c npix / nc, (c + 1) npix / nc) of source s; warp w of the block pixels w, w + 8, ...
-// of that range, lane l energies l, l + 32, ... (a pixel's E means are contiguous, so
-// the loads coalesce); the boundary test is per pixel, the same in every lane.  Per
-// block the warps' partial sums are added in a fixed order into sums[s][c][e].
+// [c npix / nc, (c + 1) npix / nc) of source s; warp w of the block the runs of 32
+// pixels w, w + 8, ... of that range.  Per run each lane tests one pixel against the
+// source's boundary; then, for the inside pixels in order, lane l adds energies l,
+// l + 32, ... (a pixel's E means are contiguous, so the loads coalesce).  Per block the
+// warps' partial sums are added in a fixed order into sums[s][c][e].
 constexpr int MI_WARPS = 8;
 constexpr int MI_EQ = 8;  // energies per lane: E <= 256
 __global__ void __launch_bounds__(32 * MI_WARPS) k_mean_integral(const double* __restrict__ centers,
@@ -610,22 +636,46 @@ __global__ void __launch_bounds__(32 * MI_WARPS) k_mean_integral(const double* _
     for (int q = 0; q < MI_EQ; ++q) acc[q] = 0.;
     if (si.in_fov) {
         const float* m = mean + (size_t)s * npix * E;
-        for (int pix = p_lo + wp; pix < p_hi; pix += MI_WARPS) {
-            const int h = pix / W, w = pix - h * W;
-            const double* c = centers + 3 * (h * W1 + w);
-            const double x = si.dir[0] - c[0], y = si.dir[1] - c[1], z = si.dir[2] - c[2];
-            const double d2 = x * x + y * y + z * z;
-            bool inside;
-            if (d2 < ch2 * (1.0 - 1e-12)) inside = true;
-            else if (d2 > ch2 * (1.0 + 1e-12)) inside = false;
-            else inside = dir_diff(si.dir, c) <= si.radius_rad;
-            if (!inside) continue;
-            const double om = omega[pix];
-            const float* mp = m + (size_t)pix * E;
+        // 32 pixels per round: each lane tests its own pixel against the boundary, then
+        // the warp sums the inside pixels' rows (lane = energy), two rows per step so
+        // that two loads are in flight
+        for (int pix0 = p_lo + 32 * wp; pix0 < p_hi; pix0 += 32 * MI_WARPS) {
+            const int pix = pix0 + lane;
+            bool inside = false;
+            double om = 0.;
+            if (pix < p_hi) {
+                const int h = pix / W, w = pix - h * W;
+                const double* c = centers + 3 * (h * W1 + w);
+                const double x = si.dir[0] - c[0], y = si.dir[1] - c[1], z = si.dir[2] - c[2];
+                const double d2 = x * x + y * y + z * z;
+                if (d2 < ch2 * (1.0 - 1e-12)) inside = true;
+                else if (d2 > ch2 * (1.0 + 1e-12)) inside = false;
+                else inside = dir_diff(si.dir, c) <= si.radius_rad;
+                if (inside) om = omega[pix];
+            }
+            unsigned mask = __ballot_sync(0xffffffffu, inside);
+            while (mask) {
+                const int l1 = __ffs(mask) - 1;
+                mask &= mask - 1;
+                const int l2 = mask ? __ffs(mask) - 1 : -1;
+                if (l2 >= 0) mask &= mask - 1;
+                const double om1 = __shfl_sync(0xffffffffu, om, l1);
+                const double om2 = __shfl_sync(0xffffffffu, om, l2 < 0 ? l1 : l2);
+                const float* mp1 = m + (size_t)(pix0 + l1) * E;
+                const float* mp2 = m + (size_t)(pix0 + (l2 < 0 ? l1 : l2)) * E;
+                float v1[MI_EQ], v2[MI_EQ];
 #pragma unroll
-            for (int q = 0; q < MI_EQ; ++q) {
-                const int e = lane + 32 * q;
-                if (q < nq && e < E) acc[q] += (double)mp[e] * om;
+                for (int q = 0; q < MI_EQ; ++q) {
+                    const int e = lane + 32 * q;
+                    const bool on = q < nq && e < E;
+                    v1[q] = on ? mp1[e] : 0.f;
+                    v2[q] = on && l2 >= 0 ? mp2[e] : 0.f;
+                }
+#pragma unroll
+                for (int q = 0; q < MI_EQ; ++q) {
+                    acc[q] += (double)v1[q] * om1;
+                    if (l2 >= 0) acc[q] += (double)v2[q] * om2;
+                }
             }
         }
     }
