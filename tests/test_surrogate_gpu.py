@@ -295,6 +295,15 @@ def test_trained_network_gains_over_centre_value(api):
     assert none is None
     assert last_stats(upsf2.device) == st
     assert torch.equal(m2, m)
+    # with the two-warpgroup network kernel in place of the four-tile one: the same map
+    # and counts (the kernels' outputs agree bit for bit)
+    api.set_tuning(mlp_blocks_per_sm=2)
+    try:
+        m3, _, st3 = model_map(job2.wcs, src, expo2, upsf2, partial2, job2.logEs, net, check_tol=1e-4)
+    finally:
+        api.reset_tuning()
+    assert st3 == st
+    assert torch.equal(m3, m)
 
 
 def test_surrogate_argument_errors(api):
