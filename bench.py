@@ -73,6 +73,9 @@ def parse():
     ap.add_argument("--no-tune", action="store_true", help="keep the library's default launch shapes")
     ap.add_argument("--surrogate-samples", type=int, default=10_000_000)
     ap.add_argument("--surrogate-epochs", type=int, default=60)
+    ap.add_argument("--surrogate-file", default="",
+                    help="load the trained, calibrated network from this file if it exists (no training "
+                         "launches: for a profiler's launch list), else train it and save it there")
     ap.add_argument("--cell-margin", type=float, default=0.7,
                     help="the network serves error cells whose held-out worst error is below margin x 1e-4")
     ap.add_argument("--exposure-map-nside", type=int, default=0,
@@ -356,7 +359,15 @@ def run_ours(args, rank, world, local_rank):
 
     net, train = (None, None)
     if not args.no_surrogate:
-        net, train = train_surrogate(args, A, dev)
+        if args.surrogate_file and os.path.exists(args.surrogate_file):
+            from xtsrcmaps_b200.surrogate import Surrogate
+
+            net = Surrogate.load(args.surrogate_file, device=dev)
+            train = {"loaded": args.surrogate_file}
+        else:
+            net, train = train_surrogate(args, A, dev)
+            if args.surrogate_file:
+                net.save(args.surrogate_file)
 
     # launch shapes by measurement on this job (window-pass, write-pass and
     # network blocks per SM), set for everything timed below
