@@ -158,7 +158,8 @@ def test_cli_and_bench_expose_the_surrogate():
         assert opt in out, opt
     out = subprocess.run([sys.executable, "bench.py", "--help"], cwd=root, capture_output=True, text=True,
                          check=True).stdout
-    for opt in ("--no-surrogate", "--surrogate-samples", "--surrogate-epochs", "--no-c4", "--no-f64"):
+    for opt in ("--no-surrogate", "--surrogate-samples", "--surrogate-epochs", "--surrogate-file", "--no-c4",
+                "--no-f64"):
         assert opt in out, opt
 
 
