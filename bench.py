@@ -883,6 +883,10 @@ def measure_c4(args, A, net, torch, dev, stream, flush, rank, chunk: int = 250):
         res["surrogate_vs_plain"] = res["value"] / res["plain_value"]
         with torch.cuda.stream(stream):
             res["surrogate_stats_last_chunk"] = last_stats(dev)
+        if res["surrogate_stats_last_chunk"].get("accepted", 0) == 0:
+            res["surrogate_note"] = ("no value served by the network: c4's 0.025 deg CAR pixels have solid angles "
+                                     "below the smallest training pixel's (0.025^2 deg^2), so the feature-range "
+                                     "check gives every value to the 12-point rule")
     if rank == 0 and not args.no_oracle:
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         import copy
